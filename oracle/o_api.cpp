@@ -1,0 +1,213 @@
+// Test infrastructure (oracle): setup, the host step driver and a C API for the Python test harness.
+// Restates Sim.reset (sim.js:613-623), writeParams (sim.js:625-639) and step/encodeFrame (sim.js:681-701).
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <sstream>
+
+#include "oracle.h"
+
+namespace orc {
+
+static bool parse_consts(const char* text, std::map<std::string, double>& kv) {
+  std::istringstream in(text);
+  std::string line;
+  while (std::getline(in, line)) {
+    if (line.empty()) continue;
+    size_t eq = line.find('=');
+    if (eq == std::string::npos) return false;
+    kv[line.substr(0, eq)] = std::strtod(line.c_str() + eq + 1, nullptr);
+  }
+  return true;
+}
+
+bool Oracle::init(const char* constants, const float* statF_, size_t nF, const uint32_t* statU_, size_t nU,
+                  const float* body_pose, const float* body_vel, const float* art_init, size_t nArt) {
+  std::map<std::string, double> kv;
+  if (!parse_consts(constants, kv)) { error = "bad constants text"; return false; }
+  auto get = [&](const char* k, double def) { auto it = kv.find(k); return it == kv.end() ? def : it->second; };
+#define X(n) C.n = (uint32_t)get(#n, 0);
+  ORC_U32_CONSTS(X)
+#undef X
+#define X(n) C.n = (float)get(#n, 0);
+  ORC_F32_CONSTS(X)
+#undef X
+  C.fps = get("PARAM_fps", 60);
+  C.substeps = (uint32_t)get("PARAM_substeps", 4);
+  C.iterations = (uint32_t)get("PARAM_iterations", 12);
+  C.baumgarte = get("PARAM_baumgarte", 0.2);
+  C.gravity[0] = get("PARAM_gravity0", 0); C.gravity[1] = get("PARAM_gravity1", 0); C.gravity[2] = get("PARAM_gravity2", -9.81);
+  C.warm = get("PARAM_warm", 0);
+  C.target_frames = (uint32_t)get("PARAM_target_frames", 0);
+  C.driven = (uint32_t)get("PARAM_driven", 0);
+  C.integral_count = (uint32_t)get("PARAM_integral_count", 0);
+  C.reg = get("PARAM_reg", 0);
+  // The oracle restates the default-flag path (and the small features that ride on it).
+  const char* unsup = nullptr;
+  if (C.FMODE) unsup = "friction_mode";
+  else if (C.ANG || C.ANG_ART) unsup = "torsional/rolling friction";
+  else if (C.TORS) unsup = "contact torsion";
+  else if (C.COMPL) unsup = "contact_compliance";
+  else if (C.NEST) unsup = "nesterov_momentum";
+  else if (C.CTI) unsup = "row_schedule contact_then_internal";
+  else if (C.LONGEST_FIRST) unsup = "propagation_color_order longest_first";
+  else if (C.DRIVE_ROWS) unsup = "drive_mode rows";
+  else if (C.VLIM_ON) unsup = "enable_joint_velocity_limits";
+  else if (C.JFL) unsup = "joint friction load coefficient";
+  else if (C.SLEEP) unsup = "enable_sleeping";
+  else if (C.VELITERS) unsup = "velocity_iterations";
+  if (unsup) { error = std::string("unsupported solver option: ") + unsup; return false; }
+  if (nF != (size_t)C.LEN_STATF4 * 4u || nU != C.LEN_STATU || nArt != C.LEN_ART) { error = "buffer size mismatch"; return false; }
+  statF.resize(C.LEN_STATF4);
+  std::memcpy(statF.data(), statF_, nF * 4);
+  statU.assign(statU_, statU_ + nU);
+  init_poses.assign(C.NB * 4u + C.NS * 4u, mk4(0, 0, 0, 0));
+  std::memcpy(init_poses.data(), body_pose, C.NB * 8u * 4u);
+  init_vel.assign(C.NB * 2u, mk4(0, 0, 0, 0));
+  std::memcpy(init_vel.data(), body_vel, C.NB * 8u * 4u);
+  init_art.assign(art_init, art_init + nArt);
+  pairs.assign(C.MAXP * 2u, 0u);
+  contacts.assign(C.MAXC * 6u, mk4(0, 0, 0, 0));
+  craw.assign(C.MAXC * 6u, mk4(0, 0, 0, 0));
+  sched.assign(C.LEN_SCHED, 0u);
+  rows.assign(C.MAXC * (C.ROWS + 2u), mk4(0, 0, 0, 0));
+  warm.assign(10u * C.WH + 30u * C.AH, 0u);
+  scratch.assign(C.MAXC, u4{0, 0, 0, 0});
+  wkey.assign(C.MAXU, 0u);
+  wcol.assign(C.MAXU, 0u);
+  wmask.assign(C.NBP * C.NCOLW, 0u);
+  wcount.assign(C.NCOL + 2u, 0u);
+  wlinkhit.assign(C.NBP, 0u);
+  wjsplit.assign(C.NL > 0 ? C.NL : 1u, 0u);
+  tw.assign(C.NBP * 2u, mk4(0, 0, 0, 0));
+  imp.assign(C.NBP * 2u, mk4(0, 0, 0, 0));
+  aqd.assign(C.ND > 0 ? C.ND : 1u, 0.0f);
+  wcs.assign(C.NCOL + 2u, 0u);
+  reset();
+  return true;
+}
+
+void Oracle::reset() {
+  poses = init_poses;
+  std::fill(poses.begin() + C.NB * 2u, poses.end(), mk4(0, 0, 0, 0));
+  vel = init_vel;
+  art = init_art;
+  std::fill(warm.begin(), warm.end(), 0u);
+  std::memset(counters, 0, sizeof(counters));
+  std::memset(stats, 0, sizeof(stats));
+  phase = 0.0; time = 0.0; frame = 0; substep_count = 0;
+}
+
+void Oracle::write_params(uint32_t substep) {
+  double dt = 1.0 / C.fps / C.substeps;
+  P = Params{};
+  P.dt = (float)dt;
+  P.substep = substep;
+  P.parity = (uint32_t)(substep_count % 2u);
+  P.iterations = C.iterations;
+  P.phase = (float)phase;
+  P.frame_dt = (float)(1.0 / C.fps);
+  P.beta = (float)C.baumgarte;
+  P.max_depen = 2.0f;
+  P.gravity = mk4((float)C.gravity[0], (float)C.gravity[1], (float)C.gravity[2], 0.0f);
+  P.warm_scale = (float)C.warm;
+  P.path_frames = C.target_frames;
+  P.driven = user_targets ? 0u : C.driven;
+  P.integral_count = C.integral_count;
+  P.reg = (float)C.reg;
+}
+
+void Oracle::substep_kernels() {
+  k_shapes();
+  k_broad();
+  k_narrow();
+  k_csort();
+  k_prepare();
+  k_solve();
+}
+
+void Oracle::step(uint32_t frames) {
+  for (uint32_t f = 0; f < frames; f++) {
+    for (uint32_t s = 0; s < C.substeps; s++) {
+      write_params(s);
+      substep_count++;
+      substep_kernels();
+    }
+    frame++;
+    time += 1.0 / C.fps;
+    phase += 1.0 / C.fps;
+  }
+}
+
+}  // namespace orc
+
+using orc::Oracle;
+
+extern "C" {
+
+void* oracle_create(const char* constants, const float* statF, size_t nF, const uint32_t* statU, size_t nU,
+                    const float* poses, const float* vel, const float* art, size_t nArt, char* err, size_t errlen) {
+  Oracle* o = new Oracle();
+  if (!o->init(constants, statF, nF, statU, nU, poses, vel, art, nArt)) {
+    if (err && errlen) { std::strncpy(err, o->error.c_str(), errlen - 1); err[errlen - 1] = 0; }
+    delete o;
+    return nullptr;
+  }
+  return o;
+}
+void oracle_destroy(void* h) { delete (Oracle*)h; }
+void oracle_reset(void* h) { ((Oracle*)h)->reset(); }
+void oracle_step(void* h, uint32_t frames) { ((Oracle*)h)->step(frames); }
+void oracle_set_user_targets(void* h, int on) { ((Oracle*)h)->user_targets = on != 0; }
+
+// Runs shapes, broad, narrow and csort for the current state (substep 0 parameters) and leaves
+// pairs/contacts in place; the state is not advanced. Used for the pair-set and sort parity tests.
+void oracle_collide(void* h) {
+  Oracle* o = (Oracle*)h;
+  o->counters[0] = o->counters[1] = 0u;
+  o->write_params(0);
+  o->k_shapes();
+  o->k_broad();
+  o->k_narrow();
+  o->k_csort();
+}
+// Runs prepare on the state oracle_collide left (colors, units, rows).
+void oracle_prepare(void* h) { ((Oracle*)h)->k_prepare(); }
+
+// Buffer access by name: float buffers copy 4-byte words; returns the element count copied.
+size_t oracle_read(void* h, const char* name, void* out, size_t max_words) {
+  Oracle* o = (Oracle*)h;
+  const void* src = nullptr;
+  size_t n = 0;
+  std::string s(name);
+  if (s == "poses") { src = o->poses.data(); n = o->poses.size() * 4; }
+  else if (s == "vel") { src = o->vel.data(); n = o->vel.size() * 4; }
+  else if (s == "art") { src = o->art.data(); n = o->art.size(); }
+  else if (s == "contacts") { src = o->contacts.data(); n = o->contacts.size() * 4; }
+  else if (s == "craw") { src = o->craw.data(); n = o->craw.size() * 4; }
+  else if (s == "pairs") { src = o->pairs.data(); n = o->pairs.size(); }
+  else if (s == "sched") { src = o->sched.data(); n = o->sched.size(); }
+  else if (s == "rows") { src = o->rows.data(); n = o->rows.size() * 4; }
+  else if (s == "warm") { src = o->warm.data(); n = o->warm.size(); }
+  else if (s == "counters") { src = o->counters; n = 16; }
+  else if (s == "stats") { src = o->stats; n = 16; }
+  else return 0;
+  if (n > max_words) n = max_words;
+  std::memcpy(out, src, n * 4);
+  return n;
+}
+// Write words into a named state buffer at a word offset (the Sim setters, sim.js:716-785).
+int oracle_write(void* h, const char* name, size_t offset, const void* data, size_t words) {
+  Oracle* o = (Oracle*)h;
+  std::string s(name);
+  uint32_t* dst = nullptr;
+  size_t n = 0;
+  if (s == "poses") { dst = (uint32_t*)o->poses.data(); n = o->poses.size() * 4; }
+  else if (s == "vel") { dst = (uint32_t*)o->vel.data(); n = o->vel.size() * 4; }
+  else if (s == "art") { dst = (uint32_t*)o->art.data(); n = o->art.size(); }
+  else return -1;
+  if (offset + words > n) return -1;
+  std::memcpy(dst + offset, data, words * 4);
+  return 0;
+}
+}

@@ -1,0 +1,596 @@
+// Test infrastructure (oracle): the solve kernel, wgsl.js:2501-3891 restated (default flag set).
+#include <algorithm>
+#include <cmath>
+
+#include "oracle.h"
+#include "smath_o.h"
+
+namespace orc {
+
+enum : uint32_t { L_V = 147, L_P = 201, L_ROT = 216, L_COM = 220, L_TAU = 223 };
+static const uint32_t AVN = 14u;
+static inline uint32_t anchor_hash(uint32_t pair, uint32_t k) { return std::max(hash_u32(pair * 2u + k), 1u); }
+static inline m3 skew(v3 r) { return mcols(mk3(0.0f, r.z, -r.y), mk3(-r.z, 0.0f, r.x), mk3(r.y, -r.x, 0.0f)); }
+
+m3 Oracle::gyro_inverse3(const m3& m) const {
+  v3 a = m.c[0], b = m.c[1], c = m.c[2];
+  v3 r0 = cross(b, c), r1 = cross(c, a), r2 = cross(a, b);
+  float det = dot(a, r0);
+  return mscale(transpose(mcols(r0, r1, r2)), 1.0f / det);
+}
+// gyroscopic_velocity (wgsl.js:2543-2562)
+v3 Oracle::gyroscopic_velocity(const m3& inertia, v3 u0, float dt) const {
+  m3 a = mscale(inertia, 1.0f / fmaxf_(inertia.c[0].x, fmaxf_(inertia.c[1].y, inertia.c[2].z)));
+  m3 inv = gyro_inverse3(a);
+  float speed = std::sqrt(fmaxf_(dot(u0, mul(a, u0)) * ((inv.c[0].x + inv.c[1].y) + inv.c[2].z), 0.0f));
+  uint32_t n = f2u(clampf(std::ceil((2.0f * std::fabs(dt)) * speed), 1.0f, 32.0f));
+  float h = dt / (float)n;
+  v3 w = u0;
+  for (uint32_t m = 0; m < n; m++) {
+    v3 u = w;
+    float energy = dot(u, mul(a, u));
+    for (uint32_t it = 0; it < 8u; it++) {
+      m3 S = mscale(0.5f * h, skew(mul(a, 0.5f * (u + w))));
+      v3 c = mul(gyro_inverse3(msub(a, S)), mul(madd(a, S), u));
+      v3 d = c - w;
+      w = c;
+      if (dot(d, mul(a, d)) <= 1e-12f * energy) break;
+    }
+  }
+  return w;
+}
+
+// friction_pair_solve (wgsl.js:2952-3011)
+v2 Oracle::friction_pair_solve(float a0, float c0, float d0, float r0, float r1, float old0, float old1, float radius,
+                               float omega) const {
+  if (radius <= 0.0f) return mk2(0.0f, 0.0f);
+  float scale = fmaxf_(fmaxf_(a0, d0), 1e-20f);
+  float a = a0 / scale, c = c0 / scale, d = d0 / scale;
+  float largest = 0.5f * ((a + d) + std::sqrt((a - d) * (a - d) + (4.0f * c) * c));
+  float smallest = largest > 0.0f ? fmaxf_((a * d - c * c) / largest, 0.0f) : 0.0f;
+  float vx = c, vy = largest - a;
+  if (a >= d) { vx = largest - d; vy = c; }
+  float vn = std::sqrt(vx * vx + vy * vy);
+  if (vn > 0.0f) { vx /= vn; vy /= vn; } else { vx = 1.0f; vy = 0.0f; }
+  float r0r = (vx * r0 + vy * r1) / scale;
+  float r1r = ((-vy) * r0 + vx * r1) / scale;
+  v2 res = mk2(old0, old1);
+  bool sticking = false;
+  if (largest > 0.0f && (smallest > 0.0f || r1r == 0.0f)) {
+    float dx = r0r / largest;
+    float dy = smallest > 0.0f ? r1r / smallest : 0.0f;
+    res = mk2(old0 - (vx * dx - vy * dy), old1 - (vy * dx + vx * dy));
+    sticking = length(res) <= radius;
+  }
+  if (!sticking) {
+    float on = length(mk2(old0, old1)), rn = length(mk2(r0, r1));
+    if (on > 0.0f && on <= radius && radius - on <= 2e-7f * radius && r0 * old0 + r1 * old1 <= 0.0f &&
+        std::fabs(r0 * old1 - r1 * old0) <= (2e-7f * on) * rn)
+      return mk2(old0, old1);
+    float ox = vx * old0 + vy * old1, oy = (-vy) * old0 + vx * old1;
+    float b0 = largest * ox - r0r, b1 = smallest * oy - r1r;
+    float x = 0.0f, y = 0.0f;
+    float hi = std::sqrt(b0 * b0 + b1 * b1) / radius;
+    if (hi > 0.0f) {
+      float lo = fmaxf_(fmaxf_(hi - largest, std::fabs(b1) / radius - smallest), 0.0f);
+      float alpha = lo;
+      bool done = false;
+      for (uint32_t it = 0; it < 8u; it++) {
+        float i0 = 1.0f / (largest + alpha);
+        float i1 = smallest + alpha > 0.0f ? 1.0f / (smallest + alpha) : 0.0f;
+        float tx = ox - (r0r + alpha * ox) * i0, ty = oy - (r1r + alpha * oy) * i1;
+        float nrm = std::sqrt(tx * tx + ty * ty);
+        if (std::fabs(nrm - radius) <= 2e-7f * radius || (alpha == 0.0f && nrm <= radius)) { x = tx; y = ty; done = true; break; }
+        if (nrm > radius) lo = alpha; else hi = alpha;
+        float slope = (tx * tx) * i0 + (ty * ty) * i1;
+        float cand = alpha;
+        if (slope > 0.0f) cand = alpha + (((nrm / radius - 1.0f) * nrm) * nrm) / slope;
+        alpha = (cand > lo && cand < hi) ? cand : 0.5f * (lo + hi);
+      }
+      if (!done) {
+        for (uint32_t it = 0; it < 24u; it++) {
+          alpha = 0.5f * (lo + hi);
+          if (length(mk2(b0 / (largest + alpha), b1 / (smallest + alpha))) > radius) lo = alpha; else hi = alpha;
+        }
+        x = b0 / (largest + hi);
+        y = b1 / (smallest + hi);
+      }
+    }
+    res = mk2((old0 + vx * (x - ox)) - vy * (y - oy), (old1 + vy * (x - ox)) + vx * (y - oy));
+  }
+  v2 old = mk2(old0, old1);
+  v2 relaxed = old + omega * (res - old);
+  float m = length(relaxed);
+  return m > radius ? relaxed * (radius / m) : relaxed;
+}
+
+void Oracle::load_tw(int b, v3 out[2]) const {
+  if (b < 0) { out[0] = splat3(0.0f); out[1] = splat3(0.0f); return; }
+  out[0] = xyz(tw[(uint32_t)b * 2u]);
+  out[1] = xyz(tw[(uint32_t)b * 2u + 1u]);
+}
+void Oracle::add_imp(int b, v3 f, v3 t) {
+  if (b < 0) return;
+  if (body_kind(b) != 2u) return;
+  imp[(uint32_t)b * 2u] = imp[(uint32_t)b * 2u] + mk4(f, 0.0f);
+  imp[(uint32_t)b * 2u + 1u] = imp[(uint32_t)b * 2u + 1u] + mk4(t, 0.0f);
+}
+
+void Oracle::solve_slot(uint32_t u, uint32_t mode, uint32_t it) {
+  v4 sl = rows[C.MAXC * C.ROWS + 2u * u], sr = rows[C.MAXC * C.ROWS + 2u * u + 1u];
+  solve_unit(f2u(sl.y), f2u(sl.x), f2i(sl.z), f2i(sl.w), f2u(sr.x), f2u(sr.y), mode, it);
+}
+
+// solve_unit (wgsl.js:3033-3231), fixed_normal friction with anchors.
+void Oracle::solve_unit(uint32_t us, uint32_t row, int a, int b, uint32_t /*s0*/, uint32_t /*s1*/, uint32_t mode,
+                        uint32_t it) {
+  const uint32_t ROWS = C.ROWS, PO = C.PO;
+  v3 ta[2], tb[2];
+  load_tw(a, ta);
+  load_tw(b, tb);
+  uint32_t o = row * ROWS;
+  v4 r0 = rows[o], r1 = rows[o + 1u], r2 = rows[o + 2u];
+  v3 ra = xyz(rows[o + 3u]), rb = xyz(rows[o + 4u]);
+  v3 n = xyz(r0), t1 = xyz(r1), t2 = xyz(r2);
+  v4 lam = rows[o + 6u];
+  float dn = 0.0f, dt1 = 0.0f, dt2 = 0.0f;
+  if (mode == 0u) {
+    dn = lam.x; dt1 = lam.y; dt2 = lam.z;
+    for (uint32_t r = 0; r < 3u; r++) {
+      float d = r == 0u ? dn : (r == 1u ? dt1 : dt2);
+      ta[0] += xyz(rows[o + 7u + r * 4u]) * d; ta[1] += xyz(rows[o + 8u + r * 4u]) * d;
+      tb[0] += xyz(rows[o + 9u + r * 4u]) * d; tb[1] += xyz(rows[o + 10u + r * 4u]) * d;
+    }
+    v3 fra = ra, frb = rb;
+    if (C.EXTRA == 1u) { fra = xyz(rows[o + PO]); frb = xyz(rows[o + PO + 1u]); }
+    v3 fn_ = n * dn, ft = t1 * dt1 + t2 * dt2;
+    add_imp(a, -fn_ - ft, -cross(ra, fn_) - cross(fra, ft));
+    add_imp(b, fn_ + ft, cross(rb, fn_) + cross(frb, ft));
+  } else {
+    v3 vrel = (tb[0] + cross(tb[1], rb)) - (ta[0] + cross(ta[1], ra));
+    float jv = dot(n, vrel);
+    float w = rows[o + 5u].w;
+    float res = jv + r1.w;
+    float nl = fmaxf_(lam.x + C.F_OMEGA * ((((-res) * r0.w) * w) - (1.0f - w) * lam.x), 0.0f);
+    dn = nl - lam.x;
+    lam.x = nl;
+    ta[0] += xyz(rows[o + 7u]) * dn; ta[1] += xyz(rows[o + 8u]) * dn;
+    tb[0] += xyz(rows[o + 9u]) * dn; tb[1] += xyz(rows[o + 10u]) * dn;
+    add_imp(a, -n * dn, -cross(ra, n * dn));
+    add_imp(b, n * dn, cross(rb, n * dn));
+    v3 fra = ra, frb = rb;
+    float lim = r2.w * nl;
+    v2 bias = mk2(0.0f, 0.0f);
+    float role = 1.0f;
+    if (C.EXTRA == 1u) {
+      role = rows[o + PO].w;
+      if (C.PATCH == 1u && role != 1.0f) art[C.A_ULOAD + us] += dn;
+      fra = xyz(rows[o + PO]);
+      frb = xyz(rows[o + PO + 1u]);
+      if (C.PATCH == 1u && role == 2.0f) {
+        float load = art[C.A_ULOAD + us];
+        lim = r2.w * load;
+        v3 e = xyz(rows[o + PO + 2u]);
+        bias = (C.F_ANCHOR_BETA * mk2(dot(t1, e), dot(t2, e))) / P.dt;
+        rows[o + PO + 2u].w = lim;
+      }
+    }
+    if (it < C.FSTART) { lam.y = 0.0f; lam.z = 0.0f; }
+    if (role != 0.0f && it >= C.FSTART) {
+      v3 vr2 = (tb[0] + cross(tb[1], frb)) - (ta[0] + cross(ta[1], fra));
+      v4 ki = rows[o + 5u];
+      float v1 = dot(t1, vr2) + bias.x, v2_ = dot(t2, vr2) + bias.y;
+      float kd = ki.x * ki.z - ki.y * ki.y;
+      v2 lt = friction_pair_solve(ki.z / kd, -ki.y / kd, ki.x / kd, v1, v2_, lam.y, lam.z, lim, C.F_OMEGA);
+      dt1 = lt.x - lam.y;
+      dt2 = lt.y - lam.z;
+      lam.y = lt.x;
+      lam.z = lt.y;
+      ta[0] += xyz(rows[o + 11u]) * dt1 + xyz(rows[o + 15u]) * dt2;
+      ta[1] += xyz(rows[o + 12u]) * dt1 + xyz(rows[o + 16u]) * dt2;
+      tb[0] += xyz(rows[o + 13u]) * dt1 + xyz(rows[o + 17u]) * dt2;
+      tb[1] += xyz(rows[o + 14u]) * dt1 + xyz(rows[o + 18u]) * dt2;
+      v3 f = t1 * dt1 + t2 * dt2;
+      add_imp(a, -f, -cross(fra, f));
+      add_imp(b, f, cross(frb, f));
+    }
+    rows[o + 6u] = lam;
+  }
+  if (a >= 0) { tw[(uint32_t)a * 2u] = mk4(ta[0], 0.0f); tw[(uint32_t)a * 2u + 1u] = mk4(ta[1], 0.0f); }
+  if (b >= 0) { tw[(uint32_t)b * 2u] = mk4(tb[0], 0.0f); tw[(uint32_t)b * 2u + 1u] = mk4(tb[1], 0.0f); }
+}
+
+// art_dense (wgsl.js:3306-3364), sequential sums (the reference's no-subgroup form).
+bool Oracle::art_dense(uint32_t a, uint32_t mode, uint32_t it, uint32_t ph) {
+  const uint32_t NDA = C.NDA, DHDR = C.DHDR, DPS = C.DPS;
+  uint32_t nd = std::min(sched[C.S_META + 3u], C.MAXDENSE);
+  u4 ai = art_info(a);
+  bool touched = false;
+  for (uint32_t i = 0; i < nd; i++) {
+    uint32_t o = C.A_DENSE + i * DPS;
+    if (f2u(art[o]) != a) continue;
+    touched = true;
+    uint32_t jo = o + DHDR, yo = o + DHDR + 3u * NDA;
+    v3 lam = mk3(art[o + 9u], art[o + 10u], art[o + 11u]);
+    if ((art[o + 21u] > 0.5f) == (ph == 1u) && ph != 0u) continue;
+    if (art[o + 21u] > 0.5f) {
+      if (mode == 0u) continue;
+      v3 nlam = lam;
+      for (uint32_t r = 0; r < f2u(art[o + 21u]); r++) {
+        float part = 0.0f;
+        for (uint32_t k = 0; k < ai.w; k++) part += art[jo + r * NDA + k] * aqd[ai.z + k];
+        float jv = part;
+        float rhs = r == 0u ? art[o + 4u] : (r == 1u ? art[o + 22u] : art[o + 23u]);
+        float dl = ((-C.F_OMEGA) * (jv + rhs)) * art[o + 5u + r];
+        setat(nlam, (int)r, at(nlam, (int)r) + dl);
+        for (uint32_t k = 0; k < ai.w; k++) aqd[ai.z + k] += art[yo + r * NDA + k] * dl;
+      }
+      art[o + 9u] = nlam.x; art[o + 10u] = nlam.y; art[o + 11u] = nlam.z;
+      continue;
+    }
+    if (mode == 0u) {
+      for (uint32_t k = 0; k < ai.w; k++)
+        aqd[ai.z + k] += (art[yo + k] * lam.x + art[yo + NDA + k] * lam.y) + art[yo + 2u * NDA + k] * lam.z;
+      continue;
+    }
+    float part = 0.0f;
+    for (uint32_t k = 0; k < ai.w; k++) part += art[jo + k] * aqd[ai.z + k];
+    float jv = part;
+    float w = art[o + 24u];
+    float nl = fmaxf_(lam.x + C.F_OMEGA * ((((-(jv + art[o + 4u])) * art[o + 5u]) * w) - (1.0f - w) * lam.x), 0.0f);
+    float dn = nl - lam.x;
+    float p1 = 0.0f, p2 = 0.0f;
+    for (uint32_t k = 0; k < ai.w; k++) {
+      aqd[ai.z + k] += art[yo + k] * dn;
+      p1 += art[jo + NDA + k] * aqd[ai.z + k];
+      p2 += art[jo + 2u * NDA + k] * aqd[ai.z + k];
+    }
+    float lim = it < C.FSTART ? 0.0f : art[o + 3u] * nl;
+    float kd = art[o + 6u] * art[o + 8u] - art[o + 7u] * art[o + 7u];
+    v2 lt = friction_pair_solve(art[o + 8u] / kd, -art[o + 7u] / kd, art[o + 6u] / kd, p1, p2, lam.y, lam.z, lim,
+                                C.F_OMEGA);
+    float d1 = lt.x - lam.y, d2 = lt.y - lam.z;
+    for (uint32_t k = 0; k < ai.w; k++) aqd[ai.z + k] += art[yo + NDA + k] * d1 + art[yo + 2u * NDA + k] * d2;
+    art[o + 9u] = nl; art[o + 10u] = lt.x; art[o + 11u] = lt.y;
+  }
+  return touched;
+}
+void Oracle::dense_phase(uint32_t mode, uint32_t it, uint32_t ph) {
+  for (uint32_t a = 0; a < C.NA; a++)
+    if (art_dense(a, mode, it, ph)) art_twists(a);
+}
+void Oracle::art_contact_impulses(uint32_t a) {
+  u4 ai = art_info(a);
+  bool hit = false;
+  for (uint32_t k = 0; k < ai.y; k++) {
+    uint32_t l = ai.x + k;
+    uint32_t b = (uint32_t)link_body(l);
+    v3 f = xyz(imp[b * 2u]), t = xyz(imp[b * 2u + 1u]);
+    if (any_ne0(f) || any_ne0(t)) {
+      hit = true;
+      stsv(lo(l) + L_P, SV{-t, -f});
+      imp[b * 2u] = mk4(0, 0, 0, 0);
+      imp[b * 2u + 1u] = mk4(0, 0, 0, 0);
+    }
+  }
+  if (hit) art_apply(a);
+}
+void Oracle::art_dof_impulse(uint32_t a, uint32_t l, uint32_t r, float dl) {
+  art[lo(l) + L_TAU + r] = dl;
+  art_apply(a);
+}
+void Oracle::art_propagate(uint32_t a, bool /*vlim*/, bool rowsOn) {
+  u4 ai = art_info(a);
+  if (rowsOn) {
+    uint32_t n = f2u(art[C.A_RLN + a]);
+    for (uint32_t i = 0; i < n; i++) {
+      uint32_t d = f2u(art[C.A_RL + ai.z + i]);
+      uint32_t l = f2u(dof_limit(d).w);
+      art_dof_rows(a, l, d - link_dof(l), d, false, true);
+    }
+  }
+}
+// art_dof_rows (wgsl.js:3421-3468), joint friction and limit rows.
+void Oracle::art_dof_rows(uint32_t a, uint32_t l, uint32_t r, uint32_t d, bool /*vlim*/, bool rowsOn) {
+  float hinv = fmaxf_(art[C.A_HINV + d], 1e-12f);
+  v4 pv = dof_passive(d);
+  float fr = pv.y;
+  if (rowsOn && fr > 0.0f) {
+    float lam = art[C.A_FRIC + d];
+    float nl = clampf(lam - (C.F_OMEGA * aqd[d]) / hinv, -fr * P.dt, fr * P.dt);
+    if (nl != lam) { art[C.A_FRIC + d] = nl; art_dof_impulse(a, l, r, nl - lam); }
+  }
+  v4 lim = dof_limit(d);
+  if (rowsOn && art[C.A_LG + d] > 0.5f) {
+    float q = art[C.A_Q + link_qs(l) + r];
+    for (uint32_t side = 0; side < 2u; side++) {
+      float sg = side == 0u ? 1.0f : -1.0f;
+      float gap = side == 0u ? q - lim.x : lim.y - q;
+      float lam = art[C.A_LIM + 2u * d + side];
+      float rhs = gap / P.dt;
+      if (gap < 0.0f) rhs = fmaxf_((P.beta * gap) / P.dt, -P.max_depen);
+      float nl = fmaxf_(lam - (C.F_OMEGA * (sg * aqd[d] + rhs)) / hinv, 0.0f);
+      if (nl == lam) continue;
+      art[C.A_LIM + 2u * d + side] = nl;
+      art_dof_impulse(a, l, r, sg * (nl - lam));
+    }
+  }
+}
+// body_motion (wgsl.js:3472-3489)
+v3 Oracle::body_motion(int b, v3 x) const {
+  if (b < 0) return splat3(0.0f);
+  v3 p0 = xyz(poses[C.P_PREV + (uint32_t)b * 2u]);
+  v4 q0 = poses[C.P_PREV + (uint32_t)b * 2u + 1u];
+  v3 p1 = xyz(poses[C.P_BODY + (uint32_t)b * 2u]);
+  v4 q1 = poses[C.P_BODY + (uint32_t)b * 2u + 1u];
+  v4 r = qmul(q1, qconj(q0));
+  if (r.w < 0.0f) r = -r;
+  float sn = length(xyz(r));
+  v3 ang = 2.0f * xyz(r);
+  v3 tr = p1 - p0;
+  v3 lin = tr;
+  if (sn > 1e-6f) {
+    float half = atan2_o(sn, r.w);
+    v3 axis = xyz(r) / sn;
+    ang = (2.0f * half) * axis;
+    float sc = (half * r.w) / sn;
+    lin = sc * tr + ((1.0f - sc) * dot(axis, tr)) * axis;
+  }
+  return lin + cross(ang, x - 0.5f * (p0 + p1));
+}
+
+void Oracle::sweep(uint32_t mode, uint32_t ncol0, uint32_t it, uint32_t ph) {
+  const uint32_t NCOL = C.NCOL;
+  uint32_t ncol = ph == 2u ? 0u : ncol0;
+  if (ph != 1u) for (uint32_t a = 0; a < C.NA; a++) art_propagate(a, false, true);
+  if (C.PATCH == 1u && mode == 1u) {
+    for (uint32_t us = 0; us < wn_x; us++) {
+      uint32_t s0 = sched[C.S_USTART + us];
+      float load = 0.0f;
+      for (uint32_t m = s0; m < s0 + sched[C.S_USIZE + us]; m++)
+        if (rows[m * C.ROWS + C.PO].w != 1.0f) load += rows[m * C.ROWS + 6u].x;
+      art[C.A_ULOAD + us] = load;
+    }
+  }
+  dense_phase(1u, it, ph);
+  for (uint32_t c = 0; c < NCOL; c++) {
+    if (c >= ncol) break;
+    for (uint32_t u = wcs[c]; u < wcs[c + 1u]; u++) solve_slot(u, mode, it);
+  }
+  if (ph != 2u)
+    for (uint32_t u = wcs[NCOL]; u < wcs[NCOL + 1u]; u++) solve_slot(std::min(u, C.MAXC - 1u), mode, it);
+  for (uint32_t a = 0; a < C.NA; a++) { art_contact_impulses(a); if (ph != 1u) art_propagate(a, true, false); }
+  if (C.VLIM_FREE == 1u) {
+    for (uint32_t b = 0; b < C.NB; b++) {
+      if (body_kind((int)b) != 1u || (body_flags((int)b) & 1u) != 0u) continue;
+      v4 lim = body_limits((int)b);
+      uint32_t g = C.A_VLG + C.ND + b * 6u;
+      if (lim.y > 0.0f) {
+        v3 v = xyz(tw[b * 2u]);
+        for (int k = 0; k < 3; k++) if (art[g + k] > 0.5f) setat(v, k, clampf(at(v, k), -lim.y, lim.y));
+        tw[b * 2u] = mk4(v, 0.0f);
+      }
+      if (lim.z > 0.0f) {
+        v3 w = xyz(tw[b * 2u + 1u]);
+        for (int k = 0; k < 3; k++) {
+          float over = at(w, k) - clampf(at(w, k), -lim.z, lim.z);
+          if (over == 0.0f || art[g + 3u + k] < 0.5f) continue;
+          v3 e = splat3(0.0f);
+          setat(e, k, 1.0f);
+          m3 R = qmat(poses[C.P_BODY + b * 2u + 1u]);
+          v3 iw = mul(R, mul(body_inv_inertia((int)b), mul(transpose(R), e)));
+          w -= iw * (over / at(iw, k));
+        }
+        tw[b * 2u + 1u] = mk4(w, 0.0f);
+      }
+    }
+  }
+}
+
+v4 Oracle::warm_row_value(uint32_t i, uint32_t nc) const {
+  if (i < nc) {
+    uint32_t o = i * C.ROWS;
+    v4 lam = rows[o + 6u];
+    return mk4(lam.x, xyz(rows[o + 1u]) * lam.y + xyz(rows[o + 2u]) * lam.z);
+  }
+  uint32_t o = C.A_DENSE + (i - nc) * C.DPS;
+  return mk4(art[o + 9u], ld3(o + 12u) * art[o + 10u] + ld3(o + 15u) * art[o + 11u]);
+}
+uint32_t Oracle::warm_row_rank(uint32_t i, uint32_t nc) const {
+  return std::min(fbits(fmaxf_(warm_row_value(i, nc).x, 0.0f)), 0xfffffffeu) + 1u;
+}
+uint32_t Oracle::warm_row_key(uint32_t i, uint32_t nc) const {
+  if (i < nc) {
+    uint32_t o = i * C.ROWS;
+    return f2u(rows[o + 3u].w) | (f2u(rows[o + 4u].w) << 16u);
+  }
+  uint32_t o = C.A_DENSE + (i - nc) * C.DPS;
+  if (art[o + 21u] > 0.5f) return 0xffffffffu;
+  return f2u(art[o + 1u]) | (f2u(art[o + 2u]) << 16u);
+}
+
+// The solve kernel (wgsl.js:3634-3891).
+void Oracle::k_solve() {
+  const uint32_t NCOL = C.NCOL, WH = C.WH, ROWS = C.ROWS, PO = C.PO;
+  uint32_t* sc = sched.data();
+  wn_x = sc[C.S_META];
+  wn_y = std::min(sc[C.S_META + 1u], NCOL);
+  for (uint32_t i = 0; i < NCOL + 2u; i++) wcs[i] = sc[C.S_CSTART + i];
+  for (uint32_t i = 0; i < C.ND; i++) aqd[i] = art[C.A_QDH + i];
+  for (uint32_t b = 0; b < C.NB; b++) {
+    uint32_t kind = body_kind((int)b);
+    imp[b * 2u] = mk4(0, 0, 0, 0);
+    imp[b * 2u + 1u] = mk4(0, 0, 0, 0);
+    if (kind == 1u) {
+      uint32_t fl = body_flags((int)b);
+      v3 v = xyz(vel[b * 2u]) + (fl != 0u ? splat3(0.0f) : xyz(P.gravity) * P.dt);
+      v3 w = xyz(vel[b * 2u + 1u]);
+      uint32_t bfo = C.A_BF + b * 8u;
+      if ((fl & 1u) == 0u && (any_ne0(ld3(bfo)) || any_ne0(ld3(bfo + 4u)))) {
+        m3 R = qmat(poses[C.P_BODY + b * 2u + 1u]);
+        v += (ld3(bfo) * body_inv_mass((int)b)) * P.dt;
+        w += mul(R, mul(body_inv_inertia((int)b), mul(transpose(R), ld3(bfo + 4u)))) * P.dt;
+      }
+      m3 I = body_inertia((int)b);
+      bool iso = I.c[0].x == I.c[1].y && I.c[1].y == I.c[2].z && I.c[0].y == 0.0f && I.c[0].z == 0.0f && I.c[1].z == 0.0f;
+      if ((fl & 1u) == 0u && !iso && any_ne0(w)) {
+        m3 R = qmat(poses[C.P_BODY + b * 2u + 1u]);
+        w = mul(R, gyroscopic_velocity(I, mul(transpose(R), w), P.dt));
+      }
+      tw[b * 2u] = mk4(v, 0.0f);
+      tw[b * 2u + 1u] = mk4(w, 0.0f);
+    }
+  }
+  for (uint32_t i = 0; i < 2u * C.ND; i++) art[C.A_LIM + i] = 0.0f;
+  for (uint32_t i = 0; i < C.ND; i++) { art[C.A_FRIC + i] = 0.0f; art[C.A_DRV + i] = 0.0f; }
+  uint32_t nslot = std::min(sc[C.S_CSTART + NCOL + 1u], C.MAXC);
+  for (uint32_t u = 0; u < nslot; u++) {
+    uint32_t row = sc[C.S_PORD + u], us = sc[C.S_RUNIT + row], key = sc[C.S_UKEY + us], s0 = sc[C.S_USTART + us];
+    rows[C.MAXC * ROWS + 2u * u] = mk4((float)row, (float)us, (float)((int)(key & 0xffffu) - 1), (float)((int)(key >> 16u) - 1));
+    rows[C.MAXC * ROWS + 2u * u + 1u] = mk4((float)s0, (float)(s0 + sc[C.S_USIZE + us]), 0.0f, 0.0f);
+  }
+  for (uint32_t a = 0; a < C.NA; a++) art_twists(a);
+  dense_phase(0u, 0u, 0u);
+  sweep(0u, wn_y, 0u, 0u);
+  for (uint32_t it = 0; it < P.iterations; it++) sweep(1u, wn_y, it, 0u);
+  // Warm-start table store (wgsl.js:3737-3767).
+  uint32_t nc = sc[C.S_USTART + wn_x];
+  uint32_t ndense = std::min(sc[C.S_META + 3u], C.MAXDENSE);
+  uint32_t wbase = (1u - P.parity) * WH;
+  for (uint32_t i = 0; i < nc + ndense; i++) {
+    uint32_t key = warm_row_key(i, nc);
+    sc[C.S_WSLOT + i] = 0xffffffffu;
+    if (key == 0xffffffffu) continue;
+    uint32_t h = key % WH;
+    for (uint32_t probe = 0; probe < 32u; probe++) {
+      uint32_t old = warm[wbase + h];
+      if (old == 0u) warm[wbase + h] = key;
+      if (old == 0u || old == key) {
+        sc[C.S_WWIN + h] = std::max(sc[C.S_WWIN + h], warm_row_rank(i, nc));
+        sc[C.S_WSLOT + i] = h;
+        break;
+      }
+      h = (h + 1u) % WH;
+    }
+  }
+  for (uint32_t i = 0; i < nc + ndense; i++) {
+    uint32_t key = warm_row_key(i, nc);
+    if (key == 0xffffffffu) continue;
+    uint32_t h = sc[C.S_WSLOT + i];
+    if (h >= WH || warm[wbase + h] != key || sc[C.S_WWIN + h] != warm_row_rank(i, nc)) continue;
+    v4 v = warm_row_value(i, nc);
+    uint32_t vo = 2u * WH + (wbase + h) * 4u;
+    warm[vo] = fbits(v.x); warm[vo + 1u] = fbits(v.y); warm[vo + 2u] = fbits(v.z); warm[vo + 3u] = fbits(v.w);
+  }
+  // Integrate.
+  if (C.PATCH == 1u) for (uint32_t b = 0; b < C.NB * 2u; b++) poses[C.P_PREV + b] = poses[C.P_BODY + b];
+  for (uint32_t b = 0; b < C.NB; b++) {
+    if (body_kind((int)b) != 1u) continue;
+    v3 v = xyz(tw[b * 2u]), w = xyz(tw[b * 2u + 1u]);
+    float damp = (body_flags((int)b) & 1u) != 0u ? 1.0f : 1.0f - body_limits((int)b).x * P.dt;
+    vel[b * 2u] = mk4(v, 0.0f);
+    vel[b * 2u + 1u] = mk4(w * damp, 0.0f);
+    v3 c = xyz(poses[C.P_BODY + b * 2u]) + v * P.dt;
+    v4 q = poses[C.P_BODY + b * 2u + 1u];
+    q = normalize(q + (0.5f * P.dt) * qmul(mk4(w, 0.0f), q));
+    poses[C.P_BODY + b * 2u] = mk4(c, 0.0f);
+    poses[C.P_BODY + b * 2u + 1u] = q;
+  }
+  for (uint32_t i = 0; i < C.ND; i++) art[C.A_QD + i] = aqd[i];
+  for (uint32_t l = 0; l < C.NL; l++) {
+    if (link_type(l) != 4u || link_parent(l) >= 0) continue;
+    float k = 1.0f - body_limits(link_body(l)).x * P.dt;
+    uint32_t d = link_dof(l);
+    art[C.A_QD + d + 3u] *= k; art[C.A_QD + d + 4u] *= k; art[C.A_QD + d + 5u] *= k;
+  }
+  for (uint32_t a = 0; a < C.NA; a++) {
+    u4 ai = art_info(a);
+    for (uint32_t k = 0; k < ai.y; k++) {
+      uint32_t l = ai.x + k, qs = link_qs(l), d = link_dof(l), t = link_type(l);
+      float* Q = &art[C.A_Q];
+      if (t == 1u || t == 0u || t == 6u)
+        for (uint32_t r = 0; r < link_ndof(l); r++) Q[qs + r] += aqd[d + r] * P.dt;
+      if (t == 2u) {
+        v3 w = mk3(aqd[d], aqd[d + 1u], aqd[d + 2u]);
+        v4 q = mk4(Q[qs], Q[qs + 1], Q[qs + 2], Q[qs + 3]);
+        q = normalize(q + (0.5f * P.dt) * qmul(mk4(w, 0.0f), q));
+        Q[qs] = q.x; Q[qs + 1] = q.y; Q[qs + 2] = q.z; Q[qs + 3] = q.w;
+      }
+      if (t == 4u) {
+        for (uint32_t c = 0; c < 3u; c++) Q[qs + c] += aqd[d + c] * P.dt;
+        v3 w = mk3(aqd[d + 3u], aqd[d + 4u], aqd[d + 5u]);
+        v4 q = mk4(Q[qs + 3], Q[qs + 4], Q[qs + 5], Q[qs + 6]);
+        q = normalize(q + (0.5f * P.dt) * qmul(mk4(w, 0.0f), q));
+        Q[qs + 3] = q.x; Q[qs + 4] = q.y; Q[qs + 5] = q.z; Q[qs + 6] = q.w;
+      }
+    }
+    art_fk(a);
+    for (uint32_t k = 0; k < ai.y; k++) {
+      uint32_t l = ai.x + k;
+      uint32_t b = (uint32_t)link_body(l);
+      poses[C.P_BODY + b * 2u] = mk4(ld3(lo(l) + L_COM), 0.0f);
+      poses[C.P_BODY + b * 2u + 1u] = link_rot(l);
+    }
+  }
+  // Friction anchors: advance and store (wgsl.js:3832-3878).
+  if (C.PATCH == 1u) {
+    uint32_t ab = AK() + (1u - P.parity) * C.AH;
+    const float keep_frac = (float)(1.0 - 1e-5);
+    for (uint32_t i = 0; i < nc; i++) {
+      uint32_t o = i * ROWS;
+      if (rows[o + PO].w != 2.0f) continue;
+      uint32_t pair = fbits(rows[o + PO + 3u].w);
+      int a = (int)(pair & 0xffffu) - 1, b = (int)(pair >> 16u) - 1;
+      v3 fra = xyz(rows[o + PO]), frb = xyz(rows[o + PO + 1u]);
+      uint32_t k = f2u(rows[o + PO + 1u].w);
+      v4 ex = rows[o + PO + 2u];
+      float lim = ex.w;
+      if (lim <= 0.0f) continue;
+      v3 n = xyz(rows[o]), t1 = xyz(rows[o + 1u]), t2 = xyz(rows[o + 2u]);
+      v3 ta[2], tb[2];
+      load_tw(a, ta);
+      load_tw(b, tb);
+      v3 vrel = (tb[0] + cross(tb[1], frb)) - (ta[0] + cross(ta[1], fra));
+      v4 lam = rows[o + 6u];
+      v3 lt = t1 * lam.y + t2 * lam.z;
+      float r = fmaxf_(fminf_(body_radius(a), body_radius(b)), 1e-4f);
+      if (length(lt) >= keep_frac * lim && dot(vrel, lt) < (((-lim) * 1e-5f) * r) / P.dt) continue;
+      v4 qa = mk4(0, 0, 0, 1);
+      v3 ca = splat3(0.0f);
+      if (a >= 0) { qa = poses[C.P_BODY + (uint32_t)a * 2u + 1u]; ca = xyz(poses[C.P_BODY + (uint32_t)a * 2u]); }
+      v3 ll = xyz(rows[o + PO + 3u]);
+      v3 x = ca + qrot(qa, ll);
+      v3 e = (xyz(ex) + body_motion(b, x)) - body_motion(a, x);
+      e -= n * dot(n, e);
+      v3 el = qinvrot(qa, e);
+      uint32_t hk = anchor_hash(pair, k);
+      uint32_t h = hk % C.AH;
+      for (uint32_t probe = 0; probe < 32u; probe++) {
+        if (warm[ab + h] == 0u) {
+          warm[ab + h] = hk;
+          uint32_t vo = AV() + ((1u - P.parity) * C.AH + h) * AVN;
+          v3 il = qinvrot(qa, lt), nl_ = qinvrot(qa, n);
+          warm[vo + 11u] = fbits(nl_.x); warm[vo + 12u] = fbits(nl_.y); warm[vo + 13u] = fbits(nl_.z);
+          warm[vo + 8u] = fbits(il.x); warm[vo + 9u] = fbits(il.y); warm[vo + 10u] = fbits(il.z);
+          warm[vo] = pair; warm[vo + 1u] = k;
+          warm[vo + 2u] = fbits(ll.x); warm[vo + 3u] = fbits(ll.y); warm[vo + 4u] = fbits(ll.z);
+          warm[vo + 5u] = fbits(el.x); warm[vo + 6u] = fbits(el.y); warm[vo + 7u] = fbits(el.z);
+          break;
+        }
+        h = (h + 1u) % C.AH;
+      }
+    }
+  }
+  stats[1] = std::max(stats[1], counters[1]);
+  stats[2] = std::max(stats[2], wn_y);
+  stats[3] = std::max(stats[3], wn_x);
+  stats[4] = std::max(stats[4], counters[0]);
+  stats[5] = counters[1];
+  stats[6] = wn_y;
+  stats[8] = sc[C.S_META + 5u];
+  stats[7] = std::max(stats[7], sc[C.S_META + 3u]);
+  counters[0] = 0u;
+  counters[1] = 0u;
+}
+
+}  // namespace orc

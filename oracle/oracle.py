@@ -1,0 +1,96 @@
+"""Test infrastructure: ctypes harness of the CPU oracle (oracle/_build/liboracle.so).
+
+ORACLE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU baseline as the
+checker. The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build(quiet: bool = True) -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True, capture_output=quiet)
+    return _LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = ctypes.CDLL(_LIB)
+        L.oracle_create.restype = ctypes.c_void_p
+        L.oracle_create.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                    ctypes.c_char_p, ctypes.c_size_t]
+        for f in ("oracle_destroy", "oracle_reset", "oracle_collide", "oracle_prepare"):
+            getattr(L, f).argtypes = [ctypes.c_void_p]
+        L.oracle_step.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
+        L.oracle_set_user_targets.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.oracle_read.restype = ctypes.c_size_t
+        L.oracle_read.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t]
+        L.oracle_write.restype = ctypes.c_int
+        L.oracle_write.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t]
+        _lib = L
+    return _lib
+
+
+class OracleSim:
+    """One packed scene stepped by the CPU oracle, with the reference's buffer layout."""
+
+    def __init__(self, pk):
+        L = lib()
+        self.pk = pk
+        C = pk.C
+        self._keep = [np.ascontiguousarray(a) for a in (pk.statF, pk.statU, pk.body_pose, pk.body_vel, pk.art)]
+        err = ctypes.create_string_buffer(256)
+        self.h = L.oracle_create(pk.constants_text().encode(), self._keep[0].ctypes.data, self._keep[0].size,
+                                 self._keep[1].ctypes.data, self._keep[1].size, self._keep[2].ctypes.data,
+                                 self._keep[3].ctypes.data, self._keep[4].ctypes.data, self._keep[4].size, err, 256)
+        if not self.h:
+            raise ValueError(err.value.decode())
+        self.sizes = dict(poses=(C["NB"] * 4 + C["NS"] * 4) * 4, vel=C["NB"] * 8, art=C["LEN_ART"],
+                          contacts=C["MAXC"] * 6 * 4, craw=C["MAXC"] * 6 * 4, pairs=C["MAXP"] * 2,
+                          sched=C["LEN_SCHED"], rows=C["MAXC"] * (C["ROWS"] + 2) * 4,
+                          warm=10 * C["WH"] + 30 * C["AH"], counters=16, stats=16)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_destroy(self.h)
+            self.h = None
+
+    def step(self, frames=1):
+        lib().oracle_step(self.h, frames)
+
+    def reset(self):
+        lib().oracle_reset(self.h)
+
+    def collide(self):
+        lib().oracle_collide(self.h)
+
+    def prepare(self):
+        lib().oracle_prepare(self.h)
+
+    def read(self, name, dtype=np.float32):
+        n = self.sizes[name]
+        out = np.zeros(n, dtype=np.uint32)
+        got = lib().oracle_read(self.h, name.encode(), out.ctypes.data, n)
+        return out[:got].view(dtype)
+
+    def write(self, name, offset, values, dtype=np.float32):
+        a = np.ascontiguousarray(np.asarray(values, dtype=dtype))
+        if lib().oracle_write(self.h, name.encode(), offset, a.ctypes.data, a.size) != 0:
+            raise IndexError(name)
+
+    def body_poses(self):
+        """(NB, 8): COM position, 0, quaternion."""
+        nb = self.pk.NB
+        return self.read("poses")[:nb * 8].reshape(nb, 8)
