@@ -1,0 +1,122 @@
+/* C ABI of the B200 implementation of steel-webgpu's Sim.step hot path.
+ *
+ * The reference's host (packages/steel-webgpu/src/sim.js, class Sim) packs a scene into its
+ * static buffers statF/statU and a constant table C (sim.js:95-477), uploads them with
+ * queue.writeBuffer, and per frame dispatches seven WGSL kernels per substep
+ * (sim.js:648-701). This library takes exactly that packed form (plus the initial state of
+ * sim.js:486-502) and runs the substeps on one GPU as CUDA kernels. Scenes are grouped into a
+ * batch that steps together; a single Sim is a batch of one.
+ *
+ * Every call returns 0 on success or a STEEL_E_* code; steel_last_error() then describes the
+ * failure (thread-local). A batch is used by one host thread at a time.
+ */
+#ifndef STEEL_B200_H
+#define STEEL_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STEEL_OK 0
+#define STEEL_E_INVALID 1     /* bad argument or malformed scene; Sim's throw new Error(...) */
+#define STEEL_E_UNSUPPORTED 2 /* solver option outside the supported set (sim.js:412-420) */
+#define STEEL_E_CAPACITY 3    /* a device capacity was exceeded and work was dropped */
+#define STEEL_E_CUDA 4        /* CUDA runtime error */
+#define STEEL_E_NOMEM 5       /* device allocation failed */
+#define STEEL_E_NODEVICE 6    /* no CUDA device; the reference's UnsupportedError (device.js:2-9) */
+
+typedef struct steel_ctx steel_ctx;
+typedef struct steel_batch steel_batch;
+
+/* One packed scene, in the reference's layout. */
+typedef struct {
+  const char* constants;     /* "KEY=VALUE\n" lines: the C table of sim.js:456-477 plus the
+                                writeParams inputs as PARAM_fps, PARAM_substeps, PARAM_iterations,
+                                PARAM_baumgarte, PARAM_gravity0..2, PARAM_warm, PARAM_reg,
+                                PARAM_target_frames, PARAM_driven, PARAM_integral_count */
+  const float* statF;        /* statF (sim.js:225), statF_floats = 4 * vec4 count */
+  uint64_t statF_floats;
+  const uint32_t* statU;     /* statU (sim.js:237) */
+  uint64_t statU_words;
+  const float* body_pose;    /* NB * 8: COM position, 0, quaternion (sim.js:258-281) */
+  const float* body_vel;     /* NB * 8: linear, 0, angular, 0 (sim.js:490-491) */
+  const float* art;          /* the art buffer's initial contents, A_* layout of C (sim.js:486-501) */
+  uint64_t art_floats;
+} steel_scene_desc;
+
+/* SimStats (src/sim.d.ts:30-43, sim.js:822-834). overflow: bit 0 pairs, 1 contacts, 2 units,
+   3 dense rows (the buffers that filled up and dropped work). */
+typedef struct {
+  uint32_t max_contacts, max_colors, max_units, max_pairs, contacts, colors, max_dense, asleep, overflow;
+} steel_stats;
+
+/* Sizes of scene s of a batch. */
+typedef struct {
+  uint32_t NB, NS, NA, NL, ND, NQ;
+  uint32_t max_pairs, max_contacts, max_units, max_dense;
+} steel_scene_info;
+
+/* Context: one CUDA device and stream. Replaces initDevice (src/device.js:7-26). */
+int steel_ctx_create(int device, steel_ctx** out);
+int steel_ctx_destroy(steel_ctx* ctx);
+const char* steel_last_error(void);
+
+/* new Sim(device, scene) for n scenes at once (sim.js:63-75, 95-611). */
+int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t n, steel_batch** out);
+int steel_batch_destroy(steel_batch* b);                          /* Sim.destroy (sim.js:85-93) */
+int steel_scene_info_get(steel_batch* b, uint32_t scene, steel_scene_info* out);
+
+int steel_reset(steel_batch* b);                                  /* Sim.reset (sim.js:613-623) */
+int steel_step(steel_batch* b, uint32_t frames);                  /* Sim.step (sim.js:692-701), async */
+int steel_sync(steel_batch* b);                                   /* queue.onSubmittedWorkDone */
+/* Capture one frame's substeps into a CUDA graph and replay it (on by default). */
+int steel_set_graph(steel_batch* b, int enabled);
+
+/* Readback (Sim.state, sim.js:732-763; Sim.poses, sim.js:804). Caller-owned buffers. */
+int steel_read_poses(steel_batch* b, uint32_t scene, float* poses /* NB*8 */);
+int steel_read_state(steel_batch* b, uint32_t scene, float* poses /* NB*8 */, float* vel /* NB*8 */,
+                     float* q /* NQ */, float* qd /* ND */, float* link_v /* NL*6, (w, v) at the COM */);
+int steel_get_stats(steel_batch* b, uint32_t scene, steel_stats* out);  /* Sim.stats (sim.js:822-834) */
+
+/* User control (sim.js:716-785), port dof/body indices; held until changed. */
+int steel_set_joint_target(steel_batch* b, uint32_t scene, uint32_t dof, float pos, float vel);
+int steel_set_joint_force(steel_batch* b, uint32_t scene, uint32_t dof, float value);
+int steel_set_body_wrench(steel_batch* b, uint32_t scene, uint32_t body, const float force[3], const float torque[3]);
+int steel_set_body_pose(steel_batch* b, uint32_t scene, uint32_t body, const float com[3], const float quat[4]);
+int steel_set_body_twist(steel_batch* b, uint32_t scene, uint32_t body, const float twist[6]);
+
+/* Inspection for parity checks: steel_collide runs shapes, broad, narrow and the contact sort on
+   the current state (substep-0 parameters) without advancing it; the readers then copy a scene's
+   candidate pairs (2 u32 each, unordered) and its sorted contact records (5 vec4 each, then the
+   shape-mu vec4s) from that run. */
+int steel_collide(steel_batch* b);
+int steel_read_pairs(steel_batch* b, uint32_t scene, uint32_t* pairs, uint32_t cap, uint32_t* count);
+int steel_read_contacts(steel_batch* b, uint32_t scene, float* records, uint32_t cap, uint32_t* count);
+/* Stage-level inspection (parity checks), one substep at a time as steel_step runs them: stage 0
+   writes the next substep's parameters and runs the collision kernels, 1 the prepare kernel, 2 the
+   solve kernel (ending the frame after the last substep). steel_read_words copies
+   `count` 4-byte words from one of a scene's device buffers ("art", "rows", "sched", "slots", "warm",
+   "contacts") at a word offset; steel_layout_get returns a named offset of that layout (an A_* or
+   S_* offset, or ROWS). */
+int steel_debug_stage(steel_batch* b, int stage);
+int steel_read_words(steel_batch* b, uint32_t scene, const char* buffer, uint64_t offset, uint64_t count, void* out);
+int steel_layout_get(steel_batch* b, uint32_t scene, const char* key, uint64_t* value);
+/* One control step of a whole batch through host memory (a policy loop's call): joint targets for
+   every articulation dof of every scene (scene after scene, ND floats each; NULL keeps the current
+   targets) are copied in, `frames` frames run, and every scene's body poses (NB * 8 floats each,
+   scene after scene) are copied out. Targets given here replace a scene's recorded trajectory,
+   as setJointTargets does (sim.js:716-728). Blocks until the poses are on the host. */
+int steel_step_io(steel_batch* b, uint32_t frames, const float* targets, uint64_t n_targets, float* poses,
+                  uint64_t n_poses);
+/* Runs `frames` frames with CUDA events around every kernel launch and returns the mean device
+   time per launch of each kernel, in milliseconds: [params, shapes, broad, narrow, csort,
+   prepare, solve] (7 floats). */
+int steel_profile_kernels(steel_batch* b, uint32_t frames, float* ms_per_launch);
+/* Device time of the last steel_step_timed call's frames, in milliseconds (CUDA events). */
+int steel_step_timed(steel_batch* b, uint32_t frames, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

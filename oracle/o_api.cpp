@@ -170,9 +170,29 @@ void oracle_collide(void* h) {
   o->k_broad();
   o->k_narrow();
   o->k_csort();
+  // Keep the counts for the readers and leave the counters as a finished substep leaves them.
+  o->collide_counts[0] = o->counters[0];
+  o->collide_counts[1] = o->counters[1];
+  o->counters[0] = o->counters[1] = 0u;
 }
-// Runs prepare on the state oracle_collide left (colors, units, rows).
-void oracle_prepare(void* h) { ((Oracle*)h)->k_prepare(); }
+// One substep in stages, as step() runs it: stage 0 writes the substep's parameters and runs the
+// collision kernels, 1 prepare, 2 solve (ending the frame after the last substep).
+void oracle_stage(void* h, int stage) {
+  Oracle* o = (Oracle*)h;
+  if (stage == 0) {
+    o->write_params(o->debug_substep);
+    o->substep_count++;
+    o->k_shapes(); o->k_broad(); o->k_narrow(); o->k_csort();
+  } else if (stage == 1) {
+    o->k_prepare();
+  } else if (stage == 2) {
+    o->k_solve();
+    if (++o->debug_substep == o->C.substeps) {
+      o->debug_substep = 0;
+      o->frame++; o->time += 1.0 / o->C.fps; o->phase += 1.0 / o->C.fps;
+    }
+  }
+}
 
 // Buffer access by name: float buffers copy 4-byte words; returns the element count copied.
 size_t oracle_read(void* h, const char* name, void* out, size_t max_words) {
@@ -190,6 +210,7 @@ size_t oracle_read(void* h, const char* name, void* out, size_t max_words) {
   else if (s == "rows") { src = o->rows.data(); n = o->rows.size() * 4; }
   else if (s == "warm") { src = o->warm.data(); n = o->warm.size(); }
   else if (s == "counters") { src = o->counters; n = 16; }
+  else if (s == "collide_counts") { src = o->collide_counts; n = 2; }
   else if (s == "stats") { src = o->stats; n = 16; }
   else return 0;
   if (n > max_words) n = max_words;

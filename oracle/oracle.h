@@ -95,6 +95,8 @@ struct Oracle {
   double phase = 0.0, time = 0.0;
   uint64_t frame = 0, substep_count = 0;
   bool user_targets = false;
+  uint32_t debug_substep = 0;
+  uint32_t collide_counts[2] = {0, 0};  // counts of the last oracle_collide
   std::string error;
 
   // --- setup / driver ---

@@ -31,8 +31,9 @@ def lib():
         L.oracle_create.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
                                     ctypes.c_char_p, ctypes.c_size_t]
-        for f in ("oracle_destroy", "oracle_reset", "oracle_collide", "oracle_prepare"):
+        for f in ("oracle_destroy", "oracle_reset", "oracle_collide"):
             getattr(L, f).argtypes = [ctypes.c_void_p]
+        L.oracle_stage.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.oracle_step.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
         L.oracle_set_user_targets.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.oracle_read.restype = ctypes.c_size_t
@@ -60,7 +61,7 @@ class OracleSim:
         self.sizes = dict(poses=(C["NB"] * 4 + C["NS"] * 4) * 4, vel=C["NB"] * 8, art=C["LEN_ART"],
                           contacts=C["MAXC"] * 6 * 4, craw=C["MAXC"] * 6 * 4, pairs=C["MAXP"] * 2,
                           sched=C["LEN_SCHED"], rows=C["MAXC"] * (C["ROWS"] + 2) * 4,
-                          warm=10 * C["WH"] + 30 * C["AH"], counters=16, stats=16)
+                          warm=10 * C["WH"] + 30 * C["AH"], counters=16, stats=16, collide_counts=2)
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -76,8 +77,8 @@ class OracleSim:
     def collide(self):
         lib().oracle_collide(self.h)
 
-    def prepare(self):
-        lib().oracle_prepare(self.h)
+    def stage(self, k: int):
+        lib().oracle_stage(self.h, k)
 
     def read(self, name, dtype=np.float32):
         n = self.sizes[name]

@@ -285,6 +285,17 @@ def convex_hull(points):
     return {"verts": verts, "faces": out}
 
 
+def box_hull(h):
+    """Hull of a box with half extents h, built directly: the 8 corners in shape_points order and
+    6 quads counter-clockwise about their outward normals (planes n . x = d). Same solid as
+    convex_hull(shape_points(BOX, h)) in a fixed vertex and face order, at a fraction of the cost."""
+    verts = [[sx * h[0], sy * h[1], sz * h[2]] for sx in (-1, 1) for sy in (-1, 1) for sz in (-1, 1)]
+    quads = [([1.0, 0.0, 0.0], h[0], [4, 6, 7, 5]), ([-1.0, 0.0, 0.0], h[0], [0, 1, 3, 2]),
+             ([0.0, 1.0, 0.0], h[1], [2, 3, 7, 6]), ([0.0, -1.0, 0.0], h[1], [0, 4, 5, 1]),
+             ([0.0, 0.0, 1.0], h[2], [1, 5, 7, 3]), ([0.0, 0.0, -1.0], h[2], [0, 2, 6, 4])]
+    return {"verts": verts, "faces": [{"n": n, "d": float(d), "v": v} for n, d, v in quads]}
+
+
 def shape_points(gtype, s):
     """Hull sample points of the analytic shapes (builder.js:176-196)."""
     pts = []
@@ -411,7 +422,9 @@ def _hull_cached(gtype, size, pts):
 class SceneBuilder:
     """Newton-style ModelBuilder (builder.js:241-491). ``finalize()`` returns a ``LoadedScene``."""
 
-    def __init__(self, gravity=(0.0, 0.0, -9.81), fps=60):
+    def __init__(self, gravity=(0.0, 0.0, -9.81), fps=60, box_hulls="quickhull"):
+        """box_hulls: "quickhull" (builder.js:264) or "direct" (box_hull, same solid, fixed order)."""
+        self.box_hulls = box_hulls
         self.gravity = list(gravity)
         self.fps = fps
         self.bodies = []
@@ -430,7 +443,12 @@ class SceneBuilder:
     def add_shape(self, body, gtype, size, opts=None, hull_points=None):
         o = dict(SHAPE_DEFAULTS)
         o.update(opts or {})
-        hull = None if gtype == GT["PLANE"] else _hull_cached(gtype, size, hull_points)
+        if gtype == GT["PLANE"]:
+            hull = None
+        elif gtype == GT["BOX"] and hull_points is None and self.box_hulls == "direct":
+            hull = box_hull([float(x) for x in size])
+        else:
+            hull = _hull_cached(gtype, size, hull_points)
         self.shapes.append(dict(body=body, type=gtype, size=list(size), xform=list(o.get("xform", IDENTITY)),
                                 hull=hull, o=o))
         return len(self.shapes) - 1
@@ -482,6 +500,20 @@ class SceneBuilder:
 
     def add_joint_fixed(self, parent, child, **o):
         return self.add_joint(JT["FIXED"], parent, child, **o)
+
+    def add_joint_d6(self, parent, child, linear_axes=(), angular_axes=(), parent_xform=IDENTITY,
+                     child_xform=IDENTITY, q=None, label=None, collision_filter_parent=True, **shared):
+        """D6 joint (builder.js:301-307): linear axes then angular axes, each [x, y, z] or dict(axis=..., **dof)."""
+        entries = [e if isinstance(e, dict) else dict(axis=list(e)) for e in list(linear_axes) + list(angular_axes)]
+        dofs = []
+        for e in entries:
+            d = dict(DOF_DEFAULTS)
+            d.update(shared)
+            d.update({k: v for k, v in e.items() if k != "axis"})
+            dofs.append(d)
+        return self.add_joint(JT["D6"], parent, child, parent_xform=parent_xform, child_xform=child_xform,
+                              axes=[e["axis"] for e in entries], linear=len(linear_axes), q=q, label=label,
+                              collision_filter_parent=collision_filter_parent, dofs=dofs)
 
     def add_joint_free(self, child, **o):
         return self.add_joint(JT["FREE"], -1, child,
@@ -721,11 +753,14 @@ class SceneBuilder:
         pairs = {}
         for a, b in self.filters:
             pairs[(min(a, b), max(a, b))] = True
+        shape_ids_by_body = {}
+        for i, s_ in enumerate(self.shapes):
+            shape_ids_by_body.setdefault(s_["body"], []).append(i)
         for j in self.joints:
             if not j["filter"] or j["parent"] < 0:
                 continue
-            pa = [i for i, s in enumerate(self.shapes) if s["body"] == j["parent"]]
-            ch = [i for i, s in enumerate(self.shapes) if s["body"] == j["child"]]
+            pa = shape_ids_by_body.get(j["parent"], [])
+            ch = shape_ids_by_body.get(j["child"], [])
             for a in pa:
                 for b in ch:
                     if a != b:

@@ -1,0 +1,773 @@
+// Host side of the C ABI (include/steel_b200.h): batch construction from the reference's packed
+// scenes, one device arena per batch, the per-substep launch sequence (captured as a CUDA graph),
+// readback and user control.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/steel_b200.h"
+#include "batch.cuh"
+
+using namespace steel;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+#define CU(x)                                                                                      \
+  do {                                                                                             \
+    cudaError_t e_ = (x);                                                                          \
+    if (e_ != cudaSuccess) return fail(STEEL_E_CUDA, std::string(#x ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+uint64_t next_pow2(uint64_t x) {
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+struct Consts {
+  std::map<std::string, double> kv;
+  bool parse(const char* text) {
+    if (!text) return false;
+    std::istringstream in(text);
+    std::string line;
+    while (std::getline(in, line)) {
+      if (line.empty()) continue;
+      size_t eq = line.find('=');
+      if (eq == std::string::npos) return false;
+      kv[line.substr(0, eq)] = std::strtod(line.c_str() + eq + 1, nullptr);
+    }
+    return true;
+  }
+  bool has(const char* k) const { return kv.count(k) != 0; }
+  double get(const char* k, double def = 0.0) const {
+    auto it = kv.find(k);
+    return it == kv.end() ? def : it->second;
+  }
+  uint32_t u(const char* k, uint32_t def = 0) const { return (uint32_t)get(k, def); }
+  float f(const char* k, float def = 0.0f) const { return (float)get(k, def); }
+};
+
+// Sequential sub-allocation of one device arena (256-byte aligned pieces).
+struct Layout {
+  size_t bytes = 0;
+  size_t take(size_t n) {
+    size_t off = (bytes + 255) & ~(size_t)255;
+    bytes = off + n;
+    return off;
+  }
+};
+
+struct SceneHost {
+  Consts C;
+  SceneDev d{};  // device pointers filled after allocation
+  // arena offsets
+  size_t o_sf, o_su, o_pos, o_rot, o_ppos, o_prot, o_lv, o_av, o_spos, o_srot, o_alo, o_ahi, o_art, o_cnt, o_stats,
+      o_params, o_craw, o_con, o_ckeys, o_rows, o_slots, o_warm, o_sched, o_tw, o_imp, o_aqd, o_tscr;
+  size_t art_floats = 0, sched_words = 0, warm_words = 0, tscr_floats = 0;
+  std::vector<float> statF;
+  std::vector<uint32_t> statU;
+  std::vector<float4> pos0, rot0, lv0, av0;
+  std::vector<float> art0;
+  uint32_t collide_pairs = 0, collide_contacts = 0;  // counts of the last steel_collide
+};
+
+}  // namespace
+
+struct steel_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sms = 148;
+};
+
+struct steel_batch {
+  steel_ctx* ctx = nullptr;
+  std::vector<SceneHost> sc;
+  uint8_t* arena = nullptr;
+  size_t arena_bytes = 0;
+  BatchDev bd{};
+  uint32_t substeps = 4;
+  uint32_t narrow_blocks = 0;
+  uint32_t debug_substep = 0;  // substep cursor of steel_debug_stage
+  size_t sort_keys = 0;
+  bool use_graph = true;
+  cudaGraphExec_t graph = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  size_t o_scenes, o_shape_scene, o_shape_local, o_tiles, o_pairs, o_pair_count, o_phase, o_ssc, o_err;
+  std::vector<uint32_t> shape_scene, shape_local;
+  std::vector<uint4> tiles;
+  // host-I/O staging (steel_step_io): packed targets/poses on the device and their offsets
+  size_t o_tgt_off, o_pose_off, o_tgt_buf, o_pose_buf;
+  uint64_t n_targets = 0, n_poses = 0;
+};
+
+namespace {
+
+int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string& why) {
+  Consts& C = s.C;
+  if (!C.parse(in.constants)) { why = "malformed constants text"; return STEEL_E_INVALID; }
+  static const char* unsupported[][2] = {
+      {"FMODE", "friction_mode"}, {"ANG", "torsional/rolling friction"}, {"ANG_ART", "torsional/rolling friction"},
+      {"TORS", "contact torsion"}, {"COMPL", "contact_compliance"}, {"NEST", "nesterov_momentum"},
+      {"CTI", "row_schedule contact_then_internal"}, {"LONGEST_FIRST", "propagation_color_order longest_first"},
+      {"DRIVE_ROWS", "drive_mode rows"}, {"VLIM_ON", "enable_joint_velocity_limits"},
+      {"JFL", "joint friction load coefficient"}, {"SLEEP", "enable_sleeping"}, {"VELITERS", "velocity_iterations"}};
+  for (auto& u : unsupported)
+    if (C.u(u[0]) != 0u) { why = std::string("unsupported solver option: ") + u[1]; return STEEL_E_UNSUPPORTED; }
+  if (in.statF_floats != (uint64_t)C.u("LEN_STATF4") * 4u || in.statU_words != C.u("LEN_STATU") ||
+      in.art_floats != C.u("LEN_ART")) {
+    why = "statF/statU/art sizes do not match the constants";
+    return STEEL_E_INVALID;
+  }
+  SceneDev& d = s.d;
+#define K(n) d.n = C.u(#n);
+  K(SF_BODY) K(SF_SHAPE) K(SF_HAABB) K(SF_VERTS) K(SF_FPLANE) K(SF_LINK) K(SF_DOF) K(SF_PATH) K(SF_LOOP)
+  K(SF_MIMIC) K(SF_CTRL) K(SU_HULL) K(SU_FACE) K(SU_FV) K(SU_HEDGE) K(SU_EDGE) K(SU_ART) K(SU_ACON)
+  K(SU_FILTER) K(NB) K(NS) K(NA) K(NL) K(ND) K(NDA) K(JM) K(MAXPATH) K(MAXLP) K(NLOOP) K(NMIMIC) K(PATCH)
+  K(EXTRA) K(SHARED) K(FSHARED) K(REST) K(FSTART) K(TGT_HELD) K(CTRL_KIND) K(CTRL_A) K(CTRL_B) K(VLIM_FREE)
+  K(FRICTION_COMBINE) K(RESTITUTION_COMBINE) K(NCOLW) K(NCOL) K(MAXP) K(MAXC) K(MAXU) K(WH) K(AH)
+  K(MAXDENSE) K(ROWS) K(PO) K(DHDR) K(DPS)
+#undef K
+#define F(n) d.n = C.f(#n);
+  F(F_ANCHOR_BETA) F(F_CFM) F(F_OMEGA) F(F_SPEC) F(F_GAP_GATE) F(F_FGAP) F(F_FSCALE) F(F_REST_SPEED) F(F_FR_MUT)
+  F(F_FR_MUR) F(F_BP_CELL) F(F_JL_GAP) F(F_JL_SPEED)
+#undef F
+  if (d.NCOLW == 0u || d.NCOLW > 64u || d.NCOL != d.NCOLW * 32u) { why = "bad color table size"; return STEEL_E_INVALID; }
+  if (d.MAXC == 0u || d.MAXP == 0u || d.WH == 0u || d.AH == 0u) { why = "zero capacity"; return STEEL_E_INVALID; }
+  d.fps = C.get("PARAM_fps", 60.0);
+  d.substeps = C.u("PARAM_substeps", 4);
+  d.iterations = C.u("PARAM_iterations", 12);
+  d.target_frames = C.u("PARAM_target_frames");
+  d.driven = C.u("PARAM_driven");
+  d.integral_count = C.u("PARAM_integral_count");
+  d.user_targets = 0u;
+  d.beta = (float)C.get("PARAM_baumgarte", 0.2);
+  d.warm = (float)C.get("PARAM_warm", 0.0);
+  d.reg = (float)C.get("PARAM_reg", 0.0);
+  d.gx = (float)C.get("PARAM_gravity0", 0.0);
+  d.gy = (float)C.get("PARAM_gravity1", 0.0);
+  d.gz = (float)C.get("PARAM_gravity2", -9.81);
+  uint32_t NB = d.NB, NS = d.NS, NA = d.NA, NL = d.NL, ND = d.ND;
+  uint32_t NQ = C.u("A_QD") - C.u("A_Q");
+  d.NQ = NQ;
+  const uint32_t MAXC = d.MAXC;
+  // Articulation buffer (sim.js:452-455 order), sized with this scene's capacities.
+  {
+    size_t ao = 0;
+    auto put = [&](uint32_t& field, size_t n) { field = (uint32_t)ao; ao += n > 0 ? n : 1; };
+    uint32_t tmp;
+    put(d.A_Q, NQ); put(d.A_QD, ND); put(d.A_QDH, ND); put(d.A_INT, ND); put(d.A_TGT, ND); put(d.A_TGTV, ND);
+    put(d.A_LIM, 2 * ND); put(d.A_DRV, ND); put(tmp, ND); put(d.A_JF, ND); put(d.A_BF, NB * 8); put(tmp, (NB + NA) * 4);
+    put(d.A_FRIC, ND); put(d.A_HINV, ND); put(d.A_LINK, (size_t)(NL > 0 ? NL : 1) * 268); put(tmp, NB * 8 + ND);
+    put(d.A_VLG, ND + NB * 6); put(tmp, NA); put(d.A_LG, ND); put(d.A_RL, ND); put(d.A_RLN, NA);
+    put(d.A_ULOAD, d.PATCH ? (size_t)MAXC : 0); put(d.A_DENSE, (size_t)d.MAXDENSE * d.DPS);
+    s.art_floats = ao;
+  }
+  // Scheduling arrays; unit-indexed arrays are sized by MAXC (every contact may be its own unit).
+  {
+    size_t so = 0;
+    auto put = [&](uint32_t& field, size_t n) { field = (uint32_t)so; so += n > 0 ? n : 1; };
+    put(d.S_UNITOF, MAXC); put(d.S_DSLOT, MAXC); put(d.S_CORDER, MAXC); put(d.S_UKEY, MAXC);
+    put(d.S_USTART0, MAXC + 1); put(d.S_USIZE, MAXC); put(d.S_USTART, MAXC + 1); put(d.S_RK0, MAXC);
+    put(d.S_RK1, MAXC); put(d.S_RK2, MAXC); put(d.S_BPC, 4 * (size_t)MAXC); put(d.S_LEAD, MAXC);
+    put(d.S_KEEP, MAXC); put(d.S_SLOT, 26 * (size_t)MAXC); put(d.S_KEPT, MAXC); put(d.S_ROWOF, MAXC);
+    put(d.S_RUNIT, MAXC); put(d.S_RCON, MAXC); put(d.S_PCOL, MAXC); put(d.S_PORD, MAXC);
+    put(d.S_CSTART, d.NCOL + 2); put(d.S_META, 8); put(d.S_WWIN, d.WH); put(d.S_WSLOT, (size_t)MAXC + d.MAXDENSE);
+    put(d.S_WMASK, (size_t)NB * d.NCOLW); put(d.S_WCOUNT, d.NCOL + 2); put(d.S_LINKHIT, NB); put(d.S_JSPLIT, NL);
+    s.sched_words = so;
+  }
+  s.warm_words = 10ull * d.WH + 30ull * d.AH;
+  {
+    size_t a = 2ull * d.MAXPATH + 6ull * d.MAXPATH * d.JM;
+    size_t b = 5ull * d.NDA + 18ull * d.MAXLP + 8;
+    s.tscr_floats = a > b ? a : b;
+    d.TSCR = (uint32_t)s.tscr_floats;
+  }
+  // Host copies: static data and initial state (the reference's reset() contents).
+  s.statF.assign(in.statF, in.statF + in.statF_floats);
+  s.statU.assign(in.statU, in.statU + in.statU_words);
+  s.pos0.resize(NB); s.rot0.resize(NB); s.lv0.resize(NB); s.av0.resize(NB);
+  for (uint32_t b = 0; b < NB; b++) {
+    const float* p = in.body_pose + b * 8;
+    const float* v = in.body_vel + b * 8;
+    s.pos0[b] = make_float4(p[0], p[1], p[2], p[3]);
+    s.rot0[b] = make_float4(p[4], p[5], p[6], p[7]);
+    s.lv0[b] = make_float4(v[0], v[1], v[2], v[3]);
+    s.av0[b] = make_float4(v[4], v[5], v[6], v[7]);
+  }
+  s.art0.assign(s.art_floats, 0.0f);
+  auto copy_block = [&](uint32_t dst, const char* src_key, uint32_t n) {
+    uint32_t src = C.u(src_key);
+    for (uint32_t i = 0; i < n; i++) s.art0[dst + i] = in.art[src + i];
+  };
+  copy_block(d.A_Q, "A_Q", NQ);
+  copy_block(d.A_QD, "A_QD", ND);
+  copy_block(d.A_TGT, "A_TGT", ND);
+  copy_block(d.A_TGTV, "A_TGTV", ND);
+  // Arena pieces.
+  s.o_sf = L.take(s.statF.size() * 4);
+  s.o_su = L.take(s.statU.size() * 4);
+  s.o_pos = L.take((size_t)NB * 16); s.o_rot = L.take((size_t)NB * 16);
+  s.o_ppos = L.take((size_t)NB * 16); s.o_prot = L.take((size_t)NB * 16);
+  s.o_lv = L.take((size_t)NB * 16); s.o_av = L.take((size_t)NB * 16);
+  s.o_spos = L.take((size_t)NS * 16); s.o_srot = L.take((size_t)NS * 16);
+  s.o_alo = L.take((size_t)NS * 16); s.o_ahi = L.take((size_t)NS * 16);
+  s.o_art = L.take(s.art_floats * 4);
+  s.o_cnt = L.take(64); s.o_stats = L.take(64); s.o_params = L.take(sizeof(Params));
+  s.o_craw = L.take((size_t)MAXC * 6 * 16); s.o_con = L.take((size_t)MAXC * 6 * 16);
+  s.o_ckeys = L.take(next_pow2(MAXC) * 16);
+  s.o_rows = L.take((size_t)MAXC * d.ROWS * 16); s.o_slots = L.take((size_t)MAXC * 2 * 16);
+  s.o_warm = L.take(s.warm_words * 4);
+  s.o_sched = L.take(s.sched_words * 4);
+  s.o_tw = L.take((size_t)NB * 32); s.o_imp = L.take((size_t)NB * 32);
+  s.o_aqd = L.take((size_t)(ND > 0 ? ND : 1) * 4);
+  s.o_tscr = L.take((size_t)PREP_THREADS * s.tscr_floats * 4);
+  return STEEL_OK;
+}
+
+template <class T> T* at(uint8_t* base, size_t off) { return reinterpret_cast<T*>(base + off); }
+
+int upload_state(steel_batch* b) {
+  cudaStream_t st = b->ctx->stream;
+  for (auto& s : b->sc) {
+    const SceneDev& d = s.d;
+    CU(cudaMemcpyAsync(d.pos, s.pos0.data(), s.pos0.size() * 16, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(d.rot, s.rot0.data(), s.rot0.size() * 16, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(d.ppos, s.pos0.data(), s.pos0.size() * 16, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(d.prot, s.rot0.data(), s.rot0.size() * 16, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(d.lv, s.lv0.data(), s.lv0.size() * 16, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(d.av, s.av0.data(), s.av0.size() * 16, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(d.art, s.art0.data(), s.art0.size() * 4, cudaMemcpyHostToDevice, st));
+    CU(cudaMemsetAsync(d.warm_tab, 0, s.warm_words * 4, st));
+    CU(cudaMemsetAsync(d.counters, 0, 64, st));
+    CU(cudaMemsetAsync(d.stats, 0, 64, st));
+  }
+  CU(cudaMemsetAsync(b->bd.phase, 0, sizeof(double) * b->sc.size(), st));
+  CU(cudaMemsetAsync(b->bd.substep_count, 0, sizeof(unsigned long long), st));
+  CU(cudaMemsetAsync(b->bd.error, 0, sizeof(uint32_t), st));
+  return STEEL_OK;
+}
+
+void enqueue_substeps(steel_batch* b, cudaStream_t st) {
+  const BatchDev& bd = b->bd;
+  for (uint32_t s = 0; s < b->substeps; s++) {
+    launch_params(bd, s, st);
+    launch_shapes(bd, st);
+    launch_broad(bd, st);
+    launch_narrow(bd, b->narrow_blocks, st);
+    launch_csort(bd, b->sort_keys, st);
+    launch_prepare(bd, st);
+    launch_solve(bd, st);
+  }
+  launch_frame_end(bd, st);
+}
+
+int check_device_error(steel_batch* b) {
+  uint32_t e = 0;
+  CU(cudaMemcpyAsync(&e, b->bd.error, 4, cudaMemcpyDeviceToHost, b->ctx->stream));
+  CU(cudaStreamSynchronize(b->ctx->stream));
+  if (e == ERR_SORT_CAPACITY) return fail(STEEL_E_CAPACITY, "contact sort capacity exceeded");
+  if (e != 0) return fail(STEEL_E_CUDA, "device error " + std::to_string(e));
+  return STEEL_OK;
+}
+
+SceneHost* scene_of(steel_batch* b, uint32_t s) { return (b && s < b->sc.size()) ? &b->sc[s] : nullptr; }
+
+}  // namespace
+
+extern "C" {
+
+const char* steel_last_error(void) { return g_err.c_str(); }
+
+int steel_ctx_create(int device, steel_ctx** out) {
+  if (!out) return fail(STEEL_E_INVALID, "null output");
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(STEEL_E_NODEVICE, "no CUDA device");
+  if (device < 0 || device >= n) return fail(STEEL_E_INVALID, "bad device index");
+  CU(cudaSetDevice(device));
+  auto* c = new steel_ctx();
+  c->device = device;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->sms = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return fail(STEEL_E_CUDA, "stream creation failed");
+  }
+  *out = c;
+  return STEEL_OK;
+}
+
+int steel_ctx_destroy(steel_ctx* ctx) {
+  if (!ctx) return STEEL_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return STEEL_OK;
+}
+
+int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t n, steel_batch** out) {
+  if (!ctx || !scenes || !out || n == 0) return fail(STEEL_E_INVALID, "null argument or empty batch");
+  CU(cudaSetDevice(ctx->device));
+  std::unique_ptr<steel_batch> b(new steel_batch());
+  b->ctx = ctx;
+  b->sc.resize(n);
+  Layout L;
+  for (uint32_t i = 0; i < n; i++) {
+    std::string why;
+    int rc = build_scene(b->sc[i], scenes[i], L, why);
+    if (rc) return fail(rc, "scene " + std::to_string(i) + ": " + why);
+    if (i > 0 && b->sc[i].d.substeps != b->sc[0].d.substeps)
+      return fail(STEEL_E_INVALID, "scenes of one batch must share the substep count");
+  }
+  b->substeps = b->sc[0].d.substeps;
+  // Batch-level tables.
+  uint32_t pair_cap = 0;
+  size_t max_c = 1;
+  for (uint32_t i = 0; i < n; i++) {
+    const SceneDev& d = b->sc[i].d;
+    for (uint32_t s = 0; s < d.NS; s++) { b->shape_scene.push_back(i); b->shape_local.push_back(s); }
+    uint32_t nt = (d.NS + BROAD_TILE - 1) / BROAD_TILE;
+    for (uint32_t ti = 0; ti < nt; ti++)
+      for (uint32_t tj = ti; tj < nt; tj++) b->tiles.push_back(make_uint4(i, ti, tj, 0u));
+    pair_cap += d.MAXP;
+    max_c = std::max<size_t>(max_c, d.MAXC);
+  }
+  b->o_scenes = L.take(sizeof(SceneDev) * n);
+  b->o_shape_scene = L.take(4 * b->shape_scene.size() + 4);
+  b->o_shape_local = L.take(4 * b->shape_local.size() + 4);
+  b->o_tiles = L.take(16 * b->tiles.size() + 16);
+  b->o_pairs = L.take(16ull * pair_cap);
+  b->o_pair_count = L.take(4);
+  b->o_phase = L.take(8ull * n);
+  b->o_ssc = L.take(8);
+  b->o_err = L.take(4);
+  std::vector<uint64_t> tgt_off(n), pose_off(n);
+  for (uint32_t i = 0; i < n; i++) {
+    tgt_off[i] = b->n_targets;
+    pose_off[i] = b->n_poses;
+    b->n_targets += b->sc[i].d.ND;
+    b->n_poses += 8ull * b->sc[i].d.NB;
+  }
+  b->o_tgt_off = L.take(8ull * n);
+  b->o_pose_off = L.take(8ull * n);
+  b->o_tgt_buf = L.take(4ull * b->n_targets + 16);
+  b->o_pose_buf = L.take(4ull * b->n_poses + 16);
+  b->arena_bytes = L.bytes;
+  if (cudaMalloc(&b->arena, b->arena_bytes) != cudaSuccess)
+    return fail(STEEL_E_NOMEM, "device arena of " + std::to_string(b->arena_bytes) + " bytes");
+  cudaStream_t st = ctx->stream;
+  CU(cudaMemsetAsync(b->arena, 0, b->arena_bytes, st));
+  uint8_t* A = b->arena;
+  std::vector<SceneDev> dev(n);
+  for (uint32_t i = 0; i < n; i++) {
+    SceneHost& s = b->sc[i];
+    SceneDev& d = s.d;
+    d.sf = at<float4>(A, s.o_sf);
+    d.su = at<uint32_t>(A, s.o_su);
+    d.pos = at<float4>(A, s.o_pos); d.rot = at<float4>(A, s.o_rot);
+    d.ppos = at<float4>(A, s.o_ppos); d.prot = at<float4>(A, s.o_prot);
+    d.lv = at<float4>(A, s.o_lv); d.av = at<float4>(A, s.o_av);
+    d.spos = at<float4>(A, s.o_spos); d.srot = at<float4>(A, s.o_srot);
+    d.alo = at<float4>(A, s.o_alo); d.ahi = at<float4>(A, s.o_ahi);
+    d.art = at<float>(A, s.o_art);
+    d.counters = at<uint32_t>(A, s.o_cnt); d.stats = at<uint32_t>(A, s.o_stats);
+    d.params = at<Params>(A, s.o_params);
+    d.craw = at<float4>(A, s.o_craw); d.con = at<float4>(A, s.o_con); d.ckeys = at<uint4>(A, s.o_ckeys);
+    d.rows = at<float4>(A, s.o_rows); d.slots = at<float4>(A, s.o_slots);
+    d.warm_tab = at<uint32_t>(A, s.o_warm); d.sched = at<uint32_t>(A, s.o_sched);
+    d.tw = at<float4>(A, s.o_tw); d.imp = at<float4>(A, s.o_imp); d.aqd = at<float>(A, s.o_aqd);
+    d.tscr = at<float>(A, s.o_tscr);
+    d.scene_index = i;
+    dev[i] = d;
+    CU(cudaMemcpyAsync((void*)d.sf, s.statF.data(), s.statF.size() * 4, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync((void*)d.su, s.statU.data(), s.statU.size() * 4, cudaMemcpyHostToDevice, st));
+  }
+  BatchDev& bd = b->bd;
+  bd.scenes = at<SceneDev>(A, b->o_scenes);
+  bd.nscenes = n;
+  bd.nshapes = (uint32_t)b->shape_scene.size();
+  bd.shape_scene = at<uint32_t>(A, b->o_shape_scene);
+  bd.shape_local = at<uint32_t>(A, b->o_shape_local);
+  bd.tiles = at<uint4>(A, b->o_tiles);
+  bd.ntiles = (uint32_t)b->tiles.size();
+  bd.pairs = at<uint4>(A, b->o_pairs);
+  bd.pair_cap = pair_cap;
+  bd.pair_count = at<uint32_t>(A, b->o_pair_count);
+  bd.phase = at<double>(A, b->o_phase);
+  bd.substep_count = at<unsigned long long>(A, b->o_ssc);
+  bd.error = at<uint32_t>(A, b->o_err);
+  CU(cudaMemcpyAsync(bd.scenes, dev.data(), sizeof(SceneDev) * n, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync((void*)bd.shape_scene, b->shape_scene.data(), 4 * b->shape_scene.size(), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync((void*)bd.shape_local, b->shape_local.data(), 4 * b->shape_local.size(), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync((void*)bd.tiles, b->tiles.data(), 16 * b->tiles.size(), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(A + b->o_tgt_off, tgt_off.data(), 8ull * n, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(A + b->o_pose_off, pose_off.data(), 8ull * n, cudaMemcpyHostToDevice, st));
+  b->narrow_blocks = (uint32_t)ctx->sms * 8u;
+  b->sort_keys = std::min<size_t>(next_pow2(max_c), 8192);
+  CU(configure_sort(b->sort_keys));
+  CU(cudaEventCreate(&b->ev0));
+  CU(cudaEventCreate(&b->ev1));
+  int rc = upload_state(b.get());
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(st));
+  *out = b.release();
+  return STEEL_OK;
+}
+
+int steel_batch_destroy(steel_batch* b) {
+  if (!b) return STEEL_OK;
+  cudaSetDevice(b->ctx->device);
+  cudaStreamSynchronize(b->ctx->stream);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->arena) cudaFree(b->arena);
+  delete b;
+  return STEEL_OK;
+}
+
+int steel_scene_info_get(steel_batch* b, uint32_t scene, steel_scene_info* out) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || !out) return fail(STEEL_E_INVALID, "bad scene index");
+  const SceneDev& d = s->d;
+  *out = steel_scene_info{d.NB, d.NS, d.NA, d.NL, d.ND, d.NQ, d.MAXP, d.MAXC, d.MAXU, d.MAXDENSE};
+  return STEEL_OK;
+}
+
+int steel_reset(steel_batch* b) {
+  if (!b) return fail(STEEL_E_INVALID, "null batch");
+  CU(cudaSetDevice(b->ctx->device));
+  int rc = upload_state(b);
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(b->ctx->stream));
+  return STEEL_OK;
+}
+
+int steel_set_graph(steel_batch* b, int enabled) {
+  if (!b) return fail(STEEL_E_INVALID, "null batch");
+  b->use_graph = enabled != 0;
+  return STEEL_OK;
+}
+
+int steel_step(steel_batch* b, uint32_t frames) {
+  if (!b) return fail(STEEL_E_INVALID, "null batch");
+  CU(cudaSetDevice(b->ctx->device));
+  cudaStream_t st = b->ctx->stream;
+  if (b->use_graph && !b->graph) {
+    cudaGraph_t g;
+    CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    enqueue_substeps(b, st);
+    CU(cudaStreamEndCapture(st, &g));
+    cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(STEEL_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  }
+  for (uint32_t f = 0; f < frames; f++) {
+    if (b->use_graph) CU(cudaGraphLaunch(b->graph, st));
+    else enqueue_substeps(b, st);
+  }
+  CU(cudaGetLastError());
+  return STEEL_OK;
+}
+
+int steel_step_timed(steel_batch* b, uint32_t frames, float* ms) {
+  if (!b || !ms) return fail(STEEL_E_INVALID, "null argument");
+  CU(cudaSetDevice(b->ctx->device));
+  CU(cudaEventRecord(b->ev0, b->ctx->stream));
+  int rc = steel_step(b, frames);
+  if (rc) return rc;
+  CU(cudaEventRecord(b->ev1, b->ctx->stream));
+  CU(cudaEventSynchronize(b->ev1));
+  CU(cudaEventElapsedTime(ms, b->ev0, b->ev1));
+  return check_device_error(b);
+}
+
+int steel_step_io(steel_batch* b, uint32_t frames, const float* targets, uint64_t n_targets, float* poses,
+                  uint64_t n_poses) {
+  if (!b) return fail(STEEL_E_INVALID, "null batch");
+  if (targets && n_targets != b->n_targets)
+    return fail(STEEL_E_INVALID, "expected " + std::to_string(b->n_targets) + " targets");
+  if (poses && n_poses != b->n_poses) return fail(STEEL_E_INVALID, "expected " + std::to_string(b->n_poses) + " pose floats");
+  CU(cudaSetDevice(b->ctx->device));
+  cudaStream_t st = b->ctx->stream;
+  uint8_t* A = b->arena;
+  if (targets && b->n_targets) {
+    CU(cudaMemcpyAsync(A + b->o_tgt_buf, targets, 4ull * b->n_targets, cudaMemcpyHostToDevice, st));
+    launch_scatter_targets(b->bd, (const float*)(A + b->o_tgt_buf), (const uint64_t*)(A + b->o_tgt_off), st);
+    for (auto& s : b->sc) s.d.user_targets = s.d.ND ? 1u : s.d.user_targets;
+  }
+  int rc = steel_step(b, frames);
+  if (rc) return rc;
+  if (poses) {
+    launch_gather_poses(b->bd, (float*)(A + b->o_pose_buf), (const uint64_t*)(A + b->o_pose_off), st);
+    CU(cudaMemcpyAsync(poses, A + b->o_pose_buf, 4ull * b->n_poses, cudaMemcpyDeviceToHost, st));
+  }
+  CU(cudaStreamSynchronize(st));
+  return STEEL_OK;
+}
+
+int steel_profile_kernels(steel_batch* b, uint32_t frames, float* ms_per_launch) {
+  if (!b || !ms_per_launch) return fail(STEEL_E_INVALID, "null argument");
+  CU(cudaSetDevice(b->ctx->device));
+  cudaStream_t st = b->ctx->stream;
+  const int NK = 7;
+  std::vector<cudaEvent_t> ev(2 * NK * b->substeps);
+  for (auto& e : ev) CU(cudaEventCreate(&e));
+  double acc[NK] = {0};
+  for (uint32_t f = 0; f < frames; f++) {
+    for (uint32_t s = 0; s < b->substeps; s++) {
+      cudaEvent_t* e = ev.data() + 2 * NK * s;
+      CU(cudaEventRecord(e[0], st)); launch_params(b->bd, s, st); CU(cudaEventRecord(e[1], st));
+      CU(cudaEventRecord(e[2], st)); launch_shapes(b->bd, st); CU(cudaEventRecord(e[3], st));
+      CU(cudaEventRecord(e[4], st)); launch_broad(b->bd, st); CU(cudaEventRecord(e[5], st));
+      CU(cudaEventRecord(e[6], st)); launch_narrow(b->bd, b->narrow_blocks, st); CU(cudaEventRecord(e[7], st));
+      CU(cudaEventRecord(e[8], st)); launch_csort(b->bd, b->sort_keys, st); CU(cudaEventRecord(e[9], st));
+      CU(cudaEventRecord(e[10], st)); launch_prepare(b->bd, st); CU(cudaEventRecord(e[11], st));
+      CU(cudaEventRecord(e[12], st)); launch_solve(b->bd, st); CU(cudaEventRecord(e[13], st));
+    }
+    launch_frame_end(b->bd, st);
+    CU(cudaStreamSynchronize(st));
+    for (uint32_t s = 0; s < b->substeps; s++)
+      for (int k = 0; k < NK; k++) {
+        float ms = 0.0f;
+        CU(cudaEventElapsedTime(&ms, ev[2 * NK * s + 2 * k], ev[2 * NK * s + 2 * k + 1]));
+        acc[k] += ms;
+      }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (int k = 0; k < NK; k++) ms_per_launch[k] = (float)(acc[k] / ((double)frames * b->substeps));
+  return check_device_error(b);
+}
+
+int steel_sync(steel_batch* b) {
+  if (!b) return fail(STEEL_E_INVALID, "null batch");
+  CU(cudaSetDevice(b->ctx->device));
+  CU(cudaStreamSynchronize(b->ctx->stream));
+  return check_device_error(b);
+}
+
+int steel_read_poses(steel_batch* b, uint32_t scene, float* poses) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || !poses) return fail(STEEL_E_INVALID, "bad scene index or null buffer");
+  CU(cudaSetDevice(b->ctx->device));
+  const SceneDev& d = s->d;
+  std::vector<float4> p(d.NB), q(d.NB);
+  cudaStream_t st = b->ctx->stream;
+  CU(cudaMemcpyAsync(p.data(), d.pos, 16ull * d.NB, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(q.data(), d.rot, 16ull * d.NB, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  for (uint32_t i = 0; i < d.NB; i++) {
+    std::memcpy(poses + i * 8, &p[i], 16);
+    std::memcpy(poses + i * 8 + 4, &q[i], 16);
+  }
+  return STEEL_OK;
+}
+
+int steel_read_state(steel_batch* b, uint32_t scene, float* poses, float* vel, float* q, float* qd, float* link_v) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s) return fail(STEEL_E_INVALID, "bad scene index");
+  int rc = poses ? steel_read_poses(b, scene, poses) : STEEL_OK;
+  if (rc) return rc;
+  const SceneDev& d = s->d;
+  cudaStream_t st = b->ctx->stream;
+  if (vel) {
+    std::vector<float4> v(d.NB), w(d.NB);
+    CU(cudaMemcpyAsync(v.data(), d.lv, 16ull * d.NB, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(w.data(), d.av, 16ull * d.NB, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    for (uint32_t i = 0; i < d.NB; i++) { std::memcpy(vel + i * 8, &v[i], 16); std::memcpy(vel + i * 8 + 4, &w[i], 16); }
+  }
+  if (q && d.NQ) CU(cudaMemcpyAsync(q, d.art + d.A_Q, 4ull * d.NQ, cudaMemcpyDeviceToHost, st));
+  if (qd && d.ND) CU(cudaMemcpyAsync(qd, d.art + d.A_QD, 4ull * d.ND, cudaMemcpyDeviceToHost, st));
+  if (link_v)
+    for (uint32_t l = 0; l < d.NL; l++)
+      CU(cudaMemcpyAsync(link_v + l * 6, d.art + d.A_LINK + l * 268u + 147u, 24, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  return STEEL_OK;
+}
+
+int steel_get_stats(steel_batch* b, uint32_t scene, steel_stats* out) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || !out) return fail(STEEL_E_INVALID, "bad scene index or null output");
+  CU(cudaSetDevice(b->ctx->device));
+  uint32_t w[16];
+  CU(cudaMemcpyAsync(w, s->d.stats, 64, cudaMemcpyDeviceToHost, b->ctx->stream));
+  CU(cudaStreamSynchronize(b->ctx->stream));
+  const SceneDev& d = s->d;
+  out->max_contacts = w[1]; out->max_colors = w[2]; out->max_units = w[3]; out->max_pairs = w[4];
+  out->contacts = w[5]; out->colors = w[6]; out->max_dense = w[7]; out->asleep = w[8];
+  out->overflow = (w[4] >= d.MAXP ? 1u : 0u) | (w[1] >= d.MAXC ? 2u : 0u) | (w[3] >= d.MAXU ? 4u : 0u) |
+                  (w[7] >= d.MAXDENSE ? 8u : 0u);
+  return STEEL_OK;
+}
+
+static int write_dev(steel_batch* b, void* dst, const void* src, size_t bytes) {
+  CU(cudaSetDevice(b->ctx->device));
+  CU(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, b->ctx->stream));
+  CU(cudaStreamSynchronize(b->ctx->stream));
+  return STEEL_OK;
+}
+
+int steel_set_joint_target(steel_batch* b, uint32_t scene, uint32_t dof, float pos, float vel) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || dof >= s->d.ND) return fail(STEEL_E_INVALID, "bad scene or dof index");
+  int rc = write_dev(b, s->d.art + s->d.A_TGT + dof, &pos, 4);
+  if (!rc) rc = write_dev(b, s->d.art + s->d.A_TGTV + dof, &vel, 4);
+  if (!rc && !s->d.user_targets) {
+    // A user target replaces the scene's recorded trajectory (sim.js:720): driven = 0 from now on.
+    s->d.user_targets = 1u;
+    SceneDev* dd = b->bd.scenes + scene;
+    rc = write_dev(b, &dd->user_targets, &s->d.user_targets, 4);
+  }
+  return rc;
+}
+int steel_set_joint_force(steel_batch* b, uint32_t scene, uint32_t dof, float value) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || dof >= s->d.ND) return fail(STEEL_E_INVALID, "bad scene or dof index");
+  return write_dev(b, s->d.art + s->d.A_JF + dof, &value, 4);
+}
+int steel_set_body_wrench(steel_batch* b, uint32_t scene, uint32_t body, const float force[3], const float torque[3]) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || body >= s->d.NB) return fail(STEEL_E_INVALID, "bad scene or body index");
+  float w[8] = {force[0], force[1], force[2], 0.0f, torque[0], torque[1], torque[2], 0.0f};
+  return write_dev(b, s->d.art + s->d.A_BF + body * 8u, w, 32);
+}
+int steel_set_body_pose(steel_batch* b, uint32_t scene, uint32_t body, const float com[3], const float quat[4]) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || body >= s->d.NB) return fail(STEEL_E_INVALID, "bad scene or body index");
+  float4 p = make_float4(com[0], com[1], com[2], 0.0f), q = make_float4(quat[0], quat[1], quat[2], quat[3]);
+  int rc = write_dev(b, s->d.pos + body, &p, 16);
+  return rc ? rc : write_dev(b, s->d.rot + body, &q, 16);
+}
+int steel_set_body_twist(steel_batch* b, uint32_t scene, uint32_t body, const float twist[6]) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || body >= s->d.NB) return fail(STEEL_E_INVALID, "bad scene or body index");
+  float4 v = make_float4(twist[0], twist[1], twist[2], 0.0f), w = make_float4(twist[3], twist[4], twist[5], 0.0f);
+  int rc = write_dev(b, s->d.lv + body, &v, 16);
+  return rc ? rc : write_dev(b, s->d.av + body, &w, 16);
+}
+
+int steel_collide(steel_batch* b) {
+  if (!b) return fail(STEEL_E_INVALID, "null batch");
+  CU(cudaSetDevice(b->ctx->device));
+  cudaStream_t st = b->ctx->stream;
+  for (auto& s : b->sc) CU(cudaMemsetAsync(s.d.counters, 0, 8, st));
+  launch_params(b->bd, 0, st);
+  launch_shapes(b->bd, st);
+  launch_broad(b->bd, st);
+  launch_narrow(b->bd, b->narrow_blocks, st);
+  launch_csort(b->bd, b->sort_keys, st);
+  CU(cudaGetLastError());
+  int rc = steel_sync(b);
+  if (rc) return rc;
+  // Keep the counts for the readers and leave the counters as a finished substep leaves them.
+  for (auto& s : b->sc) {
+    uint32_t c[2];
+    CU(cudaMemcpy(c, s.d.counters, 8, cudaMemcpyDeviceToHost));
+    s.collide_pairs = c[0];
+    s.collide_contacts = c[1];
+    CU(cudaMemset(s.d.counters, 0, 8));
+  }
+  return STEEL_OK;
+}
+
+int steel_debug_stage(steel_batch* b, int stage) {
+  if (!b) return fail(STEEL_E_INVALID, "null batch");
+  CU(cudaSetDevice(b->ctx->device));
+  cudaStream_t st = b->ctx->stream;
+  if (stage == 0) {
+    launch_params(b->bd, b->debug_substep, st);
+    launch_shapes(b->bd, st);
+    launch_broad(b->bd, st);
+    launch_narrow(b->bd, b->narrow_blocks, st);
+    launch_csort(b->bd, b->sort_keys, st);
+  } else if (stage == 1) {
+    launch_prepare(b->bd, st);
+  } else if (stage == 2) {
+    launch_solve(b->bd, st);
+    if (++b->debug_substep == b->substeps) { launch_frame_end(b->bd, st); b->debug_substep = 0; }
+  } else {
+    return fail(STEEL_E_INVALID, "bad stage");
+  }
+  CU(cudaGetLastError());
+  return steel_sync(b);
+}
+
+int steel_read_words(steel_batch* b, uint32_t scene, const char* buffer, uint64_t offset, uint64_t count, void* out) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || !buffer || !out) return fail(STEEL_E_INVALID, "bad scene index or null argument");
+  const SceneDev& d = s->d;
+  std::string n(buffer);
+  const void* base = nullptr;
+  uint64_t words = 0;
+  if (n == "art") { base = d.art; words = s->art_floats; }
+  else if (n == "rows") { base = d.rows; words = (uint64_t)d.MAXC * d.ROWS * 4; }
+  else if (n == "sched") { base = d.sched; words = s->sched_words; }
+  else if (n == "slots") { base = d.slots; words = (uint64_t)d.MAXC * 8; }
+  else if (n == "warm") { base = d.warm_tab; words = s->warm_words; }
+  else if (n == "contacts") { base = d.con; words = (uint64_t)d.MAXC * 24; }
+  else return fail(STEEL_E_INVALID, "unknown buffer " + n);
+  if (offset + count > words) return fail(STEEL_E_INVALID, "read past the end of " + n);
+  CU(cudaSetDevice(b->ctx->device));
+  CU(cudaMemcpy(out, (const uint32_t*)base + offset, count * 4, cudaMemcpyDeviceToHost));
+  return STEEL_OK;
+}
+
+int steel_layout_get(steel_batch* b, uint32_t scene, const char* key, uint64_t* value) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || !key || !value) return fail(STEEL_E_INVALID, "bad scene index or null argument");
+  const SceneDev& d = s->d;
+#define L1(k) if (!std::strcmp(key, #k)) { *value = d.k; return STEEL_OK; }
+  L1(A_Q) L1(A_QD) L1(A_QDH) L1(A_INT) L1(A_TGT) L1(A_TGTV) L1(A_LIM) L1(A_DRV) L1(A_JF) L1(A_BF) L1(A_FRIC)
+  L1(A_HINV) L1(A_LINK) L1(A_VLG) L1(A_LG) L1(A_RL) L1(A_RLN) L1(A_ULOAD) L1(A_DENSE) L1(ROWS) L1(PO)
+  L1(S_UKEY) L1(S_USIZE) L1(S_USTART) L1(S_RUNIT) L1(S_RCON) L1(S_PCOL) L1(S_PORD) L1(S_CSTART) L1(S_META)
+  L1(S_KEEP) L1(S_CORDER) L1(S_KEPT)
+#undef L1
+  return fail(STEEL_E_INVALID, std::string("unknown layout key ") + key);
+}
+
+int steel_read_pairs(steel_batch* b, uint32_t scene, uint32_t* pairs, uint32_t cap, uint32_t* count) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || !count) return fail(STEEL_E_INVALID, "bad scene index or null output");
+  CU(cudaSetDevice(b->ctx->device));
+  uint32_t total = 0;
+  CU(cudaMemcpy(&total, b->bd.pair_count, 4, cudaMemcpyDeviceToHost));
+  std::vector<uint4> all(total);
+  if (total) CU(cudaMemcpy(all.data(), b->bd.pairs, 16ull * total, cudaMemcpyDeviceToHost));
+  uint32_t n = 0;
+  for (auto& p : all) {
+    if (p.x != scene) continue;
+    if (pairs && n < cap) { pairs[2 * n] = p.y; pairs[2 * n + 1] = p.z; }
+    n++;
+  }
+  *count = n;
+  return STEEL_OK;
+}
+
+int steel_read_contacts(steel_batch* b, uint32_t scene, float* records, uint32_t cap, uint32_t* count) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || !count) return fail(STEEL_E_INVALID, "bad scene index or null output");
+  CU(cudaSetDevice(b->ctx->device));
+  const SceneDev& d = s->d;
+  uint32_t nc = std::min(s->collide_contacts, d.MAXC);
+  *count = nc;
+  if (!records) return STEEL_OK;
+  uint32_t n = std::min(nc, cap);
+  if (n) {
+    CU(cudaMemcpy(records, d.con, 80ull * n, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(records + 20ull * n, d.con + (size_t)d.MAXC * 5, 16ull * n, cudaMemcpyDeviceToHost));
+  }
+  return STEEL_OK;
+}
+
+}  // extern "C"

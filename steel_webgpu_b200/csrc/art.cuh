@@ -1,0 +1,567 @@
+// Articulated-body (Featherstone) device library for one articulation per thread.
+//
+// Follows packages/steel-webgpu/src/artwgsl.js: link FK (artwgsl.js:98-187), the articulated
+// inertia factorisation with implicit PD drives in D (artwgsl.js:210-369), the split COM
+// response of a contact-bearing link (artwgsl.js:431-510), the H^-1 diagonal of a dof
+// (artwgsl.js:513-518), generalized Jacobians and solves (artwgsl.js:525-596) and the impulse
+// propagation of the solve (wgsl.js:3240-3299). Spatial quantities are expressed at each link's
+// COM with world orientation. Per-link records keep the reference's 268-float block layout in
+// the scene's articulation buffer; path-length temporaries live in a per-thread slice of global
+// scratch (deep chains do not fit in registers).
+#pragma once
+#include "common.cuh"
+
+namespace steel {
+
+enum : uint32_t {
+  L_S = 0, L_U = 36, L_DI = 72, L_IA = 108, L_C = 135, L_PA = 141, L_V = 147, L_W = 153, L_A = 189, L_UU = 195,
+  L_P = 201, L_DV = 207, L_POS = 213, L_ROT = 216, L_COM = 220, L_TAU = 223, L_JR = 229, L_W2 = 232, LBLK = 268
+};
+
+struct SVec { f3 a, l; };
+SD SVec sv0() { return SVec{sp3(0.0f), sp3(0.0f)}; }
+SD SVec sadd(SVec x, SVec y) { return SVec{x.a + y.a, x.l + y.l}; }
+SD SVec sscl(SVec x, float s) { return SVec{x.a * s, x.l * s}; }
+SD float sdot(SVec m, SVec f) { return dot(m.a, f.a) + dot(m.l, f.l); }
+SD SVec crm(SVec v, SVec m) { return SVec{cross(v.a, m.a), cross(v.a, m.l) + cross(v.l, m.a)}; }
+SD SVec crf(SVec v, SVec f) { return SVec{cross(v.a, f.a) + cross(v.l, f.l), cross(v.a, f.l)}; }
+SD m3 skew(f3 r) { return mcols(mf3(0.0f, r.z, -r.y), mf3(-r.z, 0.0f, r.x), mf3(r.y, -r.x, 0.0f)); }
+SD m3 outer(f3 x, f3 y) { return mcols(x * y.x, x * y.y, x * y.z); }
+SD SVec mshift(SVec m, f3 r) { return SVec{m.a, m.l + cross(m.a, r)}; }
+SD SVec fshift(SVec f, f3 r) { return SVec{f.a + cross(r, f.l), f.l}; }
+SD float4 qaxis(f3 axis, float angle) { return mf4(axis * fsin(0.5f * angle), fcos(0.5f * angle)); }
+SD f3 unit_axis(uint32_t c) { return c == 0 ? mf3(1, 0, 0) : (c == 1 ? mf3(0, 1, 0) : mf3(0, 0, 1)); }
+
+struct Art {
+  const SceneDev& S;
+  float* A;  // the scene's articulation buffer
+  __device__ Art(const SceneDev& s) : S(s), A(s.art) {}
+
+  __device__ float4 lrec(uint32_t l, uint32_t k) const { return S.sf[S.SF_LINK + l * 6u + k]; }
+  __device__ uint32_t ltype(uint32_t l) const { return f2u(lrec(l, 0).x); }
+  __device__ int lparent(uint32_t l) const { return f2i(lrec(l, 0).y); }
+  __device__ uint32_t ldof(uint32_t l) const { return f2u(lrec(l, 0).z); }
+  __device__ int lbody(uint32_t l) const { return f2i(lrec(l, 0).w); }
+  __device__ uint32_t lndof(uint32_t l) const { return f2u(lrec(l, 1).w); }
+  __device__ uint32_t lqs(uint32_t l) const { return f2u(lrec(l, 3).w); }
+  __device__ float4 dof_drive(uint32_t d) const { return S.sf[S.SF_DOF + d * 5u]; }
+  __device__ float4 dof_limit(uint32_t d) const { return S.sf[S.SF_DOF + d * 5u + 1u]; }
+  __device__ float4 dof_passive(uint32_t d) const { return S.sf[S.SF_DOF + d * 5u + 2u]; }
+  __device__ f3 dof_axis(uint32_t d) const { return v3(S.sf[S.SF_DOF + d * 5u + 3u]); }
+  __device__ bool scalar_dof(uint32_t d) const { return S.sf[S.SF_DOF + d * 5u + 2u].w > 0.5f; }
+  __device__ uint4 info(uint32_t a) const {
+    const uint32_t* p = S.su + S.SU_ART + a * 4u;
+    return make_uint4(p[0], p[1], p[2], p[3]);
+  }
+  __device__ float bmass(int b) const { return S.sf[S.SF_BODY + (uint32_t)b * 8u + 1u].w; }
+  __device__ m3 binertia(int b) const {
+    const float4* o = S.sf + S.SF_BODY + (uint32_t)b * 8u;
+    return tr(mcols(v3(o[2]), v3(o[3]), v3(o[4])));
+  }
+  __device__ uint32_t lo(uint32_t l) const { return S.A_LINK + l * LBLK; }
+  __device__ f3 ld3(uint32_t o) const { return mf3(A[o], A[o + 1], A[o + 2]); }
+  __device__ void st3(uint32_t o, f3 v) const { A[o] = v.x; A[o + 1] = v.y; A[o + 2] = v.z; }
+  __device__ SVec ldsv(uint32_t o) const { return SVec{ld3(o), ld3(o + 3u)}; }
+  __device__ void stsv(uint32_t o, SVec s) const { st3(o, s.a); st3(o + 3u, s.l); }
+  __device__ m3 ldm(uint32_t o) const { return mcols(ld3(o), ld3(o + 3u), ld3(o + 6u)); }
+  __device__ void stm(uint32_t o, const m3& m) const { st3(o, m.c[0]); st3(o + 3u, m.c[1]); st3(o + 6u, m.c[2]); }
+  __device__ SVec imul(uint32_t o, SVec m) const {
+    m3 Am = ldm(o), Bm = ldm(o + 9u), Cm = ldm(o + 18u);
+    return SVec{mul(Am, m.a) + mul(Bm, m.l), mul(tr(Bm), m.a) + mul(Cm, m.l)};
+  }
+  __device__ SVec ldS(uint32_t l, uint32_t k) const { return ldsv(lo(l) + L_S + k * 6u); }
+  __device__ SVec ldU(uint32_t l, uint32_t k) const { return ldsv(lo(l) + L_U + k * 6u); }
+  __device__ float ldDI(uint32_t l, uint32_t r, uint32_t c) const { return A[lo(l) + L_DI + r * S.JM + c]; }
+  __device__ f3 link_r(uint32_t l) const {
+    int par = lparent(l);
+    if (par < 0) return sp3(0.0f);
+    return ld3(lo(l) + L_COM) - ld3(lo((uint32_t)par) + L_COM);
+  }
+  __device__ float4 link_rot(uint32_t l) const { return mf4(ld3(lo(l) + L_ROT), A[lo(l) + L_ROT + 3u]); }
+
+  // Link poses, COMs and world motion subspaces (artwgsl.js:98-187).
+  __device__ void fk(uint32_t a) const {
+    uint4 ai = info(a);
+    const float* Q = A + S.A_Q;
+    for (uint32_t k = 0; k < ai.y; k++) {
+      uint32_t l = ai.x + k;
+      float4 r0 = lrec(l, 0), r1 = lrec(l, 1), r2 = lrec(l, 2), r3 = lrec(l, 3), r4 = lrec(l, 4), r5 = lrec(l, 5);
+      f3 pp = sp3(0.0f);
+      float4 pq = make_float4(0, 0, 0, 1);
+      int par = f2i(r0.y);
+      if (par >= 0) { pp = ld3(lo((uint32_t)par) + L_POS); pq = link_rot((uint32_t)par); }
+      f3 jp = pp + qrot(pq, v3(r1));
+      float4 jq = qmul(pq, r2);
+      f3 axis = v3(r5);
+      float4 mq = make_float4(0, 0, 0, 1);
+      f3 mp = sp3(0.0f);
+      uint32_t t = f2u(r0.x), qs = f2u(r3.w), d0 = f2u(r0.z);
+      if (t == 1u) mq = qaxis(axis, Q[qs]);
+      if (t == 0u) mp = axis * Q[qs];
+      if (t == 2u) mq = nrm4(make_float4(Q[qs], Q[qs + 1], Q[qs + 2], Q[qs + 3]));
+      uint32_t nlin = f2u(r5.w), nang = f2u(r1.w) - nlin;
+      f3 ang[3] = {sp3(0.0f), sp3(0.0f), sp3(0.0f)};
+      if (t == 6u) {
+        for (uint32_t c = 0; c < nlin; c++) mp += dof_axis(d0 + c) * Q[qs + c];
+        uint32_t iq = qs + nlin;
+        if (nang == 1u) { ang[0] = dof_axis(d0 + nlin); mq = qaxis(ang[0], Q[iq]); }
+        if (nang == 2u) {
+          f3 x0 = nrm(dof_axis(d0 + nlin));
+          f3 x2 = nrm(cross(x0, dof_axis(d0 + nlin + 1u)));
+          ang[0] = x0;
+          float4 q0 = qaxis(x0, Q[iq]);
+          ang[1] = qrot(q0, cross(x2, x0));
+          mq = qmul(qaxis(ang[1], Q[iq + 1u]), q0);
+        }
+        if (nang == 3u) {
+          ang[0] = dof_axis(d0 + nlin);
+          float4 q0 = qaxis(ang[0], Q[iq]);
+          ang[1] = qrot(q0, dof_axis(d0 + nlin + 1u));
+          float4 q1 = qaxis(ang[1], Q[iq + 1u]);
+          ang[2] = qrot(qmul(q1, q0), dof_axis(d0 + nlin + 2u));
+          mq = qmul(qaxis(ang[2], Q[iq + 2u]), qmul(q1, q0));
+        }
+      }
+      if (t == 4u) {
+        mp = mf3(Q[qs], Q[qs + 1], Q[qs + 2]);
+        mq = nrm4(make_float4(Q[qs + 3], Q[qs + 4], Q[qs + 5], Q[qs + 6]));
+      }
+      float4 cq = qmul(jq, mq);
+      f3 cp = jp + qrot(jq, mp);
+      float4 iq = qconj(r4);
+      float4 lq = nrm4(qmul(cq, iq));
+      f3 lp = cp + qrot(cq, -qrot(iq, v3(r3)));
+      uint32_t L = lo(l);
+      st3(L + L_POS, lp);
+      st3(L + L_ROT, v3(lq));
+      A[L + L_ROT + 3u] = lq.w;
+      f3 com = lp + qrot(lq, v3(S.sf[S.SF_BODY + (uint32_t)f2i(r0.w) * 8u + 1u]));
+      st3(L + L_COM, com);
+      f3 aw = qrot(jq, axis);
+      f3 rj = com - jp;
+      for (uint32_t c = 0; c < S.JM; c++) stsv(L + L_S + c * 6u, sv0());
+      if (t == 1u) stsv(L + L_S, SVec{aw, cross(aw, rj)});
+      if (t == 0u) stsv(L + L_S, SVec{sp3(0.0f), aw});
+      if (t == 2u)
+        for (uint32_t c = 0; c < 3u; c++) { f3 ew = qrot(jq, unit_axis(c)); stsv(L + L_S + c * 6u, SVec{ew, cross(ew, rj)}); }
+      f3 rf = com - cp;
+      st3(L + L_JR, rf);
+      if (t == 6u) {
+        for (uint32_t c = 0; c < nlin; c++) stsv(L + L_S + c * 6u, SVec{sp3(0.0f), qrot(jq, dof_axis(d0 + c))});
+        for (uint32_t c = 0; c < nang; c++) { f3 ew = qrot(jq, ang[c]); stsv(L + L_S + (nlin + c) * 6u, SVec{ew, cross(ew, rf)}); }
+      }
+      if (t == 4u) {
+        for (uint32_t c = 0; c < 3u; c++) {
+          f3 ew = qrot(jq, unit_axis(c));
+          stsv(L + L_S + c * 6u, SVec{sp3(0.0f), ew});
+          stsv(L + L_S + (c + 3u) * 6u, SVec{ew, cross(ew, rf)});
+        }
+      }
+    }
+  }
+
+  // Gauss-Jordan inverse of the leading n x n block (artwgsl.js:192-207).
+  static __device__ void inv_spd(float* D, uint32_t n, uint32_t JM, float* Di) {
+    for (uint32_t i = 0; i < JM * JM; i++) Di[i] = 0.0f;
+    for (uint32_t i = 0; i < n; i++) Di[i * JM + i] = 1.0f;
+    for (uint32_t c = 0; c < n; c++) {
+      float pv = 1.0f / fmx(D[c * JM + c], 1e-12f);
+      for (uint32_t k = 0; k < n; k++) { D[c * JM + k] *= pv; Di[c * JM + k] *= pv; }
+      for (uint32_t r = 0; r < n; r++) {
+        if (r == c) continue;
+        float f = D[r * JM + c];
+        if (f == 0.0f) continue;
+        for (uint32_t k = 0; k < n; k++) { D[r * JM + k] -= f * D[c * JM + k]; Di[r * JM + k] -= f * Di[c * JM + k]; }
+      }
+    }
+  }
+
+  // Articulated inertias, U = I^A S, D^-1 with implicit drives, free velocity (artwgsl.js:210-369).
+  __device__ void factor(uint32_t a, const Params& P) const {
+    uint4 ai = info(a);
+    f3 g = v3(P.gravity);
+    const uint32_t JM = S.JM;
+    for (uint32_t k = 0; k < ai.y; k++) {
+      uint32_t l = ai.x + k, L = lo(l);
+      int par = lparent(l);
+      SVec vp = sv0();
+      if (par >= 0) vp = mshift(ldsv(lo((uint32_t)par) + L_V), link_r(l));
+      SVec sq = sv0();
+      uint32_t nd = lndof(l), d0 = ldof(l);
+      for (uint32_t c = 0; c < nd; c++) sq = sadd(sq, sscl(ldS(l, c), A[S.A_QD + d0 + c]));
+      SVec v = sadd(vp, sq);
+      stsv(L + L_V, v);
+      SVec cb = crm(vp, sq);
+      uint32_t jt = ltype(l);
+      if (jt == 6u) {
+        uint32_t nlin = f2u(lrec(l, 5).w);
+        f3 ca = sp3(0.0f);
+        for (uint32_t j = nlin; j < nd; j++)
+          for (uint32_t kk = j + 1u; kk < nd; kk++)
+            ca += (cross(ldS(l, j).a, ldS(l, kk).a) * A[S.A_QD + d0 + j]) * A[S.A_QD + d0 + kk];
+        cb = sadd(cb, SVec{ca, cross(ca, ld3(L + L_JR))});
+      }
+      if (jt == 4u || jt == 6u) {
+        uint32_t nlin = jt == 4u ? 3u : f2u(lrec(l, 5).w);
+        f3 vo = sp3(0.0f), wj = sp3(0.0f);
+        for (uint32_t c = 0; c < nd; c++) {
+          SVec sc = ldS(l, c);
+          float q = A[S.A_QD + d0 + c];
+          if (c < nlin) vo += sc.l * q; else wj += sc.a * q;
+        }
+        cb = sadd(cb, SVec{sp3(0.0f), -cross(wj, vo)});
+      }
+      stsv(L + L_C, cb);
+      int b = lbody(l);
+      float m = bmass(b);
+      m3 R = qmat(link_rot(l));
+      m3 Ic = mul(mul(R, binertia(b)), tr(R));
+      stm(L + L_IA, Ic);
+      stm(L + L_IA + 9u, mcols(sp3(0), sp3(0), sp3(0)));
+      stm(L + L_IA + 18u, mcols(mf3(m, 0, 0), mf3(0, m, 0), mf3(0, 0, m)));
+      SVec pa0 = crf(v, imul(L + L_IA, v));
+      if ((f2u(S.sf[S.SF_BODY + (uint32_t)b * 8u + 7u].w) & 2u) != 0u) pa0 = sadd(pa0, SVec{sp3(0.0f), m * g});
+      pa0 = sadd(pa0, SVec{-ld3(S.A_BF + (uint32_t)b * 8u + 4u), -ld3(S.A_BF + (uint32_t)b * 8u)});
+      stsv(L + L_PA, pa0);
+    }
+    for (uint32_t kk = 0; kk < ai.y; kk++) {
+      uint32_t l = ai.x + ai.y - 1u - kk, L = lo(l);
+      uint32_t n = lndof(l), d0 = ldof(l), qs = lqs(l);
+      SVec pA = ldsv(L + L_PA);
+      float D[36];
+      for (uint32_t i = 0; i < 36u; i++) D[i] = 0.0f;
+      float u[6] = {0, 0, 0, 0, 0, 0};
+      for (uint32_t c = 0; c < n; c++) stsv(L + L_U + c * 6u, imul(L + L_IA, ldS(l, c)));
+      for (uint32_t r = 0; r < n; r++) {
+        uint32_t d = d0 + r;
+        for (uint32_t c = 0; c < n; c++) D[r * JM + c] = sdot(ldS(l, r), ldU(l, c));
+        float4 dr = dof_drive(d);
+        D[r * JM + r] += dr.x;
+        float damp = dof_passive(d).x;
+        D[r * JM + r] += P.dt * damp;
+        float tau = (-damp) * A[S.A_QD + d] + A[S.A_JF + d];
+        float4 spr = S.sf[S.SF_DOF + d * 5u + 4u];
+        if (spr.x != 0.0f) tau += spr.x * (spr.y - A[S.A_Q + qs + r]);
+        if (dr.y > 0.0f || dr.z > 0.0f) {
+          float q = A[S.A_Q + qs + r], qd = A[S.A_QD + d];
+          float err = A[S.A_TGT + d] - q;
+          float tv = A[S.A_TGTV + d];
+          float mm = fmx(D[r * JM + r], 1e-9f);
+          float qdn = (mm * qd + P.dt * (dr.y * err + dr.z * tv)) / ((mm + P.dt * dr.z) + (P.dt * P.dt) * dr.y);
+          float ti = dr.y * (err - P.dt * qdn) + dr.z * (tv - qdn);
+          if (fabsf(ti) <= dr.w || dr.w <= 0.0f) {
+            D[r * JM + r] += (P.dt * P.dt) * dr.y + P.dt * dr.z;
+            tau += (dr.y * err - (P.dt * dr.y) * qd) + dr.z * (tv - qd);
+          } else {
+            tau += clmp(ti, -dr.w, dr.w);
+          }
+        }
+        u[r] = tau - sdot(ldS(l, r), pA);
+      }
+      float Di[36];
+      inv_spd(D, n, JM, Di);
+      for (uint32_t i = 0; i < JM * JM; i++) A[L + L_DI + i] = Di[i];
+      for (uint32_t r = 0; r < JM; r++) A[L + L_UU + r] = u[r];
+      int par = lparent(l);
+      if (par < 0) continue;
+      m3 Am = ldm(L + L_IA), Bm = ldm(L + L_IA + 9u), Cm = ldm(L + L_IA + 18u);
+      SVec Duu = sv0();
+      for (uint32_t r = 0; r < n; r++) {
+        SVec Ur = ldU(l, r);
+        float du = 0.0f;
+        for (uint32_t c = 0; c < n; c++) {
+          SVec Uc = ldU(l, c);
+          float w = ldDI(l, r, c);
+          Am = msub(Am, mscl(w, outer(Ur.a, Uc.a)));
+          Bm = msub(Bm, mscl(w, outer(Ur.a, Uc.l)));
+          Cm = msub(Cm, mscl(w, outer(Ur.l, Uc.l)));
+          du += w * u[c];
+        }
+        Duu = sadd(Duu, sscl(Ur, du));
+      }
+      stm(L + L_IA, Am);
+      stm(L + L_IA + 9u, Bm);
+      stm(L + L_IA + 18u, Cm);
+      SVec pa = sadd(sadd(pA, imul(L + L_IA, ldsv(L + L_C))), Duu);
+      uint32_t P0 = lo((uint32_t)par);
+      f3 r = link_r(l);
+      m3 Rs = skew(r);
+      stm(P0 + L_IA, msub(madd(msub(madd(ldm(P0 + L_IA), Am), mul(Bm, Rs)), mul(Rs, tr(Bm))), mul(mul(Rs, Cm), Rs)));
+      stm(P0 + L_IA + 9u, madd(madd(ldm(P0 + L_IA + 9u), Bm), mul(Rs, Cm)));
+      stm(P0 + L_IA + 18u, madd(ldm(P0 + L_IA + 18u), Cm));
+      stsv(P0 + L_PA, sadd(ldsv(P0 + L_PA), fshift(pa, r)));
+    }
+    for (uint32_t k = 0; k < ai.y; k++) {
+      uint32_t l = ai.x + k, L = lo(l);
+      int par = lparent(l);
+      SVec ap = SVec{sp3(0.0f), -g};
+      if (par >= 0) ap = mshift(ldsv(lo((uint32_t)par) + L_A), link_r(l));
+      SVec a1 = sadd(ap, ldsv(L + L_C));
+      uint32_t n = lndof(l), d0 = ldof(l);
+      SVec acc = a1;
+      for (uint32_t r = 0; r < n; r++) {
+        float qdd = 0.0f;
+        for (uint32_t c = 0; c < n; c++) qdd += ldDI(l, r, c) * (A[L + L_UU + c] - sdot(ldU(l, c), a1));
+        A[S.A_QDH + d0 + r] = A[S.A_QD + d0 + r] + P.dt * qdd;
+        acc = sadd(acc, sscl(ldS(l, r), qdd));
+      }
+      stsv(L + L_A, acc);
+    }
+  }
+
+  __device__ uint32_t path(uint32_t l0, uint32_t* pth) const {
+    uint32_t n = 0;
+    int l = (int)l0;
+    while (l >= 0 && n < S.MAXPATH) { pth[n] = (uint32_t)l; n++; l = lparent((uint32_t)l); }
+    return n;
+  }
+
+  // Diagonal of H^-1 for dof r of link l (path_test with F = 0, artwgsl.js:375-414, 513-518).
+  // ub: scratch of MAXPATH * JM floats.
+  __device__ float dof_hinv(uint32_t l, uint32_t rr, uint32_t* pth, float* ub) const {
+    const uint32_t JM = S.JM;
+    uint32_t np = path(l, pth);
+    SVec p = sscl(sv0(), -1.0f);
+    for (uint32_t i = 0; i < np; i++) {
+      uint32_t pl = pth[i], n = lndof(pl);
+      float u[6] = {0, 0, 0, 0, 0, 0};
+      for (uint32_t r = 0; r < n; r++) {
+        float t = (pl == l && r == rr) ? 1.0f : 0.0f;
+        u[r] = t - sdot(ldS(pl, r), p);
+        ub[i * JM + r] = u[r];
+      }
+      for (uint32_t r = 0; r < n; r++) {
+        float du = 0.0f;
+        for (uint32_t c = 0; c < n; c++) du += ldDI(pl, r, c) * u[c];
+        p = sadd(p, sscl(ldU(pl, r), du));
+      }
+      p = fshift(p, link_r(pl));
+    }
+    SVec dv = sv0();
+    float out = 0.0f;
+    for (uint32_t ii = 0; ii < np; ii++) {
+      uint32_t i = np - 1u - ii, pl = pth[i], n = lndof(pl);
+      dv = mshift(dv, link_r(pl));
+      float dq[6] = {0, 0, 0, 0, 0, 0};
+      for (uint32_t r = 0; r < n; r++) {
+        dq[r] = 0.0f;
+        for (uint32_t c = 0; c < n; c++) dq[r] += ldDI(pl, r, c) * (ub[i * JM + c] - sdot(ldU(pl, c), dv));
+      }
+      for (uint32_t r = 0; r < n; r++) {
+        dv = sadd(dv, sscl(ldS(pl, r), dq[r]));
+        if (pl == l && r == rr) out = dq[r];
+      }
+    }
+    return out;
+  }
+
+  // Split COM response of link l (artwgsl.js:431-510). split: per path link, the number of
+  // contact-bearing links whose root path crosses it. ub: scratch of 6 * MAXPATH * JM floats.
+  __device__ void response(uint32_t l, const uint32_t* split, uint32_t* pth, float* ub) const {
+    const uint32_t JM = S.JM, PD = S.MAXPATH * JM;
+    uint32_t np = path(l, pth);
+    SVec p[6];
+    for (uint32_t e = 0; e < 6u; e++) {
+      f3 f = sp3(0.0f), t = sp3(0.0f);
+      if (e < 3u) setc(f, (int)e, 1.0f); else setc(t, (int)e - 3, 1.0f);
+      p[e] = SVec{-t, -f};
+    }
+    for (uint32_t i = 0; i < np; i++) {
+      uint32_t pl = pth[i], n = lndof(pl);
+      f3 r = link_r(pl);
+      for (uint32_t e = 0; e < 6u; e++) {
+        float u[6] = {0, 0, 0, 0, 0, 0};
+        for (uint32_t c = 0; c < n; c++) { u[c] = 0.0f - sdot(ldS(pl, c), p[e]); ub[e * PD + i * JM + c] = u[c]; }
+        SVec pe = p[e];
+        for (uint32_t rr = 0; rr < n; rr++) {
+          float du = 0.0f;
+          for (uint32_t c = 0; c < n; c++) du += ldDI(pl, rr, c) * u[c];
+          pe = sadd(pe, sscl(ldU(pl, rr), du));
+        }
+        p[e] = fshift(pe, r);
+      }
+    }
+    SVec dv[6];
+    for (uint32_t e = 0; e < 6u; e++) dv[e] = sv0();
+    for (uint32_t ii = 0; ii < np; ii++) {
+      uint32_t i = np - 1u - ii, pl = pth[i], n = lndof(pl);
+      f3 r = link_r(pl);
+      for (uint32_t e = 0; e < 6u; e++) {
+        SVec d = mshift(dv[e], r);
+        float dq[6] = {0, 0, 0, 0, 0, 0};
+        for (uint32_t rr = 0; rr < n; rr++) {
+          dq[rr] = 0.0f;
+          for (uint32_t c = 0; c < n; c++) dq[rr] += ldDI(pl, rr, c) * (ub[e * PD + i * JM + c] - sdot(ldU(pl, c), d));
+        }
+        for (uint32_t rr = 0; rr < n; rr++) d = sadd(d, sscl(ldS(pl, rr), dq[rr]));
+        dv[e] = d;
+      }
+    }
+    float W[36];
+    for (uint32_t e = 0; e < 6u; e++) {
+      W[0 * 6 + e] = dv[e].l.x; W[1 * 6 + e] = dv[e].l.y; W[2 * 6 + e] = dv[e].l.z;
+      W[3 * 6 + e] = dv[e].a.x; W[4 * 6 + e] = dv[e].a.y; W[5 * 6 + e] = dv[e].a.z;
+    }
+    for (uint32_t k = 0; k < 36u; k++) A[lo(l) + L_W2 + k] = W[k];
+    for (uint32_t i = 0; i < np; i++) {
+      float extra = (float)split[i] - 1.0f;
+      if (extra <= 0.0f) continue;
+      uint32_t pl = pth[i], n = lndof(pl);
+      float t[36];
+      for (uint32_t cc = 0; cc < 6u; cc++)
+        for (uint32_t x = 0; x < n; x++) {
+          float v = 0.0f;
+          for (uint32_t y = 0; y < n; y++) v += ldDI(pl, x, y) * ub[cc * PD + i * JM + y];
+          t[cc * 6u + x] = v;
+        }
+      for (uint32_t rr = 0; rr < 6u; rr++)
+        for (uint32_t cc = 0; cc < 6u; cc++) {
+          float sv = 0.0f;
+          for (uint32_t x = 0; x < n; x++) sv += ub[rr * PD + i * JM + x] * t[cc * 6u + x];
+          W[rr * 6u + cc] += extra * sv;
+        }
+    }
+    for (uint32_t k = 0; k < 36u; k++) A[lo(l) + L_W + k] = W[k];
+  }
+
+  // Generalized Jacobians (artwgsl.js:525-554).
+  __device__ void gen_jac(uint32_t x, f3 p, float sgn, f3 d0, f3 d1, f3 d2, uint32_t ds, float* J) const {
+    int l = (int)x;
+    while (l >= 0) {
+      uint32_t k = (uint32_t)l;
+      f3 c = ld3(lo(k) + L_COM);
+      for (uint32_t r = 0; r < lndof(k); r++) {
+        SVec Sv = ldS(k, r);
+        f3 v = Sv.l + cross(Sv.a, p - c);
+        uint32_t i = ldof(k) + r - ds;
+        J[i] += sgn * dot(d0, v);
+        J[S.NDA + i] += sgn * dot(d1, v);
+        J[2u * S.NDA + i] += sgn * dot(d2, v);
+      }
+      l = lparent(k);
+    }
+  }
+  __device__ void gen_ang(uint32_t x, float sgn, f3 d0, f3 d1, uint32_t ds, float* J) const {
+    int l = (int)x;
+    while (l >= 0) {
+      uint32_t k = (uint32_t)l;
+      for (uint32_t r = 0; r < lndof(k); r++) {
+        f3 w = ldS(k, r).a;
+        uint32_t i = ldof(k) + r - ds;
+        J[i] += sgn * dot(d0, w);
+        J[S.NDA + i] += sgn * dot(d1, w);
+      }
+      l = lparent(k);
+    }
+  }
+  // qd change of articulation a for generalized impulse tau (artwgsl.js:557-596).
+  // scratch: 18 * MAXLP floats.
+  __device__ void solve_gen(uint32_t a, const float* tau, float* out, float* scr) const {
+    uint4 ai = info(a);
+    float* p = scr;                  // 6 per link
+    float* uu = scr + 6u * S.MAXLP;  // 6 per link
+    float* dvs = scr + 12u * S.MAXLP;
+    for (uint32_t k = 0; k < 6u * ai.y; k++) p[k] = 0.0f;
+    auto ldp = [&](float* base, uint32_t k) { return SVec{mf3(base[k * 6], base[k * 6 + 1], base[k * 6 + 2]), mf3(base[k * 6 + 3], base[k * 6 + 4], base[k * 6 + 5])}; };
+    auto stp = [&](float* base, uint32_t k, SVec v) {
+      base[k * 6] = v.a.x; base[k * 6 + 1] = v.a.y; base[k * 6 + 2] = v.a.z;
+      base[k * 6 + 3] = v.l.x; base[k * 6 + 4] = v.l.y; base[k * 6 + 5] = v.l.z;
+    };
+    for (uint32_t kk = 0; kk < ai.y; kk++) {
+      uint32_t k = ai.y - 1u - kk, l = ai.x + k, n = lndof(l);
+      float u[6] = {0, 0, 0, 0, 0, 0};
+      SVec pk = ldp(p, k);
+      for (uint32_t r = 0; r < n; r++) u[r] = tau[ldof(l) + r - ai.z] - sdot(ldS(l, r), pk);
+      for (uint32_t r = 0; r < 6u; r++) uu[k * 6u + r] = u[r];
+      int par = lparent(l);
+      if (par >= 0) {
+        SVec pp = pk;
+        for (uint32_t r = 0; r < n; r++) {
+          float du = 0.0f;
+          for (uint32_t c = 0; c < n; c++) du += ldDI(l, r, c) * u[c];
+          pp = sadd(pp, sscl(ldU(l, r), du));
+        }
+        uint32_t pi = (uint32_t)par - ai.x;
+        stp(p, pi, sadd(ldp(p, pi), fshift(pp, link_r(l))));
+      }
+    }
+    for (uint32_t k = 0; k < ai.y; k++) {
+      uint32_t l = ai.x + k;
+      int par = lparent(l);
+      SVec dv = sv0();
+      if (par >= 0) dv = mshift(ldp(dvs, (uint32_t)par - ai.x), link_r(l));
+      uint32_t n = lndof(l);
+      float dq[6] = {0, 0, 0, 0, 0, 0};
+      for (uint32_t r = 0; r < n; r++) {
+        dq[r] = 0.0f;
+        for (uint32_t c = 0; c < n; c++) dq[r] += ldDI(l, r, c) * (uu[k * 6u + c] - sdot(ldU(l, c), dv));
+      }
+      for (uint32_t r = 0; r < n; r++) {
+        dv = sadd(dv, sscl(ldS(l, r), dq[r]));
+        out[ldof(l) + r - ai.z] = dq[r];
+      }
+      stp(dvs, k, dv);
+    }
+  }
+
+  // Solve-side propagation (wgsl.js:3233-3299). tw: body twists (v, w), aqd: generalized velocities.
+  __device__ void set_twist(uint32_t l, SVec v, float4* tw) const {
+    uint32_t b = (uint32_t)lbody(l);
+    tw[b * 2u] = mf4(v.l, 0.0f);
+    tw[b * 2u + 1u] = mf4(v.a, 0.0f);
+  }
+  __device__ void twists(uint32_t a, const float* aqd, float4* tw) const {
+    uint4 ai = info(a);
+    for (uint32_t k = 0; k < ai.y; k++) {
+      uint32_t l = ai.x + k;
+      int par = lparent(l);
+      SVec v = sv0();
+      if (par >= 0) v = mshift(ldsv(lo((uint32_t)par) + L_V), link_r(l));
+      for (uint32_t r = 0; r < lndof(l); r++) v = sadd(v, sscl(ldS(l, r), aqd[ldof(l) + r]));
+      stsv(lo(l) + L_V, v);
+      set_twist(l, v, tw);
+    }
+  }
+  __device__ void apply(uint32_t a, float* aqd, float4* tw) const {
+    uint4 ai = info(a);
+    for (uint32_t kk = 0; kk < ai.y; kk++) {
+      uint32_t l = ai.x + ai.y - 1u - kk, L = lo(l);
+      uint32_t n = lndof(l);
+      SVec p = ldsv(L + L_P);
+      float u[6] = {0, 0, 0, 0, 0, 0};
+      for (uint32_t r = 0; r < n; r++) { u[r] = A[L + L_TAU + r] - sdot(ldS(l, r), p); A[L + L_UU + r] = u[r]; }
+      int par = lparent(l);
+      if (par >= 0) {
+        SVec pp = p;
+        for (uint32_t r = 0; r < n; r++) {
+          float du = 0.0f;
+          for (uint32_t c = 0; c < n; c++) du += ldDI(l, r, c) * u[c];
+          pp = sadd(pp, sscl(ldU(l, r), du));
+        }
+        uint32_t P0 = lo((uint32_t)par) + L_P;
+        stsv(P0, sadd(ldsv(P0), fshift(pp, link_r(l))));
+      }
+    }
+    for (uint32_t k = 0; k < ai.y; k++) {
+      uint32_t l = ai.x + k, L = lo(l);
+      int par = lparent(l);
+      SVec dv = sv0();
+      if (par >= 0) dv = mshift(ldsv(lo((uint32_t)par) + L_DV), link_r(l));
+      uint32_t n = lndof(l);
+      float dq[6] = {0, 0, 0, 0, 0, 0};
+      for (uint32_t r = 0; r < n; r++) {
+        dq[r] = 0.0f;
+        for (uint32_t c = 0; c < n; c++) dq[r] += ldDI(l, r, c) * (A[L + L_UU + c] - sdot(ldU(l, c), dv));
+      }
+      for (uint32_t r = 0; r < n; r++) { dv = sadd(dv, sscl(ldS(l, r), dq[r])); aqd[ldof(l) + r] += dq[r]; }
+      stsv(L + L_DV, dv);
+      SVec v = sadd(ldsv(L + L_V), dv);
+      stsv(L + L_V, v);
+      set_twist(l, v, tw);
+      stsv(L + L_P, sv0());
+      for (uint32_t r = 0; r < S.JM; r++) A[L + L_TAU + r] = 0.0f;
+    }
+  }
+};
+
+}  // namespace steel

@@ -16,7 +16,8 @@ No public dataset exists for this path; these generators build scenes through th
 * ``uneven_batch``     a list of independent scenes with log-U[8, 512] bodies from the box mix,
                        each with one revolute chain of U[2, 40] links and its own ground plane.
 
-Every draw comes from one ``numpy.random.default_rng(seed)``.
+Every draw comes from one ``numpy.random.default_rng(seed)``. Box hulls are built directly
+(``builder.box_hull``) rather than by quickhull, for generation speed at batch scale.
 """
 from __future__ import annotations
 
@@ -37,7 +38,7 @@ def _rand_quat(rng):
 
 def boxes_on_plane(n=64, seed=0, fps=240, substeps=4, iterations=12, volume=2.0, z0=0.2, mu=0.6):
     rng = np.random.default_rng(seed)
-    b = SceneBuilder(fps=fps)
+    b = SceneBuilder(fps=fps, box_hulls="direct")
     b.add_ground_plane(mu=mu)
     placed = []
     for _ in range(n):
@@ -64,7 +65,7 @@ def _ellipsoid_points(rng, k):
 def convex_pour(n=8192, seed=0, fps=240, substeps=4, iterations=12, bin_size=4.0, wall_h=1.0, layer=0.25):
     """Bodies on a jittered lattice above a 4x4 m bin (floor + 4 walls, 5 static boxes)."""
     rng = np.random.default_rng(seed)
-    b = SceneBuilder(fps=fps)
+    b = SceneBuilder(fps=fps, box_hulls="direct")
     half = bin_size / 2
     t = 0.1
     walls = [([0, 0, -t], [half + t, half + t, t]),
@@ -136,7 +137,7 @@ def _add_quadruped(b, rng, pos, ke=60.0, kd=2.0):
 
 def quadrupeds(n_quad=1024, n_chains=64, chain_links=40, seed=0, fps=500, substeps=4, iterations=12, spacing=1.2):
     rng = np.random.default_rng(seed)
-    b = SceneBuilder(fps=fps)
+    b = SceneBuilder(fps=fps, box_hulls="direct")
     b.add_ground_plane(mu=0.8)
     side = int(math.ceil(math.sqrt(n_quad + n_chains)))
     joints = []
@@ -159,7 +160,7 @@ def uneven_batch(n_scenes=2048, seed=0, fps=240, substeps=4, iterations=12, lo=8
     scenes = []
     for s in range(n_scenes):
         nb = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
-        b = SceneBuilder(fps=fps)
+        b = SceneBuilder(fps=fps, box_hulls="direct")
         b.add_ground_plane(mu=0.6)
         side = max(int(math.ceil(math.sqrt(nb))), 1)
         for i in range(nb):

@@ -1,0 +1,71 @@
+"""Small seeded scenes covering the features of the hot path, built with the SceneBuilder mirror."""
+import math
+
+import numpy as np
+
+from steel_webgpu_b200 import SceneBuilder, synth
+
+
+def boxes(n=64, seed=1):
+    return synth.boxes_on_plane(n, seed=seed)
+
+
+def mixed_prims(seed=3, n=24):
+    """Boxes, spheres, capsules, cylinders and random hulls (<= 16 and > 16 points) on a plane."""
+    rng = np.random.default_rng(seed)
+    b = SceneBuilder(fps=240)
+    b.add_ground_plane(mu=0.7)
+    for i in range(n):
+        p = [float(rng.uniform(-0.6, 0.6)), float(rng.uniform(-0.6, 0.6)), 0.15 + 0.22 * i]
+        body = b.add_body(xform=p + synth._rand_quat(rng))
+        k = i % 6
+        if k == 0:
+            b.add_shape_box(body, hx=0.08, hy=0.05, hz=0.06, mu=0.6)
+        elif k == 1:
+            b.add_shape_sphere(body, radius=0.06, mu=0.5)
+        elif k == 2:
+            b.add_shape_capsule(body, radius=0.04, half_height=0.07, mu=0.6)
+        elif k == 3:
+            b.add_shape_cylinder(body, radius=0.05, half_height=0.06, mu=0.6)
+        elif k == 4:
+            b.add_shape_convex_hull(body, vertices=synth._ellipsoid_points(rng, 12), mu=0.6)
+        else:
+            b.add_shape_convex_hull(body, vertices=synth._ellipsoid_points(rng, 24), mu=0.6)
+    return b.finalize()
+
+
+def articulated(seed=5):
+    """Two quadrupeds with PD drives and limits, one hanging revolute chain, a D6 and a ball pendulum."""
+    rng = np.random.default_rng(seed)
+    b = SceneBuilder(fps=500)
+    b.add_ground_plane(mu=0.8)
+    synth._add_quadruped(b, rng, [0.0, 0.0, 0.9])
+    synth._add_quadruped(b, rng, [1.5, 0.0, 0.9])
+    synth._add_chain(b, rng, [3.0, 0.0, 2.2], 8, ratio_max=100.0)
+    base = b.add_body(xform=[-1.5, 0, 1.0, 0, 0, 0, 1])
+    b.add_shape_box(base, hx=0.1, hy=0.1, hz=0.1)
+    b.add_joint_fixed(-1, base, parent_xform=[-1.5, 0, 1.0, 0, 0, 0, 1])
+    arm = b.add_body(xform=[-1.5, 0, 0.7, 0, 0, 0, 1])
+    b.add_shape_capsule(arm, radius=0.03, half_height=0.12)
+    b.add_joint_d6(base, arm, linear_axes=[[0, 0, 1]], angular_axes=[[1, 0, 0], [0, 1, 0]],
+                   parent_xform=[0, 0, -0.1, 0, 0, 0, 1], child_xform=[0, 0, 0.2, 0, 0, 0, 1], q=[0.0, 0.3, -0.2])
+    bob = b.add_body(xform=[-2.5, 0, 1.5, 0, 0, 0, 1])
+    b.add_shape_sphere(bob, radius=0.08)
+    b.add_joint_ball(-1, bob, parent_xform=[-2.5, 0, 2.0, 0, 0, 0, 1], child_xform=[0, 0, 0.4, 0, 0, 0, 1],
+                     q=[math.sin(0.2), 0.0, 0.0, math.cos(0.2)])
+    return b.finalize()
+
+
+def chains_and_quads(seed=7, n_quad=4, chain_links=40):
+    """Quadrupeds plus one 40-link chain with link mass ratios up to 1e3 (the articulation workload)."""
+    return synth.quadrupeds(n_quad=n_quad, n_chains=1, chain_links=chain_links, seed=seed)
+
+
+def hull_bin(seed=11, n=160):
+    """Hulls, boxes and capsules poured into a bin of 5 static boxes (the convex-pour workload)."""
+    return synth.convex_pour(n=n, seed=seed, bin_size=1.5, layer=0.25)
+
+
+def small_batch(seed=13, n=6):
+    """Independent scenes of uneven size (the uneven-batch workload)."""
+    return synth.uneven_batch(n_scenes=n, seed=seed, lo=8, hi=96, chain_lo=2, chain_hi=12)

@@ -1,0 +1,129 @@
+"""Parity of the CUDA path with the CPU oracle on the same packed scenes.
+
+Integer and order outputs (pair sets, the canonical contact order, colors) must match exactly;
+the float pipeline is pinned to IEEE operations in a fixed order on both sides (no FMA), so
+contact records, rows, poses and velocities are compared bit for bit as well.
+"""
+import numpy as np
+import pytest
+
+from steel_webgpu_b200 import pack
+from steel_webgpu_b200.sim import Batch
+from tests import scenes
+
+pytestmark = pytest.mark.gpu
+
+SCENES = {"boxes": scenes.boxes, "mixed_prims": scenes.mixed_prims, "articulated": scenes.articulated,
+          "chains_and_quads": scenes.chains_and_quads, "hull_bin": scenes.hull_bin}
+
+
+def _pair_set(p):
+    return {(int(min(a, b)), int(max(a, b))) for a, b in p}
+
+
+def _bits(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+@pytest.mark.parametrize("name", ["boxes", "mixed_prims", "articulated", "hull_bin"])
+def test_pairs_and_sorted_contacts(name, steel, oracle_lib):
+    pk = pack(SCENES[name]())
+    o = oracle_lib.OracleSim(pk)
+    g = Batch([pk])
+    for frames in (0, 30, 60):
+        if frames:
+            o.step(30)
+            g.step(30)
+        o.collide()
+        g.collide()
+        cnt = o.read("collide_counts", np.uint32)
+        op = o.read("pairs", np.uint32)[:min(cnt[0], pk.C["MAXP"]) * 2].reshape(-1, 2)
+        assert _pair_set(g.pairs()) == _pair_set(op), f"pair set differs after {frames} frames"
+        nc = min(cnt[1], pk.C["MAXC"])
+        rec, smu = g.contacts()
+        oc = o.read("contacts")
+        assert rec.shape[0] == nc
+        assert np.array_equal(_bits(rec.reshape(-1)), _bits(oc[:nc * 20])), "contact records differ"
+        assert np.array_equal(_bits(smu.reshape(-1)), _bits(oc[pk.C["MAXC"] * 20:pk.C["MAXC"] * 20 + nc * 4]))
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_trajectory_bit_exact(name, steel, oracle_lib):
+    pk = pack(SCENES[name]())
+    o = oracle_lib.OracleSim(pk)
+    g = Batch([pk])
+    nb = pk.NB
+    for chunk in range(4):
+        o.step(15)
+        g.step(15)
+        op = o.read("poses")[:nb * 8]
+        gp = g.poses()
+        if not np.array_equal(_bits(op), _bits(gp)):
+            pytest.fail(f"{name}: poses differ after {(chunk + 1) * 15} frames (max |d| {np.abs(op - gp).max():g})")
+        _, gv, gq, gqd, _ = g.raw_state()
+        assert np.array_equal(_bits(o.read("vel")[:nb * 8]), _bits(gv)), "velocities differ"
+        oa = o.read("art")
+        assert np.array_equal(_bits(oa[pk.C["A_Q"]:pk.C["A_Q"] + pk.NQ]), _bits(gq)), "joint coordinates differ"
+        assert np.array_equal(_bits(oa[pk.C["A_QD"]:pk.C["A_QD"] + pk.ND]), _bits(gqd)), "joint velocities differ"
+    ost = o.read("stats", np.uint32)
+    gst = g.stats()
+    assert (gst["contacts"], gst["colors"], gst["max_pairs"], gst["max_units"]) == (ost[5], ost[6], ost[4], ost[3])
+
+
+@pytest.mark.parametrize("name", ["boxes", "articulated"])
+def test_stage_by_stage(name, steel, oracle_lib):
+    """Each substep's colors, rows and state agree after every kernel, warm-table parity included."""
+    pk = pack(SCENES[name]())
+    C = pk.C
+    R = C["ROWS"]
+    o = oracle_lib.OracleSim(pk)
+    g = Batch([pk])
+    for sub in range(40):
+        o.stage(0)
+        g.debug_stage(0)
+        o.stage(1)
+        g.debug_stage(1)
+        osch = o.read("sched", np.uint32)
+        nu = osch[C["S_META"]]
+        tot = osch[C["S_USTART"] + nu]
+        assert g.read_words("sched", g.layout("S_META"), 2, dtype=np.uint32).tolist() == [nu, osch[C["S_META"] + 1]]
+        gcol = g.read_words("sched", g.layout("S_PCOL"), tot, dtype=np.uint32)
+        assert np.array_equal(gcol, osch[C["S_PCOL"]:C["S_PCOL"] + tot]), f"colors differ at substep {sub}"
+        assert np.array_equal(_bits(g.read_words("rows", 0, tot * R * 4)), _bits(o.read("rows")[:tot * R * 4])), \
+            f"rows differ at substep {sub}"
+        if pk.NL:
+            assert np.array_equal(_bits(g.read_words("art", g.layout("A_LINK"), pk.NL * 268)),
+                                  _bits(o.read("art")[C["A_LINK"]:C["A_LINK"] + pk.NL * 268]))
+        o.stage(2)
+        g.debug_stage(2)
+        assert np.array_equal(_bits(g.poses()), _bits(o.read("poses")[:pk.NB * 8])), f"poses differ at substep {sub}"
+
+
+def test_batch_matches_each_scene_alone(steel, oracle_lib):
+    """Scenes stepped together in one batch give the same bits as each scene alone on the oracle."""
+    pks = [pack(s) for s in scenes.small_batch()]
+    g = Batch(pks)
+    orcs = [oracle_lib.OracleSim(pk) for pk in pks]
+    g.step(40)
+    for i, (pk, o) in enumerate(zip(pks, orcs)):
+        o.step(40)
+        assert np.array_equal(_bits(g.poses(i)), _bits(o.read("poses")[:pk.NB * 8])), f"scene {i} differs"
+
+
+def test_reset_replays_identically(steel):
+    pk = pack(scenes.boxes(24))
+    g = Batch([pk])
+    g.step(30)
+    a = g.poses().copy()
+    g.reset()
+    g.step(30)
+    assert np.array_equal(_bits(a), _bits(g.poses()))
+
+
+def test_graph_and_eager_launches_agree(steel):
+    pk = pack(scenes.articulated())
+    g1 = Batch([pk], graph=True)
+    g2 = Batch([pk], graph=False)
+    g1.step(20)
+    g2.step(20)
+    assert np.array_equal(_bits(g1.poses()), _bits(g2.poses()))
