@@ -116,6 +116,24 @@ int steel_profile_kernels(steel_batch* b, uint32_t frames, float* ms_per_launch)
 /* Device time of the last steel_step_timed call's frames, in milliseconds (CUDA events). */
 int steel_step_timed(steel_batch* b, uint32_t frames, float* ms);
 
+/* Canonical contact sort that allocates no device memory. No counterpart in the reference (its
+   sort runs only inside Sim.step); it exists for callers that cannot call cudaMalloc: a robot
+   controller on a fixed-rate loop, where cudaMalloc/cudaFree may block and synchronise the whole
+   device, or a host engine that hands all device memory out of its own pool sized at start-up.
+   Sorts n raw contact records into the order steel_collide/steel_read_contacts produce. Both
+   buffers are caller-owned device memory of the calling thread's current device (or mapped host
+   memory), 16-byte aligned, not overlapping, 24 * n floats each, laid out as steel_read_contacts
+   returns them: n records of 5 vec4, then n shape-mu vec4. `stream` is a cudaStream_t of that
+   device (NULL: the default stream); the call only enqueues the work.
+   The key scratch is a static device array of STEEL_NOALLOC_MAX_CONTACTS keys (1 MiB) that every
+   GPU which loads this library holds until exit; n above that maximum fails with
+   STEEL_E_CAPACITY before anything is launched. The first call on a device looks up the array's
+   device address (set-up); make that first call before any stream capture. All calls on a device
+   share the array: calls whose kernels overlap on the GPU race and corrupt each other's results,
+   so order them (for example on one stream). */
+#define STEEL_NOALLOC_MAX_CONTACTS 65536
+int steel_sort_contacts_noalloc(const float* raw, uint32_t n, float* sorted, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

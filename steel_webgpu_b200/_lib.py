@@ -70,6 +70,7 @@ SIGNATURES = {
     "steel_step_timed": [_VP, _U32, ctypes.POINTER(_F32)],
     "steel_step_io": [_VP, _U32, _VP, ctypes.c_uint64, _VP, ctypes.c_uint64],
     "steel_profile_kernels": [_VP, _U32, _VP],
+    "steel_sort_contacts_noalloc": [_VP, _U32, _VP, _VP],
 }
 
 _lib = None

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libsteel_b200.so")
-SOURCES = ["collide.cu", "prepare.cu", "solve.cu", "api.cu"]
+SOURCES = ["collide.cu", "prepare.cu", "solve.cu", "api.cu", "sort_noalloc.cu"]
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "--fmad=false", "-prec-div=true",
          "-prec-sqrt=true", "-ftz=false", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]

@@ -35,6 +35,16 @@ uint64_t next_pow2(uint64_t x) {
   return p;
 }
 
+}  // namespace
+
+namespace steel {
+// Records the calling thread's error for steel_last_error(); for the entry points that live in
+// other translation units.
+int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace steel
+
+namespace {
+
 struct Consts {
   std::map<std::string, double> kv;
   bool parse(const char* text) {

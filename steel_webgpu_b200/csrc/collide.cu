@@ -9,6 +9,7 @@
 // narrowphase runs one warp per pair with shuffle reductions over faces, edge pairs and
 // support points; each scene's contacts are sorted by one block.
 #include "batch.cuh"
+#include "contact_key.cuh"
 
 namespace steel {
 
@@ -1124,20 +1125,6 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32) k_narrow(BatchDev B) {
 // --------------------------------------------------------------------------------------------
 // Canonical contact sort (wgsl.js:3899-3982): key (pair, feature key, point-bit hash, raw index),
 // one block per scene, bitonic sort over a power-of-two key array in shared memory.
-SD bool key_gt(uint4 a, uint4 b) {
-  if (a.x != b.x) return a.x > b.x;
-  if (a.y != b.y) return a.y > b.y;
-  if (a.z != b.z) return a.z > b.z;
-  return a.w > b.w;
-}
-SD uint4 contact_key(const float4* craw, uint32_t c) {
-  float4 p = craw[c * 5u], m = craw[c * 5u + 2u];
-  uint32_t pair = (uint32_t)(f2i(m.x) + 1) | ((uint32_t)(f2i(m.y) + 1) << 16u);
-  uint32_t feat = f2u(m.z) | (f2u(m.w) << 16u);
-  uint32_t bits = mix32(mix32(mix32(fbits(p.x)) ^ fbits(p.y)) ^ fbits(p.z)) ^ fbits(p.w);
-  return make_uint4(pair, feat, bits, c);
-}
-
 __global__ void __launch_bounds__(SORT_THREADS) k_csort(BatchDev B, uint32_t smem_keys) {
   extern __shared__ uint4 sk[];
   const SceneDev& S = B.scenes[blockIdx.x];
