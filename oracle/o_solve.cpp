@@ -200,12 +200,28 @@ void Oracle::solve_unit(uint32_t us, uint32_t row, int a, int b, uint32_t /*s0*/
   if (b >= 0) { tw[(uint32_t)b * 2u] = mk4(tb[0], 0.0f); tw[(uint32_t)b * 2u + 1u] = mk4(tb[1], 0.0f); }
 }
 
-// art_dense (wgsl.js:3306-3364), sequential sums (the reference's no-subgroup form).
+// subgroupAdd of a 32-lane subgroup (wgsl.js:3305 with SG = 1), pinned to a fixed order: an xor
+// butterfly over lane offsets 16, 8, 4, 2, 1, each step adding lane l and lane l ^ offset. IEEE
+// addition commutes, so every lane ends with the same bits; lane 0's value is returned.
+static float lane_sum32(const float* part) {
+  float v[32], t[32];
+  for (uint32_t l = 0; l < 32u; l++) v[l] = part[l];
+  for (uint32_t off = 16u; off > 0u; off >>= 1u) {
+    for (uint32_t l = 0; l < 32u; l++) t[l] = v[l] + v[l ^ off];
+    for (uint32_t l = 0; l < 32u; l++) v[l] = t[l];
+  }
+  return v[0];
+}
+
+// art_dense (wgsl.js:3306-3364) in its subgroup form: one 32-lane subgroup per articulation, lane
+// l owns dofs l, l + 32, ... and accumulates its partial sums in dof order; lane_sum32 combines
+// them. Per-dof updates are the same operations in either form.
 bool Oracle::art_dense(uint32_t a, uint32_t mode, uint32_t it, uint32_t ph) {
   const uint32_t NDA = C.NDA, DHDR = C.DHDR, DPS = C.DPS;
   uint32_t nd = std::min(sched[C.S_META + 3u], C.MAXDENSE);
   u4 ai = art_info(a);
   bool touched = false;
+  float part[32], p1[32], p2[32];
   for (uint32_t i = 0; i < nd; i++) {
     uint32_t o = C.A_DENSE + i * DPS;
     if (f2u(art[o]) != a) continue;
@@ -217,9 +233,9 @@ bool Oracle::art_dense(uint32_t a, uint32_t mode, uint32_t it, uint32_t ph) {
       if (mode == 0u) continue;
       v3 nlam = lam;
       for (uint32_t r = 0; r < f2u(art[o + 21u]); r++) {
-        float part = 0.0f;
-        for (uint32_t k = 0; k < ai.w; k++) part += art[jo + r * NDA + k] * aqd[ai.z + k];
-        float jv = part;
+        for (uint32_t l = 0; l < 32u; l++) part[l] = 0.0f;
+        for (uint32_t k = 0; k < ai.w; k++) part[k % 32u] += art[jo + r * NDA + k] * aqd[ai.z + k];
+        float jv = lane_sum32(part);
         float rhs = r == 0u ? art[o + 4u] : (r == 1u ? art[o + 22u] : art[o + 23u]);
         float dl = ((-C.F_OMEGA) * (jv + rhs)) * art[o + 5u + r];
         setat(nlam, (int)r, at(nlam, (int)r) + dl);
@@ -233,21 +249,22 @@ bool Oracle::art_dense(uint32_t a, uint32_t mode, uint32_t it, uint32_t ph) {
         aqd[ai.z + k] += (art[yo + k] * lam.x + art[yo + NDA + k] * lam.y) + art[yo + 2u * NDA + k] * lam.z;
       continue;
     }
-    float part = 0.0f;
-    for (uint32_t k = 0; k < ai.w; k++) part += art[jo + k] * aqd[ai.z + k];
-    float jv = part;
+    for (uint32_t l = 0; l < 32u; l++) part[l] = 0.0f;
+    for (uint32_t k = 0; k < ai.w; k++) part[k % 32u] += art[jo + k] * aqd[ai.z + k];
+    float jv = lane_sum32(part);
     float w = art[o + 24u];
     float nl = fmaxf_(lam.x + C.F_OMEGA * ((((-(jv + art[o + 4u])) * art[o + 5u]) * w) - (1.0f - w) * lam.x), 0.0f);
     float dn = nl - lam.x;
-    float p1 = 0.0f, p2 = 0.0f;
+    for (uint32_t l = 0; l < 32u; l++) { p1[l] = 0.0f; p2[l] = 0.0f; }
     for (uint32_t k = 0; k < ai.w; k++) {
       aqd[ai.z + k] += art[yo + k] * dn;
-      p1 += art[jo + NDA + k] * aqd[ai.z + k];
-      p2 += art[jo + 2u * NDA + k] * aqd[ai.z + k];
+      p1[k % 32u] += art[jo + NDA + k] * aqd[ai.z + k];
+      p2[k % 32u] += art[jo + 2u * NDA + k] * aqd[ai.z + k];
     }
+    float s1 = lane_sum32(p1), s2 = lane_sum32(p2);
     float lim = it < C.FSTART ? 0.0f : art[o + 3u] * nl;
     float kd = art[o + 6u] * art[o + 8u] - art[o + 7u] * art[o + 7u];
-    v2 lt = friction_pair_solve(art[o + 8u] / kd, -art[o + 7u] / kd, art[o + 6u] / kd, p1, p2, lam.y, lam.z, lim,
+    v2 lt = friction_pair_solve(art[o + 8u] / kd, -art[o + 7u] / kd, art[o + 6u] / kd, s1, s2, lam.y, lam.z, lim,
                                 C.F_OMEGA);
     float d1 = lt.x - lam.y, d2 = lt.y - lam.z;
     for (uint32_t k = 0; k < ai.w; k++) aqd[ai.z + k] += art[yo + NDA + k] * d1 + art[yo + 2u * NDA + k] * d2;
@@ -421,6 +438,9 @@ void Oracle::k_solve() {
     uint32_t kind = body_kind((int)b);
     imp[b * 2u] = mk4(0, 0, 0, 0);
     imp[b * 2u + 1u] = mk4(0, 0, 0, 0);
+    // tw is workgroup memory in the reference (wgsl.js:2504), zero at the start of every dispatch.
+    tw[b * 2u] = mk4(0, 0, 0, 0);
+    tw[b * 2u + 1u] = mk4(0, 0, 0, 0);
     if (kind == 1u) {
       uint32_t fl = body_flags((int)b);
       v3 v = xyz(vel[b * 2u]) + (fl != 0u ? splat3(0.0f) : xyz(P.gravity) * P.dt);

@@ -379,6 +379,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   CU(cudaMemsetAsync(b->arena, 0, b->arena_bytes, st));
   uint8_t* A = b->arena;
   std::vector<SceneDev> dev(n);
+  size_t prep_smem = 0, solve_smem = 0;
   for (uint32_t i = 0; i < n; i++) {
     SceneHost& s = b->sc[i];
     SceneDev& d = s.d;
@@ -398,6 +399,13 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
     d.tw = at<float4>(A, s.o_tw); d.imp = at<float4>(A, s.o_imp); d.aqd = at<float>(A, s.o_aqd);
     d.tscr = at<float>(A, s.o_tscr);
     d.scene_index = i;
+    d.stage = 0u;
+    if (d.NL > 0u && 4ull * d.NL * 268u <= STAGE_LINK_CAP) d.stage |= STAGE_LINKS;
+    if (64ull * d.NB <= STAGE_BODY_CAP) d.stage |= STAGE_BODIES;
+    if (4ull * d.ND <= STAGE_QD_CAP) d.stage |= STAGE_QD;
+    if (4ull * d.NB * d.NCOLW <= STAGE_WMASK_CAP) d.stage |= STAGE_WMASK;
+    prep_smem = std::max<size_t>(prep_smem, prep_smem_layout(d.stage, d.NL, d.NB, d.NCOLW, d.NCOL).total);
+    solve_smem = std::max<size_t>(solve_smem, solve_smem_layout(d.stage, d.NB, d.ND, d.NCOL, d.NL).total);
     dev[i] = d;
     CU(cudaMemcpyAsync((void*)d.sf, s.statF.data(), s.statF.size() * 4, cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync((void*)d.su, s.statU.data(), s.statU.size() * 4, cudaMemcpyHostToDevice, st));
@@ -416,13 +424,17 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   bd.phase = at<double>(A, b->o_phase);
   bd.substep_count = at<unsigned long long>(A, b->o_ssc);
   bd.error = at<uint32_t>(A, b->o_err);
+  bd.prep_smem = (uint32_t)prep_smem;
+  bd.solve_smem = (uint32_t)solve_smem;
+  CU(configure_prepare(prep_smem));
+  CU(configure_solve(solve_smem));
   CU(cudaMemcpyAsync(bd.scenes, dev.data(), sizeof(SceneDev) * n, cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync((void*)bd.shape_scene, b->shape_scene.data(), 4 * b->shape_scene.size(), cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync((void*)bd.shape_local, b->shape_local.data(), 4 * b->shape_local.size(), cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync((void*)bd.tiles, b->tiles.data(), 16 * b->tiles.size(), cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(A + b->o_tgt_off, tgt_off.data(), 8ull * n, cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(A + b->o_pose_off, pose_off.data(), 8ull * n, cudaMemcpyHostToDevice, st));
-  b->narrow_blocks = (uint32_t)ctx->sms * 8u;
+  b->narrow_blocks = (uint32_t)ctx->sms * (uint32_t)narrow_blocks_per_sm();
   b->sort_keys = std::min<size_t>(next_pow2(max_c), 8192);
   CU(configure_sort(b->sort_keys));
   CU(cudaEventCreate(&b->ev0));

@@ -34,8 +34,10 @@ SD f3 unit_axis(uint32_t c) { return c == 0 ? mf3(1, 0, 0) : (c == 1 ? mf3(0, 1,
 
 struct Art {
   const SceneDev& S;
-  float* A;  // the scene's articulation buffer
-  __device__ Art(const SceneDev& s) : S(s), A(s.art) {}
+  float* A;   // the scene's articulation buffer
+  float* LB;  // link blocks: LB + lo(l) is link l's LBLK floats
+  __device__ Art(const SceneDev& s) : S(s), A(s.art), LB(s.art + s.A_LINK) {}
+  __device__ Art(const SceneDev& s, float* lb) : S(s), A(s.art), LB(lb) {}
 
   __device__ float4 lrec(uint32_t l, uint32_t k) const { return S.sf[S.SF_LINK + l * 6u + k]; }
   __device__ uint32_t ltype(uint32_t l) const { return f2u(lrec(l, 0).x); }
@@ -58,9 +60,13 @@ struct Art {
     const float4* o = S.sf + S.SF_BODY + (uint32_t)b * 8u;
     return tr(mcols(v3(o[2]), v3(o[3]), v3(o[4])));
   }
-  __device__ uint32_t lo(uint32_t l) const { return S.A_LINK + l * LBLK; }
-  __device__ f3 ld3(uint32_t o) const { return mf3(A[o], A[o + 1], A[o + 2]); }
-  __device__ void st3(uint32_t o, f3 v) const { A[o] = v.x; A[o + 1] = v.y; A[o + 2] = v.z; }
+  __device__ uint32_t lo(uint32_t l) const { return l * LBLK; }
+  // Link-block fields (offsets from lo(l)) live at LB, which is either the scene's art buffer or a
+  // shared-memory copy of its link blocks; every other art field is addressed through A.
+  __device__ f3 ld3(uint32_t o) const { return mf3(LB[o], LB[o + 1], LB[o + 2]); }
+  __device__ void st3(uint32_t o, f3 v) const { LB[o] = v.x; LB[o + 1] = v.y; LB[o + 2] = v.z; }
+  __device__ f3 ald3(uint32_t o) const { return mf3(A[o], A[o + 1], A[o + 2]); }
+  __device__ void ast3(uint32_t o, f3 v) const { A[o] = v.x; A[o + 1] = v.y; A[o + 2] = v.z; }
   __device__ SVec ldsv(uint32_t o) const { return SVec{ld3(o), ld3(o + 3u)}; }
   __device__ void stsv(uint32_t o, SVec s) const { st3(o, s.a); st3(o + 3u, s.l); }
   __device__ m3 ldm(uint32_t o) const { return mcols(ld3(o), ld3(o + 3u), ld3(o + 6u)); }
@@ -71,13 +77,13 @@ struct Art {
   }
   __device__ SVec ldS(uint32_t l, uint32_t k) const { return ldsv(lo(l) + L_S + k * 6u); }
   __device__ SVec ldU(uint32_t l, uint32_t k) const { return ldsv(lo(l) + L_U + k * 6u); }
-  __device__ float ldDI(uint32_t l, uint32_t r, uint32_t c) const { return A[lo(l) + L_DI + r * S.JM + c]; }
+  __device__ float ldDI(uint32_t l, uint32_t r, uint32_t c) const { return LB[lo(l) + L_DI + r * S.JM + c]; }
   __device__ f3 link_r(uint32_t l) const {
     int par = lparent(l);
     if (par < 0) return sp3(0.0f);
     return ld3(lo(l) + L_COM) - ld3(lo((uint32_t)par) + L_COM);
   }
-  __device__ float4 link_rot(uint32_t l) const { return mf4(ld3(lo(l) + L_ROT), A[lo(l) + L_ROT + 3u]); }
+  __device__ float4 link_rot(uint32_t l) const { return mf4(ld3(lo(l) + L_ROT), LB[lo(l) + L_ROT + 3u]); }
 
   // Link poses, COMs and world motion subspaces (artwgsl.js:98-187).
   __device__ void fk(uint32_t a) const {
@@ -134,7 +140,7 @@ struct Art {
       uint32_t L = lo(l);
       st3(L + L_POS, lp);
       st3(L + L_ROT, v3(lq));
-      A[L + L_ROT + 3u] = lq.w;
+      LB[L + L_ROT + 3u] = lq.w;
       f3 com = lp + qrot(lq, v3(S.sf[S.SF_BODY + (uint32_t)f2i(r0.w) * 8u + 1u]));
       st3(L + L_COM, com);
       f3 aw = qrot(jq, axis);
@@ -221,7 +227,7 @@ struct Art {
       stm(L + L_IA + 18u, mcols(mf3(m, 0, 0), mf3(0, m, 0), mf3(0, 0, m)));
       SVec pa0 = crf(v, imul(L + L_IA, v));
       if ((f2u(S.sf[S.SF_BODY + (uint32_t)b * 8u + 7u].w) & 2u) != 0u) pa0 = sadd(pa0, SVec{sp3(0.0f), m * g});
-      pa0 = sadd(pa0, SVec{-ld3(S.A_BF + (uint32_t)b * 8u + 4u), -ld3(S.A_BF + (uint32_t)b * 8u)});
+      pa0 = sadd(pa0, SVec{-ald3(S.A_BF + (uint32_t)b * 8u + 4u), -ald3(S.A_BF + (uint32_t)b * 8u)});
       stsv(L + L_PA, pa0);
     }
     for (uint32_t kk = 0; kk < ai.y; kk++) {
@@ -260,8 +266,8 @@ struct Art {
       }
       float Di[36];
       inv_spd(D, n, JM, Di);
-      for (uint32_t i = 0; i < JM * JM; i++) A[L + L_DI + i] = Di[i];
-      for (uint32_t r = 0; r < JM; r++) A[L + L_UU + r] = u[r];
+      for (uint32_t i = 0; i < JM * JM; i++) LB[L + L_DI + i] = Di[i];
+      for (uint32_t r = 0; r < JM; r++) LB[L + L_UU + r] = u[r];
       int par = lparent(l);
       if (par < 0) continue;
       m3 Am = ldm(L + L_IA), Bm = ldm(L + L_IA + 9u), Cm = ldm(L + L_IA + 18u);
@@ -301,7 +307,7 @@ struct Art {
       SVec acc = a1;
       for (uint32_t r = 0; r < n; r++) {
         float qdd = 0.0f;
-        for (uint32_t c = 0; c < n; c++) qdd += ldDI(l, r, c) * (A[L + L_UU + c] - sdot(ldU(l, c), a1));
+        for (uint32_t c = 0; c < n; c++) qdd += ldDI(l, r, c) * (LB[L + L_UU + c] - sdot(ldU(l, c), a1));
         A[S.A_QDH + d0 + r] = A[S.A_QD + d0 + r] + P.dt * qdd;
         acc = sadd(acc, sscl(ldS(l, r), qdd));
       }
@@ -402,7 +408,7 @@ struct Art {
       W[0 * 6 + e] = dv[e].l.x; W[1 * 6 + e] = dv[e].l.y; W[2 * 6 + e] = dv[e].l.z;
       W[3 * 6 + e] = dv[e].a.x; W[4 * 6 + e] = dv[e].a.y; W[5 * 6 + e] = dv[e].a.z;
     }
-    for (uint32_t k = 0; k < 36u; k++) A[lo(l) + L_W2 + k] = W[k];
+    for (uint32_t k = 0; k < 36u; k++) LB[lo(l) + L_W2 + k] = W[k];
     for (uint32_t i = 0; i < np; i++) {
       float extra = (float)split[i] - 1.0f;
       if (extra <= 0.0f) continue;
@@ -421,7 +427,7 @@ struct Art {
           W[rr * 6u + cc] += extra * sv;
         }
     }
-    for (uint32_t k = 0; k < 36u; k++) A[lo(l) + L_W + k] = W[k];
+    for (uint32_t k = 0; k < 36u; k++) LB[lo(l) + L_W + k] = W[k];
   }
 
   // Generalized Jacobians (artwgsl.js:525-554).
@@ -529,7 +535,7 @@ struct Art {
       uint32_t n = lndof(l);
       SVec p = ldsv(L + L_P);
       float u[6] = {0, 0, 0, 0, 0, 0};
-      for (uint32_t r = 0; r < n; r++) { u[r] = A[L + L_TAU + r] - sdot(ldS(l, r), p); A[L + L_UU + r] = u[r]; }
+      for (uint32_t r = 0; r < n; r++) { u[r] = LB[L + L_TAU + r] - sdot(ldS(l, r), p); LB[L + L_UU + r] = u[r]; }
       int par = lparent(l);
       if (par >= 0) {
         SVec pp = p;
@@ -551,7 +557,7 @@ struct Art {
       float dq[6] = {0, 0, 0, 0, 0, 0};
       for (uint32_t r = 0; r < n; r++) {
         dq[r] = 0.0f;
-        for (uint32_t c = 0; c < n; c++) dq[r] += ldDI(l, r, c) * (A[L + L_UU + c] - sdot(ldU(l, c), dv));
+        for (uint32_t c = 0; c < n; c++) dq[r] += ldDI(l, r, c) * (LB[L + L_UU + c] - sdot(ldU(l, c), dv));
       }
       for (uint32_t r = 0; r < n; r++) { dv = sadd(dv, sscl(ldS(l, r), dq[r])); aqd[ldof(l) + r] += dq[r]; }
       stsv(L + L_DV, dv);
@@ -559,7 +565,7 @@ struct Art {
       stsv(L + L_V, v);
       set_twist(l, v, tw);
       stsv(L + L_P, sv0());
-      for (uint32_t r = 0; r < S.JM; r++) A[L + L_TAU + r] = 0.0f;
+      for (uint32_t r = 0; r < S.JM; r++) LB[L + L_TAU + r] = 0.0f;
     }
   }
 };

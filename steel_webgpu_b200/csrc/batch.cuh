@@ -19,23 +19,84 @@ struct BatchDev {
   double* phase;              // per-scene clock (sim.js:674-678)
   unsigned long long* substep_count;  // [1]
   uint32_t* error;            // [1] first device-side error code (0 = none)
+  uint32_t prep_smem;         // dynamic shared memory of k_prepare / k_solve launches (bytes)
+  uint32_t solve_smem;
 };
 
 constexpr uint32_t BROAD_TILE = 32;
 constexpr int NARROW_WARPS = 8;          // warps per narrowphase block
 constexpr int SORT_THREADS = 512;
-constexpr int PREP_THREADS = 512;
-constexpr int SOLVE_THREADS = 256;
+constexpr int PREP_THREADS = 128;
+constexpr int SOLVE_THREADS = 128;
 
 // Device error codes written to BatchDev::error.
 enum : uint32_t { ERR_NONE = 0, ERR_SORT_CAPACITY = 1 };
+
+// Shared-memory staging of a scene inside k_prepare / k_solve. A scene is staged when its part
+// fits the cap; the launch's dynamic shared memory is the largest staged scene's need.
+enum : uint32_t { STAGE_LINKS = 1u, STAGE_BODIES = 2u, STAGE_QD = 4u, STAGE_WMASK = 8u };
+// Caps keep four prepare / solve blocks resident per SM.
+constexpr uint32_t STAGE_LINK_CAP = 44u * 1024u;   // link blocks (NL * 1072 B)
+constexpr uint32_t STAGE_BODY_CAP = 8u * 1024u;    // twists + impulses (NB * 64 B)
+constexpr uint32_t STAGE_QD_CAP = 8u * 1024u;      // generalized velocities of the solve (ND * 4 B)
+constexpr uint32_t STAGE_WMASK_CAP = 16u * 1024u;  // per-body color masks (NB * NCOLW words)
+constexpr uint32_t COLOR_CHUNK = 512u;             // row keys staged per round of the serial coloring
+// Byte offsets of a scene's parts in k_prepare's dynamic shared memory: link blocks (if staged),
+// coloring key chunk, color counts, color masks (if staged).
+struct PrepSmem { uint32_t links, ckey, wcount, wmask, total; };
+__host__ __device__ inline PrepSmem prep_smem_layout(uint32_t stage, uint32_t NL, uint32_t NB, uint32_t NCOLW,
+                                                     uint32_t NCOL) {
+  PrepSmem m{};
+  uint32_t o = 0;
+  m.links = o;
+  if (stage & STAGE_LINKS) o += 4u * NL * 268u;
+  m.ckey = o;
+  o += 4u * COLOR_CHUNK;
+  m.wcount = o;
+  o += 4u * (NCOL + 2u);
+  m.wmask = o;
+  if (stage & STAGE_WMASK) o += 4u * NB * NCOLW;
+  m.total = (o + 15u) & ~15u;
+  return m;
+}
+// Byte offsets of a scene's parts in k_solve's dynamic shared memory: [tw | imp] (if bodies
+// are staged), qd (if staged), color starts, link blocks (if staged).
+struct SolveSmem { uint32_t tw, imp, aqd, wcs, links, total; };
+__host__ __device__ inline SolveSmem solve_smem_layout(uint32_t stage, uint32_t NB, uint32_t ND, uint32_t NCOL,
+                                                       uint32_t NL) {
+  SolveSmem m{};
+  uint32_t o = 0;
+  if (stage & STAGE_BODIES) { m.tw = 0; m.imp = 32u * NB; o = 64u * NB; }
+  m.aqd = o;
+  if (stage & STAGE_QD) o += 4u * ND;
+  m.wcs = o;
+  o += 4u * (NCOL + 2u);
+  o = (o + 15u) & ~15u;
+  m.links = o;
+  if (stage & STAGE_LINKS) o += 4u * NL * 268u;
+  m.total = o;
+  return m;
+}
+
+// Copies a scene's descriptor into shared memory (all threads of the block call it; ends with a
+// barrier), so the per-scene kernels read offsets and sizes at shared-memory latency.
+__device__ inline void copy_scene(SceneDev& dst, const SceneDev& src) {
+  static_assert(sizeof(SceneDev) % 4 == 0, "SceneDev is copied as words");
+  const uint32_t* s = reinterpret_cast<const uint32_t*>(&src);
+  uint32_t* d = reinterpret_cast<uint32_t*>(&dst);
+  for (uint32_t i = threadIdx.x; i < sizeof(SceneDev) / 4u; i += blockDim.x) d[i] = s[i];
+  __syncthreads();
+}
 
 void launch_params(const BatchDev& b, uint32_t substep, cudaStream_t st);
 void launch_shapes(const BatchDev& b, cudaStream_t st);
 void launch_broad(const BatchDev& b, cudaStream_t st);
 void launch_narrow(const BatchDev& b, uint32_t narrow_blocks, cudaStream_t st);
+int narrow_blocks_per_sm();
 void launch_csort(const BatchDev& b, size_t smem_keys, cudaStream_t st);
 cudaError_t configure_sort(size_t smem_keys);
+cudaError_t configure_prepare(size_t smem_bytes);
+cudaError_t configure_solve(size_t smem_bytes);
 void launch_prepare(const BatchDev& b, cudaStream_t st);
 void launch_solve(const BatchDev& b, cudaStream_t st);
 void launch_frame_end(const BatchDev& b, cudaStream_t st);

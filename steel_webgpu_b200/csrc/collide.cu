@@ -1110,7 +1110,7 @@ struct Narrow {
   }
 };
 
-__global__ void __launch_bounds__(NARROW_WARPS * 32) k_narrow(BatchDev B) {
+__global__ void __launch_bounds__(NARROW_WARPS * 32, 2) k_narrow(BatchDev B) {
   uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5u;
   uint32_t nwarps = (gridDim.x * blockDim.x) >> 5u;
   uint32_t total = *B.pair_count;
@@ -1191,6 +1191,12 @@ void launch_shapes(const BatchDev& b, cudaStream_t st) {
 }
 void launch_broad(const BatchDev& b, cudaStream_t st) {
   if (b.ntiles) k_broad<<<b.ntiles, 256, 0, st>>>(b);
+}
+// Resident narrowphase blocks per SM (the persistent grid is this times the SM count).
+int narrow_blocks_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_narrow, NARROW_WARPS * 32, 0) != cudaSuccess || n < 1) n = 1;
+  return n;
 }
 void launch_narrow(const BatchDev& b, uint32_t narrow_blocks, cudaStream_t st) {
   k_narrow<<<narrow_blocks, NARROW_WARPS * 32, 0, st>>>(b);

@@ -114,21 +114,22 @@ SHD uint32_t mix32(uint32_t x) {
 // reduction by pi/2 (nearest multiple), then the Taylor series of sin/cos on
 // |r| <= pi/4 to degree 21/20; atan by two half-angle reductions
 // t -> t / (1 + sqrt(1 + t^2)) followed by its Taylor series to degree 41.
+// Series are evaluated in Horner form; the coefficients (-1)^n/(2n+1)!, (-1)^n/(2n)! and
+// (-1)^n/(2n+1) are written as their nearest doubles (hexadecimal literals).
 SHD double ser_sin(double r) {
-  double r2 = r * r, t = r, s = r;
-  for (int n = 1; n <= 10; n++) { t = -t * r2 / (double)((2 * n) * (2 * n + 1)); s = s + t; }
-  return s;
+  double r2 = r * r;
+  double q = -0x1.5555555555555p-3 + r2 * (0x1.1111111111111p-7 + r2 * (-0x1.a01a01a01a01ap-13 + r2 * (0x1.71de3a556c734p-19 + r2 * (-0x1.ae64567f544e4p-26 + r2 * (0x1.6124613a86d09p-33 + r2 * (-0x1.ae7f3e733b81fp-41 + r2 * (0x1.952c77030ad4ap-49 + r2 * (-0x1.2f49b46814157p-57 + r2 * (0x1.71b8ef6dcf572p-66)))))))));
+  return r + (r * r2) * q;
 }
 SHD double ser_cos(double r) {
-  double r2 = r * r, t = 1.0, s = 1.0;
-  for (int n = 1; n <= 10; n++) { t = -t * r2 / (double)((2 * n - 1) * (2 * n)); s = s + t; }
-  return s;
+  double r2 = r * r;
+  double q = -0x1.0000000000000p-1 + r2 * (0x1.5555555555555p-5 + r2 * (-0x1.6c16c16c16c17p-10 + r2 * (0x1.a01a01a01a01ap-16 + r2 * (-0x1.27e4fb7789f5cp-22 + r2 * (0x1.1eed8eff8d898p-29 + r2 * (-0x1.93974a8c07c9dp-37 + r2 * (0x1.ae7f3e733b81fp-45 + r2 * (-0x1.6827863b97d97p-53 + r2 * (0x1.e542ba4020225p-62)))))))));
+  return 1.0 + r2 * q;
 }
 SHD void quadrant(double x, double* r, int* q) {
   double k = nearbyint(x * 0.6366197723675814);
   *r = x - k * 1.5707963267948966;
-  long long kk = (long long)k;
-  *q = (int)(((kk % 4) + 4) % 4);
+  *q = (int)((long long)k & 3);
 }
 SHD float fsin(float xf) {
   double r; int q; quadrant((double)xf, &r, &q);
@@ -141,9 +142,9 @@ SHD float fcos(float xf) {
   return (float)v;
 }
 SHD double ser_atan(double t) {
-  double t2 = t * t, p = t, s = t;
-  for (int n = 1; n <= 20; n++) { p = -p * t2; s = s + p / (double)(2 * n + 1); }
-  return s;
+  double t2 = t * t;
+  double q = -0x1.5555555555555p-2 + t2 * (0x1.999999999999ap-3 + t2 * (-0x1.2492492492492p-3 + t2 * (0x1.c71c71c71c71cp-4 + t2 * (-0x1.745d1745d1746p-4 + t2 * (0x1.3b13b13b13b14p-4 + t2 * (-0x1.1111111111111p-4 + t2 * (0x1.e1e1e1e1e1e1ep-5 + t2 * (-0x1.af286bca1af28p-5 + t2 * (0x1.8618618618618p-5 + t2 * (-0x1.642c8590b2164p-5 + t2 * (0x1.47ae147ae147bp-5 + t2 * (-0x1.2f684bda12f68p-5 + t2 * (0x1.1a7b9611a7b96p-5 + t2 * (-0x1.0842108421084p-5 + t2 * (0x1.f07c1f07c1f08p-6 + t2 * (-0x1.d41d41d41d41dp-6 + t2 * (0x1.bacf914c1bad0p-6 + t2 * (-0x1.a41a41a41a41ap-6 + t2 * (0x1.8f9c18f9c18fap-6)))))))))))))))))));
+  return t + (t * t2) * q;
 }
 SHD double atan_unit(double t) {
   double a = t / (1.0 + sqrt(1.0 + t * t));
@@ -218,6 +219,8 @@ struct SceneDev {
   float* tscr;                       // per-thread scratch slices (path temporaries), TSCR floats each
   uint32_t TSCR;
   float4 *tw, *imp;                  // solve: body twists and link impulses [NB * 2]
+  uint32_t stage;                    // shared-memory staging: bit 0 link blocks (prepare, solve),
+                                     // bit 1 twists, impulses and qd (solve)
   float* aqd;                        // solve: generalized velocities [ND]
   uint32_t scene_index;
 };

@@ -36,7 +36,7 @@ struct Prep {
   const SceneDev& S;
   const Params& P;
   Art ar;
-  __device__ Prep(const SceneDev& s, const Params& p) : S(s), P(p), ar(s) {}
+  __device__ Prep(const SceneDev& s, const Params& p, float* lb) : S(s), P(p), ar(s, lb) {}
 
   __device__ uint32_t bkind(int b) const { return f2u(S.sf[S.SF_BODY + (uint32_t)b * 8u].y); }
   __device__ int bart(int b) const { return f2i(S.sf[S.SF_BODY + (uint32_t)b * 8u].z); }
@@ -65,7 +65,7 @@ struct Prep {
     }
     // Kind 2 links answer the unsplit query from L_W2; immovable links (kind 3) from L_W.
     uint32_t wo = ar.lo((uint32_t)blink(b)) + ((unsplit && k == 2u) ? L_W2 : L_W);
-    const float* W = S.art + wo;
+    const float* W = ar.LB + wo;
     float x[6] = {f.x, f.y, f.z, t.x, t.y, t.z}, o[6];
     for (uint32_t r = 0; r < 6u; r++) {
       float s = 0.0f;
@@ -469,7 +469,7 @@ struct Prep {
     A[o + 4u] = rhs; A[o + 5u] = effn;
     A[o + 6u] = k11 / det; A[o + 7u] = -k01 / det; A[o + 8u] = k00 / det;
     A[o + 9u] = ln; A[o + 10u] = lt.x; A[o + 11u] = lt.y;
-    ar.st3(o + 12u, t1); ar.st3(o + 15u, t2); ar.st3(o + 18u, n);
+    ar.ast3(o + 12u, t1); ar.ast3(o + 15u, t2); ar.ast3(o + 18u, n);
     A[o + 21u] = 0.0f;
     A[o + 24u] = bounce ? 1.0f : row_weight(phi);
     A[o + 22u] = bounce ? 1e30f : phi;
@@ -501,14 +501,23 @@ struct Prep {
 };
 
 __global__ void __launch_bounds__(PREP_THREADS) k_prepare(BatchDev B) {
+  extern __shared__ float4 psm4[];  // prep_smem_layout: link blocks, coloring
   __shared__ uint32_t stmp[40];
   __shared__ Params Ps;
-  const SceneDev& S = B.scenes[blockIdx.x];
+  __shared__ SceneDev Ss;  // the scene's offsets and sizes, read everywhere in the serial passes
   const uint32_t tid = threadIdx.x, nt = blockDim.x;
-  if (tid == 0u) Ps = *S.params;
+  copy_scene(Ss, B.scenes[blockIdx.x]);
+  const SceneDev& S = Ss;
+  if (tid == 0u) Ps = *B.scenes[blockIdx.x].params;
+  uint8_t* pb = reinterpret_cast<uint8_t*>(psm4);
+  const PrepSmem lay = prep_smem_layout(S.stage, S.NL, S.NB, S.NCOLW, S.NCOL);
+  const bool staged = (S.stage & STAGE_LINKS) != 0u;
+  float* lb = staged ? reinterpret_cast<float*>(pb + lay.links) : S.art + S.A_LINK;
+  if (staged)
+    for (uint32_t i = tid; i < S.NL * LBLK; i += nt) lb[i] = S.art[S.A_LINK + i];
   __syncthreads();
   const Params& P = Ps;
-  Prep pr(S, P);
+  Prep pr(S, P, lb);
   const Art& ar = pr.ar;
   float* A = S.art;
   uint32_t* sch = S.sched;
@@ -723,44 +732,76 @@ __global__ void __launch_bounds__(PREP_THREADS) k_prepare(BatchDev B) {
   if (S.PATCH == 1u)
     for (uint32_t u = tid; u < nu; u += nt) pr.build_patch(u);
   __syncthreads();
-  // Phase 6c: greedy first-fit coloring of the rows in contact order (serial, as the reference),
-  // then the rows bucketed by color in row order.
-  if (tid == 0u) {
-    uint32_t* wmask = sch + S.S_WMASK;
-    uint32_t* wcount = sch + S.S_WCOUNT;
+  // Phase 6c: greedy first-fit coloring of the rows in contact order (serial on one thread, as
+  // the reference), with the per-body color masks and the color counts in shared memory and the
+  // rows' body-pair keys staged COLOR_CHUNK at a time; then the rows bucketed by color in row
+  // order (warp 0, match/ballot ranks).
+  {
+    uint32_t* ckey = reinterpret_cast<uint32_t*>(pb + lay.ckey);
+    uint32_t* wcount = reinterpret_cast<uint32_t*>(pb + lay.wcount);
+    uint32_t* wmask = (S.stage & STAGE_WMASK) ? reinterpret_cast<uint32_t*>(pb + lay.wmask) : sch + S.S_WMASK;
     const uint32_t NCOLW = S.NCOLW;
-    for (uint32_t row = 0; row < total; row++) {
-      uint32_t key = sch[S.S_UKEY + sch[S.S_RUNIT + row]];
-      int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
-      uint32_t col = S.NCOL;
-      for (uint32_t w = 0; w < NCOLW; w++) {
-        uint32_t used = 0u;
-        if (a >= 0) used |= wmask[(uint32_t)a * NCOLW + w];
-        if (b >= 0) used |= wmask[(uint32_t)b * NCOLW + w];
-        if (used != 0xffffffffu) {
-          uint32_t k = (uint32_t)__ffs(~used) - 1u;
-          if (a >= 0) wmask[(uint32_t)a * NCOLW + w] |= 1u << k;
-          if (b >= 0) wmask[(uint32_t)b * NCOLW + w] |= 1u << k;
-          col = w * 32u + k;
-          break;
+    for (uint32_t i = tid; i < S.NCOL + 2u; i += nt) wcount[i] = 0u;
+    if (S.stage & STAGE_WMASK)
+      for (uint32_t i = tid; i < S.NB * NCOLW; i += nt) wmask[i] = 0u;
+    for (uint32_t r0 = 0; r0 < total; r0 += COLOR_CHUNK) {
+      const uint32_t nrow = min(COLOR_CHUNK, total - r0);
+      __syncthreads();
+      for (uint32_t i = tid; i < nrow; i += nt) ckey[i] = sch[S.S_UKEY + sch[S.S_RUNIT + r0 + i]];
+      __syncthreads();
+      if (tid == 0u) {
+        for (uint32_t i = 0; i < nrow; i++) {
+          uint32_t key = ckey[i];
+          int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
+          uint32_t col = S.NCOL;
+          for (uint32_t w = 0; w < NCOLW; w++) {
+            uint32_t used = 0u;
+            if (a >= 0) used |= wmask[(uint32_t)a * NCOLW + w];
+            if (b >= 0) used |= wmask[(uint32_t)b * NCOLW + w];
+            if (used != 0xffffffffu) {
+              uint32_t k = (uint32_t)__ffs(~used) - 1u;
+              if (a >= 0) wmask[(uint32_t)a * NCOLW + w] |= 1u << k;
+              if (b >= 0) wmask[(uint32_t)b * NCOLW + w] |= 1u << k;
+              col = w * 32u + k;
+              break;
+            }
+          }
+          sch[S.S_PCOL + r0 + i] = col;
+          wcount[col]++;
         }
       }
-      sch[S.S_PCOL + row] = col;
-      wcount[col]++;
     }
-    uint32_t acc = 0u, ncol = 0u;
-    for (uint32_t c = 0; c <= S.NCOL; c++) {
-      uint32_t n = wcount[c];
-      sch[S.S_CSTART + c] = acc;
-      wcount[c] = acc;
-      acc += n;
-      if (n > 0u) ncol = c + 1u;
+    __syncthreads();
+    if (tid == 0u) {
+      uint32_t acc = 0u, ncol = 0u;
+      for (uint32_t c = 0; c <= S.NCOL; c++) {
+        uint32_t n = wcount[c];
+        sch[S.S_CSTART + c] = acc;
+        wcount[c] = acc;
+        acc += n;
+        if (n > 0u) ncol = c + 1u;
+      }
+      sch[S.S_CSTART + S.NCOL + 1u] = acc;
+      sch[S.S_META + 0u] = nu;
+      sch[S.S_META + 1u] = ncol;
+      sch[S.S_META + 2u] = nc;
     }
-    sch[S.S_CSTART + S.NCOL + 1u] = acc;
-    for (uint32_t row = 0; row < total; row++) sch[S.S_PORD + wcount[sch[S.S_PCOL + row]]++] = row;
-    sch[S.S_META + 0u] = nu;
-    sch[S.S_META + 1u] = ncol;
-    sch[S.S_META + 2u] = nc;
+    __syncthreads();
+    if (tid < 32u) {
+      for (uint32_t r0 = 0; r0 < total; r0 += 32u) {
+        const uint32_t row = r0 + tid;
+        const bool in = row < total;
+        const uint32_t col = in ? sch[S.S_PCOL + row] : 0xffffffffu;
+        const uint32_t same = __match_any_sync(0xffffffffu, col);
+        const uint32_t base = in ? wcount[col] : 0u;
+        __syncwarp();
+        if (in) {
+          sch[S.S_PORD + base + (uint32_t)__popc(same & ((1u << tid) - 1u))] = row;
+          if (tid == 31u - (uint32_t)__clz(same)) wcount[col] = base + (uint32_t)__popc(same);
+        }
+        __syncwarp();
+      }
+    }
   }
   // Phase 7: dense rows for same-articulation contacts (slots in contact order), loops, mimics.
   uint32_t nloop_rows = 0u;
@@ -820,8 +861,15 @@ __global__ void __launch_bounds__(PREP_THREADS) k_prepare(BatchDev B) {
     float phi = (A[S.A_Q + f2u(M1.x)] - M0.w * A[S.A_Q + f2u(M1.y)]) - M1.z;
     pr.put_bilateral(S.A_DENSE + slot * S.DPS, f2u(M0.x), J, 1u, mf3((P.beta * phi) / P.dt, 0.0f, 0.0f), tscr + JDIM);
   }
+  if (staged) {
+    __syncthreads();
+    for (uint32_t i = tid; i < S.NL * LBLK; i += nt) S.art[S.A_LINK + i] = lb[i];
+  }
 }
 
-void launch_prepare(const BatchDev& b, cudaStream_t st) { k_prepare<<<b.nscenes, PREP_THREADS, 0, st>>>(b); }
+cudaError_t configure_prepare(size_t smem_bytes) {
+  return cudaFuncSetAttribute(k_prepare, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+}
+void launch_prepare(const BatchDev& b, cudaStream_t st) { k_prepare<<<b.nscenes, PREP_THREADS, b.prep_smem, st>>>(b); }
 
 }  // namespace steel

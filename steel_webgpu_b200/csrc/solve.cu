@@ -24,7 +24,8 @@ struct Solver {
   float4* tw;
   float4* imp;
   float* aqd;
-  __device__ Solver(const SceneDev& s, const Params& p) : S(s), P(p), ar(s), tw(s.tw), imp(s.imp), aqd(s.aqd) {}
+  __device__ Solver(const SceneDev& s, const Params& p, float* lb, float4* tw_, float4* imp_, float* aqd_)
+      : S(s), P(p), ar(s, lb), tw(tw_), imp(imp_), aqd(aqd_) {}
 
   __device__ uint32_t bkind(int b) const { return f2u(S.sf[S.SF_BODY + (uint32_t)b * 8u].y); }
   __device__ uint32_t bflags(int b) const { return b < 0 ? 0u : f2u(S.sf[S.SF_BODY + (uint32_t)b * 8u + 7u].w); }
@@ -216,12 +217,118 @@ struct Solver {
     solve_row(f2u(sl.y), f2u(sl.x), f2i(sl.z), f2i(sl.w), mode, it);
   }
 
-  // Dense same-articulation rows of articulation a (wgsl.js:3306-3364), sequential sums.
-  __device__ bool dense(uint32_t a, uint32_t mode, uint32_t it, uint32_t ph) const {
+  // subgroupAdd over the warp (wgsl.js:3305, subgroups on), pinned to an xor butterfly over lane
+  // offsets 16, 8, 4, 2, 1. IEEE addition commutes, so every lane ends with the same bits.
+  static __device__ float lane_sum(float x) {
+    for (uint32_t off = 16u; off > 0u; off >>= 1u) x += __shfl_xor_sync(0xffffffffu, x, off);
+    return x;
+  }
+  // Dense same-articulation rows of articulation a (wgsl.js:3306-3364), one warp: lane l owns
+  // dofs l, l + 32, ... (so lanes never touch each other's qd entries) and its partial sums
+  // are combined with lane_sum. Each lane first loads its slice of the row (J and Y rows of its
+  // dofs, up to DENSE_REG of them) into registers. Called by all 32 lanes; returns whether a
+  // row belongs to a.
+  static constexpr uint32_t DENSE_REG = 2u;  // articulations of up to 64 dofs keep rows in registers
+  __device__ bool dense(uint32_t a, uint32_t mode, uint32_t it, uint32_t ph, uint32_t lane) const {
     const uint32_t NDA = S.NDA, DHDR = S.DHDR, DPS = S.DPS;
     float* A = S.art;
     uint32_t nd = min(S.sched[S.S_META + 3u], S.MAXDENSE);
     uint4 ai = ar.info(a);
+    if (ai.w > 32u * DENSE_REG) return dense_wide(a, mode, it, ph, lane, nd, ai);
+    float* q = aqd + ai.z;
+    bool touched = false;
+    for (uint32_t i = 0; i < nd; i++) {
+      uint32_t o = S.A_DENSE + i * DPS;
+      if (f2u(A[o]) != a) continue;
+      touched = true;
+      uint32_t jo = o + DHDR, yo = o + DHDR + 3u * NDA;
+      float J[3][DENSE_REG], Y[3][DENSE_REG];
+#pragma unroll
+      for (uint32_t j = 0; j < DENSE_REG; j++) {
+        uint32_t k = lane + 32u * j;
+        bool v = k < ai.w;
+#pragma unroll
+        for (uint32_t r = 0; r < 3u; r++) {
+          J[r][j] = v ? A[jo + r * NDA + k] : 0.0f;
+          Y[r][j] = v ? A[yo + r * NDA + k] : 0.0f;
+        }
+      }
+      const float m3_ = A[o + 3u], m4 = A[o + 4u], m5 = A[o + 5u], m6 = A[o + 6u], m7 = A[o + 7u], m8 = A[o + 8u];
+      const float nbil = A[o + 21u], m22 = A[o + 22u], m23 = A[o + 23u], m24 = A[o + 24u];
+      f3 lam = mf3(A[o + 9u], A[o + 10u], A[o + 11u]);
+      if ((nbil > 0.5f) == (ph == 1u) && ph != 0u) continue;
+      if (nbil > 0.5f) {
+        if (mode == 0u) continue;
+        f3 nlam = lam;
+        const uint32_t nr = f2u(nbil);
+#pragma unroll
+        for (uint32_t r = 0; r < 3u; r++) {
+          if (r >= nr) break;
+          float part = 0.0f;
+#pragma unroll
+          for (uint32_t j = 0; j < DENSE_REG; j++) {
+            uint32_t k = lane + 32u * j;
+            if (k < ai.w) part += J[r][j] * q[k];
+          }
+          float jv = lane_sum(part);
+          float rhs = r == 0u ? m4 : (r == 1u ? m22 : m23);
+          float dl = ((-S.F_OMEGA) * (jv + rhs)) * A[o + 5u + r];
+          setc(nlam, (int)r, comp(nlam, (int)r) + dl);
+#pragma unroll
+          for (uint32_t j = 0; j < DENSE_REG; j++) {
+            uint32_t k = lane + 32u * j;
+            if (k < ai.w) q[k] += Y[r][j] * dl;
+          }
+        }
+        if (lane == 0u) { A[o + 9u] = nlam.x; A[o + 10u] = nlam.y; A[o + 11u] = nlam.z; }
+        continue;
+      }
+      if (mode == 0u) {
+#pragma unroll
+        for (uint32_t j = 0; j < DENSE_REG; j++) {
+          uint32_t k = lane + 32u * j;
+          if (k < ai.w) q[k] += (Y[0][j] * lam.x + Y[1][j] * lam.y) + Y[2][j] * lam.z;
+        }
+        continue;
+      }
+      float part = 0.0f;
+#pragma unroll
+      for (uint32_t j = 0; j < DENSE_REG; j++) {
+        uint32_t k = lane + 32u * j;
+        if (k < ai.w) part += J[0][j] * q[k];
+      }
+      float jv = lane_sum(part);
+      float nl = fmx(lam.x + S.F_OMEGA * ((((-(jv + m4)) * m5) * m24) - (1.0f - m24) * lam.x), 0.0f);
+      float dn = nl - lam.x;
+      float p1 = 0.0f, p2 = 0.0f;
+#pragma unroll
+      for (uint32_t j = 0; j < DENSE_REG; j++) {
+        uint32_t k = lane + 32u * j;
+        if (k < ai.w) {
+          q[k] += Y[0][j] * dn;
+          p1 += J[1][j] * q[k];
+          p2 += J[2][j] * q[k];
+        }
+      }
+      float s1 = lane_sum(p1), s2 = lane_sum(p2);
+      float lim = it < S.FSTART ? 0.0f : m3_ * nl;
+      float kd = m6 * m8 - m7 * m7;
+      f2 lt = friction_pair(m8 / kd, -m7 / kd, m6 / kd, s1, s2, lam.y, lam.z, lim, S.F_OMEGA);
+      float d1 = lt.x - lam.y, d2 = lt.y - lam.z;
+#pragma unroll
+      for (uint32_t j = 0; j < DENSE_REG; j++) {
+        uint32_t k = lane + 32u * j;
+        if (k < ai.w) q[k] += Y[1][j] * d1 + Y[2][j] * d2;
+      }
+      if (lane == 0u) { A[o + 9u] = nl; A[o + 10u] = lt.x; A[o + 11u] = lt.y; }
+    }
+    return touched;
+  }
+  // The same for articulations of more than 32 * DENSE_REG dofs, reading rows as it goes.
+  __device__ bool dense_wide(uint32_t a, uint32_t mode, uint32_t it, uint32_t ph, uint32_t lane, uint32_t nd,
+                             uint4 ai) const {
+    const uint32_t NDA = S.NDA, DHDR = S.DHDR, DPS = S.DPS;
+    float* A = S.art;
     bool touched = false;
     for (uint32_t i = 0; i < nd; i++) {
       uint32_t o = S.A_DENSE + i * DPS;
@@ -235,37 +342,40 @@ struct Solver {
         f3 nlam = lam;
         for (uint32_t r = 0; r < f2u(A[o + 21u]); r++) {
           float part = 0.0f;
-          for (uint32_t k = 0; k < ai.w; k++) part += A[jo + r * NDA + k] * aqd[ai.z + k];
+          for (uint32_t k = lane; k < ai.w; k += 32u) part += A[jo + r * NDA + k] * aqd[ai.z + k];
+          float jv = lane_sum(part);
           float rhs = r == 0u ? A[o + 4u] : (r == 1u ? A[o + 22u] : A[o + 23u]);
-          float dl = ((-S.F_OMEGA) * (part + rhs)) * A[o + 5u + r];
+          float dl = ((-S.F_OMEGA) * (jv + rhs)) * A[o + 5u + r];
           setc(nlam, (int)r, comp(nlam, (int)r) + dl);
-          for (uint32_t k = 0; k < ai.w; k++) aqd[ai.z + k] += A[yo + r * NDA + k] * dl;
+          for (uint32_t k = lane; k < ai.w; k += 32u) aqd[ai.z + k] += A[yo + r * NDA + k] * dl;
         }
-        A[o + 9u] = nlam.x; A[o + 10u] = nlam.y; A[o + 11u] = nlam.z;
+        if (lane == 0u) { A[o + 9u] = nlam.x; A[o + 10u] = nlam.y; A[o + 11u] = nlam.z; }
         continue;
       }
       if (mode == 0u) {
-        for (uint32_t k = 0; k < ai.w; k++)
+        for (uint32_t k = lane; k < ai.w; k += 32u)
           aqd[ai.z + k] += (A[yo + k] * lam.x + A[yo + NDA + k] * lam.y) + A[yo + 2u * NDA + k] * lam.z;
         continue;
       }
-      float jv = 0.0f;
-      for (uint32_t k = 0; k < ai.w; k++) jv += A[jo + k] * aqd[ai.z + k];
+      float part = 0.0f;
+      for (uint32_t k = lane; k < ai.w; k += 32u) part += A[jo + k] * aqd[ai.z + k];
+      float jv = lane_sum(part);
       float w = A[o + 24u];
       float nl = fmx(lam.x + S.F_OMEGA * ((((-(jv + A[o + 4u])) * A[o + 5u]) * w) - (1.0f - w) * lam.x), 0.0f);
       float dn = nl - lam.x;
       float p1 = 0.0f, p2 = 0.0f;
-      for (uint32_t k = 0; k < ai.w; k++) {
+      for (uint32_t k = lane; k < ai.w; k += 32u) {
         aqd[ai.z + k] += A[yo + k] * dn;
         p1 += A[jo + NDA + k] * aqd[ai.z + k];
         p2 += A[jo + 2u * NDA + k] * aqd[ai.z + k];
       }
+      float s1 = lane_sum(p1), s2 = lane_sum(p2);
       float lim = it < S.FSTART ? 0.0f : A[o + 3u] * nl;
       float kd = A[o + 6u] * A[o + 8u] - A[o + 7u] * A[o + 7u];
-      f2 lt = friction_pair(A[o + 8u] / kd, -A[o + 7u] / kd, A[o + 6u] / kd, p1, p2, lam.y, lam.z, lim, S.F_OMEGA);
+      f2 lt = friction_pair(A[o + 8u] / kd, -A[o + 7u] / kd, A[o + 6u] / kd, s1, s2, lam.y, lam.z, lim, S.F_OMEGA);
       float d1 = lt.x - lam.y, d2 = lt.y - lam.z;
-      for (uint32_t k = 0; k < ai.w; k++) aqd[ai.z + k] += A[yo + NDA + k] * d1 + A[yo + 2u * NDA + k] * d2;
-      A[o + 9u] = nl; A[o + 10u] = lt.x; A[o + 11u] = lt.y;
+      for (uint32_t k = lane; k < ai.w; k += 32u) aqd[ai.z + k] += A[yo + NDA + k] * d1 + A[yo + 2u * NDA + k] * d2;
+      if (lane == 0u) { A[o + 9u] = nl; A[o + 10u] = lt.x; A[o + 11u] = lt.y; }
     }
     return touched;
   }
@@ -300,7 +410,7 @@ struct Solver {
       if (fr > 0.0f) {
         float lam = A[S.A_FRIC + d];
         float nl = clmp(lam - (S.F_OMEGA * aqd[d]) / hinv, -fr * P.dt, fr * P.dt);
-        if (nl != lam) { A[S.A_FRIC + d] = nl; A[ar.lo(l) + L_TAU + r] = nl - lam; ar.apply(a, aqd, tw); }
+        if (nl != lam) { A[S.A_FRIC + d] = nl; ar.LB[ar.lo(l) + L_TAU + r] = nl - lam; ar.apply(a, aqd, tw); }
       }
       float4 lim = ar.dof_limit(d);
       if (A[S.A_LG + d] > 0.5f) {
@@ -314,7 +424,7 @@ struct Solver {
           float nl = fmx(lam - (S.F_OMEGA * (sg * aqd[d] + rhs)) / hinv, 0.0f);
           if (nl == lam) continue;
           A[S.A_LIM + 2u * d + side] = nl;
-          A[ar.lo(l) + L_TAU + r] = sg * (nl - lam);
+          ar.LB[ar.lo(l) + L_TAU + r] = sg * (nl - lam);
           ar.apply(a, aqd, tw);
         }
       }
@@ -341,9 +451,17 @@ struct Solver {
     return lin + cross(ang, x - 0.5f * (p0 + p1));
   }
 
+  // Dense rows of every articulation, one warp each, then the twists of the articulations they
+  // moved (wgsl.js:3366-3377). Articulations share no qd, rows or links, so each warp goes on to
+  // its next articulation without a block barrier.
   __device__ void dense_phase(uint32_t mode, uint32_t it, uint32_t ph) const {
-    for (uint32_t a = threadIdx.x; a < S.NA; a += blockDim.x)
-      if (dense(a, mode, it, ph)) ar.twists(a, aqd, tw);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5u, nw = blockDim.x >> 5u;
+    for (uint32_t a = warp; a < S.NA; a += nw) {
+      bool touched = dense(a, mode, it, ph, lane);
+      __syncwarp();
+      if (lane == 0u && touched) ar.twists(a, aqd, tw);
+      __syncwarp();
+    }
     __syncthreads();
   }
   // One sweep (wgsl.js:3559-3611).
@@ -405,7 +523,7 @@ struct Solver {
       return mf4(lam.x, v3(S.rows[o + 1u]) * lam.y + v3(S.rows[o + 2u]) * lam.z);
     }
     uint32_t o = S.A_DENSE + (i - nc) * S.DPS;
-    return mf4(S.art[o + 9u], ar.ld3(o + 12u) * S.art[o + 10u] + ar.ld3(o + 15u) * S.art[o + 11u]);
+    return mf4(S.art[o + 9u], ar.ald3(o + 12u) * S.art[o + 10u] + ar.ald3(o + 15u) * S.art[o + 11u]);
   }
   __device__ uint32_t warm_rank(uint32_t i, uint32_t nc) const {
     return min(__float_as_uint(fmx(warm_value(i, nc).x, 0.0f)), 0xfffffffeu) + 1u;
@@ -419,17 +537,28 @@ struct Solver {
 };
 
 __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(BatchDev B) {
-  extern __shared__ uint32_t wcs[];  // color starts [NCOL + 2]
+  extern __shared__ float4 ssm4[];  // solve_smem_layout: [tw | imp], qd, color starts, link blocks
   __shared__ Params Ps;
-  const SceneDev& S = B.scenes[blockIdx.x];
+  __shared__ SceneDev Ss;  // the scene's offsets and sizes, read everywhere in the serial passes
   const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  copy_scene(Ss, B.scenes[blockIdx.x]);
+  const SceneDev& S = Ss;
   if (tid == 0u) Ps = *S.params;
+  uint8_t* sb = reinterpret_cast<uint8_t*>(ssm4);
+  const SolveSmem lay = solve_smem_layout(S.stage, S.NB, S.ND, S.NCOL, S.NL);
+  const bool staged_links = (S.stage & STAGE_LINKS) != 0u, staged_bodies = (S.stage & STAGE_BODIES) != 0u;
+  uint32_t* wcs = reinterpret_cast<uint32_t*>(sb + lay.wcs);
+  float* lb = staged_links ? reinterpret_cast<float*>(sb + lay.links) : S.art + S.A_LINK;
   const uint32_t nu = S.sched[S.S_META];
   const uint32_t ncol = min(S.sched[S.S_META + 1u], S.NCOL);
   for (uint32_t i = tid; i < S.NCOL + 2u; i += nt) wcs[i] = S.sched[S.S_CSTART + i];
+  if (staged_links)
+    for (uint32_t i = tid; i < S.NL * LBLK; i += nt) lb[i] = S.art[S.A_LINK + i];
   __syncthreads();
   const Params& P = Ps;
-  Solver sv(S, P);
+  Solver sv(S, P, lb, staged_bodies ? reinterpret_cast<float4*>(sb + lay.tw) : S.tw,
+            staged_bodies ? reinterpret_cast<float4*>(sb + lay.imp) : S.imp,
+            (S.stage & STAGE_QD) ? reinterpret_cast<float*>(sb + lay.aqd) : S.aqd);
   float* A = S.art;
   // Prologue (wgsl.js:3635-3691).
   for (uint32_t i = tid; i < S.ND; i += nt) sv.aqd[i] = A[S.A_QDH + i];
@@ -437,6 +566,9 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(BatchDev B) {
     uint32_t kind = sv.bkind((int)b);
     sv.imp[b * 2u] = make_float4(0, 0, 0, 0);
     sv.imp[b * 2u + 1u] = make_float4(0, 0, 0, 0);
+    // The reference keeps twists in workgroup memory, which starts at zero in every dispatch.
+    sv.tw[b * 2u] = make_float4(0, 0, 0, 0);
+    sv.tw[b * 2u + 1u] = make_float4(0, 0, 0, 0);
     if (kind != 1u) continue;
     uint32_t fl = sv.bflags((int)b);
     f3 v = v3(S.lv[b]) + (fl != 0u ? sp3(0.0f) : v3(P.gravity) * P.dt);
@@ -619,11 +751,15 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(BatchDev B) {
     S.counters[0] = 0u;
     S.counters[1] = 0u;
   }
+  if (staged_links) {
+    __syncthreads();
+    for (uint32_t i = tid; i < S.NL * LBLK; i += nt) S.art[S.A_LINK + i] = lb[i];
+  }
 }
 
-void launch_solve(const BatchDev& b, cudaStream_t st) {
-  // Dynamic shared memory: the color starts of the widest color table in the batch.
-  k_solve<<<b.nscenes, SOLVE_THREADS, (64u * 32u + 2u) * sizeof(uint32_t), st>>>(b);
+cudaError_t configure_solve(size_t smem_bytes) {
+  return cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
 }
+void launch_solve(const BatchDev& b, cudaStream_t st) { k_solve<<<b.nscenes, SOLVE_THREADS, b.solve_smem, st>>>(b); }
 
 }  // namespace steel
