@@ -31,6 +31,7 @@ WORKLOADS = {
     # name: (generator kwargs, description)
     "uneven_batch_2048": dict(n_scenes=2048),
     "uneven_batch_256": dict(n_scenes=256),
+    "uneven_batch_64": dict(n_scenes=64),  # small case for profiler captures
 }
 
 
@@ -309,6 +310,8 @@ def run_steel(args):
     # Roofline of the dominant kernel: per-launch device time from CUDA events around each launch.
     prof = batch.profile_kernels(max(2, min(args.steps, 8)))
     counts = scene_counts(batch, pks)
+    # Capacities change results only when a buffer overflows; count the scenes where one did.
+    overflow_scenes = sum(1 for i in range(len(pks)) if batch.stats(i)["overflow"])
     rows_vec4 = pks[0].C["ROWS"]
     total_ms = sum(prof.values())
     dom = max(prof, key=prof.get)
@@ -328,7 +331,7 @@ def run_steel(args):
                    "fps": 240, "substeps": substeps, "iterations": iterations, "parallelism": f"replicas x{world}",
                    "graph": True, "l2": "per-scene state is resident and re-read every substep; no L2 flush",
                    "contact_steps_per_s": world * counts["contacts"] * substeps * args.steps / (ms / 1000.0),
-                   "build_s": round(build_s, 1)},
+                   "build_s": round(build_s, 1), "overflow_scenes": overflow_scenes},
         "e2e": {"value": e2e, "unit": "body-steps/s", "h2d_bytes_per_step": 4 * nd, "d2h_bytes_per_step": 4 * npose},
         "gpu_launches": args.steps * (substeps * 7 + 1),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -213,7 +213,7 @@ struct Narrow {
   __device__ uint32_t body_kind(int b) const { return f2u(S.sf[S.SF_BODY + (uint32_t)b * 8u].y); }
 
   // --- warp-cooperative queries ---
-  __device__ FaceQ face_query(uint32_t ha, uint32_t hb, float4 rq, f3 t) const {
+  __device__ __noinline__ FaceQ face_query(uint32_t ha, uint32_t hb, float4 rq, f3 t) const {
     FaceQ best{-1e30f, 0u};
     uint32_t fo = hfo(ha), nf = hnf(ha), nv = hnv(hb);
     for (uint32_t f = lane; f < nf; f += 32u) {
@@ -237,7 +237,7 @@ struct Narrow {
     for (uint32_t v = 0; v < hnv(h); v++) m = fmx(m, dot(n, hv(h, v)));
     return m;
   }
-  __device__ EdgeQ edge_query(uint32_t ha, uint32_t hb, float4 rq, f3 t) const {
+  __device__ __noinline__ EdgeQ edge_query(uint32_t ha, uint32_t hb, float4 rq, f3 t) const {
     EdgeQ best{-1e30f, sp3(0), sp3(0), sp3(0), sp3(0), sp3(0), 0u};
     uint32_t foa = hfo(ha), fob = hfo(hb);
     f3 cena = v3(S.sf[S.SF_HAABB + ha * 2u]);
@@ -419,7 +419,7 @@ struct Narrow {
     return 0.5f * (a + b);
   }
   // emit (wgsl.js:269-307)
-  __device__ void emit(uint32_t sa, uint32_t sb, f3 p, f3 n, float phi, uint32_t key) const {
+  __device__ __noinline__ void emit(uint32_t sa, uint32_t sb, f3 p, f3 n, float phi, uint32_t key) const {
     float4 A0 = shp(sa, 0), B0 = shp(sb, 0);
     int ba = f2i(A0.x), bb = f2i(B0.x);
     float4 ma = shp(sa, 4), mb = shp(sb, 4);
@@ -460,7 +460,7 @@ struct Narrow {
     out[0] = mf4(p1 + n * (r1 + 0.5f * d), d);
     out[1] = mf4(n, 0.0f);
   }
-  __device__ void prim_prim(uint32_t sa, uint32_t sb, f3 pa, float4 qa, f3 pb, float4 qb, float thresh) const {
+  __device__ __noinline__ void prim_prim(uint32_t sa, uint32_t sb, f3 pa, float4 qa, f3 pb, float4 qb, float thresh) const {
     float4 A = shp(sa, 6), Bq = shp(sb, 6);
     f3 ua = qrot(qa, mf3(0.0f, 0.0f, A.z)), ub = qrot(qb, mf3(0.0f, 0.0f, Bq.z));
     uint32_t base = mix32(sa * 7919u + sb * 104729u);
@@ -492,7 +492,7 @@ struct Narrow {
     for (uint32_t i = 0; i < nc; i++)
       if (c[i][0].w <= thresh) emit(sa, sb, v3(c[i][0]), v3(c[0][1]), c[i][0].w, mix32(base ^ (i * 977u + 13u)));
   }
-  __device__ void plane_contacts(uint32_t pl, uint32_t os, f3 pp, float4 pq, f3 op, float4 oq, float thresh) const {
+  __device__ __noinline__ void plane_contacts(uint32_t pl, uint32_t os, f3 pp, float4 pq, f3 op, float4 oq, float thresh) const {
     f3 n = qrot(pq, mf3(0.0f, 0.0f, 1.0f));
     uint32_t sa = pl, sb = os;
     uint32_t base = mix32(sa * 7919u + sb * 104729u);
@@ -576,7 +576,7 @@ struct Narrow {
     for (uint32_t i = 0; i < nc; i++)
       if (d[i] <= thresh) emit(sa, sb, x[i], n, d[i], mix32(base ^ (i + 7u)));
   }
-  __device__ void seg_on_face(uint32_t hs, uint32_t ps, uint32_t h, uint32_t f, f3 e0, f3 e1, float r, f3 wp,
+  __device__ __noinline__ void seg_on_face(uint32_t hs, uint32_t ps, uint32_t h, uint32_t f, f3 e0, f3 e1, float r, f3 wp,
                               float4 wq, float thresh, bool flip) const {
     float4 pl = fplane(hfo(h) + f);
     float t0 = 0.0f, t1 = 1.0f;
@@ -837,7 +837,7 @@ struct Narrow {
   static __device__ bool is_discrete(uint32_t t) { return t == GT_BOX || t == GT_CONVEX || t == GT_PLANE; }
 
   // build_manifold + gen_run (wgsl.js:875-977)
-  __device__ void gen_run(uint32_t sa, uint32_t sb, const Geo& ga, const Geo& gb, f3 pa, float4 qa, float4 rq, f3 rt,
+  __device__ __noinline__ void gen_run(uint32_t sa, uint32_t sb, const Geo& ga, const Geo& gb, f3 pa, float4 qa, float4 rq, f3 rt,
                           f3 wa, f3 wb, f3 n, float thresh) const {
     f3 mp[5];
     float md[5];
@@ -966,7 +966,7 @@ struct Narrow {
     if ((refA && !(oa < ob - 1e-6f)) || (!refA && ob < oa - 1e-6f)) { out[0] = wb0; out[1] = wb1; return; }
     out[0] = wa0; out[1] = wa1;
   }
-  __device__ void sat_generic(uint32_t sa, uint32_t sb, uint32_t ha, uint32_t hb, f3 pa, float4 qa, float4 rBA, f3 tBA,
+  __device__ __noinline__ void sat_generic(uint32_t sa, uint32_t sb, uint32_t ha, uint32_t hb, f3 pa, float4 qa, float4 rBA, f3 tBA,
                               float thresh, FaceQ fa, FaceQ fb, const EdgeQ& eq) const {
     Geo ga = geo(sa), gb = geo(sb);
     if (eq.sep > fmx(fa.sep, fb.sep) + SAT_TIE) {
@@ -981,7 +981,7 @@ struct Narrow {
     sup_witness(ga, gb, rBA, tBA, n, refA, w);
     gen_run(sa, sb, ga, gb, pa, qa, rBA, tBA, w[0], w[1], n, thresh);
   }
-  __device__ void plane_convex(uint32_t sa, uint32_t sb, f3 pa, float4 qa, f3 pb, float4 qb, float thresh) const {
+  __device__ __noinline__ void plane_convex(uint32_t sa, uint32_t sb, f3 pa, float4 qa, f3 pb, float4 qb, float thresh) const {
     Geo gb = geo(sb);
     f3 nw = qrot(qa, mf3(0.0f, 0.0f, 1.0f));
     float L = 10.0f * (len(v3(S.sf[S.SF_HAABB + gb.h * 2u])) + len(v3(S.sf[S.SF_HAABB + gb.h * 2u + 1u])));
@@ -994,14 +994,14 @@ struct Narrow {
     if (sep > thresh) return;
     gen_run(sa, sb, Geo{GT_BOX, mf3(L, L, L), 0u}, gb, c, qa, rq, rt, wb - n * sep, wb, n, thresh);
   }
-  __device__ void capsule_generic(uint32_t c, uint32_t h, f3 pc, float4 qc, f3 wp, float4 wq, f3 wc, f3 wh, f3 nh,
+  __device__ __noinline__ void capsule_generic(uint32_t c, uint32_t h, f3 pc, float4 qc, f3 wp, float4 wq, f3 wc, f3 wh, f3 nh,
                                   float thresh) const {
     if (dot(wh - wc, nh) - shp(c, 6).y > thresh) return;
     float4 rq = qmul(qconj(qc), wq);
     f3 rt = qinv(qc, wp - pc);
     gen_run(c, h, geo(c), geo(h), pc, qc, rq, rt, qrot(rq, wc) + rt, qrot(rq, wh) + rt, qrot(rq, nh), thresh);
   }
-  __device__ void mpr_generic(uint32_t sa, uint32_t sb, uint32_t ha, uint32_t hb, f3 pa, float4 qa, float4 rBA, f3 tBA,
+  __device__ __noinline__ void mpr_generic(uint32_t sa, uint32_t sb, uint32_t ha, uint32_t hb, f3 pa, float4 qa, float4 rBA, f3 tBA,
                               float thresh, f3 n) const {
     float alA = -2.0f;
     for (uint32_t f = 0; f < hnf(ha); f++) alA = fmx(alA, dot(v3(fplane(hfo(ha) + f)), n));

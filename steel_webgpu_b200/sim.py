@@ -23,8 +23,9 @@ def auto_caps(scene: LoadedScene) -> dict:
     Results depend on capacities only when one overflows; the hash tables (WH, AH) only need room.
     """
     ns = sum(1 for s in scene.json["shapes"] if s.get("hull") or s.get("plane"))
-    maxp = int(min(max(256, 12 * ns), 1 << 22))
-    maxc = int(min(max(512, 6 * maxp), 1 << 24))
+    # Piles of the uneven batch peak near 4 pairs and 2.5 contacts per shape; these leave 2-5x room.
+    maxp = int(min(max(256, 8 * ns), 1 << 22))
+    maxc = int(min(max(512, 12 * ns), 1 << 24))
 
     def p2(x):
         return 1 << max(int(x) - 1, 1).bit_length()
