@@ -333,7 +333,7 @@ def run_steel(args):
                    "contact_steps_per_s": world * counts["contacts"] * substeps * args.steps / (ms / 1000.0),
                    "build_s": round(build_s, 1), "overflow_scenes": overflow_scenes},
         "e2e": {"value": e2e, "unit": "body-steps/s", "h2d_bytes_per_step": 4 * nd, "d2h_bytes_per_step": 4 * npose},
-        "gpu_launches": args.steps * (substeps * 7 + 1),
+        "gpu_launches": args.steps * (substeps * 8 + 1),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
                      "algorithmic_bytes_per_launch": bytes_dom, "ms_per_launch": prof[dom],

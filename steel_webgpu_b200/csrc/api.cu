@@ -113,7 +113,7 @@ struct steel_batch {
   bool use_graph = true;
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  size_t o_scenes, o_shape_scene, o_shape_local, o_tiles, o_pairs, o_pair_count, o_phase, o_ssc, o_err;
+  size_t o_scenes, o_shape_scene, o_shape_local, o_tiles, o_pairs, o_pair_count, o_jobs, o_phase, o_ssc, o_err;
   std::vector<uint32_t> shape_scene, shape_local;
   std::vector<uint4> tiles;
   // host-I/O staging (steel_step_io): packed targets/poses on the device and their offsets
@@ -287,6 +287,7 @@ int check_device_error(steel_batch* b) {
   CU(cudaMemcpyAsync(&e, b->bd.error, 4, cudaMemcpyDeviceToHost, b->ctx->stream));
   CU(cudaStreamSynchronize(b->ctx->stream));
   if (e == ERR_SORT_CAPACITY) return fail(STEEL_E_CAPACITY, "contact sort capacity exceeded");
+  if (e == ERR_JOB_CAPACITY) return fail(STEEL_E_CAPACITY, "narrowphase job capacity exceeded");
   if (e != 0) return fail(STEEL_E_CUDA, "device error " + std::to_string(e));
   return STEEL_OK;
 }
@@ -357,7 +358,8 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   b->o_shape_local = L.take(4 * b->shape_local.size() + 4);
   b->o_tiles = L.take(16 * b->tiles.size() + 16);
   b->o_pairs = L.take(16ull * pair_cap);
-  b->o_pair_count = L.take(4);
+  b->o_pair_count = L.take(8);
+  b->o_jobs = L.take(4ull * NJOB_WORDS * pair_cap + 16);
   b->o_phase = L.take(8ull * n);
   b->o_ssc = L.take(8);
   b->o_err = L.take(4);
@@ -421,6 +423,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   bd.pairs = at<uint4>(A, b->o_pairs);
   bd.pair_cap = pair_cap;
   bd.pair_count = at<uint32_t>(A, b->o_pair_count);
+  bd.jobs = at<uint4>(A, b->o_jobs);
   bd.phase = at<double>(A, b->o_phase);
   bd.substep_count = at<unsigned long long>(A, b->o_ssc);
   bd.error = at<uint32_t>(A, b->o_err);

@@ -15,7 +15,8 @@ struct BatchDev {
   uint32_t ntiles;
   uint4* pairs;               // candidate pairs over all scenes: (scene, shape i, shape j, 0)
   uint32_t pair_cap;
-  uint32_t* pair_count;       // [1]
+  uint32_t* pair_count;       // [2]: candidate pairs, narrowphase jobs
+  uint4* jobs;                // narrowphase jobs [pair_cap][NJOB_WORDS / 4]
   double* phase;              // per-scene clock (sim.js:674-678)
   unsigned long long* substep_count;  // [1]
   uint32_t* error;            // [1] first device-side error code (0 = none)
@@ -25,12 +26,14 @@ struct BatchDev {
 
 constexpr uint32_t BROAD_TILE = 32;
 constexpr int NARROW_WARPS = 8;          // warps per narrowphase block
+constexpr int NARROW_JOB_THREADS = 128;  // threads per block of the narrowphase job kernel
+constexpr uint32_t NJOB_WORDS = 44;     // words per narrowphase job record
 constexpr int SORT_THREADS = 512;
 constexpr int PREP_THREADS = 128;
 constexpr int SOLVE_THREADS = 128;
 
 // Device error codes written to BatchDev::error.
-enum : uint32_t { ERR_NONE = 0, ERR_SORT_CAPACITY = 1 };
+enum : uint32_t { ERR_NONE = 0, ERR_SORT_CAPACITY = 1, ERR_JOB_CAPACITY = 2 };
 
 // Shared-memory staging of a scene inside k_prepare / k_solve. A scene is staged when its part
 // fits the cap; the launch's dynamic shared memory is the largest staged scene's need.

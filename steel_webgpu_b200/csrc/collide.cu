@@ -37,7 +37,7 @@ __global__ void k_params(BatchDev B, uint32_t substep) {
   P.reg = S.reg;
   P.pad[0] = P.pad[1] = P.pad[2] = 0u;
   *S.params = P;
-  if (s == 0u && threadIdx.x == 0u) *B.pair_count = 0u;
+  if (s == 0u && threadIdx.x == 0u) { B.pair_count[0] = 0u; B.pair_count[1] = 0u; }
 }
 // Frame end (sim.js:674-678): advance the clocks.
 __global__ void k_frame_end(BatchDev B) {
@@ -190,10 +190,108 @@ SD f3 shfl3(f3 v, uint32_t src) {
   return mf3(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src), __shfl_sync(0xffffffffu, v.z, src));
 }
 
+// Serial narrowphase work that k_narrow hands to k_narrow_jobs: the routine and its argument
+// values, stored bit for bit in a record of NJOB_WORDS words (word 0 the routine, word 1 the
+// scene). The routines run one per thread there instead of on lane 0 of a warp.
+enum : uint32_t { J_PLANE_CONVEX = 1u, J_PLANE = 2u, J_PRIM = 3u, J_CAPSULE = 4u, J_SEGFACE = 5u, J_SAT = 6u, J_MPR = 7u };
+struct JobW {
+  uint32_t w[NJOB_WORDS];
+  uint32_t n = 2u;
+  __device__ void u(uint32_t x) { w[n++] = x; }
+  __device__ void f(float x) { w[n++] = __float_as_uint(x); }
+  __device__ void v(f3 x) { f(x.x); f(x.y); f(x.z); }
+  __device__ void q(float4 x) { f(x.x); f(x.y); f(x.z); f(x.w); }
+  __device__ void fq(FaceQ x) { f(x.sep); u(x.face); }
+  __device__ void eq(const EdgeQ& x) { f(x.sep); v(x.axis); v(x.a0); v(x.a1); v(x.b0); v(x.b1); u(x.id); }
+};
+struct JobR {
+  uint32_t w[NJOB_WORDS];
+  uint32_t n = 2u;
+  __device__ explicit JobR(const uint4* p) {
+#pragma unroll
+    for (uint32_t k = 0; k < NJOB_WORDS / 4u; k++) {
+      uint4 x = p[k];
+      w[4u * k] = x.x; w[4u * k + 1u] = x.y; w[4u * k + 2u] = x.z; w[4u * k + 3u] = x.w;
+    }
+  }
+  __device__ uint32_t u() { return w[n++]; }
+  __device__ float f() { return __uint_as_float(w[n++]); }
+  __device__ f3 v() { float x = f(), y = f(), z = f(); return mf3(x, y, z); }
+  __device__ float4 q() { float x = f(), y = f(), z = f(), ww = f(); return make_float4(x, y, z, ww); }
+  __device__ FaceQ fq() { float sp = f(); uint32_t fc = u(); return FaceQ{sp, fc}; }
+  __device__ EdgeQ eq() {
+    EdgeQ e;
+    e.sep = f(); e.axis = v(); e.a0 = v(); e.a1 = v(); e.b0 = v(); e.b1 = v(); e.id = u();
+    return e;
+  }
+};
+
 struct Narrow {
   const SceneDev& S;
   uint32_t lane;
-  __device__ Narrow(const SceneDev& s) : S(s), lane(threadIdx.x & 31u) {}
+  const BatchDev* B;  // job list of the batch
+  uint32_t scene;
+  __device__ Narrow(const SceneDev& s, const BatchDev* b, uint32_t sc) : S(s), lane(threadIdx.x & 31u), B(b), scene(sc) {}
+
+  // Appends a job (lane 0 of k_narrow). Each pair adds at most one, so the list holds pair_cap.
+  __device__ void defer(uint32_t kind, JobW& j) const {
+    uint32_t slot = atomicAdd(B->pair_count + 1, 1u);
+    if (slot >= B->pair_cap) { atomicCAS(B->error, 0u, (uint32_t)ERR_JOB_CAPACITY); return; }
+    j.w[0] = kind;
+    j.w[1] = scene;
+    uint4* dst = B->jobs + (size_t)slot * (NJOB_WORDS / 4u);
+    for (uint32_t k = 0; 4u * k < j.n; k++) dst[k] = make_uint4(j.w[4u * k], j.w[4u * k + 1u], j.w[4u * k + 2u], j.w[4u * k + 3u]);
+  }
+  __device__ void defer_capsule(uint32_t c, uint32_t h, f3 pc, float4 qc, f3 wp, float4 wq, f3 wc, f3 wh, f3 nh,
+                                float thresh) const {
+    JobW j;
+    j.u(c); j.u(h); j.v(pc); j.q(qc); j.v(wp); j.q(wq); j.v(wc); j.v(wh); j.v(nh); j.f(thresh);
+    defer(J_CAPSULE, j);
+  }
+  __device__ void defer_segface(uint32_t hs, uint32_t ps, uint32_t h, uint32_t f, f3 e0, f3 e1, float r, f3 wp,
+                                float4 wq, float thresh, bool flip) const {
+    JobW j;
+    j.u(hs); j.u(ps); j.u(h); j.u(f); j.v(e0); j.v(e1); j.f(r); j.v(wp); j.q(wq); j.f(thresh); j.u(flip ? 1u : 0u);
+    defer(J_SEGFACE, j);
+  }
+  __device__ void defer_sat(uint32_t sa, uint32_t sb, uint32_t ha, uint32_t hb, f3 pa, float4 qa, float4 rBA, f3 tBA,
+                            float thresh, FaceQ fa, FaceQ fb, const EdgeQ& eq) const {
+    JobW j;
+    j.u(sa); j.u(sb); j.u(ha); j.u(hb); j.v(pa); j.q(qa); j.q(rBA); j.v(tBA); j.f(thresh); j.fq(fa); j.fq(fb); j.eq(eq);
+    defer(J_SAT, j);
+  }
+  // Runs one job (k_narrow_jobs, one per thread).
+  __device__ void run_job(JobR& r) const {
+    const uint32_t kind = r.w[0];
+    if (kind == J_PLANE_CONVEX || kind == J_PLANE || kind == J_PRIM) {
+      uint32_t sa = r.u(), sb = r.u();
+      f3 pa = r.v(); float4 qa = r.q(); f3 pb = r.v(); float4 qb = r.q(); float thresh = r.f();
+      if (kind == J_PLANE_CONVEX) plane_convex(sa, sb, pa, qa, pb, qb, thresh);
+      else if (kind == J_PLANE) plane_contacts(sa, sb, pa, qa, pb, qb, thresh);
+      else prim_prim(sa, sb, pa, qa, pb, qb, thresh);
+    } else if (kind == J_CAPSULE) {
+      uint32_t c = r.u(), h = r.u();
+      f3 pc = r.v(); float4 qc = r.q(); f3 wp = r.v(); float4 wq = r.q(); f3 wc = r.v(); f3 wh = r.v(); f3 nh = r.v();
+      float thresh = r.f();
+      capsule_generic(c, h, pc, qc, wp, wq, wc, wh, nh, thresh);
+    } else if (kind == J_SEGFACE) {
+      uint32_t hs = r.u(), ps = r.u(), h = r.u(), f = r.u();
+      f3 e0 = r.v(); f3 e1 = r.v(); float rad = r.f(); f3 wp = r.v(); float4 wq = r.q(); float thresh = r.f();
+      bool flip = r.u() != 0u;
+      seg_on_face(hs, ps, h, f, e0, e1, rad, wp, wq, thresh, flip);
+    } else if (kind == J_SAT || kind == J_MPR) {
+      uint32_t sa = r.u(), sb = r.u(), ha = r.u(), hb = r.u();
+      f3 pa = r.v(); float4 qa = r.q(); float4 rBA = r.q(); f3 tBA = r.v(); float thresh = r.f();
+      if (kind == J_SAT) {
+        FaceQ fa = r.fq(), fb = r.fq();
+        EdgeQ eq = r.eq();
+        sat_generic(sa, sb, ha, hb, pa, qa, rBA, tBA, thresh, fa, fb, eq);
+      } else {
+        f3 n = r.v();
+        mpr_generic(sa, sb, ha, hb, pa, qa, rBA, tBA, thresh, n);
+      }
+    }
+  }
 
   __device__ f3 hv(uint32_t h, uint32_t i) const { return v3(S.sf[S.SF_VERTS + S.su[S.SU_HULL + h * 4u] + i]); }
   __device__ uint32_t hnv(uint32_t h) const { return S.su[S.SU_HULL + h * 4u + 1u]; }
@@ -1013,7 +1111,7 @@ struct Narrow {
     gen_run(sa, sb, ga, gb, pa, qa, rBA, tBA, w[0], w[1], n, thresh);
   }
 
-  // narrow_pair (wgsl.js:1072-1195): all lanes enter; lane 0 runs the serial paths.
+  // narrow_pair (wgsl.js:1072-1195): all lanes enter; the serial paths become jobs of lane 0.
   __device__ void pair(uint32_t p0, uint32_t p1) const {
     bool swp = geo_type(p0) > geo_type(p1);
     uint32_t sa = swp ? p1 : p0, sb = swp ? p0 : p1;
@@ -1030,13 +1128,18 @@ struct Narrow {
     float4 ka = shp(sa, 3), kb = shp(sb, 3);
     if (ka.x == 4.0f || kb.x == 4.0f) {
       if (lane == 0u) {
-        if (geo_type(sb) == GT_CONVEX) plane_convex(sa, sb, pa, qa, pb, qb, thresh);
-        else plane_contacts(sa, sb, pa, qa, pb, qb, thresh);
+        JobW j;
+        j.u(sa); j.u(sb); j.v(pa); j.q(qa); j.v(pb); j.q(qb); j.f(thresh);
+        defer(geo_type(sb) == GT_CONVEX ? J_PLANE_CONVEX : J_PLANE, j);
       }
       return;
     }
     if (ka.x != 0.0f && kb.x != 0.0f) {
-      if (lane == 0u) prim_prim(sa, sb, pa, qa, pb, qb, thresh);
+      if (lane == 0u) {
+        JobW j;
+        j.u(sa); j.u(sb); j.v(pa); j.q(qa); j.v(pb); j.q(qb); j.f(thresh);
+        defer(J_PRIM, j);
+      }
       return;
     }
     if (ka.x != 0.0f || kb.x != 0.0f) {
@@ -1059,7 +1162,7 @@ struct Narrow {
           float d = sqrtf(q.d2);
           if (d >= 1e-9f) {
             f3 nh = (q.ph - q.ps) / d;
-            capsule_generic(ps, hs, flip ? pa : pb, flip ? qa : qb, wp, wq, q.ps + nh * 1e-4f, q.ph, nh, thresh);
+            defer_capsule(ps, hs, flip ? pa : pb, flip ? qa : qb, wp, wq, q.ps + nh * 1e-4f, q.ph, nh, thresh);
           }
         } else {
           float d = sqrtf(q.d2);
@@ -1067,7 +1170,7 @@ struct Narrow {
           f3 n = (q.ps - q.ph) / fmx(d, 1e-9f);
           if (phi > thresh || d < 1e-9f) {
           } else if (dot(n, v3(fplane(hfo(h) + fq.face))) > 0.999f) {
-            seg_on_face(hs, ps, h, fq.face, e0, e1, pr.y, wp, wq, thresh, flip);
+            defer_segface(hs, ps, h, fq.face, e0, e1, pr.y, wp, wq, thresh, flip);
           } else {
             uint32_t sa2 = flip ? ps : hs, sb2 = flip ? hs : ps;
             f3 nw = qrot(wq, n);
@@ -1081,10 +1184,10 @@ struct Narrow {
       if (pr.x == 2.0f) {
         float4 pl = fplane(hfo(h) + fq.face);
         f3 x = dot(v3(pl), e0) <= dot(v3(pl), e1) ? e0 : e1;
-        capsule_generic(ps, hs, flip ? pa : pb, flip ? qa : qb, wp, wq, x - v3(pl) * 1e-4f,
-                        x - v3(pl) * (dot(v3(pl), x) - pl.w), -v3(pl), thresh);
+        defer_capsule(ps, hs, flip ? pa : pb, flip ? qa : qb, wp, wq, x - v3(pl) * 1e-4f,
+                      x - v3(pl) * (dot(v3(pl), x) - pl.w), -v3(pl), thresh);
       } else {
-        seg_on_face(hs, ps, h, fq.face, e0, e1, pr.y, wp, wq, thresh, flip);
+        defer_segface(hs, ps, h, fq.face, e0, e1, pr.y, wp, wq, thresh, flip);
       }
       return;
     }
@@ -1099,14 +1202,19 @@ struct Narrow {
       if (lane == 0u && m.w >= 0.0f) {
         f3 n = -v3(m);
         float sep = (dot(n, tBA) + support_min(hb, qinv(rBA, n))) - support_max(ha, n);
-        if (fmx(fa.sep, fb.sep) > sep + 1e-4f) sat_generic(sa, sb, ha, hb, pa, qa, rBA, tBA, thresh, fa, fb, none);
-        else mpr_generic(sa, sb, ha, hb, pa, qa, rBA, tBA, thresh, n);
+        if (fmx(fa.sep, fb.sep) > sep + 1e-4f) {
+          defer_sat(sa, sb, ha, hb, pa, qa, rBA, tBA, thresh, fa, fb, none);
+        } else {
+          JobW j;
+          j.u(sa); j.u(sb); j.u(ha); j.u(hb); j.v(pa); j.q(qa); j.q(rBA); j.v(tBA); j.f(thresh); j.v(n);
+          defer(J_MPR, j);
+        }
       }
       return;
     }
     EdgeQ eq = edge_query(ha, hb, rBA, tBA);
     if (eq.sep > thresh) return;
-    if (lane == 0u) sat_generic(sa, sb, ha, hb, pa, qa, rBA, tBA, thresh, fa, fb, eq);
+    if (lane == 0u) defer_sat(sa, sb, ha, hb, pa, qa, rBA, tBA, thresh, fa, fb, eq);
   }
 };
 
@@ -1116,9 +1224,20 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, 2) k_narrow(BatchDev B) {
   uint32_t total = *B.pair_count;
   for (uint32_t g = warp; g < total; g += nwarps) {
     uint4 pr = B.pairs[g];
-    Narrow N(B.scenes[pr.x]);
+    Narrow N(B.scenes[pr.x], &B, pr.x);
     N.pair(pr.y, pr.z);
     __syncwarp();
+  }
+}
+
+// The jobs k_narrow deferred, one per thread (grid-stride).
+__global__ void __launch_bounds__(NARROW_JOB_THREADS, 4) k_narrow_jobs(BatchDev B) {
+  const uint32_t total = min(B.pair_count[1], B.pair_cap);
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
+    JobR r(B.jobs + (size_t)j * (NJOB_WORDS / 4u));
+    const uint32_t scene = r.w[1];
+    Narrow N(B.scenes[scene], &B, scene);
+    N.run_job(r);
   }
 }
 
@@ -1200,6 +1319,7 @@ int narrow_blocks_per_sm() {
 }
 void launch_narrow(const BatchDev& b, uint32_t narrow_blocks, cudaStream_t st) {
   k_narrow<<<narrow_blocks, NARROW_WARPS * 32, 0, st>>>(b);
+  k_narrow_jobs<<<narrow_blocks * 2u, NARROW_JOB_THREADS, 0, st>>>(b);
 }
 cudaError_t configure_sort(size_t smem_keys) {
   return cudaFuncSetAttribute(k_csort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smem_keys * sizeof(uint4)));
