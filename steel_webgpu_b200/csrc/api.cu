@@ -385,8 +385,8 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   for (uint32_t i = 0; i < n; i++) {
     SceneHost& s = b->sc[i];
     SceneDev& d = s.d;
-    d.sf = at<float4>(A, s.o_sf);
-    d.su = at<uint32_t>(A, s.o_su);
+    d.sf = RO<float4>{at<float4>(A, s.o_sf)};
+    d.su = RO<uint32_t>{at<uint32_t>(A, s.o_su)};
     d.pos = at<float4>(A, s.o_pos); d.rot = at<float4>(A, s.o_rot);
     d.ppos = at<float4>(A, s.o_ppos); d.prot = at<float4>(A, s.o_prot);
     d.lv = at<float4>(A, s.o_lv); d.av = at<float4>(A, s.o_av);
@@ -409,8 +409,8 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
     prep_smem = std::max<size_t>(prep_smem, prep_smem_layout(d.stage, d.NL, d.NB, d.NCOLW, d.NCOL).total);
     solve_smem = std::max<size_t>(solve_smem, solve_smem_layout(d.stage, d.NB, d.ND, d.NCOL, d.NL).total);
     dev[i] = d;
-    CU(cudaMemcpyAsync((void*)d.sf, s.statF.data(), s.statF.size() * 4, cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync((void*)d.su, s.statU.data(), s.statU.size() * 4, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync((void*)d.sf.p, s.statF.data(), s.statF.size() * 4, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync((void*)d.su.p, s.statU.data(), s.statU.size() * 4, cudaMemcpyHostToDevice, st));
   }
   BatchDev& bd = b->bd;
   bd.scenes = at<SceneDev>(A, b->o_scenes);

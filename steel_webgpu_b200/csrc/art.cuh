@@ -52,12 +52,12 @@ struct Art {
   __device__ f3 dof_axis(uint32_t d) const { return v3(S.sf[S.SF_DOF + d * 5u + 3u]); }
   __device__ bool scalar_dof(uint32_t d) const { return S.sf[S.SF_DOF + d * 5u + 2u].w > 0.5f; }
   __device__ uint4 info(uint32_t a) const {
-    const uint32_t* p = S.su + S.SU_ART + a * 4u;
+    RO<uint32_t> p = S.su + S.SU_ART + a * 4u;
     return make_uint4(p[0], p[1], p[2], p[3]);
   }
   __device__ float bmass(int b) const { return S.sf[S.SF_BODY + (uint32_t)b * 8u + 1u].w; }
   __device__ m3 binertia(int b) const {
-    const float4* o = S.sf + S.SF_BODY + (uint32_t)b * 8u;
+    RO<float4> o = S.sf + S.SF_BODY + (uint32_t)b * 8u;
     return tr(mcols(v3(o[2]), v3(o[3]), v3(o[4])));
   }
   __device__ uint32_t lo(uint32_t l) const { return l * LBLK; }
@@ -182,6 +182,34 @@ struct Art {
     }
   }
 
+  // Diagonal terms and generalized force of dof d (the r-th of its link, joint coordinates from
+  // qs): joint damping, spring, and the implicit PD drive folded into D (artwgsl.js:290-318).
+  // Drr holds D[r][r] = S_r . U_r on entry and gains the drive and damping terms.
+  __device__ float dof_tau(uint32_t d, uint32_t qs, uint32_t r, float& Drr, const Params& P) const {
+    float4 dr = dof_drive(d);
+    Drr += dr.x;
+    float damp = dof_passive(d).x;
+    Drr += P.dt * damp;
+    float tau = (-damp) * A[S.A_QD + d] + A[S.A_JF + d];
+    float4 spr = S.sf[S.SF_DOF + d * 5u + 4u];
+    if (spr.x != 0.0f) tau += spr.x * (spr.y - A[S.A_Q + qs + r]);
+    if (dr.y > 0.0f || dr.z > 0.0f) {
+      float q = A[S.A_Q + qs + r], qd = A[S.A_QD + d];
+      float err = A[S.A_TGT + d] - q;
+      float tv = A[S.A_TGTV + d];
+      float mm = fmx(Drr, 1e-9f);
+      float qdn = (mm * qd + P.dt * (dr.y * err + dr.z * tv)) / ((mm + P.dt * dr.z) + (P.dt * P.dt) * dr.y);
+      float ti = dr.y * (err - P.dt * qdn) + dr.z * (tv - qdn);
+      if (fabsf(ti) <= dr.w || dr.w <= 0.0f) {
+        Drr += (P.dt * P.dt) * dr.y + P.dt * dr.z;
+        tau += (dr.y * err - (P.dt * dr.y) * qd) + dr.z * (tv - qd);
+      } else {
+        tau += clmp(ti, -dr.w, dr.w);
+      }
+    }
+    return tau;
+  }
+
   // Articulated inertias, U = I^A S, D^-1 with implicit drives, free velocity (artwgsl.js:210-369).
   __device__ void factor(uint32_t a, const Params& P) const {
     uint4 ai = info(a);
@@ -234,40 +262,33 @@ struct Art {
       uint32_t l = ai.x + ai.y - 1u - kk, L = lo(l);
       uint32_t n = lndof(l), d0 = ldof(l), qs = lqs(l);
       SVec pA = ldsv(L + L_PA);
-      float D[36];
-      for (uint32_t i = 0; i < 36u; i++) D[i] = 0.0f;
       float u[6] = {0, 0, 0, 0, 0, 0};
-      for (uint32_t c = 0; c < n; c++) stsv(L + L_U + c * 6u, imul(L + L_IA, ldS(l, c)));
-      for (uint32_t r = 0; r < n; r++) {
-        uint32_t d = d0 + r;
-        for (uint32_t c = 0; c < n; c++) D[r * JM + c] = sdot(ldS(l, r), ldU(l, c));
-        float4 dr = dof_drive(d);
-        D[r * JM + r] += dr.x;
-        float damp = dof_passive(d).x;
-        D[r * JM + r] += P.dt * damp;
-        float tau = (-damp) * A[S.A_QD + d] + A[S.A_JF + d];
-        float4 spr = S.sf[S.SF_DOF + d * 5u + 4u];
-        if (spr.x != 0.0f) tau += spr.x * (spr.y - A[S.A_Q + qs + r]);
-        if (dr.y > 0.0f || dr.z > 0.0f) {
-          float q = A[S.A_Q + qs + r], qd = A[S.A_QD + d];
-          float err = A[S.A_TGT + d] - q;
-          float tv = A[S.A_TGTV + d];
-          float mm = fmx(D[r * JM + r], 1e-9f);
-          float qdn = (mm * qd + P.dt * (dr.y * err + dr.z * tv)) / ((mm + P.dt * dr.z) + (P.dt * P.dt) * dr.y);
-          float ti = dr.y * (err - P.dt * qdn) + dr.z * (tv - qdn);
-          if (fabsf(ti) <= dr.w || dr.w <= 0.0f) {
-            D[r * JM + r] += (P.dt * P.dt) * dr.y + P.dt * dr.z;
-            tau += (dr.y * err - (P.dt * dr.y) * qd) + dr.z * (tv - qd);
-          } else {
-            tau += clmp(ti, -dr.w, dr.w);
-          }
+#pragma unroll
+      for (uint32_t c = 0; c < 6u; c++)
+        if (c < n) stsv(L + L_U + c * 6u, imul(L + L_IA, ldS(l, c)));
+      if (n == 1u) {
+        // One dof: D is 1 x 1 and its Gauss-Jordan inverse is 1 * (1 / max(D, 1e-12)).
+        float d00 = sdot(ldS(l, 0u), ldU(l, 0u));
+        float tau = dof_tau(d0, qs, 0u, d00, P);
+        u[0] = tau - sdot(ldS(l, 0u), pA);
+        float di = 1.0f * (1.0f / fmx(d00, 1e-12f));
+        for (uint32_t i = 0; i < JM * JM; i++) LB[L + L_DI + i] = i == 0u ? di : 0.0f;
+      } else {
+        float D[36];
+        for (uint32_t i = 0; i < 36u; i++) D[i] = 0.0f;
+        for (uint32_t r = 0; r < n; r++) {
+          for (uint32_t c = 0; c < n; c++) D[r * JM + c] = sdot(ldS(l, r), ldU(l, c));
+          float tau = dof_tau(d0 + r, qs, r, D[r * JM + r], P);
+          float ur = tau - sdot(ldS(l, r), pA);
+#pragma unroll
+          for (uint32_t c = 0; c < 6u; c++) if (c == r) u[c] = ur;
         }
-        u[r] = tau - sdot(ldS(l, r), pA);
+        float Di[36];
+        inv_spd(D, n, JM, Di);
+        for (uint32_t i = 0; i < JM * JM; i++) LB[L + L_DI + i] = Di[i];
       }
-      float Di[36];
-      inv_spd(D, n, JM, Di);
-      for (uint32_t i = 0; i < JM * JM; i++) LB[L + L_DI + i] = Di[i];
-      for (uint32_t r = 0; r < JM; r++) LB[L + L_UU + r] = u[r];
+#pragma unroll
+      for (uint32_t r = 0; r < 6u; r++) if (r < JM) LB[L + L_UU + r] = u[r];
       int par = lparent(l);
       if (par < 0) continue;
       m3 Am = ldm(L + L_IA), Bm = ldm(L + L_IA + 9u), Cm = ldm(L + L_IA + 18u);
@@ -275,7 +296,9 @@ struct Art {
       for (uint32_t r = 0; r < n; r++) {
         SVec Ur = ldU(l, r);
         float du = 0.0f;
-        for (uint32_t c = 0; c < n; c++) {
+#pragma unroll
+        for (uint32_t c = 0; c < 6u; c++) {
+          if (c >= n) break;
           SVec Uc = ldU(l, c);
           float w = ldDI(l, r, c);
           Am = msub(Am, mscl(w, outer(Ur.a, Uc.a)));
@@ -477,14 +500,25 @@ struct Art {
       uint32_t k = ai.y - 1u - kk, l = ai.x + k, n = lndof(l);
       float u[6] = {0, 0, 0, 0, 0, 0};
       SVec pk = ldp(p, k);
-      for (uint32_t r = 0; r < n; r++) u[r] = tau[ldof(l) + r - ai.z] - sdot(ldS(l, r), pk);
+#pragma unroll
+      for (uint32_t r = 0; r < 6u; r++) {
+        if (r >= n) break;
+        u[r] = tau[ldof(l) + r - ai.z] - sdot(ldS(l, r), pk);
+      }
+#pragma unroll
       for (uint32_t r = 0; r < 6u; r++) uu[k * 6u + r] = u[r];
       int par = lparent(l);
       if (par >= 0) {
         SVec pp = pk;
-        for (uint32_t r = 0; r < n; r++) {
+#pragma unroll
+        for (uint32_t r = 0; r < 6u; r++) {
+          if (r >= n) break;
           float du = 0.0f;
-          for (uint32_t c = 0; c < n; c++) du += ldDI(l, r, c) * u[c];
+#pragma unroll
+          for (uint32_t c = 0; c < 6u; c++) {
+            if (c >= n) break;
+            du += ldDI(l, r, c) * u[c];
+          }
           pp = sadd(pp, sscl(ldU(l, r), du));
         }
         uint32_t pi = (uint32_t)par - ai.x;
@@ -498,11 +532,19 @@ struct Art {
       if (par >= 0) dv = mshift(ldp(dvs, (uint32_t)par - ai.x), link_r(l));
       uint32_t n = lndof(l);
       float dq[6] = {0, 0, 0, 0, 0, 0};
-      for (uint32_t r = 0; r < n; r++) {
+#pragma unroll
+      for (uint32_t r = 0; r < 6u; r++) {
+        if (r >= n) break;
         dq[r] = 0.0f;
-        for (uint32_t c = 0; c < n; c++) dq[r] += ldDI(l, r, c) * (uu[k * 6u + c] - sdot(ldU(l, c), dv));
+#pragma unroll
+        for (uint32_t c = 0; c < 6u; c++) {
+          if (c >= n) break;
+          dq[r] += ldDI(l, r, c) * (uu[k * 6u + c] - sdot(ldU(l, c), dv));
+        }
       }
-      for (uint32_t r = 0; r < n; r++) {
+#pragma unroll
+      for (uint32_t r = 0; r < 6u; r++) {
+        if (r >= n) break;
         dv = sadd(dv, sscl(ldS(l, r), dq[r]));
         out[ldof(l) + r - ai.z] = dq[r];
       }
@@ -535,13 +577,24 @@ struct Art {
       uint32_t n = lndof(l);
       SVec p = ldsv(L + L_P);
       float u[6] = {0, 0, 0, 0, 0, 0};
-      for (uint32_t r = 0; r < n; r++) { u[r] = LB[L + L_TAU + r] - sdot(ldS(l, r), p); LB[L + L_UU + r] = u[r]; }
+#pragma unroll
+      for (uint32_t r = 0; r < 6u; r++) {
+        if (r >= n) break;
+        u[r] = LB[L + L_TAU + r] - sdot(ldS(l, r), p);
+        LB[L + L_UU + r] = u[r];
+      }
       int par = lparent(l);
       if (par >= 0) {
         SVec pp = p;
-        for (uint32_t r = 0; r < n; r++) {
+#pragma unroll
+        for (uint32_t r = 0; r < 6u; r++) {
+          if (r >= n) break;
           float du = 0.0f;
-          for (uint32_t c = 0; c < n; c++) du += ldDI(l, r, c) * u[c];
+#pragma unroll
+          for (uint32_t c = 0; c < 6u; c++) {
+            if (c >= n) break;
+            du += ldDI(l, r, c) * u[c];
+          }
           pp = sadd(pp, sscl(ldU(l, r), du));
         }
         uint32_t P0 = lo((uint32_t)par) + L_P;
@@ -555,11 +608,22 @@ struct Art {
       if (par >= 0) dv = mshift(ldsv(lo((uint32_t)par) + L_DV), link_r(l));
       uint32_t n = lndof(l);
       float dq[6] = {0, 0, 0, 0, 0, 0};
-      for (uint32_t r = 0; r < n; r++) {
+#pragma unroll
+      for (uint32_t r = 0; r < 6u; r++) {
+        if (r >= n) break;
         dq[r] = 0.0f;
-        for (uint32_t c = 0; c < n; c++) dq[r] += ldDI(l, r, c) * (LB[L + L_UU + c] - sdot(ldU(l, c), dv));
+#pragma unroll
+        for (uint32_t c = 0; c < 6u; c++) {
+          if (c >= n) break;
+          dq[r] += ldDI(l, r, c) * (LB[L + L_UU + c] - sdot(ldU(l, c), dv));
+        }
       }
-      for (uint32_t r = 0; r < n; r++) { dv = sadd(dv, sscl(ldS(l, r), dq[r])); aqd[ldof(l) + r] += dq[r]; }
+#pragma unroll
+      for (uint32_t r = 0; r < 6u; r++) {
+        if (r >= n) break;
+        dv = sadd(dv, sscl(ldS(l, r), dq[r]));
+        aqd[ldof(l) + r] += dq[r];
+      }
       stsv(L + L_DV, dv);
       SVec v = sadd(ldsv(L + L_V), dv);
       stsv(L + L_V, v);

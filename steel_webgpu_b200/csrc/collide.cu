@@ -53,7 +53,7 @@ __global__ void k_shapes(BatchDev B) {
   if (g >= B.nshapes) return;
   const SceneDev& S = B.scenes[B.shape_scene[g]];
   uint32_t s = B.shape_local[g];
-  const float4* sf = S.sf + S.SF_SHAPE + s * 7u;
+  RO<float4> sf = S.sf + S.SF_SHAPE + s * 7u;
   float4 r0 = sf[0];
   int body = f2i(r0.x);
   uint32_t hull = f2u(r0.y);
@@ -303,7 +303,7 @@ struct Narrow {
   __device__ uint32_t fvert(uint32_t k) const { return S.su[S.SU_FV + k]; }
   __device__ uint32_t hne(uint32_t h) const { return S.su[S.SU_HEDGE + h * 2u + 1u]; }
   __device__ uint4 hedge(uint32_t h, uint32_t k) const {
-    const uint32_t* e = S.su + S.SU_EDGE + (S.su[S.SU_HEDGE + h * 2u] + k) * 4u;
+    RO<uint32_t> e = S.su + S.SU_EDGE + (S.su[S.SU_HEDGE + h * 2u] + k) * 4u;
     return make_uint4(e[0], e[1], e[2], e[3]);
   }
   __device__ float4 shp(uint32_t s, uint32_t k) const { return S.sf[S.SF_SHAPE + s * 7u + k]; }

@@ -165,6 +165,15 @@ SHD float fatan2(float yf, float xf) {
   return (float)v;
 }
 
+// View of an array that no kernel writes while it runs (the scene's static data): element reads
+// go through the read-only data path, so the compiler may issue them ahead of stores.
+template <class T>
+struct RO {
+  const T* p;
+  __device__ __forceinline__ T operator[](size_t i) const { return __ldg(p + i); }
+  __host__ __device__ RO operator+(size_t i) const { return RO{p + i}; }
+};
+
 // Per-substep parameters (the reference's 112-byte Params uniform, wgsl.js:34-45).
 struct Params {
   float dt; uint32_t substep, parity, iterations;
@@ -179,8 +188,8 @@ struct Params {
 // elements of the array they index.
 struct SceneDev {
   // static, reference format
-  const float4* sf;
-  const uint32_t* su;
+  RO<float4> sf;                     // static scene data, read-only in every kernel
+  RO<uint32_t> su;
   uint32_t SF_BODY, SF_SHAPE, SF_HAABB, SF_VERTS, SF_FPLANE, SF_LINK, SF_DOF, SF_PATH, SF_LOOP, SF_MIMIC, SF_CTRL;
   uint32_t SU_HULL, SU_FACE, SU_FV, SU_HEDGE, SU_EDGE, SU_ART, SU_ACON, SU_FILTER;
   // counts

@@ -57,7 +57,7 @@ struct Prep {
     if (k == 1u) {
       float4 q = S.rot[b];
       m3 R = qmat(q);
-      const float4* o = S.sf + S.SF_BODY + (uint32_t)b * 8u;
+      RO<float4> o = S.sf + S.SF_BODY + (uint32_t)b * 8u;
       m3 Ii = tr(mcols(v3(o[5]), v3(o[6]), v3(o[7])));
       out[0] = f * o[0].x;
       out[1] = mul(R, mul(Ii, mul(tr(R), t)));
@@ -500,7 +500,7 @@ struct Prep {
   }
 };
 
-__global__ void __launch_bounds__(PREP_THREADS) k_prepare(BatchDev B) {
+__global__ void __launch_bounds__(PREP_THREADS, 4) k_prepare(BatchDev B) {
   extern __shared__ float4 psm4[];  // prep_smem_layout: link blocks, coloring
   __shared__ uint32_t stmp[40];
   __shared__ Params Ps;
@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(PREP_THREADS) k_prepare(BatchDev B) {
     float frame = clmp(S.TGT_HELD == 1u ? P.phase * 60.0f : ramp, 0.0f, (float)(P.path_frames - 1u));
     uint32_t a = f2u(frame);
     uint32_t b = min(a + 1u, P.path_frames - 1u);
-    const float* path = (const float*)(S.sf + S.SF_PATH);
+    RO<float> path{reinterpret_cast<const float*>(S.sf.p + S.SF_PATH)};
     float pa = path[a * P.driven + d], pb = path[b * P.driven + d];
     float t = frame - (float)a;
     float value = pa * (1.0f - t) + pb * t;

@@ -31,7 +31,7 @@ struct Solver {
   __device__ uint32_t bflags(int b) const { return b < 0 ? 0u : f2u(S.sf[S.SF_BODY + (uint32_t)b * 8u + 7u].w); }
   __device__ float bradius(int b) const { return b < 0 ? 1e30f : S.sf[S.SF_BODY + (uint32_t)b * 8u + 2u].w; }
   __device__ m3 binv_inertia(int b) const {
-    const float4* o = S.sf + S.SF_BODY + (uint32_t)b * 8u;
+    RO<float4> o = S.sf + S.SF_BODY + (uint32_t)b * 8u;
     return tr(mcols(v3(o[5]), v3(o[6]), v3(o[7])));
   }
   __device__ void load_tw(int b, f3 out[2]) const {
@@ -491,7 +491,7 @@ struct Solver {
     if (S.VLIM_FREE == 1u) {
       for (uint32_t b = tid; b < S.NB; b += nt) {
         if (bkind((int)b) != 1u || (bflags((int)b) & 1u) != 0u) continue;
-        const float4* o = S.sf + S.SF_BODY + b * 8u;
+        RO<float4> o = S.sf + S.SF_BODY + b * 8u;
         float limv = o[4].w, lima = o[5].w;
         uint32_t g = S.A_VLG + S.ND + b * 6u;
         if (limv > 0.0f) {
@@ -536,7 +536,7 @@ struct Solver {
   }
 };
 
-__global__ void __launch_bounds__(SOLVE_THREADS) k_solve(BatchDev B) {
+__global__ void __launch_bounds__(SOLVE_THREADS, 4) k_solve(BatchDev B) {
   extern __shared__ float4 ssm4[];  // solve_smem_layout: [tw | imp], qd, color starts, link blocks
   __shared__ Params Ps;
   __shared__ SceneDev Ss;  // the scene's offsets and sizes, read everywhere in the serial passes
@@ -575,7 +575,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(BatchDev B) {
     f3 w = v3(S.av[b]);
     uint32_t bfo = S.A_BF + b * 8u;
     f3 bf = mf3(A[bfo], A[bfo + 1], A[bfo + 2]), bt = mf3(A[bfo + 4], A[bfo + 5], A[bfo + 6]);
-    const float4* o = S.sf + S.SF_BODY + b * 8u;
+    RO<float4> o = S.sf + S.SF_BODY + b * 8u;
     if ((fl & 1u) == 0u && (nonzero(bf) || nonzero(bt))) {
       m3 R = qmat(S.rot[b]);
       v += (bf * o[0].x) * P.dt;
