@@ -138,6 +138,12 @@ def scene_counts(batch, pks):
     return tot
 
 
+# DRAM bytes (read + write) per body and launch, from one ncu capture of the 64-scene uneven batch
+# (cold cache; profiles/narrow_prepare_solve_uneven_batch_64.md). Scaled by a batch's body count
+# for the bench line's roofline traffic; the narrow stage is k_narrow + k_narrow_jobs.
+NCU_TRAFFIC_PER_BODY = {"narrow": 1660.0, "prepare": 1264.0, "solve": 1346.0}
+
+
 def kernel_bytes(k: str, c: dict, rows_vec4: int, iterations: int) -> float:
     """Algorithmic bytes per launch of kernel k over the whole batch (one substep).
 
@@ -335,7 +341,10 @@ def run_steel(args):
         "e2e": {"value": e2e, "unit": "body-steps/s", "h2d_bytes_per_step": 4 * nd, "d2h_bytes_per_step": 4 * npose},
         "gpu_launches": args.steps * (substeps * 8 + 1),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": NCU_TRAFFIC_PER_BODY[dom] * nbodies if dom in NCU_TRAFFIC_PER_BODY else None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of uneven_batch_64, "
+                                       "per body, scaled to this batch",
                      "algorithmic_bytes_per_launch": bytes_dom, "ms_per_launch": prof[dom],
                      "kernel_share": {k: round(v / total_ms, 4) for k, v in prof.items()}},
         "cpu_baseline": {"value": cpu_val, "unit": "body-steps/s", "cores": 1, "kind": "port",

@@ -6,6 +6,7 @@
 #include <sstream>
 
 #include "oracle.h"
+#include "smath_o.h"
 
 namespace orc {
 
@@ -144,6 +145,14 @@ void Oracle::step(uint32_t frames) {
 using orc::Oracle;
 
 extern "C" {
+
+// The oracle's float sin / cos / atan2 (smath_o.h), for accuracy tests.
+void oracle_trig(const float* x, float* s, float* c, size_t n) {
+  for (size_t i = 0; i < n; i++) { s[i] = orc::sin_o(x[i]); c[i] = orc::cos_o(x[i]); }
+}
+void oracle_atan2(const float* y, const float* x, float* out, size_t n) {
+  for (size_t i = 0; i < n; i++) out[i] = orc::atan2_o(y[i], x[i]);
+}
 
 void* oracle_create(const char* constants, const float* statF, size_t nF, const uint32_t* statU, size_t nU,
                     const float* poses, const float* vel, const float* art, size_t nArt, char* err, size_t errlen) {

@@ -8,9 +8,15 @@
 // own buffer layout (statF/statU/poses/vel/counters/pairs/contacts/sched/rows/
 // warm/art/stats, sim.js:503-519) and its compile-time constants C
 // (sim.js:456-477). Each workgroup phase becomes a loop over its invocations in
-// index order; barriers become phase boundaries. Subgroup reductions follow the
-// reference's own no-subgroup fallback (lane-major scans, sequential sums),
-// which defines the same tie-breaks.
+// index order; barriers become phase boundaries. Subgroup min/max reductions are
+// lane-major scans (the lowest lane wins ties, as the reference's no-subgroup
+// fallback does); the subgroup sums of the dense-row solve (SG = 1) are
+// per-lane partial sums in dof order combined by a fixed xor butterfly.
+//
+// Parity unpinned: the reference ships no golden vectors or known-answer tests for
+// this path and cannot run here (WGSL needs a WebGPU adapter and a JS runtime), so
+// this restatement is checked by construction, by physical known answers and by its
+// own committed fixtures (tests/golden), not against the reference's outputs.
 #pragma once
 #include <cstdint>
 #include <map>

@@ -1,7 +1,9 @@
 """Test infrastructure: ctypes harness of the CPU oracle (oracle/_build/liboracle.so).
 
 ORACLE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU baseline as the
-checker. The product never imports it.
+checker. The product never imports it. Parity unpinned: the reference has no golden vectors for this
+path and cannot run here, so the oracle is pinned only by construction, physical known answers and
+its own fixtures (tests/golden).
 """
 from __future__ import annotations
 
@@ -40,6 +42,8 @@ def lib():
         L.oracle_read.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t]
         L.oracle_write.restype = ctypes.c_int
         L.oracle_write.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t]
+        L.oracle_trig.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]
+        L.oracle_atan2.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]
         _lib = L
     return _lib
 
@@ -95,3 +99,20 @@ class OracleSim:
         """(NB, 8): COM position, 0, quaternion."""
         nb = self.pk.NB
         return self.read("poses")[:nb * 8].reshape(nb, 8)
+
+
+def trig(x):
+    """The oracle's float sin and cos of x (float32 array)."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    s, c = np.zeros_like(x), np.zeros_like(x)
+    lib().oracle_trig(x.ctypes.data, s.ctypes.data, c.ctypes.data, x.size)
+    return s, c
+
+
+def atan2(y, x):
+    """The oracle's float atan2(y, x)."""
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.zeros_like(y)
+    lib().oracle_atan2(y.ctypes.data, x.ctypes.data, out.ctypes.data, y.size)
+    return out

@@ -1,0 +1,133 @@
+"""CPU checks of the oracle: known physical answers, its sin/cos/atan2, its committed fixtures, and
+the scene loader and packer on the reference's own scene folders (when they are on disk).
+
+The reference has no golden vectors for this path (parity unpinned), so these tests pin the oracle
+by analytic cases and by fixtures it produced earlier (tests/golden/make_golden.py).
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from steel_webgpu_b200 import SceneBuilder, pack
+from tests import scenes
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "oracle_fixtures.npz")
+REF_SCENES = "/root/reference/assets/scenes"
+UNSUPPORTED = ("FMODE", "ANG", "ANG_ART", "TORS", "COMPL", "NEST", "CTI", "LONGEST_FIRST", "DRIVE_ROWS", "VLIM_ON",
+               "JFL", "SLEEP", "VELITERS")
+
+
+def test_trig_accuracy(oracle_lib):
+    rng = np.random.default_rng(0)
+    x = np.concatenate([rng.uniform(-10, 10, 100000), rng.uniform(-1e4, 1e4, 20000)]).astype(np.float32)
+    s, c = oracle_lib.trig(x)
+    xs = x.astype(np.float64)
+    # Within one float ulp of the correctly rounded value.
+    for got, ref in ((s, np.sin(xs)), (c, np.cos(xs))):
+        ulp = np.abs(got.view(np.int32).astype(np.int64) - ref.astype(np.float32).view(np.int32).astype(np.int64))
+        assert ulp.max() <= 1
+    y = rng.uniform(-5, 5, 100000).astype(np.float32)
+    z = rng.uniform(-5, 5, 100000).astype(np.float32)
+    a = oracle_lib.atan2(y, z)
+    ref = np.arctan2(y.astype(np.float64), z.astype(np.float64)).astype(np.float32)
+    assert np.abs(a.view(np.int32).astype(np.int64) - ref.view(np.int32).astype(np.int64)).max() <= 1
+    assert oracle_lib.atan2(np.float32([0.0]), np.float32([-1.0]))[0] == np.float32(math.pi)
+
+
+def test_free_fall_matches_semi_implicit_euler(oracle_lib):
+    b = SceneBuilder(fps=240, box_hulls="direct")
+    b.add_ground_plane()
+    body = b.add_body(xform=[0.0, 0.0, 5.0, 0, 0, 0, 1])
+    b.add_shape_box(body, hx=0.1, hy=0.1, hz=0.1)
+    pk = pack(b.finalize())
+    o = oracle_lib.OracleSim(pk)
+    frames, substeps = 30, pk.params["substeps"]
+    o.step(frames)
+    dt = np.float32(1.0 / (240 * substeps))
+    g = np.float32(-9.81)
+    v, z = np.float32(0.0), np.float32(5.0)
+    for _ in range(frames * substeps):
+        v = np.float32(v + g * dt)
+        z = np.float32(z + v * dt)
+    np.testing.assert_allclose(o.body_poses()[0, 2], z, rtol=1e-6)
+    np.testing.assert_allclose(o.read("vel")[2], v, rtol=1e-5)
+
+
+def test_box_rests_on_plane(oracle_lib):
+    b = SceneBuilder(fps=240, box_hulls="direct")
+    b.add_ground_plane(mu=0.6)
+    body = b.add_body(xform=[0.0, 0.0, 0.1, 0, 0, 0, 1])
+    b.add_shape_box(body, hx=0.2, hy=0.15, hz=0.1, mu=0.6)
+    o = oracle_lib.OracleSim(pack(b.finalize()))
+    o.step(240)
+    pose = o.body_poses()[0]
+    vel = o.read("vel")[:8]
+    assert abs(pose[2] - 0.1) < 2e-3
+    assert abs(pose[0]) < 1e-4 and abs(pose[1]) < 1e-4
+    assert np.abs(vel[[0, 1, 2, 4, 5, 6]]).max() < 1e-2
+
+
+def test_pendulum_small_angle_period(oracle_lib):
+    r, d = 0.05, 0.5
+    b = SceneBuilder(fps=240)
+    bob = b.add_body(xform=[0.0, 0.0, 2.0 - d, 0, 0, 0, 1])
+    b.add_shape_sphere(bob, radius=r)
+    b.add_joint_revolute(-1, bob, axis=[0, 1, 0], parent_xform=[0.0, 0.0, 2.0, 0, 0, 0, 1],
+                         child_xform=[0.0, 0.0, d, 0, 0, 0, 1], q=[0.05])
+    pk = pack(b.finalize())
+    o = oracle_lib.OracleSim(pk)
+    qs = []
+    for _ in range(720):
+        o.step(1)
+        qs.append(o.read("art")[pk.C["A_Q"]])
+    q = np.array(qs)
+    t = (np.arange(len(q)) + 1) / 240.0
+    cross = [t[i] - q[i] * (t[i + 1] - t[i]) / (q[i + 1] - q[i]) for i in range(len(q) - 1) if q[i] * q[i + 1] < 0]
+    period = 2.0 * float(np.mean(np.diff(cross)))
+    expected = 2.0 * math.pi * math.sqrt((0.4 * r * r + d * d) / (9.81 * d))
+    assert len(cross) >= 4
+    assert abs(period - expected) / expected < 0.01
+
+
+def _fixture_values(oracle_lib):
+    from tests.golden.make_golden import fixture_values
+    return fixture_values(oracle_lib)
+
+
+def test_oracle_matches_committed_fixtures(oracle_lib):
+    gold = np.load(GOLDEN)
+    now = _fixture_values(oracle_lib)
+    assert sorted(now) == sorted(gold.files)
+    for k in gold.files:
+        a, b = np.ascontiguousarray(gold[k]), np.ascontiguousarray(now[k])
+        assert a.shape == b.shape, k
+        assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), f"fixture {k} changed"
+
+
+def test_oracle_refuses_unsupported_options(oracle_lib):
+    sc = scenes.boxes(n=4, seed=2)
+    pk = pack(sc, opts={"solver": {"enable_sleeping": True}})
+    if pk.C.get("SLEEP", 0) == 0:
+        pytest.skip("option not carried by the packer")
+    with pytest.raises(ValueError):
+        oracle_lib.OracleSim(pk)
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_SCENES), reason="reference scene folders not on disk")
+def test_reference_scenes_load_and_pack(oracle_lib):
+    from steel_webgpu_b200.builder import load_scene
+    names = sorted(d for d in os.listdir(REF_SCENES) if os.path.exists(os.path.join(REF_SCENES, d, "scene.json")))
+    assert len(names) >= 40
+    supported = []
+    for name in names:
+        pk = pack(load_scene(os.path.join(REF_SCENES, name)))
+        assert pk.statF.size == pk.C["LEN_STATF4"] * 4 and pk.statU.size == pk.C["LEN_STATU"]
+        if not any(pk.C.get(k, 0) for k in UNSUPPORTED):
+            supported.append((name, pk))
+    assert len(supported) >= 5
+    for name, pk in supported:
+        o = oracle_lib.OracleSim(pk)
+        o.step(5)
+        assert np.isfinite(o.body_poses()).all(), name
