@@ -199,7 +199,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
   s.warm_words = 10ull * d.WH + 30ull * d.AH;
   {
     size_t a = 2ull * d.MAXPATH + 6ull * d.MAXPATH * d.JM;
-    size_t b = 5ull * d.NDA + 18ull * d.MAXLP + 8;
+    size_t b = 6ull * d.NDA + 54ull * d.MAXLP + 8;  // dense rows: J, Y, three-way generalized solve
     s.tscr_floats = a > b ? a : b;
     d.TSCR = (uint32_t)s.tscr_floats;
   }

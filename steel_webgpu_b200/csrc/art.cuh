@@ -186,17 +186,17 @@ struct Art {
   // qs): joint damping, spring, and the implicit PD drive folded into D (artwgsl.js:290-318).
   // Drr holds D[r][r] = S_r . U_r on entry and gains the drive and damping terms.
   __device__ float dof_tau(uint32_t d, uint32_t qs, uint32_t r, float& Drr, const Params& P) const {
-    float4 dr = dof_drive(d);
+    // Every input is loaded first, so the loads overlap.
+    const float4 dr = dof_drive(d), pas = dof_passive(d), spr = S.sf[S.SF_DOF + d * 5u + 4u];
+    const float qd = A[S.A_QD + d], jf = A[S.A_JF + d], q = A[S.A_Q + qs + r];
+    const float tgt = A[S.A_TGT + d], tv = A[S.A_TGTV + d];
     Drr += dr.x;
-    float damp = dof_passive(d).x;
+    float damp = pas.x;
     Drr += P.dt * damp;
-    float tau = (-damp) * A[S.A_QD + d] + A[S.A_JF + d];
-    float4 spr = S.sf[S.SF_DOF + d * 5u + 4u];
-    if (spr.x != 0.0f) tau += spr.x * (spr.y - A[S.A_Q + qs + r]);
+    float tau = (-damp) * qd + jf;
+    if (spr.x != 0.0f) tau += spr.x * (spr.y - q);
     if (dr.y > 0.0f || dr.z > 0.0f) {
-      float q = A[S.A_Q + qs + r], qd = A[S.A_QD + d];
-      float err = A[S.A_TGT + d] - q;
-      float tv = A[S.A_TGTV + d];
+      float err = tgt - q;
       float mm = fmx(Drr, 1e-9f);
       float qdn = (mm * qd + P.dt * (dr.y * err + dr.z * tv)) / ((mm + P.dt * dr.z) + (P.dt * P.dt) * dr.y);
       float ti = dr.y * (err - P.dt * qdn) + dr.z * (tv - qdn);
@@ -218,11 +218,21 @@ struct Art {
     for (uint32_t k = 0; k < ai.y; k++) {
       uint32_t l = ai.x + k, L = lo(l);
       int par = lparent(l);
+      uint32_t nd = lndof(l), d0 = ldof(l);
+      // Global inputs first (qd of the link's dofs, the body's applied wrench), so they overlap.
+      const uint32_t bo = S.A_BF + (uint32_t)lbody(l) * 8u;
+      const f3 bforce = ald3(bo), btorque = ald3(bo + 4u);
+      float qdv[6];
+#pragma unroll
+      for (uint32_t c = 0; c < 6u; c++) qdv[c] = c < nd ? A[S.A_QD + d0 + c] : 0.0f;
       SVec vp = sv0();
       if (par >= 0) vp = mshift(ldsv(lo((uint32_t)par) + L_V), link_r(l));
       SVec sq = sv0();
-      uint32_t nd = lndof(l), d0 = ldof(l);
-      for (uint32_t c = 0; c < nd; c++) sq = sadd(sq, sscl(ldS(l, c), A[S.A_QD + d0 + c]));
+#pragma unroll
+      for (uint32_t c = 0; c < 6u; c++) {
+        if (c >= nd) break;
+        sq = sadd(sq, sscl(ldS(l, c), qdv[c]));
+      }
       SVec v = sadd(vp, sq);
       stsv(L + L_V, v);
       SVec cb = crm(vp, sq);
@@ -255,7 +265,7 @@ struct Art {
       stm(L + L_IA + 18u, mcols(mf3(m, 0, 0), mf3(0, m, 0), mf3(0, 0, m)));
       SVec pa0 = crf(v, imul(L + L_IA, v));
       if ((f2u(S.sf[S.SF_BODY + (uint32_t)b * 8u + 7u].w) & 2u) != 0u) pa0 = sadd(pa0, SVec{sp3(0.0f), m * g});
-      pa0 = sadd(pa0, SVec{-ald3(S.A_BF + (uint32_t)b * 8u + 4u), -ald3(S.A_BF + (uint32_t)b * 8u)});
+      pa0 = sadd(pa0, SVec{-btorque, -bforce});
       stsv(L + L_PA, pa0);
     }
     for (uint32_t kk = 0; kk < ai.y; kk++) {
@@ -549,6 +559,167 @@ struct Art {
         out[ldof(l) + r - ai.z] = dq[r];
       }
       stp(dvs, k, dv);
+    }
+  }
+
+  // solve_gen3 on a serial chain: p and dv carried in registers, u staged in uu (18 per link).
+  __device__ void solve_gen3_chain(uint4 ai, const float* __restrict__ J, float* __restrict__ Y,
+                                   float* __restrict__ uu) const {
+    const uint32_t NDA = S.NDA;
+    SVec pc[3] = {sv0(), sv0(), sv0()};  // p of the link being visited (its child's contribution)
+    for (uint32_t kk = 0; kk < ai.y; kk++) {
+      uint32_t k = ai.y - 1u - kk, l = ai.x + k, n = lndof(l);
+      bool has_parent = k > 0u || lparent(l) >= 0;
+      f3 rl = link_r(l);
+      uint32_t dl = ldof(l) - ai.z;
+#pragma unroll
+      for (uint32_t rs = 0; rs < 3u; rs++) {
+        const float* tau = J + rs * NDA;
+        float u[6] = {0, 0, 0, 0, 0, 0};
+        SVec pk = pc[rs];
+#pragma unroll
+        for (uint32_t r = 0; r < 6u; r++) {
+          if (r >= n) break;
+          u[r] = tau[dl + r] - sdot(ldS(l, r), pk);
+        }
+#pragma unroll
+        for (uint32_t r = 0; r < 6u; r++) uu[(k * 3u + rs) * 6u + r] = u[r];
+        if (has_parent) {
+          SVec pp = pk;
+#pragma unroll
+          for (uint32_t r = 0; r < 6u; r++) {
+            if (r >= n) break;
+            float du = 0.0f;
+#pragma unroll
+            for (uint32_t c = 0; c < 6u; c++) {
+              if (c >= n) break;
+              du += ldDI(l, r, c) * u[c];
+            }
+            pp = sadd(pp, sscl(ldU(l, r), du));
+          }
+          pc[rs] = sadd(sv0(), fshift(pp, rl));
+        }
+      }
+    }
+    SVec dc[3] = {sv0(), sv0(), sv0()};  // dv of the parent of the link being visited
+    for (uint32_t k = 0; k < ai.y; k++) {
+      uint32_t l = ai.x + k;
+      bool has_parent = lparent(l) >= 0;
+      f3 rl = link_r(l);
+      uint32_t n = lndof(l), dl = ldof(l) - ai.z;
+#pragma unroll
+      for (uint32_t rs = 0; rs < 3u; rs++) {
+        SVec dv = sv0();
+        if (has_parent) dv = mshift(dc[rs], rl);
+        float dq[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (uint32_t r = 0; r < 6u; r++) {
+          if (r >= n) break;
+          dq[r] = 0.0f;
+#pragma unroll
+          for (uint32_t c = 0; c < 6u; c++) {
+            if (c >= n) break;
+            dq[r] += ldDI(l, r, c) * (uu[(k * 3u + rs) * 6u + c] - sdot(ldU(l, c), dv));
+          }
+        }
+#pragma unroll
+        for (uint32_t r = 0; r < 6u; r++) {
+          if (r >= n) break;
+          dv = sadd(dv, sscl(ldS(l, r), dq[r]));
+          Y[rs * NDA + dl + r] = dq[r];
+        }
+        dc[rs] = dv;
+      }
+    }
+  }
+
+  // solve_gen for three right-hand sides in one walk of the articulation: row r of J (NDA
+  // floats, zero beyond the articulation's dofs) is the generalized impulse of right-hand side r,
+  // row r of Y receives its qd change. Each right-hand side goes through exactly the operations of
+  // solve_gen. scratch: 54 * MAXLP floats.
+  __device__ void solve_gen3(uint32_t a, const float* __restrict__ J, float* __restrict__ Y, float* __restrict__ scr) const {
+    uint4 ai = info(a);
+    const uint32_t NDA = S.NDA, M = S.MAXLP;
+    // A serial chain (every link's parent is the previous link) has one child per link, so the
+    // impulse accumulated into a parent and the velocity change handed to a child can stay in
+    // registers; the sums are the same (the parent's accumulator starts at zero).
+    bool chain = true;
+    for (uint32_t k = 1; k < ai.y; k++) chain = chain && lparent(ai.x + k) == (int)(ai.x + k - 1u);
+    if (chain) { solve_gen3_chain(ai, J, Y, scr + 18u * M); return; }
+    float* p = scr;                 // per link, 3 x 6
+    float* uu = scr + 18u * M;      // per link, 3 x 6
+    float* dvs = scr + 36u * M;     // per link, 3 x 6
+    for (uint32_t k = 0; k < 18u * ai.y; k++) p[k] = 0.0f;
+    auto ldp = [&](const float* base, uint32_t k) {
+      return SVec{mf3(base[k * 6], base[k * 6 + 1], base[k * 6 + 2]), mf3(base[k * 6 + 3], base[k * 6 + 4], base[k * 6 + 5])};
+    };
+    auto stp = [&](float* base, uint32_t k, SVec v) {
+      base[k * 6] = v.a.x; base[k * 6 + 1] = v.a.y; base[k * 6 + 2] = v.a.z;
+      base[k * 6 + 3] = v.l.x; base[k * 6 + 4] = v.l.y; base[k * 6 + 5] = v.l.z;
+    };
+    for (uint32_t kk = 0; kk < ai.y; kk++) {
+      uint32_t k = ai.y - 1u - kk, l = ai.x + k, n = lndof(l);
+      int par = lparent(l);
+      f3 rl = link_r(l);
+      uint32_t dl = ldof(l) - ai.z;
+#pragma unroll
+      for (uint32_t rs = 0; rs < 3u; rs++) {
+        const float* tau = J + rs * NDA;
+        float u[6] = {0, 0, 0, 0, 0, 0};
+        SVec pk = ldp(p, k * 3u + rs);
+#pragma unroll
+        for (uint32_t r = 0; r < 6u; r++) {
+          if (r >= n) break;
+          u[r] = tau[dl + r] - sdot(ldS(l, r), pk);
+        }
+#pragma unroll
+        for (uint32_t r = 0; r < 6u; r++) uu[(k * 3u + rs) * 6u + r] = u[r];
+        if (par >= 0) {
+          SVec pp = pk;
+#pragma unroll
+          for (uint32_t r = 0; r < 6u; r++) {
+            if (r >= n) break;
+            float du = 0.0f;
+#pragma unroll
+            for (uint32_t c = 0; c < 6u; c++) {
+              if (c >= n) break;
+              du += ldDI(l, r, c) * u[c];
+            }
+            pp = sadd(pp, sscl(ldU(l, r), du));
+          }
+          uint32_t pi = ((uint32_t)par - ai.x) * 3u + rs;
+          stp(p, pi, sadd(ldp(p, pi), fshift(pp, rl)));
+        }
+      }
+    }
+    for (uint32_t k = 0; k < ai.y; k++) {
+      uint32_t l = ai.x + k;
+      int par = lparent(l);
+      f3 rl = link_r(l);
+      uint32_t n = lndof(l), dl = ldof(l) - ai.z;
+#pragma unroll
+      for (uint32_t rs = 0; rs < 3u; rs++) {
+        SVec dv = sv0();
+        if (par >= 0) dv = mshift(ldp(dvs, ((uint32_t)par - ai.x) * 3u + rs), rl);
+        float dq[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (uint32_t r = 0; r < 6u; r++) {
+          if (r >= n) break;
+          dq[r] = 0.0f;
+#pragma unroll
+          for (uint32_t c = 0; c < 6u; c++) {
+            if (c >= n) break;
+            dq[r] += ldDI(l, r, c) * (uu[(k * 3u + rs) * 6u + c] - sdot(ldU(l, c), dv));
+          }
+        }
+#pragma unroll
+        for (uint32_t r = 0; r < 6u; r++) {
+          if (r >= n) break;
+          dv = sadd(dv, sscl(ldS(l, r), dq[r]));
+          Y[rs * NDA + dl + r] = dq[r];
+        }
+        stp(dvs, k * 3u + rs, dv);
+      }
     }
   }
 

@@ -425,17 +425,17 @@ struct Prep {
     uint32_t art_id = (uint32_t)bart(a);
     uint4 ai = ar.info(art_id);
     float* J = scr;
-    float* tau = scr + 3u * NDA;
-    float* y = tau + NDA;
-    float* gs = y + NDA;
-    for (uint32_t k = 0; k < 3u * NDA; k++) J[k] = 0.0f;
+    float* Y = scr + 3u * NDA;
+    float* gs = Y + 3u * NDA;
+    for (uint32_t k = 0; k < 3u * NDA; k++) { J[k] = 0.0f; Y[k] = 0.0f; }
     ar.gen_jac((uint32_t)blink(b), p, 1.0f, n, t1, t2, ai.z, J);
     ar.gen_jac((uint32_t)blink(a), p, -1.0f, n, t1, t2, ai.z, J);
     uint32_t o = S.A_DENSE + slot * DPS;
     float K[9];
+    // Row r's right-hand side is J row r (zero beyond the articulation's dofs, as gen_jac leaves it).
+    ar.solve_gen3(art_id, J, Y, gs);
     for (uint32_t r = 0; r < 3u; r++) {
-      for (uint32_t k = 0; k < NDA; k++) { tau[k] = k < ai.w ? J[r * NDA + k] : 0.0f; y[k] = 0.0f; }
-      ar.solve_gen(art_id, tau, y, gs);
+      const float* y = Y + r * NDA;
       for (uint32_t k = 0; k < ai.w; k++) {
         A[o + DHDR + r * NDA + k] = J[r * NDA + k];
         A[o + DHDR + 3u * NDA + r * NDA + k] = y[k];
