@@ -227,16 +227,54 @@ def cpu_baseline_sample(pks, frames: int):
     return sum(pk.NB for pk in pks) * frames / dt, dt
 
 
-def dist_setup(n_gpus: int):
+def dist_setup(n_gpus: int, backend: str = "nccl"):
+    """Rank, world size and local device from the torchrun environment (single process otherwise)."""
     if n_gpus <= 1 or "RANK" not in os.environ:
         return 0, 1, 0
     import torch
     import torch.distributed as dist
     import datetime
     rank, world, local = int(os.environ["RANK"]), int(os.environ["WORLD_SIZE"]), int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(local)
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return rank, world, local
+
+
+def max_over_ranks(x: float, world: int, local: int = 0) -> float:
+    """The maximum of x over all ranks (x itself for one rank): times are max-over-ranks."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = f"cuda:{local}" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def whole_job_rate(world: int, units_per_rank: int, steps: int, seconds: float) -> float:
+    """Units of all ranks per second of the slowest rank (every rank steps the same workload size)."""
+    return world * units_per_rank * steps / seconds
+
+
+def plain_path_sample(pks, frames: int, device: int):
+    """The plain path: each scene alone, one batch of one scene per launch sequence; body-steps/s."""
+    from steel_webgpu_b200.sim import Batch
+    bodies, ms = 0, 0.0
+    for pk in pks:
+        b = Batch([pk], device=device)
+        b.step(3)
+        ms += b.step_timed(frames)
+        bodies += pk.NB * frames
+        b.close()
+    return bodies / (ms / 1000.0)
 
 
 def run_reference(args):
@@ -279,19 +317,13 @@ def run_steel(args):
     substeps = pks[0].params["substeps"]
     batch.step(max(args.warmup, 3))
     batch.sync()
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    barrier(world)
     torch.cuda.synchronize(local)
     with ClockSampler(local) as clk:
         ms = batch.step_timed(args.steps)
     torch.cuda.synchronize(local)
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * nbodies * args.steps / (ms / 1000.0)
+    ms = max_over_ranks(ms, world, local)
+    value = whole_job_rate(world, nbodies, args.steps, ms / 1000.0)
     # End to end through the C ABI with pinned host buffers: joint targets in, body poses out.
     nd = sum(pk.ND for pk in pks)
     npose = sum(pk.NB * 8 for pk in pks)
@@ -299,20 +331,16 @@ def run_steel(args):
     h_pose = torch.zeros(npose, dtype=torch.float32, pin_memory=True).numpy()
     rng = np.random.default_rng(1)
     batch.step_io(1, h_tgt if nd else None, h_pose)
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    barrier(world)
+    frame_ms = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
+        f0 = time.perf_counter()
         h_tgt[:] = rng.uniform(-0.5, 0.5, nd).astype(np.float32)
         batch.step_io(1, h_tgt if nd else None, h_pose)
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * nbodies * args.steps / e2e_s
+        frame_ms.append((time.perf_counter() - f0) * 1000.0)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, local)
+    e2e = whole_job_rate(world, nbodies, args.steps, e2e_s)
     # Roofline of the dominant kernel: per-launch device time from CUDA events around each launch.
     prof = batch.profile_kernels(max(2, min(args.steps, 8)))
     counts = scene_counts(batch, pks)
@@ -326,6 +354,7 @@ def run_steel(args):
     achieved = bytes_dom / (prof[dom] / 1000.0) / 1e9
     if rank != 0:
         return
+    plain = plain_path_sample(pks[:args.plain_scenes], 2, local) if args.plain_scenes > 0 else None
     cpu_sample = pks[:args.cpu_scenes]
     cpu_val, cpu_dt = cpu_baseline_sample(cpu_sample, args.cpu_frames)
     clocks = clk.summary()
@@ -337,7 +366,13 @@ def run_steel(args):
                    "fps": 240, "substeps": substeps, "iterations": iterations, "parallelism": f"replicas x{world}",
                    "graph": True, "l2": "per-scene state is resident and re-read every substep; no L2 flush",
                    "contact_steps_per_s": world * counts["contacts"] * substeps * args.steps / (ms / 1000.0),
-                   "build_s": round(build_s, 1), "overflow_scenes": overflow_scenes},
+                   "build_s": round(build_s, 1), "overflow_scenes": overflow_scenes,
+                   "frame_latency_ms": {"p50": float(np.percentile(frame_ms, 50)),
+                                        "p99": float(np.percentile(frame_ms, 99)),
+                                        "what": "one frame of the whole batch through steel_step_io, host clock"},
+                   "plain_path": None if plain is None else {
+                       "body_steps_per_s": plain, "batched_over_plain": value / world / plain,
+                       "sample": f"first {args.plain_scenes} scenes, each alone (one scene per launch sequence), 2 frames"}},
         "e2e": {"value": e2e, "unit": "body-steps/s", "h2d_bytes_per_step": 4 * nd, "d2h_bytes_per_step": 4 * npose},
         "gpu_launches": args.steps * (substeps * 8 + 1),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -369,6 +404,7 @@ def main():
     ap.add_argument("--cpu-scenes", type=int, default=16)
     ap.add_argument("--cpu-frames", type=int, default=4)
     ap.add_argument("--ref-scenes", type=int, default=128)
+    ap.add_argument("--plain-scenes", type=int, default=16)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
