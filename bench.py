@@ -393,6 +393,48 @@ def run_steel(args):
         dist.destroy_process_group()
 
 
+def run_serve(args):
+    """Serving: Poisson arrivals of 1-32-frame requests for random resident instances, continuous
+    batching (steel_serve_*); p50/p99 request latency and served body-steps/s (one JSON line)."""
+    from steel_webgpu_b200.sim import Batch, Server
+    pks = build_workload(args.workload, args.seed, limit=args.serve_instances)
+    batch = Batch(pks)
+    batch.step(3)
+    batch.sync()
+    srv = Server(batch, max_active=args.serve_max_active)
+    rng = np.random.default_rng(args.seed)
+    n = args.serve_requests
+    gaps = rng.exponential(1.0 / args.serve_rate, n)
+    arrive = np.cumsum(gaps)
+    inst = rng.integers(0, len(pks), n)
+    frames = rng.integers(1, 33, n)
+    done, k, lat = 0, 0, []
+    body_frames = 0
+    t0 = time.perf_counter()
+    while done < n:
+        now = time.perf_counter() - t0
+        while k < n and arrive[k] <= now:
+            srv.submit(int(inst[k]), int(frames[k]))
+            body_frames += pks[int(inst[k])].NB * int(frames[k])
+            k += 1
+        if srv.tick() == 0 and k < n:
+            time.sleep(max(0.0, min(arrive[k] - (time.perf_counter() - t0), 0.001)))
+        for _, _, ms in srv.poll():
+            lat.append(ms)
+            done += 1
+    wall = time.perf_counter() - t0
+    srv.close()
+    print(json.dumps({
+        "metric": "served body-steps/s", "value": body_frames / wall, "unit": "body-steps/s", "n_gpus": 1,
+        "higher_is_better": True, "data": "synthetic (seeded scenes, no dataset)",
+        "config": {"workload": args.workload, "instances": len(pks), "requests": n, "rate_per_s": args.serve_rate,
+                   "frames_per_request": "uniform 1-32", "max_active": args.serve_max_active or len(pks)},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "mean": float(np.mean(lat))},
+        "wall_s": wall}), flush=True)
+    batch.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -405,9 +447,16 @@ def main():
     ap.add_argument("--cpu-frames", type=int, default=4)
     ap.add_argument("--ref-scenes", type=int, default=128)
     ap.add_argument("--plain-scenes", type=int, default=16)
+    ap.add_argument("--mode", default="bench", choices=["bench", "serve"])
+    ap.add_argument("--serve-instances", type=int, default=512)
+    ap.add_argument("--serve-requests", type=int, default=3000)
+    ap.add_argument("--serve-rate", type=float, default=2000.0)
+    ap.add_argument("--serve-max-active", type=int, default=0)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.mode == "serve":
+        run_serve(args)
     else:
         run_steel(args)
 

@@ -116,6 +116,23 @@ int steel_profile_kernels(steel_batch* b, uint32_t frames, float* ms_per_launch)
 /* Device time of the last steel_step_timed call's frames, in milliseconds (CUDA events). */
 int steel_step_timed(steel_batch* b, uint32_t frames, float* ms);
 
+/* Serving loop: continuous batching over the batch's scenes as resident instances. No direct
+   counterpart in the reference; the closest is Sim.run (sim.js:705-712), which keeps up to four
+   frames of one scene in flight. Requests of `frames` frames queue per instance; up to max_active
+   instances are admitted at a time, first come first served (0 or a value above the scene count:
+   all). Each tick steps every admitted instance by one frame and waits for it; an instance whose
+   request is done takes its next queued request or makes room for the next waiting instance.
+   Latency is measured from submit to the end of the request's last tick. While the loop runs,
+   steel_step and steel_collide step only the admitted instances; steel_serve_end makes every
+   scene step again. Scenes are independent, so an instance's result is the same alone and in any
+   mix. */
+int steel_serve_config(steel_batch* b, uint32_t max_active);
+int steel_serve_submit(steel_batch* b, uint32_t instance, uint32_t frames, uint64_t* id);
+int steel_serve_tick(steel_batch* b, uint32_t* stepped /* instances stepped in this tick */);
+int steel_serve_poll(steel_batch* b, uint64_t* ids, uint32_t* instances, double* latency_ms, uint32_t cap,
+                     uint32_t* count /* finished requests returned (and removed) */);
+int steel_serve_end(steel_batch* b);
+
 /* Canonical contact sort that allocates no device memory. No counterpart in the reference (its
    sort runs only inside Sim.step); it exists for callers that cannot call cudaMalloc: a robot
    controller on a fixed-rate loop, where cudaMalloc/cudaFree may block and synchronise the whole

@@ -1,9 +1,11 @@
 // Host side of the C ABI (include/steel_b200.h): batch construction from the reference's packed
 // scenes, one device arena per batch, the per-substep launch sequence (captured as a CUDA graph),
 // readback and user control.
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
 #include <sstream>
@@ -113,12 +115,23 @@ struct steel_batch {
   bool use_graph = true;
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  size_t o_scenes, o_shape_scene, o_shape_local, o_tiles, o_pairs, o_pair_count, o_jobs, o_phase, o_ssc, o_err;
+  size_t o_scenes, o_shape_scene, o_shape_local, o_tiles, o_pairs, o_pair_count, o_jobs, o_phase, o_ssc, o_active, o_err;
   std::vector<uint32_t> shape_scene, shape_local;
   std::vector<uint4> tiles;
   // host-I/O staging (steel_step_io): packed targets/poses on the device and their offsets
   size_t o_tgt_off, o_pose_off, o_tgt_buf, o_pose_buf;
   uint64_t n_targets = 0, n_poses = 0;
+  // Serving loop (steel_serve_*): per-instance request queues, the admitted set and finished work.
+  struct Req { uint64_t id; uint32_t frames_left, frames; double t_submit; };
+  struct Done { uint64_t id; uint32_t instance, frames; double latency_ms; };
+  std::vector<std::deque<Req>> serve_queue;
+  std::deque<uint32_t> serve_waiting;          // instances with queued work, not admitted, FIFO
+  std::vector<uint8_t> serve_state;            // 0 idle, 1 waiting, 2 admitted
+  std::vector<uint32_t> serve_mask;            // host copy of the device activity mask
+  std::vector<Done> serve_done;
+  uint32_t serve_admitted = 0, serve_max_active = 0;
+  uint64_t serve_next_id = 1;
+  bool serve_on = false;
 };
 
 namespace {
@@ -263,7 +276,7 @@ int upload_state(steel_batch* b) {
     CU(cudaMemsetAsync(d.stats, 0, 64, st));
   }
   CU(cudaMemsetAsync(b->bd.phase, 0, sizeof(double) * b->sc.size(), st));
-  CU(cudaMemsetAsync(b->bd.substep_count, 0, sizeof(unsigned long long), st));
+  CU(cudaMemsetAsync(b->bd.substep_count, 0, sizeof(unsigned long long) * b->sc.size(), st));
   CU(cudaMemsetAsync(b->bd.error, 0, sizeof(uint32_t), st));
   return STEEL_OK;
 }
@@ -361,7 +374,8 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   b->o_pair_count = L.take(8);
   b->o_jobs = L.take(4ull * NJOB_WORDS * pair_cap + 16);
   b->o_phase = L.take(8ull * n);
-  b->o_ssc = L.take(8);
+  b->o_ssc = L.take(8ull * n);
+  b->o_active = L.take(4ull * n);
   b->o_err = L.take(4);
   std::vector<uint64_t> tgt_off(n), pose_off(n);
   for (uint32_t i = 0; i < n; i++) {
@@ -426,6 +440,8 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   bd.jobs = at<uint4>(A, b->o_jobs);
   bd.phase = at<double>(A, b->o_phase);
   bd.substep_count = at<unsigned long long>(A, b->o_ssc);
+  bd.active = at<uint32_t>(A, b->o_active);
+  CU(cudaMemsetAsync(A + b->o_active, 1, 4ull * n, st));  // every scene steps (nonzero words)
   bd.error = at<uint32_t>(A, b->o_err);
   bd.prep_smem = (uint32_t)prep_smem;
   bd.solve_smem = (uint32_t)solve_smem;
@@ -776,6 +792,118 @@ int steel_read_pairs(steel_batch* b, uint32_t scene, uint32_t* pairs, uint32_t c
     n++;
   }
   *count = n;
+  return STEEL_OK;
+}
+
+
+// --- Serving loop -----------------------------------------------------------------------------
+// Continuous batching over the batch's scenes as resident instances. Requests (instance, frames)
+// queue per instance; up to max_active instances are admitted at a time (FIFO), each tick steps
+// every admitted instance by one frame (the other scenes' blocks return at once), and an instance
+// whose request is done takes its next queued request or leaves the admitted set, which admits the
+// next waiting instance. Scenes are independent, so an instance's result does not depend on what
+// else is admitted.
+static double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+static int serve_begin(steel_batch* b) {
+  if (b->serve_on) return STEEL_OK;
+  const uint32_t n = (uint32_t)b->sc.size();
+  b->serve_queue.assign(n, {});
+  b->serve_state.assign(n, 0);
+  b->serve_mask.assign(n, 0u);
+  b->serve_waiting.clear();
+  b->serve_done.clear();
+  b->serve_admitted = 0;
+  if (b->serve_max_active == 0 || b->serve_max_active > n) b->serve_max_active = n;
+  CU(cudaSetDevice(b->ctx->device));
+  CU(cudaMemcpyAsync(b->arena + b->o_active, b->serve_mask.data(), 4ull * n, cudaMemcpyHostToDevice, b->ctx->stream));
+  b->serve_on = true;
+  return STEEL_OK;
+}
+
+int steel_serve_config(steel_batch* b, uint32_t max_active) {
+  if (!b) return fail(STEEL_E_INVALID, "null batch");
+  b->serve_max_active = max_active;
+  return STEEL_OK;
+}
+
+int steel_serve_submit(steel_batch* b, uint32_t instance, uint32_t frames, uint64_t* id) {
+  if (!b || !id) return fail(STEEL_E_INVALID, "null argument");
+  if (instance >= b->sc.size()) return fail(STEEL_E_INVALID, "bad instance index");
+  if (frames == 0) return fail(STEEL_E_INVALID, "a request needs at least one frame");
+  if (int rc = serve_begin(b)) return rc;
+  *id = b->serve_next_id++;
+  b->serve_queue[instance].push_back({*id, frames, frames, now_ms()});
+  if (b->serve_state[instance] == 0) {
+    b->serve_state[instance] = 1;
+    b->serve_waiting.push_back(instance);
+  }
+  return STEEL_OK;
+}
+
+int steel_serve_tick(steel_batch* b, uint32_t* stepped) {
+  if (!b) return fail(STEEL_E_INVALID, "null batch");
+  if (int rc = serve_begin(b)) return rc;
+  CU(cudaSetDevice(b->ctx->device));
+  cudaStream_t st = b->ctx->stream;
+  bool changed = false;
+  while (b->serve_admitted < b->serve_max_active && !b->serve_waiting.empty()) {
+    uint32_t i = b->serve_waiting.front();
+    b->serve_waiting.pop_front();
+    b->serve_state[i] = 2;
+    b->serve_mask[i] = 1u;
+    b->serve_admitted++;
+    changed = true;
+  }
+  if (stepped) *stepped = b->serve_admitted;
+  if (b->serve_admitted == 0) return STEEL_OK;
+  if (changed)
+    CU(cudaMemcpyAsync(b->arena + b->o_active, b->serve_mask.data(), 4ull * b->sc.size(), cudaMemcpyHostToDevice, st));
+  if (int rc = steel_step(b, 1)) return rc;
+  CU(cudaStreamSynchronize(st));
+  const double t = now_ms();
+  changed = false;
+  for (uint32_t i = 0; i < (uint32_t)b->sc.size(); i++) {
+    if (b->serve_state[i] != 2) continue;
+    auto& q = b->serve_queue[i];
+    steel_batch::Req& r = q.front();
+    if (--r.frames_left > 0) continue;
+    b->serve_done.push_back({r.id, i, r.frames, t - r.t_submit});
+    q.pop_front();
+    if (q.empty()) {
+      b->serve_state[i] = 0;
+      b->serve_mask[i] = 0u;
+      b->serve_admitted--;
+      changed = true;
+    }
+  }
+  if (changed)
+    CU(cudaMemcpyAsync(b->arena + b->o_active, b->serve_mask.data(), 4ull * b->sc.size(), cudaMemcpyHostToDevice, st));
+  return STEEL_OK;
+}
+
+int steel_serve_poll(steel_batch* b, uint64_t* ids, uint32_t* instances, double* latency_ms, uint32_t cap,
+                     uint32_t* count) {
+  if (!b || !count) return fail(STEEL_E_INVALID, "null argument");
+  uint32_t n = (uint32_t)std::min<size_t>(cap, b->serve_done.size());
+  for (uint32_t k = 0; k < n; k++) {
+    if (ids) ids[k] = b->serve_done[k].id;
+    if (instances) instances[k] = b->serve_done[k].instance;
+    if (latency_ms) latency_ms[k] = b->serve_done[k].latency_ms;
+  }
+  b->serve_done.erase(b->serve_done.begin(), b->serve_done.begin() + n);
+  *count = n;
+  return STEEL_OK;
+}
+
+int steel_serve_end(steel_batch* b) {
+  if (!b) return fail(STEEL_E_INVALID, "null batch");
+  if (!b->serve_on) return STEEL_OK;
+  CU(cudaSetDevice(b->ctx->device));
+  CU(cudaMemsetAsync(b->arena + b->o_active, 1, 4ull * b->sc.size(), b->ctx->stream));
+  b->serve_on = false;
   return STEEL_OK;
 }
 

@@ -18,7 +18,8 @@ struct BatchDev {
   uint32_t* pair_count;       // [2]: candidate pairs, narrowphase jobs
   uint4* jobs;                // narrowphase jobs [pair_cap][NJOB_WORDS / 4]
   double* phase;              // per-scene clock (sim.js:674-678)
-  unsigned long long* substep_count;  // [1]
+  unsigned long long* substep_count;  // [nscenes] substeps each scene has run (warm-table parity)
+  const uint32_t* active;     // [nscenes] nonzero: the scene steps in this frame (serving loop mask)
   uint32_t* error;            // [1] first device-side error code (0 = none)
   uint32_t prep_smem;         // dynamic shared memory of k_prepare / k_solve launches (bytes)
   uint32_t solve_smem;

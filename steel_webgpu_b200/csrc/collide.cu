@@ -17,13 +17,14 @@ namespace steel {
 // Per-substep parameters (sim.js:625-639): one thread per scene.
 __global__ void k_params(BatchDev B, uint32_t substep) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= B.nscenes) return;
+  if (s == 0u) { B.pair_count[0] = 0u; B.pair_count[1] = 0u; }
+  if (s >= B.nscenes || B.active[s] == 0u) return;
   const SceneDev& S = B.scenes[s];
   Params P;
   double dt = 1.0 / S.fps / (double)S.substeps;
   P.dt = (float)dt;
   P.substep = substep;
-  P.parity = (uint32_t)((*B.substep_count + substep) % 2ull);
+  P.parity = (uint32_t)((B.substep_count[s] + substep) % 2ull);
   P.iterations = S.iterations;
   P.phase = (float)B.phase[s];
   P.frame_dt = (float)(1.0 / S.fps);
@@ -37,20 +38,20 @@ __global__ void k_params(BatchDev B, uint32_t substep) {
   P.reg = S.reg;
   P.pad[0] = P.pad[1] = P.pad[2] = 0u;
   *S.params = P;
-  if (s == 0u && threadIdx.x == 0u) { B.pair_count[0] = 0u; B.pair_count[1] = 0u; }
 }
 // Frame end (sim.js:674-678): advance the clocks.
 __global__ void k_frame_end(BatchDev B) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < B.nscenes) B.phase[s] += 1.0 / B.scenes[s].fps;
-  if (s == 0u) *B.substep_count += (unsigned long long)B.scenes[0].substeps;
+  if (s >= B.nscenes || B.active[s] == 0u) return;
+  B.phase[s] += 1.0 / B.scenes[s].fps;
+  B.substep_count[s] += (unsigned long long)B.scenes[s].substeps;
 }
 
 // --------------------------------------------------------------------------------------------
 // Shape world poses and AABBs (wgsl.js:117-150): one thread per shape of the batch.
 __global__ void k_shapes(BatchDev B) {
   uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= B.nshapes) return;
+  if (g >= B.nshapes || B.active[B.shape_scene[g]] == 0u) return;
   const SceneDev& S = B.scenes[B.shape_scene[g]];
   uint32_t s = B.shape_local[g];
   RO<float4> sf = S.sf + S.SF_SHAPE + s * 7u;
@@ -92,6 +93,7 @@ struct TileShape { float4 lo, hi; int body; uint32_t fixed; };
 __global__ void __launch_bounds__(256) k_broad(BatchDev B) {
   __shared__ TileShape ti_[BROAD_TILE], tj_[BROAD_TILE];
   uint4 job = B.tiles[blockIdx.x];
+  if (B.active[job.x] == 0u) return;
   const SceneDev& S = B.scenes[job.x];
   const uint32_t i0 = job.y * BROAD_TILE, j0 = job.z * BROAD_TILE;
   const uint32_t t = threadIdx.x;
@@ -1246,6 +1248,7 @@ __global__ void __launch_bounds__(NARROW_JOB_THREADS, 4) k_narrow_jobs(BatchDev 
 // one block per scene, bitonic sort over a power-of-two key array in shared memory.
 __global__ void __launch_bounds__(SORT_THREADS) k_csort(BatchDev B, uint32_t smem_keys) {
   extern __shared__ uint4 sk[];
+  if (B.active[blockIdx.x] == 0u) return;
   const SceneDev& S = B.scenes[blockIdx.x];
   uint32_t nc = min(S.counters[1], S.MAXC);
   if (nc == 0u) return;

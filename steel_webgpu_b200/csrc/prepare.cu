@@ -506,6 +506,7 @@ __global__ void __launch_bounds__(PREP_THREADS, 4) k_prepare(BatchDev B) {
   __shared__ Params Ps;
   __shared__ SceneDev Ss;  // the scene's offsets and sizes, read everywhere in the serial passes
   const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  if (B.active[blockIdx.x] == 0u) return;  // not stepping in this frame (serving loop)
   copy_scene(Ss, B.scenes[blockIdx.x]);
   const SceneDev& S = Ss;
   if (tid == 0u) Ps = *B.scenes[blockIdx.x].params;

@@ -541,6 +541,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 4) k_solve(BatchDev B) {
   __shared__ Params Ps;
   __shared__ SceneDev Ss;  // the scene's offsets and sizes, read everywhere in the serial passes
   const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  if (B.active[blockIdx.x] == 0u) return;  // not stepping in this frame (serving loop)
   copy_scene(Ss, B.scenes[blockIdx.x]);
   const SceneDev& S = Ss;
   if (tid == 0u) Ps = *S.params;

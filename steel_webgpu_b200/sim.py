@@ -173,6 +173,40 @@ class Batch:
         return out[:nc * 20].reshape(nc, 5, 4), out[nc * 20:nc * 24].reshape(nc, 4)
 
 
+class Server:
+    """Continuous batching over a Batch's scenes as resident instances (steel_serve_*).
+
+    ``submit(instance, frames)`` queues a request; ``tick()`` steps every admitted instance by one
+    frame; ``poll()`` returns finished requests with their latency (submit to completion, ms).
+    """
+
+    def __init__(self, batch: Batch, max_active: int = 0):
+        self.batch = batch
+        _lib.check(_lib.load().steel_serve_config(batch.h, max_active))
+
+    def submit(self, instance: int, frames: int) -> int:
+        rid = ctypes.c_uint64()
+        _lib.check(_lib.load().steel_serve_submit(self.batch.h, instance, frames, ctypes.byref(rid)))
+        return rid.value
+
+    def tick(self) -> int:
+        n = ctypes.c_uint32()
+        _lib.check(_lib.load().steel_serve_tick(self.batch.h, ctypes.byref(n)))
+        return n.value
+
+    def poll(self, cap: int = 4096) -> list:
+        ids = np.zeros(cap, dtype=np.uint64)
+        inst = np.zeros(cap, dtype=np.uint32)
+        lat = np.zeros(cap, dtype=np.float64)
+        n = ctypes.c_uint32()
+        _lib.check(_lib.load().steel_serve_poll(self.batch.h, ids.ctypes.data, inst.ctypes.data, lat.ctypes.data,
+                                                cap, ctypes.byref(n)))
+        return [(int(ids[k]), int(inst[k]), float(lat[k])) for k in range(n.value)]
+
+    def close(self):
+        _lib.check(_lib.load().steel_serve_end(self.batch.h))
+
+
 class Sim:
     """``new Sim(device, scene, opts)`` (sim.js:63-75) as a batch of one scene."""
 
