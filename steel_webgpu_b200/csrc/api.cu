@@ -191,7 +191,9 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
     uint32_t tmp;
     put(d.A_Q, NQ); put(d.A_QD, ND); put(d.A_QDH, ND); put(d.A_INT, ND); put(d.A_TGT, ND); put(d.A_TGTV, ND);
     put(d.A_LIM, 2 * ND); put(d.A_DRV, ND); put(tmp, ND); put(d.A_JF, ND); put(d.A_BF, NB * 8); put(tmp, (NB + NA) * 4);
-    put(d.A_FRIC, ND); put(d.A_HINV, ND); put(d.A_LINK, (size_t)(NL > 0 ? NL : 1) * 268); put(tmp, NB * 8 + ND);
+    put(d.A_FRIC, ND); put(d.A_HINV, ND);
+    ao = (ao + 3) & ~(size_t)3;  // link blocks start on a 16-byte boundary (bulk copies)
+    put(d.A_LINK, (size_t)(NL > 0 ? NL : 1) * 268); put(tmp, NB * 8 + ND);
     put(d.A_VLG, ND + NB * 6); put(tmp, NA); put(d.A_LG, ND); put(d.A_RL, ND); put(d.A_RLN, NA);
     put(d.A_ULOAD, d.PATCH ? (size_t)MAXC : 0); put(d.A_DENSE, (size_t)d.MAXDENSE * d.DPS);
     s.art_floats = ao;
@@ -301,6 +303,7 @@ int check_device_error(steel_batch* b) {
   CU(cudaStreamSynchronize(b->ctx->stream));
   if (e == ERR_SORT_CAPACITY) return fail(STEEL_E_CAPACITY, "contact sort capacity exceeded");
   if (e == ERR_JOB_CAPACITY) return fail(STEEL_E_CAPACITY, "narrowphase job capacity exceeded");
+  if (e == ERR_STAGE_TIMEOUT) return fail(STEEL_E_CUDA, "a shared-memory bulk copy did not complete");
   if (e != 0) return fail(STEEL_E_CUDA, "device error " + std::to_string(e));
   return STEEL_OK;
 }

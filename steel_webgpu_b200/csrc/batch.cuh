@@ -34,7 +34,7 @@ constexpr int PREP_THREADS = 128;
 constexpr int SOLVE_THREADS = 128;
 
 // Device error codes written to BatchDev::error.
-enum : uint32_t { ERR_NONE = 0, ERR_SORT_CAPACITY = 1, ERR_JOB_CAPACITY = 2 };
+enum : uint32_t { ERR_NONE = 0, ERR_SORT_CAPACITY = 1, ERR_JOB_CAPACITY = 2, ERR_STAGE_TIMEOUT = 3 };
 
 // Shared-memory staging of a scene inside k_prepare / k_solve. A scene is staged when its part
 // fits the cap; the launch's dynamic shared memory is the largest staged scene's need.

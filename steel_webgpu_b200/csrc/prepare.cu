@@ -14,6 +14,7 @@
 // the serial overflow color's contact-order sort the identity.
 #include "art.cuh"
 #include "batch.cuh"
+#include "bulk.cuh"
 #include "block.cuh"
 
 namespace steel {
@@ -514,8 +515,10 @@ __global__ void __launch_bounds__(PREP_THREADS, 4) k_prepare(BatchDev B) {
   const PrepSmem lay = prep_smem_layout(S.stage, S.NL, S.NB, S.NCOLW, S.NCOL);
   const bool staged = (S.stage & STAGE_LINKS) != 0u;
   float* lb = staged ? reinterpret_cast<float*>(pb + lay.links) : S.art + S.A_LINK;
-  if (staged)
-    for (uint32_t i = tid; i < S.NL * LBLK; i += nt) lb[i] = S.art[S.A_LINK + i];
+  // Link blocks into shared memory with one bulk copy (A_LINK is 16-byte aligned).
+  __shared__ __align__(8) uint64_t stage_bar;
+  if (staged && !stage_to_shared(lb, S.art + S.A_LINK, 4u * S.NL * LBLK, &stage_bar) && tid == 0u)
+    atomicCAS(B.error, 0u, (uint32_t)ERR_STAGE_TIMEOUT);
   __syncthreads();
   const Params& P = Ps;
   Prep pr(S, P, lb);

@@ -12,6 +12,7 @@
 // with one barrier per color; the overflow color runs serially in contact order.
 #include "art.cuh"
 #include "batch.cuh"
+#include "bulk.cuh"
 
 namespace steel {
 
@@ -553,8 +554,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 4) k_solve(BatchDev B) {
   const uint32_t nu = S.sched[S.S_META];
   const uint32_t ncol = min(S.sched[S.S_META + 1u], S.NCOL);
   for (uint32_t i = tid; i < S.NCOL + 2u; i += nt) wcs[i] = S.sched[S.S_CSTART + i];
-  if (staged_links)
-    for (uint32_t i = tid; i < S.NL * LBLK; i += nt) lb[i] = S.art[S.A_LINK + i];
+  // Link blocks into shared memory with one bulk copy (A_LINK is 16-byte aligned).
+  __shared__ __align__(8) uint64_t stage_bar;
+  if (staged_links && !stage_to_shared(lb, S.art + S.A_LINK, 4u * S.NL * LBLK, &stage_bar) && tid == 0u)
+    atomicCAS(B.error, 0u, (uint32_t)ERR_STAGE_TIMEOUT);
   __syncthreads();
   const Params& P = Ps;
   Solver sv(S, P, lb, staged_bodies ? reinterpret_cast<float4*>(sb + lay.tw) : S.tw,
