@@ -53,7 +53,6 @@ bool Oracle::init(const char* constants, const float* statF_, size_t nF, const u
   else if (C.CTI) unsup = "row_schedule contact_then_internal";
   else if (C.LONGEST_FIRST) unsup = "propagation_color_order longest_first";
   else if (C.DRIVE_ROWS) unsup = "drive_mode rows";
-  else if (C.VLIM_ON) unsup = "enable_joint_velocity_limits";
   else if (C.JFL) unsup = "joint friction load coefficient";
   else if (C.SLEEP) unsup = "enable_sleeping";
   else if (C.VELITERS) unsup = "velocity_iterations";

@@ -387,6 +387,35 @@ void Oracle::k_prepare() {
   std::fill(wjsplit.begin(), wjsplit.end(), 0u);
   for (uint32_t tid = 0; tid < C.NA; tid++) {
     u4 ai = art_info(tid);
+    // Joint velocity limits (wgsl.js:1829-1854): scale the articulation's scalar dof speeds so the
+    // most exceeded limit is met, then mark the dofs near their limit (rows exist only there).
+    if (C.VLIM_ON == 1u) {
+      auto fused = [&](uint32_t d) {
+        v4 dr = dof_drive(d);
+        return C.DRIVE_ROWS == 1u && C.FUSE_VLIM == 1u && (dr.y > 0.0f || dr.z > 0.0f);
+      };
+      float ratio = 1.0f;
+      for (uint32_t k = 0; k < ai.w; k++) {
+        uint32_t d = ai.z + k;
+        float vl = dof_passive(d).z;
+        if (vl < 0.0f || fused(d)) continue;
+        float sp = std::fabs(art[C.A_QD + d]);
+        if (sp > vl) ratio = fminf_(ratio, vl / sp);
+      }
+      if (ratio < 1.0f)
+        for (uint32_t k = 0; k < ai.w; k++) {
+          uint32_t d = ai.z + k;
+          if (scalar_dof(d) && !fused(d)) art[C.A_QD + d] *= ratio;
+        }
+      bool any = false;
+      for (uint32_t k = 0; k < ai.w; k++) {
+        uint32_t d = ai.z + k;
+        bool on = std::fabs(art[C.A_QD + d]) >= C.F_VLIM_FRAC * dof_passive(d).z;
+        art[C.A_VLG + d] = on ? 1.0f : 0.0f;
+        any = any || (on && dof_passive(d).z >= 0.0f && scalar_dof(d));
+      }
+      art[C.A_AVL + tid] = any ? 1.0f : 0.0f;
+    }
     uint32_t n = 0u;
     for (uint32_t k = 0; k < ai.w; k++) {
       uint32_t d = ai.z + k;

@@ -296,7 +296,7 @@ void Oracle::art_dof_impulse(uint32_t a, uint32_t l, uint32_t r, float dl) {
   art[lo(l) + L_TAU + r] = dl;
   art_apply(a);
 }
-void Oracle::art_propagate(uint32_t a, bool /*vlim*/, bool rowsOn) {
+void Oracle::art_propagate(uint32_t a, bool vlim, bool rowsOn) {
   u4 ai = art_info(a);
   if (rowsOn) {
     uint32_t n = f2u(art[C.A_RLN + a]);
@@ -306,9 +306,16 @@ void Oracle::art_propagate(uint32_t a, bool /*vlim*/, bool rowsOn) {
       art_dof_rows(a, l, d - link_dof(l), d, false, true);
     }
   }
+  if (!(vlim && C.VLIM_ON == 1u && art[C.A_AVL + a] > 0.5f)) return;
+  for (uint32_t k = 0; k < ai.y; k++) {
+    uint32_t l = ai.x + k;
+    uint32_t t = link_type(l);
+    if (t != 1u && t != 0u && t != 6u) continue;  // revolute, prismatic, D6
+    for (uint32_t r = 0; r < link_ndof(l); r++) art_dof_rows(a, l, r, link_dof(l) + r, true, false);
+  }
 }
 // art_dof_rows (wgsl.js:3421-3468), joint friction and limit rows.
-void Oracle::art_dof_rows(uint32_t a, uint32_t l, uint32_t r, uint32_t d, bool /*vlim*/, bool rowsOn) {
+void Oracle::art_dof_rows(uint32_t a, uint32_t l, uint32_t r, uint32_t d, bool vlim, bool rowsOn) {
   float hinv = fmaxf_(art[C.A_HINV + d], 1e-12f);
   v4 pv = dof_passive(d);
   float fr = pv.y;
@@ -331,6 +338,11 @@ void Oracle::art_dof_rows(uint32_t a, uint32_t l, uint32_t r, uint32_t d, bool /
       art[C.A_LIM + 2u * d + side] = nl;
       art_dof_impulse(a, l, r, sg * (nl - lam));
     }
+  }
+  // Velocity limit (wgsl.js:3462-3467): a stateless push back onto |qd| <= limit, no bias.
+  if (vlim && pv.z >= 0.0f && art[C.A_VLG + d] > 0.5f) {
+    float over = aqd[d] - clampf(aqd[d], -pv.z, pv.z);
+    if (over != 0.0f) art_dof_impulse(a, l, r, (-over) / hinv);
   }
 }
 // body_motion (wgsl.js:3472-3489)

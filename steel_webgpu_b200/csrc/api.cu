@@ -143,7 +143,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
       {"FMODE", "friction_mode"}, {"ANG", "torsional/rolling friction"}, {"ANG_ART", "torsional/rolling friction"},
       {"TORS", "contact torsion"}, {"COMPL", "contact_compliance"}, {"NEST", "nesterov_momentum"},
       {"CTI", "row_schedule contact_then_internal"}, {"LONGEST_FIRST", "propagation_color_order longest_first"},
-      {"DRIVE_ROWS", "drive_mode rows"}, {"VLIM_ON", "enable_joint_velocity_limits"},
+      {"DRIVE_ROWS", "drive_mode rows"},
       {"JFL", "joint friction load coefficient"}, {"SLEEP", "enable_sleeping"}, {"VELITERS", "velocity_iterations"}};
   for (auto& u : unsupported)
     if (C.u(u[0]) != 0u) { why = std::string("unsupported solver option: ") + u[1]; return STEEL_E_UNSUPPORTED; }
@@ -157,13 +157,13 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
   K(SF_BODY) K(SF_SHAPE) K(SF_HAABB) K(SF_VERTS) K(SF_FPLANE) K(SF_LINK) K(SF_DOF) K(SF_PATH) K(SF_LOOP)
   K(SF_MIMIC) K(SF_CTRL) K(SU_HULL) K(SU_FACE) K(SU_FV) K(SU_HEDGE) K(SU_EDGE) K(SU_ART) K(SU_ACON)
   K(SU_FILTER) K(NB) K(NS) K(NA) K(NL) K(ND) K(NDA) K(JM) K(MAXPATH) K(MAXLP) K(NLOOP) K(NMIMIC) K(PATCH)
-  K(EXTRA) K(SHARED) K(FSHARED) K(REST) K(FSTART) K(TGT_HELD) K(CTRL_KIND) K(CTRL_A) K(CTRL_B) K(VLIM_FREE)
+  K(EXTRA) K(SHARED) K(FSHARED) K(REST) K(FSTART) K(TGT_HELD) K(CTRL_KIND) K(CTRL_A) K(CTRL_B) K(VLIM_FREE) K(VLIM_ON)
   K(FRICTION_COMBINE) K(RESTITUTION_COMBINE) K(NCOLW) K(NCOL) K(MAXP) K(MAXC) K(MAXU) K(WH) K(AH)
   K(MAXDENSE) K(ROWS) K(PO) K(DHDR) K(DPS)
 #undef K
 #define F(n) d.n = C.f(#n);
   F(F_ANCHOR_BETA) F(F_CFM) F(F_OMEGA) F(F_SPEC) F(F_GAP_GATE) F(F_FGAP) F(F_FSCALE) F(F_REST_SPEED) F(F_FR_MUT)
-  F(F_FR_MUR) F(F_BP_CELL) F(F_JL_GAP) F(F_JL_SPEED)
+  F(F_FR_MUR) F(F_BP_CELL) F(F_JL_GAP) F(F_JL_SPEED) F(F_VLIM_FRAC)
 #undef F
   if (d.NCOLW == 0u || d.NCOLW > 64u || d.NCOL != d.NCOLW * 32u) { why = "bad color table size"; return STEEL_E_INVALID; }
   if (d.MAXC == 0u || d.MAXP == 0u || d.WH == 0u || d.AH == 0u) { why = "zero capacity"; return STEEL_E_INVALID; }
@@ -194,7 +194,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
     put(d.A_FRIC, ND); put(d.A_HINV, ND);
     ao = (ao + 3) & ~(size_t)3;  // link blocks start on a 16-byte boundary (bulk copies)
     put(d.A_LINK, (size_t)(NL > 0 ? NL : 1) * 268); put(tmp, NB * 8 + ND);
-    put(d.A_VLG, ND + NB * 6); put(tmp, NA); put(d.A_LG, ND); put(d.A_RL, ND); put(d.A_RLN, NA);
+    put(d.A_VLG, ND + NB * 6); put(d.A_AVL, NA); put(d.A_LG, ND); put(d.A_RL, ND); put(d.A_RLN, NA);
     put(d.A_ULOAD, d.PATCH ? (size_t)MAXC : 0); put(d.A_DENSE, (size_t)d.MAXDENSE * d.DPS);
     s.art_floats = ao;
   }

@@ -562,6 +562,30 @@ __global__ void __launch_bounds__(PREP_THREADS, 4) k_prepare(BatchDev B) {
   // Joint-limit gating, listed joint rows, FK and factorisation per articulation.
   for (uint32_t a = tid; a < S.NA; a += nt) {
     uint4 ai = ar.info(a);
+    // Joint velocity limits (wgsl.js:1829-1854): scale the articulation's scalar dof speeds so the
+    // most exceeded limit is met, then mark the dofs near their limit (rows exist only there).
+    // Drive rows are unsupported, so no dof has the fused drive clamp.
+    if (S.VLIM_ON == 1u) {
+      float ratio = 1.0f;
+      for (uint32_t k = 0; k < ai.w; k++) {
+        uint32_t d = ai.z + k;
+        float vl = ar.dof_passive(d).z;
+        if (vl < 0.0f) continue;
+        float sp = fabsf(A[S.A_QD + d]);
+        if (sp > vl) ratio = fmn(ratio, vl / sp);
+      }
+      if (ratio < 1.0f)
+        for (uint32_t k = 0; k < ai.w; k++)
+          if (ar.scalar_dof(ai.z + k)) A[S.A_QD + ai.z + k] *= ratio;
+      bool any = false;
+      for (uint32_t k = 0; k < ai.w; k++) {
+        uint32_t d = ai.z + k;
+        bool on = fabsf(A[S.A_QD + d]) >= S.F_VLIM_FRAC * ar.dof_passive(d).z;
+        A[S.A_VLG + d] = on ? 1.0f : 0.0f;
+        any = any || (on && ar.dof_passive(d).z >= 0.0f && ar.scalar_dof(d));
+      }
+      A[S.A_AVL + a] = any ? 1.0f : 0.0f;
+    }
     uint32_t n = 0u;
     for (uint32_t k = 0; k < ai.w; k++) {
       uint32_t d = ai.z + k;

@@ -431,6 +431,26 @@ struct Solver {
       }
     }
   }
+  // Joint velocity limits after the contact impulses (wgsl.js:3413-3419, 3462-3467): a stateless
+  // push back onto |qd| <= limit for the marked dofs of revolute, prismatic and D6 links.
+  __device__ void vlim_rows(uint32_t a) const {
+    float* A = S.art;
+    if (A[S.A_AVL + a] <= 0.5f) return;
+    uint4 ai = ar.info(a);
+    for (uint32_t k = 0; k < ai.y; k++) {
+      uint32_t l = ai.x + k, t = ar.ltype(l);
+      if (t != 1u && t != 0u && t != 6u) continue;
+      for (uint32_t r = 0; r < ar.lndof(l); r++) {
+        uint32_t d = ar.ldof(l) + r;
+        float hinv = fmx(A[S.A_HINV + d], 1e-12f);
+        float4 pv = ar.dof_passive(d);
+        if (pv.z >= 0.0f && A[S.A_VLG + d] > 0.5f) {
+          float over = aqd[d] - clmp(aqd[d], -pv.z, pv.z);
+          if (over != 0.0f) { ar.LB[ar.lo(l) + L_TAU + r] = (-over) / hinv; ar.apply(a, aqd, tw); }
+        }
+      }
+    }
+  }
   // Displacement of world point x under body b's motion this substep (wgsl.js:3472-3489).
   __device__ f3 body_motion(int b, f3 x) const {
     if (b < 0) return sp3(0.0f);
@@ -487,7 +507,10 @@ struct Solver {
     if (tid == 0u)
       for (uint32_t u = wcs[S.NCOL]; u < wcs[S.NCOL + 1u]; u++) solve_slot(u, mode, it);
     __syncthreads();
-    for (uint32_t a = tid; a < S.NA; a += nt) contact_impulses(a);
+    for (uint32_t a = tid; a < S.NA; a += nt) {
+      contact_impulses(a);
+      if (S.VLIM_ON == 1u) vlim_rows(a);
+    }
     __syncthreads();
     if (S.VLIM_FREE == 1u) {
       for (uint32_t b = tid; b < S.NB; b += nt) {

@@ -69,3 +69,22 @@ def hull_bin(seed=11, n=160):
 def small_batch(seed=13, n=6):
     """Independent scenes of uneven size (the uneven-batch workload)."""
     return synth.uneven_batch(n_scenes=n, seed=seed, lo=8, hi=96, chain_lo=2, chain_hi=12)
+
+
+def vel_limited(seed=17):
+    """A 10-link revolute chain released from a steep angle with joint velocity limits of 2 rad/s
+    (enable_joint_velocity_limits), next to a PD-driven quadruped without limits."""
+    rng = np.random.default_rng(seed)
+    b = SceneBuilder(fps=240)
+    b.add_ground_plane(mu=0.7)
+    parent = -1
+    top = [0.0, 0.0, 2.5]
+    for k in range(10):
+        body = b.add_body(xform=[top[0], top[1], top[2] - 0.1 * (k + 0.5), 0, 0, 0, 1])
+        b.add_shape_capsule(body, radius=0.02, half_height=0.04, mass=float(0.1 * math.exp(rng.uniform(0.0, 2.0))))
+        b.add_joint_revolute(parent, body, axis=[0, 1, 0],
+                             parent_xform=[0, 0, -0.05, 0, 0, 0, 1] if parent >= 0 else top + [0, 0, 0, 1],
+                             child_xform=[0, 0, 0.05, 0, 0, 0, 1], q=[1.3] if k == 0 else [0.2], velocityLimit=2.0)
+        parent = body
+    synth._add_quadruped(b, rng, [1.5, 0.0, 0.9])
+    return b.finalize(solver=dict(enable_joint_velocity_limits=True))

@@ -15,8 +15,8 @@ from tests import scenes
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "oracle_fixtures.npz")
 REF_SCENES = "/root/reference/assets/scenes"
-UNSUPPORTED = ("FMODE", "ANG", "ANG_ART", "TORS", "COMPL", "NEST", "CTI", "LONGEST_FIRST", "DRIVE_ROWS", "VLIM_ON",
-               "JFL", "SLEEP", "VELITERS")
+UNSUPPORTED = ("FMODE", "ANG", "ANG_ART", "TORS", "COMPL", "NEST", "CTI", "LONGEST_FIRST", "DRIVE_ROWS", "JFL",
+               "SLEEP", "VELITERS")
 
 
 def test_trig_accuracy(oracle_lib):
@@ -126,8 +126,24 @@ def test_reference_scenes_load_and_pack(oracle_lib):
         assert pk.statF.size == pk.C["LEN_STATF4"] * 4 and pk.statU.size == pk.C["LEN_STATU"]
         if not any(pk.C.get(k, 0) for k in UNSUPPORTED):
             supported.append((name, pk))
-    assert len(supported) >= 5
+    assert len(supported) >= 15
     for name, pk in supported:
         o = oracle_lib.OracleSim(pk)
         o.step(5)
         assert np.isfinite(o.body_poses()).all(), name
+
+
+def test_joint_velocity_limits_hold(oracle_lib):
+    def peak(opts):
+        pk = pack(scenes.vel_limited(), opts=opts)
+        o = oracle_lib.OracleSim(pk)
+        m = 0.0
+        for _ in range(120):
+            o.step(1)
+            m = max(m, float(np.abs(o.read("art")[pk.C["A_QD"]:pk.C["A_QD"] + 10]).max()))
+        return pk.C["VLIM_ON"], m
+    on, limited = peak(None)
+    off, free = peak({"solver": {"enable_joint_velocity_limits": False}})
+    assert on == 1 and off == 0
+    assert limited < 2.05
+    assert free > 2.5

@@ -14,7 +14,7 @@ from tests import scenes
 pytestmark = pytest.mark.gpu
 
 SCENES = {"boxes": scenes.boxes, "mixed_prims": scenes.mixed_prims, "articulated": scenes.articulated,
-          "chains_and_quads": scenes.chains_and_quads, "hull_bin": scenes.hull_bin}
+          "chains_and_quads": scenes.chains_and_quads, "hull_bin": scenes.hull_bin, "vel_limited": scenes.vel_limited}
 
 
 def _pair_set(p):
