@@ -36,28 +36,34 @@ struct Art {
   const SceneDev& S;
   float* A;   // the scene's articulation buffer
   float* LB;  // link blocks: LB + lo(l) is link l's LBLK floats
-  __device__ Art(const SceneDev& s) : S(s), A(s.art), LB(s.art + s.A_LINK) {}
-  __device__ Art(const SceneDev& s, float* lb) : S(s), A(s.art), LB(lb) {}
+  // Static records and the dof stride, read once: the serial passes address them on every link.
+  RO<float4> LR, DR, BR;  // link (6 vec4), dof (5 vec4) and body (8 vec4) records
+  uint32_t JMc;
+  __device__ Art(const SceneDev& s)
+      : S(s), A(s.art), LB(s.art + s.A_LINK), LR(s.sf + s.SF_LINK), DR(s.sf + s.SF_DOF), BR(s.sf + s.SF_BODY),
+        JMc(s.JM) {}
+  __device__ Art(const SceneDev& s, float* lb)
+      : S(s), A(s.art), LB(lb), LR(s.sf + s.SF_LINK), DR(s.sf + s.SF_DOF), BR(s.sf + s.SF_BODY), JMc(s.JM) {}
 
-  __device__ float4 lrec(uint32_t l, uint32_t k) const { return S.sf[S.SF_LINK + l * 6u + k]; }
+  __device__ float4 lrec(uint32_t l, uint32_t k) const { return LR[l * 6u + k]; }
   __device__ uint32_t ltype(uint32_t l) const { return f2u(lrec(l, 0).x); }
   __device__ int lparent(uint32_t l) const { return f2i(lrec(l, 0).y); }
   __device__ uint32_t ldof(uint32_t l) const { return f2u(lrec(l, 0).z); }
   __device__ int lbody(uint32_t l) const { return f2i(lrec(l, 0).w); }
   __device__ uint32_t lndof(uint32_t l) const { return f2u(lrec(l, 1).w); }
   __device__ uint32_t lqs(uint32_t l) const { return f2u(lrec(l, 3).w); }
-  __device__ float4 dof_drive(uint32_t d) const { return S.sf[S.SF_DOF + d * 5u]; }
-  __device__ float4 dof_limit(uint32_t d) const { return S.sf[S.SF_DOF + d * 5u + 1u]; }
-  __device__ float4 dof_passive(uint32_t d) const { return S.sf[S.SF_DOF + d * 5u + 2u]; }
-  __device__ f3 dof_axis(uint32_t d) const { return v3(S.sf[S.SF_DOF + d * 5u + 3u]); }
-  __device__ bool scalar_dof(uint32_t d) const { return S.sf[S.SF_DOF + d * 5u + 2u].w > 0.5f; }
+  __device__ float4 dof_drive(uint32_t d) const { return DR[d * 5u]; }
+  __device__ float4 dof_limit(uint32_t d) const { return DR[d * 5u + 1u]; }
+  __device__ float4 dof_passive(uint32_t d) const { return DR[d * 5u + 2u]; }
+  __device__ f3 dof_axis(uint32_t d) const { return v3(DR[d * 5u + 3u]); }
+  __device__ bool scalar_dof(uint32_t d) const { return DR[d * 5u + 2u].w > 0.5f; }
   __device__ uint4 info(uint32_t a) const {
     RO<uint32_t> p = S.su + S.SU_ART + a * 4u;
     return make_uint4(p[0], p[1], p[2], p[3]);
   }
-  __device__ float bmass(int b) const { return S.sf[S.SF_BODY + (uint32_t)b * 8u + 1u].w; }
+  __device__ float bmass(int b) const { return BR[(uint32_t)b * 8u + 1u].w; }
   __device__ m3 binertia(int b) const {
-    RO<float4> o = S.sf + S.SF_BODY + (uint32_t)b * 8u;
+    RO<float4> o = BR + (uint32_t)b * 8u;
     return tr(mcols(v3(o[2]), v3(o[3]), v3(o[4])));
   }
   __device__ uint32_t lo(uint32_t l) const { return l * LBLK; }
@@ -77,7 +83,7 @@ struct Art {
   }
   __device__ SVec ldS(uint32_t l, uint32_t k) const { return ldsv(lo(l) + L_S + k * 6u); }
   __device__ SVec ldU(uint32_t l, uint32_t k) const { return ldsv(lo(l) + L_U + k * 6u); }
-  __device__ float ldDI(uint32_t l, uint32_t r, uint32_t c) const { return LB[lo(l) + L_DI + r * S.JM + c]; }
+  __device__ float ldDI(uint32_t l, uint32_t r, uint32_t c) const { return LB[lo(l) + L_DI + r * JMc + c]; }
   __device__ f3 link_r(uint32_t l) const {
     int par = lparent(l);
     if (par < 0) return sp3(0.0f);
@@ -141,7 +147,7 @@ struct Art {
       st3(L + L_POS, lp);
       st3(L + L_ROT, v3(lq));
       LB[L + L_ROT + 3u] = lq.w;
-      f3 com = lp + qrot(lq, v3(S.sf[S.SF_BODY + (uint32_t)f2i(r0.w) * 8u + 1u]));
+      f3 com = lp + qrot(lq, v3(BR[(uint32_t)f2i(r0.w) * 8u + 1u]));
       st3(L + L_COM, com);
       f3 aw = qrot(jq, axis);
       f3 rj = com - jp;
@@ -187,7 +193,7 @@ struct Art {
   // Drr holds D[r][r] = S_r . U_r on entry and gains the drive and damping terms.
   __device__ float dof_tau(uint32_t d, uint32_t qs, uint32_t r, float& Drr, const Params& P) const {
     // Every input is loaded first, so the loads overlap.
-    const float4 dr = dof_drive(d), pas = dof_passive(d), spr = S.sf[S.SF_DOF + d * 5u + 4u];
+    const float4 dr = dof_drive(d), pas = dof_passive(d), spr = DR[d * 5u + 4u];
     const float qd = A[S.A_QD + d], jf = A[S.A_JF + d], q = A[S.A_Q + qs + r];
     const float tgt = A[S.A_TGT + d], tv = A[S.A_TGTV + d];
     Drr += dr.x;
@@ -264,7 +270,7 @@ struct Art {
       stm(L + L_IA + 9u, mcols(sp3(0), sp3(0), sp3(0)));
       stm(L + L_IA + 18u, mcols(mf3(m, 0, 0), mf3(0, m, 0), mf3(0, 0, m)));
       SVec pa0 = crf(v, imul(L + L_IA, v));
-      if ((f2u(S.sf[S.SF_BODY + (uint32_t)b * 8u + 7u].w) & 2u) != 0u) pa0 = sadd(pa0, SVec{sp3(0.0f), m * g});
+      if ((f2u(BR[(uint32_t)b * 8u + 7u].w) & 2u) != 0u) pa0 = sadd(pa0, SVec{sp3(0.0f), m * g});
       pa0 = sadd(pa0, SVec{-btorque, -bforce});
       stsv(L + L_PA, pa0);
     }
