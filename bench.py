@@ -31,6 +31,7 @@ WORKLOADS = {
     # name: (generator kwargs, description)
     "uneven_batch_2048": dict(n_scenes=2048),
     "uneven_batch_256": dict(n_scenes=256),
+    "uneven_batch_512": dict(n_scenes=512),  # loaded case (several blocks per SM) for profiler captures
     "uneven_batch_64": dict(n_scenes=64),  # small case for profiler captures
 }
 

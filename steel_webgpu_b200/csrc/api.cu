@@ -1,6 +1,7 @@
 // Host side of the C ABI (include/steel_b200.h): batch construction from the reference's packed
 // scenes, one device arena per batch, the per-substep launch sequence (captured as a CUDA graph),
 // readback and user control.
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -115,7 +116,7 @@ struct steel_batch {
   bool use_graph = true;
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  size_t o_scenes, o_shape_scene, o_shape_local, o_tiles, o_pairs, o_pair_count, o_jobs, o_phase, o_ssc, o_active, o_err;
+  size_t o_scenes, o_shape_scene, o_shape_local, o_tiles, o_pairs, o_pair_count, o_jobs, o_phase, o_ssc, o_active, o_order, o_err;
   std::vector<uint32_t> shape_scene, shape_local;
   std::vector<uint4> tiles;
   // host-I/O staging (steel_step_io): packed targets/poses on the device and their offsets
@@ -130,6 +131,7 @@ struct steel_batch {
   std::vector<uint32_t> serve_mask;            // host copy of the device activity mask
   std::vector<Done> serve_done;
   uint32_t serve_admitted = 0, serve_max_active = 0;
+  std::vector<uint32_t> order_host;  // block order of the fused prepare + solve kernel
   uint64_t serve_next_id = 1;
   bool serve_on = false;
 };
@@ -291,8 +293,7 @@ void enqueue_substeps(steel_batch* b, cudaStream_t st) {
     launch_broad(bd, st);
     launch_narrow(bd, b->narrow_blocks, st);
     launch_csort(bd, b->sort_keys, st);
-    launch_prepare(bd, st);
-    launch_solve(bd, st);
+    launch_prepare_solve(bd, st);
   }
   launch_frame_end(bd, st);
 }
@@ -379,6 +380,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   b->o_phase = L.take(8ull * n);
   b->o_ssc = L.take(8ull * n);
   b->o_active = L.take(4ull * n);
+  b->o_order = L.take(4ull * n);
   b->o_err = L.take(4);
   std::vector<uint64_t> tgt_off(n), pose_off(n);
   for (uint32_t i = 0; i < n; i++) {
@@ -444,12 +446,26 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   bd.phase = at<double>(A, b->o_phase);
   bd.substep_count = at<unsigned long long>(A, b->o_ssc);
   bd.active = at<uint32_t>(A, b->o_active);
+  bd.order = at<uint32_t>(A, b->o_order);
+  {
+    // Fused prepare + solve blocks take the scenes longest first (chain length, then bodies), so
+    // short scenes fill the end of the launch.
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+      const SceneDev &a = b->sc[x].d, &c = b->sc[y].d;
+      return a.MAXLP != c.MAXLP ? a.MAXLP > c.MAXLP : a.NB > c.NB;
+    });
+    b->order_host = order;
+    CU(cudaMemcpyAsync(A + b->o_order, b->order_host.data(), 4ull * n, cudaMemcpyHostToDevice, st));
+  }
   CU(cudaMemsetAsync(A + b->o_active, 1, 4ull * n, st));  // every scene steps (nonzero words)
   bd.error = at<uint32_t>(A, b->o_err);
   bd.prep_smem = (uint32_t)prep_smem;
   bd.solve_smem = (uint32_t)solve_smem;
   CU(configure_prepare(prep_smem));
   CU(configure_solve(solve_smem));
+  CU(configure_prepare_solve(std::max(prep_smem, solve_smem)));
   CU(cudaMemcpyAsync(bd.scenes, dev.data(), sizeof(SceneDev) * n, cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync((void*)bd.shape_scene, b->shape_scene.data(), 4 * b->shape_scene.size(), cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync((void*)bd.shape_local, b->shape_local.data(), 4 * b->shape_local.size(), cudaMemcpyHostToDevice, st));

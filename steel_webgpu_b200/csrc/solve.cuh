@@ -1,0 +1,789 @@
+#pragma once
+// Solve of one scene by one block (the body of k_solve and of the fused k_prepare_solve).
+//
+// Follows the reference's solve pass (packages/steel-webgpu/src/wgsl.js:2501-3891) on its
+// default option set: free-body gravity, wrench and gyroscopic prologue (wgsl.js:3647-3675),
+// the slot table (wgsl.js:3679-3686), the warm-apply sweep and `iterations` colored
+// Gauss-Seidel sweeps (wgsl.js:3559-3611) of fixed-normal contact rows with friction anchors
+// (wgsl.js:3033-3231, 2952-3011), dense same-articulation rows (wgsl.js:3306-3377), exact
+// Featherstone impulse propagation and joint limit / friction rows after each sweep
+// (wgsl.js:3380-3468), the warm-start table (wgsl.js:3737-3767), integration of bodies and
+// joints with FK (wgsl.js:3768-3828) and the friction-anchor advance (wgsl.js:3832-3878).
+// Rows of one color touch disjoint bodies, so a color's rows run in parallel across the block
+// with one barrier per color; the overflow color runs serially in contact order.
+#include "art.cuh"
+#include "batch.cuh"
+#include "bulk.cuh"
+
+namespace steel {
+
+static constexpr uint32_t AVN_S = 14u;
+
+struct Solver {
+  const SceneDev& S;
+  const Params& P;
+  Art ar;
+  float4* tw;
+  float4* imp;
+  float* aqd;
+  __device__ Solver(const SceneDev& s, const Params& p, float* lb, float4* tw_, float4* imp_, float* aqd_)
+      : S(s), P(p), ar(s, lb), tw(tw_), imp(imp_), aqd(aqd_) {}
+
+  __device__ uint32_t bkind(int b) const { return f2u(S.sf[S.SF_BODY + (uint32_t)b * 8u].y); }
+  __device__ uint32_t bflags(int b) const { return b < 0 ? 0u : f2u(S.sf[S.SF_BODY + (uint32_t)b * 8u + 7u].w); }
+  __device__ float bradius(int b) const { return b < 0 ? 1e30f : S.sf[S.SF_BODY + (uint32_t)b * 8u + 2u].w; }
+  __device__ m3 binv_inertia(int b) const {
+    RO<float4> o = S.sf + S.SF_BODY + (uint32_t)b * 8u;
+    return tr(mcols(v3(o[5]), v3(o[6]), v3(o[7])));
+  }
+  __device__ void load_tw(int b, f3 out[2]) const {
+    if (b < 0) { out[0] = sp3(0.0f); out[1] = sp3(0.0f); return; }
+    out[0] = v3(tw[(uint32_t)b * 2u]);
+    out[1] = v3(tw[(uint32_t)b * 2u + 1u]);
+  }
+  __device__ void add_imp(int b, f3 f, f3 t) const {
+    if (b < 0 || bkind(b) != 2u) return;
+    imp[(uint32_t)b * 2u] = add4(imp[(uint32_t)b * 2u], mf4(f, 0.0f));
+    imp[(uint32_t)b * 2u + 1u] = add4(imp[(uint32_t)b * 2u + 1u], mf4(t, 0.0f));
+  }
+  static __device__ m3 inverse3(const m3& m) {
+    f3 a = m.c[0], b = m.c[1], c = m.c[2];
+    f3 r0 = cross(b, c), r1 = cross(c, a), r2 = cross(a, b);
+    float det = dot(a, r0);
+    return mscl(1.0f / det, tr(mcols(r0, r1, r2)));
+  }
+  // Energy-preserving Cayley microsteps of the free-body gyroscopic term (wgsl.js:2543-2562).
+  static __device__ f3 gyro(const m3& inertia, f3 u0, float dt) {
+    m3 a = mscl(1.0f / fmx(inertia.c[0].x, fmx(inertia.c[1].y, inertia.c[2].z)), inertia);
+    m3 inv = inverse3(a);
+    float speed = sqrtf(fmx(dot(u0, mul(a, u0)) * ((inv.c[0].x + inv.c[1].y) + inv.c[2].z), 0.0f));
+    uint32_t n = f2u(clmp(ceilf((2.0f * fabsf(dt)) * speed), 1.0f, 32.0f));
+    float h = dt / (float)n;
+    f3 w = u0;
+    for (uint32_t m = 0; m < n; m++) {
+      f3 u = w;
+      float energy = dot(u, mul(a, u));
+      for (uint32_t it = 0; it < 8u; it++) {
+        m3 Sk = mscl(0.5f * h, skew(mul(a, 0.5f * (u + w))));
+        f3 c = mul(inverse3(msub(a, Sk)), mul(madd(a, Sk), u));
+        f3 d = c - w;
+        w = c;
+        if (dot(d, mul(a, d)) <= 1e-12f * energy) break;
+      }
+    }
+    return w;
+  }
+  // Friction pair update on its 2x2 block with a disk bound (wgsl.js:2952-3011).
+  static __device__ f2 friction_pair(float a0, float c0, float d0, float r0, float r1, float old0, float old1,
+                                     float radius, float omega) {
+    if (radius <= 0.0f) return mf2(0.0f, 0.0f);
+    float scale = fmx(fmx(a0, d0), 1e-20f);
+    float a = a0 / scale, c = c0 / scale, d = d0 / scale;
+    float largest = 0.5f * ((a + d) + sqrtf((a - d) * (a - d) + (4.0f * c) * c));
+    float smallest = largest > 0.0f ? fmx((a * d - c * c) / largest, 0.0f) : 0.0f;
+    float vx = c, vy = largest - a;
+    if (a >= d) { vx = largest - d; vy = c; }
+    float vn = sqrtf(vx * vx + vy * vy);
+    if (vn > 0.0f) { vx /= vn; vy /= vn; } else { vx = 1.0f; vy = 0.0f; }
+    float r0r = (vx * r0 + vy * r1) / scale;
+    float r1r = ((-vy) * r0 + vx * r1) / scale;
+    f2 res = mf2(old0, old1);
+    bool sticking = false;
+    if (largest > 0.0f && (smallest > 0.0f || r1r == 0.0f)) {
+      float dx = r0r / largest;
+      float dy = smallest > 0.0f ? r1r / smallest : 0.0f;
+      res = mf2(old0 - (vx * dx - vy * dy), old1 - (vy * dx + vx * dy));
+      sticking = len(res) <= radius;
+    }
+    if (!sticking) {
+      float on = len(mf2(old0, old1)), rn = len(mf2(r0, r1));
+      if (on > 0.0f && on <= radius && radius - on <= 2e-7f * radius && r0 * old0 + r1 * old1 <= 0.0f &&
+          fabsf(r0 * old1 - r1 * old0) <= (2e-7f * on) * rn)
+        return mf2(old0, old1);
+      float ox = vx * old0 + vy * old1, oy = (-vy) * old0 + vx * old1;
+      float b0 = largest * ox - r0r, b1 = smallest * oy - r1r;
+      float x = 0.0f, y = 0.0f;
+      float hi = sqrtf(b0 * b0 + b1 * b1) / radius;
+      if (hi > 0.0f) {
+        float lo = fmx(fmx(hi - largest, fabsf(b1) / radius - smallest), 0.0f);
+        float alpha = lo;
+        bool done = false;
+        for (uint32_t it = 0; it < 8u; it++) {
+          float i0 = 1.0f / (largest + alpha);
+          float i1 = smallest + alpha > 0.0f ? 1.0f / (smallest + alpha) : 0.0f;
+          float tx = ox - (r0r + alpha * ox) * i0, ty = oy - (r1r + alpha * oy) * i1;
+          float nr = sqrtf(tx * tx + ty * ty);
+          if (fabsf(nr - radius) <= 2e-7f * radius || (alpha == 0.0f && nr <= radius)) { x = tx; y = ty; done = true; break; }
+          if (nr > radius) lo = alpha; else hi = alpha;
+          float slope = (tx * tx) * i0 + (ty * ty) * i1;
+          float cand = alpha;
+          if (slope > 0.0f) cand = alpha + (((nr / radius - 1.0f) * nr) * nr) / slope;
+          alpha = (cand > lo && cand < hi) ? cand : 0.5f * (lo + hi);
+        }
+        if (!done) {
+          for (uint32_t it = 0; it < 24u; it++) {
+            alpha = 0.5f * (lo + hi);
+            if (len(mf2(b0 / (largest + alpha), b1 / (smallest + alpha))) > radius) lo = alpha; else hi = alpha;
+          }
+          x = b0 / (largest + hi);
+          y = b1 / (smallest + hi);
+        }
+      }
+      res = mf2((old0 + vx * (x - ox)) - vy * (y - oy), (old1 + vy * (x - ox)) + vx * (y - oy));
+    }
+    f2 old = mf2(old0, old1);
+    f2 relaxed = old + omega * (res - old);
+    float m = len(relaxed);
+    return m > radius ? relaxed * (radius / m) : relaxed;
+  }
+
+  // One contact row of unit us (wgsl.js:3033-3231, default option set). mode 0 applies the warm
+  // impulses, mode 1 solves.
+  __device__ void solve_row(uint32_t us, uint32_t row, int a, int b, uint32_t mode, uint32_t it) const {
+    const uint32_t ROWS = S.ROWS, PO = S.PO;
+    float4* rows = S.rows;
+    f3 ta[2], tb[2];
+    load_tw(a, ta);
+    load_tw(b, tb);
+    uint32_t o = row * ROWS;
+    float4 r0 = rows[o], r1 = rows[o + 1u], r2 = rows[o + 2u];
+    f3 ra = v3(rows[o + 3u]), rb = v3(rows[o + 4u]);
+    f3 n = v3(r0), t1 = v3(r1), t2 = v3(r2);
+    float4 lam = rows[o + 6u];
+    if (mode == 0u) {
+      float dn = lam.x, dt1 = lam.y, dt2 = lam.z;
+      for (uint32_t r = 0; r < 3u; r++) {
+        float d = r == 0u ? dn : (r == 1u ? dt1 : dt2);
+        ta[0] += v3(rows[o + 7u + r * 4u]) * d; ta[1] += v3(rows[o + 8u + r * 4u]) * d;
+        tb[0] += v3(rows[o + 9u + r * 4u]) * d; tb[1] += v3(rows[o + 10u + r * 4u]) * d;
+      }
+      f3 fra = ra, frb = rb;
+      if (S.EXTRA == 1u) { fra = v3(rows[o + PO]); frb = v3(rows[o + PO + 1u]); }
+      f3 fn_ = n * dn, ft = t1 * dt1 + t2 * dt2;
+      add_imp(a, -fn_ - ft, -cross(ra, fn_) - cross(fra, ft));
+      add_imp(b, fn_ + ft, cross(rb, fn_) + cross(frb, ft));
+    } else {
+      f3 vrel = (tb[0] + cross(tb[1], rb)) - (ta[0] + cross(ta[1], ra));
+      float jv = dot(n, vrel);
+      float w = rows[o + 5u].w;
+      float res = jv + r1.w;
+      float nl = fmx(lam.x + S.F_OMEGA * ((((-res) * r0.w) * w) - (1.0f - w) * lam.x), 0.0f);
+      float dn = nl - lam.x;
+      lam.x = nl;
+      ta[0] += v3(rows[o + 7u]) * dn; ta[1] += v3(rows[o + 8u]) * dn;
+      tb[0] += v3(rows[o + 9u]) * dn; tb[1] += v3(rows[o + 10u]) * dn;
+      add_imp(a, -n * dn, -cross(ra, n * dn));
+      add_imp(b, n * dn, cross(rb, n * dn));
+      f3 fra = ra, frb = rb;
+      float lim = r2.w * nl;
+      f2 bias = mf2(0.0f, 0.0f);
+      float role = 1.0f;
+      if (S.EXTRA == 1u) {
+        role = rows[o + PO].w;
+        if (S.PATCH == 1u && role != 1.0f) S.art[S.A_ULOAD + us] += dn;
+        fra = v3(rows[o + PO]);
+        frb = v3(rows[o + PO + 1u]);
+        if (S.PATCH == 1u && role == 2.0f) {
+          float load = S.art[S.A_ULOAD + us];
+          lim = r2.w * load;
+          f3 e = v3(rows[o + PO + 2u]);
+          bias = (S.F_ANCHOR_BETA * mf2(dot(t1, e), dot(t2, e))) / P.dt;
+          rows[o + PO + 2u].w = lim;
+        }
+      }
+      if (it < S.FSTART) { lam.y = 0.0f; lam.z = 0.0f; }
+      if (role != 0.0f && it >= S.FSTART) {
+        f3 vr2 = (tb[0] + cross(tb[1], frb)) - (ta[0] + cross(ta[1], fra));
+        float4 ki = rows[o + 5u];
+        float v1 = dot(t1, vr2) + bias.x, v2_ = dot(t2, vr2) + bias.y;
+        float kd = ki.x * ki.z - ki.y * ki.y;
+        f2 lt = friction_pair(ki.z / kd, -ki.y / kd, ki.x / kd, v1, v2_, lam.y, lam.z, lim, S.F_OMEGA);
+        float dt1 = lt.x - lam.y, dt2 = lt.y - lam.z;
+        lam.y = lt.x;
+        lam.z = lt.y;
+        ta[0] += v3(rows[o + 11u]) * dt1 + v3(rows[o + 15u]) * dt2;
+        ta[1] += v3(rows[o + 12u]) * dt1 + v3(rows[o + 16u]) * dt2;
+        tb[0] += v3(rows[o + 13u]) * dt1 + v3(rows[o + 17u]) * dt2;
+        tb[1] += v3(rows[o + 14u]) * dt1 + v3(rows[o + 18u]) * dt2;
+        f3 f = t1 * dt1 + t2 * dt2;
+        add_imp(a, -f, -cross(fra, f));
+        add_imp(b, f, cross(frb, f));
+      }
+      rows[o + 6u] = lam;
+    }
+    if (a >= 0) { tw[(uint32_t)a * 2u] = mf4(ta[0], 0.0f); tw[(uint32_t)a * 2u + 1u] = mf4(ta[1], 0.0f); }
+    if (b >= 0) { tw[(uint32_t)b * 2u] = mf4(tb[0], 0.0f); tw[(uint32_t)b * 2u + 1u] = mf4(tb[1], 0.0f); }
+  }
+  __device__ void solve_slot(uint32_t u, uint32_t mode, uint32_t it) const {
+    float4 sl = S.slots[2u * u];
+    solve_row(f2u(sl.y), f2u(sl.x), f2i(sl.z), f2i(sl.w), mode, it);
+  }
+
+  // subgroupAdd over the warp (wgsl.js:3305, subgroups on), pinned to an xor butterfly over lane
+  // offsets 16, 8, 4, 2, 1. IEEE addition commutes, so every lane ends with the same bits.
+  static __device__ float lane_sum(float x) {
+    for (uint32_t off = 16u; off > 0u; off >>= 1u) x += __shfl_xor_sync(0xffffffffu, x, off);
+    return x;
+  }
+  // Dense same-articulation rows of articulation a (wgsl.js:3306-3364), one warp: lane l owns
+  // dofs l, l + 32, ... (so lanes never touch each other's qd entries) and its partial sums
+  // are combined with lane_sum. Each lane first loads its slice of the row (J and Y rows of its
+  // dofs, up to DENSE_REG of them) into registers. Called by all 32 lanes; returns whether a
+  // row belongs to a.
+  static constexpr uint32_t DENSE_REG = 2u;  // articulations of up to 64 dofs keep rows in registers
+  __device__ bool dense(uint32_t a, uint32_t mode, uint32_t it, uint32_t ph, uint32_t lane) const {
+    const uint32_t NDA = S.NDA, DHDR = S.DHDR, DPS = S.DPS;
+    float* A = S.art;
+    uint32_t nd = min(S.sched[S.S_META + 3u], S.MAXDENSE);
+    uint4 ai = ar.info(a);
+    if (ai.w > 32u * DENSE_REG) return dense_wide(a, mode, it, ph, lane, nd, ai);
+    float* q = aqd + ai.z;
+    bool touched = false;
+    for (uint32_t i = 0; i < nd; i++) {
+      uint32_t o = S.A_DENSE + i * DPS;
+      if (f2u(A[o]) != a) continue;
+      touched = true;
+      uint32_t jo = o + DHDR, yo = o + DHDR + 3u * NDA;
+      float J[3][DENSE_REG], Y[3][DENSE_REG];
+#pragma unroll
+      for (uint32_t j = 0; j < DENSE_REG; j++) {
+        uint32_t k = lane + 32u * j;
+        bool v = k < ai.w;
+#pragma unroll
+        for (uint32_t r = 0; r < 3u; r++) {
+          J[r][j] = v ? A[jo + r * NDA + k] : 0.0f;
+          Y[r][j] = v ? A[yo + r * NDA + k] : 0.0f;
+        }
+      }
+      const float m3_ = A[o + 3u], m4 = A[o + 4u], m5 = A[o + 5u], m6 = A[o + 6u], m7 = A[o + 7u], m8 = A[o + 8u];
+      const float nbil = A[o + 21u], m22 = A[o + 22u], m23 = A[o + 23u], m24 = A[o + 24u];
+      f3 lam = mf3(A[o + 9u], A[o + 10u], A[o + 11u]);
+      if ((nbil > 0.5f) == (ph == 1u) && ph != 0u) continue;
+      if (nbil > 0.5f) {
+        if (mode == 0u) continue;
+        f3 nlam = lam;
+        const uint32_t nr = f2u(nbil);
+#pragma unroll
+        for (uint32_t r = 0; r < 3u; r++) {
+          if (r >= nr) break;
+          float part = 0.0f;
+#pragma unroll
+          for (uint32_t j = 0; j < DENSE_REG; j++) {
+            uint32_t k = lane + 32u * j;
+            if (k < ai.w) part += J[r][j] * q[k];
+          }
+          float jv = lane_sum(part);
+          float rhs = r == 0u ? m4 : (r == 1u ? m22 : m23);
+          float dl = ((-S.F_OMEGA) * (jv + rhs)) * A[o + 5u + r];
+          setc(nlam, (int)r, comp(nlam, (int)r) + dl);
+#pragma unroll
+          for (uint32_t j = 0; j < DENSE_REG; j++) {
+            uint32_t k = lane + 32u * j;
+            if (k < ai.w) q[k] += Y[r][j] * dl;
+          }
+        }
+        if (lane == 0u) { A[o + 9u] = nlam.x; A[o + 10u] = nlam.y; A[o + 11u] = nlam.z; }
+        continue;
+      }
+      if (mode == 0u) {
+#pragma unroll
+        for (uint32_t j = 0; j < DENSE_REG; j++) {
+          uint32_t k = lane + 32u * j;
+          if (k < ai.w) q[k] += (Y[0][j] * lam.x + Y[1][j] * lam.y) + Y[2][j] * lam.z;
+        }
+        continue;
+      }
+      float part = 0.0f;
+#pragma unroll
+      for (uint32_t j = 0; j < DENSE_REG; j++) {
+        uint32_t k = lane + 32u * j;
+        if (k < ai.w) part += J[0][j] * q[k];
+      }
+      float jv = lane_sum(part);
+      float nl = fmx(lam.x + S.F_OMEGA * ((((-(jv + m4)) * m5) * m24) - (1.0f - m24) * lam.x), 0.0f);
+      float dn = nl - lam.x;
+      float p1 = 0.0f, p2 = 0.0f;
+#pragma unroll
+      for (uint32_t j = 0; j < DENSE_REG; j++) {
+        uint32_t k = lane + 32u * j;
+        if (k < ai.w) {
+          q[k] += Y[0][j] * dn;
+          p1 += J[1][j] * q[k];
+          p2 += J[2][j] * q[k];
+        }
+      }
+      float s1 = lane_sum(p1), s2 = lane_sum(p2);
+      float lim = it < S.FSTART ? 0.0f : m3_ * nl;
+      float kd = m6 * m8 - m7 * m7;
+      f2 lt = friction_pair(m8 / kd, -m7 / kd, m6 / kd, s1, s2, lam.y, lam.z, lim, S.F_OMEGA);
+      float d1 = lt.x - lam.y, d2 = lt.y - lam.z;
+#pragma unroll
+      for (uint32_t j = 0; j < DENSE_REG; j++) {
+        uint32_t k = lane + 32u * j;
+        if (k < ai.w) q[k] += Y[1][j] * d1 + Y[2][j] * d2;
+      }
+      if (lane == 0u) { A[o + 9u] = nl; A[o + 10u] = lt.x; A[o + 11u] = lt.y; }
+    }
+    return touched;
+  }
+  // The same for articulations of more than 32 * DENSE_REG dofs, reading rows as it goes.
+  __device__ bool dense_wide(uint32_t a, uint32_t mode, uint32_t it, uint32_t ph, uint32_t lane, uint32_t nd,
+                             uint4 ai) const {
+    const uint32_t NDA = S.NDA, DHDR = S.DHDR, DPS = S.DPS;
+    float* A = S.art;
+    bool touched = false;
+    for (uint32_t i = 0; i < nd; i++) {
+      uint32_t o = S.A_DENSE + i * DPS;
+      if (f2u(A[o]) != a) continue;
+      touched = true;
+      uint32_t jo = o + DHDR, yo = o + DHDR + 3u * NDA;
+      f3 lam = mf3(A[o + 9u], A[o + 10u], A[o + 11u]);
+      if ((A[o + 21u] > 0.5f) == (ph == 1u) && ph != 0u) continue;
+      if (A[o + 21u] > 0.5f) {
+        if (mode == 0u) continue;
+        f3 nlam = lam;
+        for (uint32_t r = 0; r < f2u(A[o + 21u]); r++) {
+          float part = 0.0f;
+          for (uint32_t k = lane; k < ai.w; k += 32u) part += A[jo + r * NDA + k] * aqd[ai.z + k];
+          float jv = lane_sum(part);
+          float rhs = r == 0u ? A[o + 4u] : (r == 1u ? A[o + 22u] : A[o + 23u]);
+          float dl = ((-S.F_OMEGA) * (jv + rhs)) * A[o + 5u + r];
+          setc(nlam, (int)r, comp(nlam, (int)r) + dl);
+          for (uint32_t k = lane; k < ai.w; k += 32u) aqd[ai.z + k] += A[yo + r * NDA + k] * dl;
+        }
+        if (lane == 0u) { A[o + 9u] = nlam.x; A[o + 10u] = nlam.y; A[o + 11u] = nlam.z; }
+        continue;
+      }
+      if (mode == 0u) {
+        for (uint32_t k = lane; k < ai.w; k += 32u)
+          aqd[ai.z + k] += (A[yo + k] * lam.x + A[yo + NDA + k] * lam.y) + A[yo + 2u * NDA + k] * lam.z;
+        continue;
+      }
+      float part = 0.0f;
+      for (uint32_t k = lane; k < ai.w; k += 32u) part += A[jo + k] * aqd[ai.z + k];
+      float jv = lane_sum(part);
+      float w = A[o + 24u];
+      float nl = fmx(lam.x + S.F_OMEGA * ((((-(jv + A[o + 4u])) * A[o + 5u]) * w) - (1.0f - w) * lam.x), 0.0f);
+      float dn = nl - lam.x;
+      float p1 = 0.0f, p2 = 0.0f;
+      for (uint32_t k = lane; k < ai.w; k += 32u) {
+        aqd[ai.z + k] += A[yo + k] * dn;
+        p1 += A[jo + NDA + k] * aqd[ai.z + k];
+        p2 += A[jo + 2u * NDA + k] * aqd[ai.z + k];
+      }
+      float s1 = lane_sum(p1), s2 = lane_sum(p2);
+      float lim = it < S.FSTART ? 0.0f : A[o + 3u] * nl;
+      float kd = A[o + 6u] * A[o + 8u] - A[o + 7u] * A[o + 7u];
+      f2 lt = friction_pair(A[o + 8u] / kd, -A[o + 7u] / kd, A[o + 6u] / kd, s1, s2, lam.y, lam.z, lim, S.F_OMEGA);
+      float d1 = lt.x - lam.y, d2 = lt.y - lam.z;
+      for (uint32_t k = lane; k < ai.w; k += 32u) aqd[ai.z + k] += A[yo + NDA + k] * d1 + A[yo + 2u * NDA + k] * d2;
+      if (lane == 0u) { A[o + 9u] = nl; A[o + 10u] = lt.x; A[o + 11u] = lt.y; }
+    }
+    return touched;
+  }
+  // Exact articulation update from the contact impulses on its links (wgsl.js:3380-3394).
+  __device__ void contact_impulses(uint32_t a) const {
+    uint4 ai = ar.info(a);
+    bool hit = false;
+    for (uint32_t k = 0; k < ai.y; k++) {
+      uint32_t l = ai.x + k;
+      uint32_t b = (uint32_t)ar.lbody(l);
+      f3 f = v3(imp[b * 2u]), t = v3(imp[b * 2u + 1u]);
+      if (nonzero(f) || nonzero(t)) {
+        hit = true;
+        ar.stsv(ar.lo(l) + L_P, SVec{-t, -f});
+        imp[b * 2u] = make_float4(0, 0, 0, 0);
+        imp[b * 2u + 1u] = make_float4(0, 0, 0, 0);
+      }
+    }
+    if (hit) ar.apply(a, aqd, tw);
+  }
+  // Joint friction and limit rows over the dofs listed in prepare (wgsl.js:3404-3468).
+  __device__ void joint_rows(uint32_t a) const {
+    float* A = S.art;
+    uint4 ai = ar.info(a);
+    uint32_t n = f2u(A[S.A_RLN + a]);
+    for (uint32_t i = 0; i < n; i++) {
+      uint32_t d = f2u(A[S.A_RL + ai.z + i]);
+      uint32_t l = f2u(ar.dof_limit(d).w);
+      uint32_t r = d - ar.ldof(l);
+      float hinv = fmx(A[S.A_HINV + d], 1e-12f);
+      float fr = ar.dof_passive(d).y;
+      if (fr > 0.0f) {
+        float lam = A[S.A_FRIC + d];
+        float nl = clmp(lam - (S.F_OMEGA * aqd[d]) / hinv, -fr * P.dt, fr * P.dt);
+        if (nl != lam) { A[S.A_FRIC + d] = nl; ar.LB[ar.lo(l) + L_TAU + r] = nl - lam; ar.apply(a, aqd, tw); }
+      }
+      float4 lim = ar.dof_limit(d);
+      if (A[S.A_LG + d] > 0.5f) {
+        float q = A[S.A_Q + ar.lqs(l) + r];
+        for (uint32_t side = 0; side < 2u; side++) {
+          float sg = side == 0u ? 1.0f : -1.0f;
+          float gap = side == 0u ? q - lim.x : lim.y - q;
+          float lam = A[S.A_LIM + 2u * d + side];
+          float rhs = gap / P.dt;
+          if (gap < 0.0f) rhs = fmx((P.beta * gap) / P.dt, -P.max_depen);
+          float nl = fmx(lam - (S.F_OMEGA * (sg * aqd[d] + rhs)) / hinv, 0.0f);
+          if (nl == lam) continue;
+          A[S.A_LIM + 2u * d + side] = nl;
+          ar.LB[ar.lo(l) + L_TAU + r] = sg * (nl - lam);
+          ar.apply(a, aqd, tw);
+        }
+      }
+    }
+  }
+  // Joint velocity limits after the contact impulses (wgsl.js:3413-3419, 3462-3467): a stateless
+  // push back onto |qd| <= limit for the marked dofs of revolute, prismatic and D6 links.
+  __device__ void vlim_rows(uint32_t a) const {
+    float* A = S.art;
+    if (A[S.A_AVL + a] <= 0.5f) return;
+    uint4 ai = ar.info(a);
+    for (uint32_t k = 0; k < ai.y; k++) {
+      uint32_t l = ai.x + k, t = ar.ltype(l);
+      if (t != 1u && t != 0u && t != 6u) continue;
+      for (uint32_t r = 0; r < ar.lndof(l); r++) {
+        uint32_t d = ar.ldof(l) + r;
+        float hinv = fmx(A[S.A_HINV + d], 1e-12f);
+        float4 pv = ar.dof_passive(d);
+        if (pv.z >= 0.0f && A[S.A_VLG + d] > 0.5f) {
+          float over = aqd[d] - clmp(aqd[d], -pv.z, pv.z);
+          if (over != 0.0f) { ar.LB[ar.lo(l) + L_TAU + r] = (-over) / hinv; ar.apply(a, aqd, tw); }
+        }
+      }
+    }
+  }
+  // Displacement of world point x under body b's motion this substep (wgsl.js:3472-3489).
+  __device__ f3 body_motion(int b, f3 x) const {
+    if (b < 0) return sp3(0.0f);
+    f3 p0 = v3(S.ppos[b]), p1 = v3(S.pos[b]);
+    float4 q0 = S.prot[b], q1 = S.rot[b];
+    float4 r = qmul(q1, qconj(q0));
+    if (r.w < 0.0f) r = neg4(r);
+    float sn = len(v3(r));
+    f3 ang = 2.0f * v3(r);
+    f3 trv = p1 - p0;
+    f3 lin = trv;
+    if (sn > 1e-6f) {
+      float half = fatan2(sn, r.w);
+      f3 axis = v3(r) / sn;
+      ang = (2.0f * half) * axis;
+      float scv = (half * r.w) / sn;
+      lin = scv * trv + ((1.0f - scv) * dot(axis, trv)) * axis;
+    }
+    return lin + cross(ang, x - 0.5f * (p0 + p1));
+  }
+
+  // Dense rows of every articulation, one warp each, then the twists of the articulations they
+  // moved (wgsl.js:3366-3377). Articulations share no qd, rows or links, so each warp goes on to
+  // its next articulation without a block barrier.
+  __device__ void dense_phase(uint32_t mode, uint32_t it, uint32_t ph) const {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5u, nw = blockDim.x >> 5u;
+    for (uint32_t a = warp; a < S.NA; a += nw) {
+      bool touched = dense(a, mode, it, ph, lane);
+      __syncwarp();
+      if (lane == 0u && touched) ar.twists(a, aqd, tw);
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+  // One sweep (wgsl.js:3559-3611).
+  __device__ void sweep(uint32_t mode, uint32_t ncol, uint32_t it, const uint32_t* wcs, uint32_t nu) const {
+    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    for (uint32_t a = tid; a < S.NA; a += nt) joint_rows(a);
+    if (S.PATCH == 1u && mode == 1u) {
+      for (uint32_t us = tid; us < nu; us += nt) {
+        uint32_t s0 = S.sched[S.S_USTART + us];
+        float load = 0.0f;
+        for (uint32_t m = s0; m < s0 + S.sched[S.S_USIZE + us]; m++)
+          if (S.rows[m * S.ROWS + S.PO].w != 1.0f) load += S.rows[m * S.ROWS + 6u].x;
+        S.art[S.A_ULOAD + us] = load;
+      }
+    }
+    __syncthreads();
+    dense_phase(1u, it, 0u);
+    for (uint32_t c = 0; c < ncol; c++) {
+      for (uint32_t u = wcs[c] + tid; u < wcs[c + 1u]; u += nt) solve_slot(u, mode, it);
+      __syncthreads();
+    }
+    if (tid == 0u)
+      for (uint32_t u = wcs[S.NCOL]; u < wcs[S.NCOL + 1u]; u++) solve_slot(u, mode, it);
+    __syncthreads();
+    for (uint32_t a = tid; a < S.NA; a += nt) {
+      contact_impulses(a);
+      if (S.VLIM_ON == 1u) vlim_rows(a);
+    }
+    __syncthreads();
+    if (S.VLIM_FREE == 1u) {
+      for (uint32_t b = tid; b < S.NB; b += nt) {
+        if (bkind((int)b) != 1u || (bflags((int)b) & 1u) != 0u) continue;
+        RO<float4> o = S.sf + S.SF_BODY + b * 8u;
+        float limv = o[4].w, lima = o[5].w;
+        uint32_t g = S.A_VLG + S.ND + b * 6u;
+        if (limv > 0.0f) {
+          f3 v = v3(tw[b * 2u]);
+          for (int k = 0; k < 3; k++) if (S.art[g + k] > 0.5f) setc(v, k, clmp(comp(v, k), -limv, limv));
+          tw[b * 2u] = mf4(v, 0.0f);
+        }
+        if (lima > 0.0f) {
+          f3 w = v3(tw[b * 2u + 1u]);
+          for (int k = 0; k < 3; k++) {
+            float over = comp(w, k) - clmp(comp(w, k), -lima, lima);
+            if (over == 0.0f || S.art[g + 3u + k] < 0.5f) continue;
+            f3 e = sp3(0.0f);
+            setc(e, k, 1.0f);
+            m3 R = qmat(S.rot[b]);
+            f3 iw = mul(R, mul(binv_inertia((int)b), mul(tr(R), e)));
+            w -= iw * (over / comp(iw, k));
+          }
+          tw[b * 2u + 1u] = mf4(w, 0.0f);
+        }
+      }
+      __syncthreads();
+    }
+  }
+  __device__ float4 warm_value(uint32_t i, uint32_t nc) const {
+    if (i < nc) {
+      uint32_t o = i * S.ROWS;
+      float4 lam = S.rows[o + 6u];
+      return mf4(lam.x, v3(S.rows[o + 1u]) * lam.y + v3(S.rows[o + 2u]) * lam.z);
+    }
+    uint32_t o = S.A_DENSE + (i - nc) * S.DPS;
+    return mf4(S.art[o + 9u], ar.ald3(o + 12u) * S.art[o + 10u] + ar.ald3(o + 15u) * S.art[o + 11u]);
+  }
+  __device__ uint32_t warm_rank(uint32_t i, uint32_t nc) const {
+    return min(__float_as_uint(fmx(warm_value(i, nc).x, 0.0f)), 0xfffffffeu) + 1u;
+  }
+  __device__ uint32_t warm_key(uint32_t i, uint32_t nc) const {
+    if (i < nc) { uint32_t o = i * S.ROWS; return f2u(S.rows[o + 3u].w) | (f2u(S.rows[o + 4u].w) << 16u); }
+    uint32_t o = S.A_DENSE + (i - nc) * S.DPS;
+    if (S.art[o + 21u] > 0.5f) return 0xffffffffu;
+    return f2u(S.art[o + 1u]) | (f2u(S.art[o + 2u]) << 16u);
+  }
+};
+
+// Solve of scene sc by the calling block (all its threads).
+__device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
+  extern __shared__ float4 ssm4[];  // solve_smem_layout: [tw | imp], qd, color starts, link blocks
+  __shared__ Params Ps;
+  __shared__ SceneDev Ss;  // the scene's offsets and sizes, read everywhere in the serial passes
+  const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  if (B.active[sc] == 0u) return;  // not stepping in this frame (serving loop)
+  copy_scene(Ss, B.scenes[sc]);
+  const SceneDev& S = Ss;
+  if (tid == 0u) Ps = *S.params;
+  uint8_t* sb = reinterpret_cast<uint8_t*>(ssm4);
+  const SolveSmem lay = solve_smem_layout(S.stage, S.NB, S.ND, S.NCOL, S.NL);
+  const bool staged_links = (S.stage & STAGE_LINKS) != 0u, staged_bodies = (S.stage & STAGE_BODIES) != 0u;
+  uint32_t* wcs = reinterpret_cast<uint32_t*>(sb + lay.wcs);
+  float* lb = staged_links ? reinterpret_cast<float*>(sb + lay.links) : S.art + S.A_LINK;
+  const uint32_t nu = S.sched[S.S_META];
+  const uint32_t ncol = min(S.sched[S.S_META + 1u], S.NCOL);
+  for (uint32_t i = tid; i < S.NCOL + 2u; i += nt) wcs[i] = S.sched[S.S_CSTART + i];
+  // Link blocks into shared memory with one bulk copy (A_LINK is 16-byte aligned).
+  __shared__ __align__(8) uint64_t stage_bar;
+  if (staged_links && !stage_to_shared(lb, S.art + S.A_LINK, 4u * S.NL * LBLK, &stage_bar) && tid == 0u)
+    atomicCAS(B.error, 0u, (uint32_t)ERR_STAGE_TIMEOUT);
+  __syncthreads();
+  const Params& P = Ps;
+  Solver sv(S, P, lb, staged_bodies ? reinterpret_cast<float4*>(sb + lay.tw) : S.tw,
+            staged_bodies ? reinterpret_cast<float4*>(sb + lay.imp) : S.imp,
+            (S.stage & STAGE_QD) ? reinterpret_cast<float*>(sb + lay.aqd) : S.aqd);
+  float* A = S.art;
+  // Prologue (wgsl.js:3635-3691).
+  for (uint32_t i = tid; i < S.ND; i += nt) sv.aqd[i] = A[S.A_QDH + i];
+  for (uint32_t b = tid; b < S.NB; b += nt) {
+    uint32_t kind = sv.bkind((int)b);
+    sv.imp[b * 2u] = make_float4(0, 0, 0, 0);
+    sv.imp[b * 2u + 1u] = make_float4(0, 0, 0, 0);
+    // The reference keeps twists in workgroup memory, which starts at zero in every dispatch.
+    sv.tw[b * 2u] = make_float4(0, 0, 0, 0);
+    sv.tw[b * 2u + 1u] = make_float4(0, 0, 0, 0);
+    if (kind != 1u) continue;
+    uint32_t fl = sv.bflags((int)b);
+    f3 v = v3(S.lv[b]) + (fl != 0u ? sp3(0.0f) : v3(P.gravity) * P.dt);
+    f3 w = v3(S.av[b]);
+    uint32_t bfo = S.A_BF + b * 8u;
+    f3 bf = mf3(A[bfo], A[bfo + 1], A[bfo + 2]), bt = mf3(A[bfo + 4], A[bfo + 5], A[bfo + 6]);
+    RO<float4> o = S.sf + S.SF_BODY + b * 8u;
+    if ((fl & 1u) == 0u && (nonzero(bf) || nonzero(bt))) {
+      m3 R = qmat(S.rot[b]);
+      v += (bf * o[0].x) * P.dt;
+      w += mul(R, mul(sv.binv_inertia((int)b), mul(tr(R), bt))) * P.dt;
+    }
+    m3 I = tr(mcols(v3(o[2]), v3(o[3]), v3(o[4])));
+    bool iso = I.c[0].x == I.c[1].y && I.c[1].y == I.c[2].z && I.c[0].y == 0.0f && I.c[0].z == 0.0f && I.c[1].z == 0.0f;
+    if ((fl & 1u) == 0u && !iso && nonzero(w)) {
+      m3 R = qmat(S.rot[b]);
+      w = mul(R, Solver::gyro(I, mul(tr(R), w), P.dt));
+    }
+    sv.tw[b * 2u] = mf4(v, 0.0f);
+    sv.tw[b * 2u + 1u] = mf4(w, 0.0f);
+  }
+  for (uint32_t i = tid; i < 2u * S.ND; i += nt) A[S.A_LIM + i] = 0.0f;
+  for (uint32_t i = tid; i < S.ND; i += nt) { A[S.A_FRIC + i] = 0.0f; A[S.A_DRV + i] = 0.0f; }
+  const uint32_t nslot = wcs[S.NCOL + 1u];
+  for (uint32_t u = tid; u < nslot; u += nt) {
+    uint32_t row = S.sched[S.S_PORD + u], us = S.sched[S.S_RUNIT + row], key = S.sched[S.S_UKEY + us];
+    S.slots[2u * u] = make_float4((float)row, (float)us, (float)((int)(key & 0xffffu) - 1), (float)((int)(key >> 16u) - 1));
+  }
+  __syncthreads();
+  for (uint32_t a = tid; a < S.NA; a += nt) sv.ar.twists(a, sv.aqd, sv.tw);
+  __syncthreads();
+  sv.dense_phase(0u, 0u, 0u);
+  sv.sweep(0u, ncol, 0u, wcs, nu);
+  for (uint32_t it = 0; it < P.iterations; it++) sv.sweep(1u, ncol, it, wcs, nu);
+  // Warm-start table (wgsl.js:3737-3767): rows sharing a key keep the largest normal impulse.
+  const uint32_t nc = S.sched[S.S_USTART + nu];
+  const uint32_t ndense = min(S.sched[S.S_META + 3u], S.MAXDENSE);
+  const uint32_t WH = S.WH, wbase = (1u - P.parity) * WH;
+  uint32_t* wslot = S.sched + S.S_WSLOT;
+  uint32_t* wwin = S.sched + S.S_WWIN;
+  for (uint32_t i = tid; i < nc + ndense; i += nt) {
+    uint32_t key = sv.warm_key(i, nc);
+    wslot[i] = 0xffffffffu;
+    if (key == 0xffffffffu) continue;
+    uint32_t h = key % WH;
+    for (uint32_t probe = 0; probe < 32u; probe++) {
+      uint32_t old = atomicCAS(&S.warm_tab[wbase + h], 0u, key);
+      if (old == 0u || old == key) { atomicMax(&wwin[h], sv.warm_rank(i, nc)); wslot[i] = h; break; }
+      h = (h + 1u) % WH;
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = tid; i < nc + ndense; i += nt) {
+    uint32_t key = sv.warm_key(i, nc);
+    if (key == 0xffffffffu) continue;
+    uint32_t h = wslot[i];
+    if (h >= WH || S.warm_tab[wbase + h] != key || wwin[h] != sv.warm_rank(i, nc)) continue;
+    float4 v = sv.warm_value(i, nc);
+    uint32_t* vo = S.warm_tab + 2u * WH + (wbase + h) * 4u;
+    vo[0] = __float_as_uint(v.x); vo[1] = __float_as_uint(v.y); vo[2] = __float_as_uint(v.z); vo[3] = __float_as_uint(v.w);
+  }
+  // Integrate (wgsl.js:3768-3828). The reference copies qd and damps the floating bases in two
+  // unsynchronised loops; here the copy completes before the damping.
+  if (S.PATCH == 1u) {
+    for (uint32_t b = tid; b < S.NB; b += nt) { S.ppos[b] = S.pos[b]; S.prot[b] = S.rot[b]; }
+    __syncthreads();
+  }
+  for (uint32_t b = tid; b < S.NB; b += nt) {
+    if (sv.bkind((int)b) != 1u) continue;
+    f3 v = v3(sv.tw[b * 2u]), w = v3(sv.tw[b * 2u + 1u]);
+    float damp = (sv.bflags((int)b) & 1u) != 0u ? 1.0f : 1.0f - S.sf[S.SF_BODY + b * 8u + 3u].w * P.dt;
+    S.lv[b] = mf4(v, 0.0f);
+    S.av[b] = mf4(w * damp, 0.0f);
+    f3 c = v3(S.pos[b]) + v * P.dt;
+    float4 q = S.rot[b];
+    q = nrm4(add4(q, scale4(0.5f * P.dt, qmul(mf4(w, 0.0f), q))));
+    S.pos[b] = mf4(c, 0.0f);
+    S.rot[b] = q;
+  }
+  for (uint32_t i = tid; i < S.ND; i += nt) A[S.A_QD + i] = sv.aqd[i];
+  __syncthreads();
+  for (uint32_t l = tid; l < S.NL; l += nt) {
+    if (sv.ar.ltype(l) != 4u || sv.ar.lparent(l) >= 0) continue;
+    float k = 1.0f - S.sf[S.SF_BODY + (uint32_t)sv.ar.lbody(l) * 8u + 3u].w * P.dt;
+    uint32_t d = sv.ar.ldof(l);
+    A[S.A_QD + d + 3u] *= k; A[S.A_QD + d + 4u] *= k; A[S.A_QD + d + 5u] *= k;
+  }
+  __syncthreads();
+  for (uint32_t a = tid; a < S.NA; a += nt) {
+    uint4 ai = sv.ar.info(a);
+    float* Q = A + S.A_Q;
+    const float* aqd = sv.aqd;
+    for (uint32_t k = 0; k < ai.y; k++) {
+      uint32_t l = ai.x + k, qs = sv.ar.lqs(l), d = sv.ar.ldof(l), t = sv.ar.ltype(l);
+      if (t == 1u || t == 0u || t == 6u)
+        for (uint32_t r = 0; r < sv.ar.lndof(l); r++) Q[qs + r] += aqd[d + r] * P.dt;
+      if (t == 2u) {
+        f3 w = mf3(aqd[d], aqd[d + 1u], aqd[d + 2u]);
+        float4 q = make_float4(Q[qs], Q[qs + 1], Q[qs + 2], Q[qs + 3]);
+        q = nrm4(add4(q, scale4(0.5f * P.dt, qmul(mf4(w, 0.0f), q))));
+        Q[qs] = q.x; Q[qs + 1] = q.y; Q[qs + 2] = q.z; Q[qs + 3] = q.w;
+      }
+      if (t == 4u) {
+        for (uint32_t c = 0; c < 3u; c++) Q[qs + c] += aqd[d + c] * P.dt;
+        f3 w = mf3(aqd[d + 3u], aqd[d + 4u], aqd[d + 5u]);
+        float4 q = make_float4(Q[qs + 3], Q[qs + 4], Q[qs + 5], Q[qs + 6]);
+        q = nrm4(add4(q, scale4(0.5f * P.dt, qmul(mf4(w, 0.0f), q))));
+        Q[qs + 3] = q.x; Q[qs + 4] = q.y; Q[qs + 5] = q.z; Q[qs + 6] = q.w;
+      }
+    }
+    sv.ar.fk(a);
+    for (uint32_t k = 0; k < ai.y; k++) {
+      uint32_t l = ai.x + k;
+      uint32_t b = (uint32_t)sv.ar.lbody(l);
+      S.pos[b] = mf4(sv.ar.ld3(sv.ar.lo(l) + L_COM), 0.0f);
+      S.rot[b] = sv.ar.link_rot(l);
+    }
+  }
+  // Friction anchors: advance and store for the next substep (wgsl.js:3832-3878).
+  if (S.PATCH == 1u) {
+    __syncthreads();
+    const uint32_t AH = S.AH, ab = 10u * WH + (1u - P.parity) * AH, AVb = 10u * WH + 2u * AH;
+    const float keep_frac = (float)(1.0 - 1e-5);
+    for (uint32_t i = tid; i < nc; i += nt) {
+      uint32_t o = i * S.ROWS;
+      const float4* rows = S.rows;
+      const uint32_t PO = S.PO;
+      if (rows[o + PO].w != 2.0f) continue;
+      uint32_t pair = __float_as_uint(rows[o + PO + 3u].w);
+      int a = (int)(pair & 0xffffu) - 1, b = (int)(pair >> 16u) - 1;
+      f3 fra = v3(rows[o + PO]), frb = v3(rows[o + PO + 1u]);
+      uint32_t k = f2u(rows[o + PO + 1u].w);
+      float4 ex = rows[o + PO + 2u];
+      float lim = ex.w;
+      if (lim <= 0.0f) continue;
+      f3 n = v3(rows[o]), t1 = v3(rows[o + 1u]), t2 = v3(rows[o + 2u]);
+      f3 ta[2], tb[2];
+      sv.load_tw(a, ta);
+      sv.load_tw(b, tb);
+      f3 vrel = (tb[0] + cross(tb[1], frb)) - (ta[0] + cross(ta[1], fra));
+      float4 lam = rows[o + 6u];
+      f3 lt = t1 * lam.y + t2 * lam.z;
+      float r = fmx(fmn(sv.bradius(a), sv.bradius(b)), 1e-4f);
+      if (len(lt) >= keep_frac * lim && dot(vrel, lt) < (((-lim) * 1e-5f) * r) / P.dt) continue;
+      float4 qa = make_float4(0, 0, 0, 1);
+      f3 ca = sp3(0.0f);
+      if (a >= 0) { qa = S.rot[a]; ca = v3(S.pos[a]); }
+      f3 ll = v3(rows[o + PO + 3u]);
+      f3 x = ca + qrot(qa, ll);
+      f3 e = (v3(ex) + sv.body_motion(b, x)) - sv.body_motion(a, x);
+      e -= n * dot(n, e);
+      f3 el = qinv(qa, e);
+      uint32_t hk = max(mix32(pair * 2u + k), 1u);
+      uint32_t h = hk % AH;
+      for (uint32_t probe = 0; probe < 32u; probe++) {
+        uint32_t old = atomicCAS(&S.warm_tab[ab + h], 0u, hk);
+        if (old == 0u) {
+          uint32_t* vo = S.warm_tab + AVb + ((1u - P.parity) * AH + h) * AVN_S;
+          f3 il = qinv(qa, lt), nl_ = qinv(qa, n);
+          vo[11] = __float_as_uint(nl_.x); vo[12] = __float_as_uint(nl_.y); vo[13] = __float_as_uint(nl_.z);
+          vo[8] = __float_as_uint(il.x); vo[9] = __float_as_uint(il.y); vo[10] = __float_as_uint(il.z);
+          vo[0] = pair; vo[1] = k;
+          vo[2] = __float_as_uint(ll.x); vo[3] = __float_as_uint(ll.y); vo[4] = __float_as_uint(ll.z);
+          vo[5] = __float_as_uint(el.x); vo[6] = __float_as_uint(el.y); vo[7] = __float_as_uint(el.z);
+          break;
+        }
+        h = (h + 1u) % AH;
+      }
+    }
+  }
+  if (tid == 0u) {
+    uint32_t* st = S.stats;
+    st[1] = max(st[1], S.counters[1]);
+    st[2] = max(st[2], ncol);
+    st[3] = max(st[3], nu);
+    st[4] = max(st[4], S.counters[0]);
+    st[5] = S.counters[1];
+    st[6] = ncol;
+    st[7] = max(st[7], S.sched[S.S_META + 3u]);
+    S.counters[0] = 0u;
+    S.counters[1] = 0u;
+  }
+  if (staged_links) {
+    __syncthreads();
+    for (uint32_t i = tid; i < S.NL * LBLK; i += nt) S.art[S.A_LINK + i] = lb[i];
+  }
+}
+
+}  // namespace steel
