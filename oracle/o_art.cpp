@@ -27,6 +27,32 @@ static inline v4 qaxis(v3 axis, float angle) {
 }
 static inline v3 unit3(uint32_t c) { return c == 0 ? mk3(1, 0, 0) : (c == 1 ? mk3(0, 1, 0) : mk3(0, 0, 1)); }
 
+// Double 3-vectors and column-major 3x3 blocks for the FP64 articulated-inertia option (ART_F64),
+// with the float path's evaluation orders.
+struct d3 { double x, y, z; };
+struct dm3 { d3 c[3]; };
+static inline d3 dv(v3 v) { return {(double)v.x, (double)v.y, (double)v.z}; }
+static inline v3 fv(d3 v) { return mk3((float)v.x, (float)v.y, (float)v.z); }
+static inline d3 operator+(d3 a, d3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline d3 operator-(d3 a, d3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline d3 operator*(d3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+static inline d3 operator*(double s, d3 a) { return {s * a.x, s * a.y, s * a.z}; }
+static inline double ddot(d3 a, d3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+static inline dm3 dcols(d3 a, d3 b, d3 c) { return {{a, b, c}}; }
+static inline dm3 dm(const m3& m) { return dcols(dv(m.c[0]), dv(m.c[1]), dv(m.c[2])); }
+static inline m3 fm(const dm3& m) { return mcols(fv(m.c[0]), fv(m.c[1]), fv(m.c[2])); }
+static inline d3 dmul(const dm3& m, d3 v) { return (m.c[0] * v.x + m.c[1] * v.y) + m.c[2] * v.z; }
+static inline dm3 dmul(const dm3& a, const dm3& b) { return dcols(dmul(a, b.c[0]), dmul(a, b.c[1]), dmul(a, b.c[2])); }
+static inline dm3 dtr(const dm3& m) {
+  return dcols(d3{m.c[0].x, m.c[1].x, m.c[2].x}, d3{m.c[0].y, m.c[1].y, m.c[2].y}, d3{m.c[0].z, m.c[1].z, m.c[2].z});
+}
+static inline dm3 dadd(const dm3& a, const dm3& b) { return dcols(a.c[0] + b.c[0], a.c[1] + b.c[1], a.c[2] + b.c[2]); }
+static inline dm3 dsub(const dm3& a, const dm3& b) { return dcols(a.c[0] - b.c[0], a.c[1] - b.c[1], a.c[2] - b.c[2]); }
+static inline dm3 dscale(double s, const dm3& a) { return dcols(s * a.c[0], s * a.c[1], s * a.c[2]); }
+static inline dm3 douter(d3 x, d3 y) { return dcols(x * y.x, x * y.y, x * y.z); }
+static inline dm3 dskew(d3 r) { return dcols(d3{0.0, r.z, -r.y}, d3{-r.z, 0.0, r.x}, d3{r.y, -r.x, 0.0}); }
+static inline double dmax(double a, double b) { return b > a ? b : a; }
+
 SV Oracle::imul(uint32_t o, SV m) const {
   m3 A = ldm(o), B = ldm(o + 9u), Cm = ldm(o + 18u);
   return SV{mul(A, m.a) + mul(B, m.l), mul(transpose(B), m.a) + mul(Cm, m.l)};
@@ -156,6 +182,111 @@ static void inv_spd(float* D, uint32_t n, uint32_t JM, float* Di) {
   }
 }
 
+// inv_spd in double, same steps (ART_F64).
+static void inv_spd64(double* D, uint32_t n, uint32_t JM, double* Di) {
+  for (uint32_t i = 0; i < JM * JM; i++) Di[i] = 0.0;
+  for (uint32_t i = 0; i < n; i++) Di[i * JM + i] = 1.0;
+  for (uint32_t c = 0; c < n; c++) {
+    double pv = 1.0 / dmax(D[c * JM + c], 1e-12);
+    for (uint32_t k = 0; k < n; k++) { D[c * JM + k] *= pv; Di[c * JM + k] *= pv; }
+    for (uint32_t r = 0; r < n; r++) {
+      if (r == c) continue;
+      double f = D[r * JM + c];
+      if (f == 0.0) continue;
+      for (uint32_t k = 0; k < n; k++) {
+        D[r * JM + k] -= f * D[c * JM + k];
+        Di[r * JM + k] -= f * Di[c * JM + k];
+      }
+    }
+  }
+}
+
+// Diagonal terms and generalized force of dof d, the r-th of link l (artwgsl.js:290-318): the
+// armature, implicit damping and the implicit PD drive are added to Drr (D[r][r], float or double);
+// the drive's saturation test reads Drr rounded to float.
+template <class T>
+float Oracle::dof_tau(uint32_t l, uint32_t r, T& Drr) const {
+  uint32_t d = link_dof(l) + r;
+  v4 dr = dof_drive(d);
+  Drr += (T)dr.x;
+  float damp = dof_passive(d).x;
+  Drr += (T)P.dt * (T)damp;
+  float tau = (-damp) * art[C.A_QD + d] + art[C.A_JF + d];
+  v2 sp = dof_spring(d);
+  if (sp.x != 0.0f) tau += sp.x * (sp.y - art[C.A_Q + link_qs(l) + r]);
+  if (C.DRIVE_ROWS == 0u && (dr.y > 0.0f || dr.z > 0.0f)) {
+    float q = art[C.A_Q + link_qs(l) + r], qd = art[C.A_QD + d];
+    float err = art[C.A_TGT + d] - q;
+    float tv = art[C.A_TGTV + d];
+    float mm = fmaxf_((float)Drr, 1e-9f);
+    float qdn = (mm * qd + P.dt * (dr.y * err + dr.z * tv)) / ((mm + P.dt * dr.z) + (P.dt * P.dt) * dr.y);
+    float ti = dr.y * (err - P.dt * qdn) + dr.z * (tv - qdn);
+    if (std::fabs(ti) <= dr.w || dr.w <= 0.0f) {
+      Drr += ((T)P.dt * (T)P.dt) * (T)dr.y + (T)P.dt * (T)dr.z;
+      tau += (dr.y * err - (P.dt * dr.y) * qd) + dr.z * (tv - qd);
+    } else {
+      tau += clampf(ti, -dr.w, dr.w);
+    }
+  }
+  return tau;
+}
+
+// Backward step of link l with the articulated-inertia branch in double (ART_F64): U = I^A S,
+// D = S^T U and its inverse, the projected inertia I^A - U D^-1 U^T and its shifted sum into the
+// parent are computed in double from the stored float blocks and rounded once on store; the bias
+// forces stay float as in the FP32 path.
+void Oracle::art_back_f64(uint32_t l) {
+  const uint32_t JM = C.JM, L = lo(l), n = link_ndof(l);
+  SV pA = ldsv(L + L_PA);
+  dm3 A = dm(ldm(L + L_IA)), B = dm(ldm(L + L_IA + 9u)), Cm = dm(ldm(L + L_IA + 18u));
+  d3 Ua[6], Ul[6];
+  for (uint32_t c = 0; c < n; c++) {
+    SV s = ldS(l, c);
+    d3 sa = dv(s.a), sl = dv(s.l);
+    Ua[c] = dmul(A, sa) + dmul(B, sl);
+    Ul[c] = dmul(dtr(B), sa) + dmul(Cm, sl);
+    stsv(L + L_U + c * 6u, SV{fv(Ua[c]), fv(Ul[c])});
+  }
+  double D[36] = {0};
+  float u[6] = {0};
+  for (uint32_t r = 0; r < n; r++) {
+    SV s = ldS(l, r);
+    for (uint32_t c = 0; c < n; c++) D[r * JM + c] = ddot(dv(s.a), Ua[c]) + ddot(dv(s.l), Ul[c]);
+    float tau = dof_tau(l, r, D[r * JM + r]);
+    u[r] = tau - sdot(s, pA);
+  }
+  double Di[36];
+  inv_spd64(D, n, JM, Di);
+  for (uint32_t i = 0; i < JM * JM; i++) art[L + L_DI + i] = (float)Di[i];
+  for (uint32_t r = 0; r < JM; r++) art[L + L_UU + r] = u[r];
+  int par = link_parent(l);
+  if (par < 0) return;
+  SV Duu = sv0();
+  for (uint32_t r = 0; r < n; r++) {
+    float du = 0.0f;
+    for (uint32_t c = 0; c < n; c++) {
+      double w = Di[r * JM + c];
+      A = dsub(A, dscale(w, douter(Ua[r], Ua[c])));
+      B = dsub(B, dscale(w, douter(Ua[r], Ul[c])));
+      Cm = dsub(Cm, dscale(w, douter(Ul[r], Ul[c])));
+      du += ldDI(l, r, c) * u[c];
+    }
+    Duu = sadd(Duu, sscale(ldU(l, r), du));
+  }
+  stm(L + L_IA, fm(A));
+  stm(L + L_IA + 9u, fm(B));
+  stm(L + L_IA + 18u, fm(Cm));
+  SV pa = sadd(sadd(pA, imul(L + L_IA, ldsv(L + L_C))), Duu);
+  uint32_t P0 = lo((uint32_t)par);
+  v3 r = link_r(l);
+  dm3 R = dskew(dv(r));
+  dm3 PA = dm(ldm(P0 + L_IA)), PB = dm(ldm(P0 + L_IA + 9u)), PC = dm(ldm(P0 + L_IA + 18u));
+  stm(P0 + L_IA, fm(dsub(dadd(dsub(dadd(PA, A), dmul(B, R)), dmul(R, dtr(B))), dmul(dmul(R, Cm), R))));
+  stm(P0 + L_IA + 9u, fm(dadd(dadd(PB, B), dmul(R, Cm))));
+  stm(P0 + L_IA + 18u, fm(dadd(PC, Cm)));
+  stsv(P0 + L_PA, sadd(ldsv(P0 + L_PA), fshift(pa, r)));
+}
+
 // art_factor (artwgsl.js:210-369)
 void Oracle::art_factor(uint32_t a) {
   u4 ai = art_info(a);
@@ -205,35 +336,18 @@ void Oracle::art_factor(uint32_t a) {
   }
   for (uint32_t kk = 0; kk < ai.y; kk++) {
     uint32_t l = ai.x + ai.y - 1u - kk, L = lo(l);
+    if (C.ART_F64 == 1u) {
+      art_back_f64(l);
+      continue;
+    }
     uint32_t n = link_ndof(l);
     SV pA = ldsv(L + L_PA);
     float D[36] = {0};
     float u[6] = {0};
     for (uint32_t c = 0; c < n; c++) stsv(L + L_U + c * 6u, imul(L + L_IA, ldS(l, c)));
     for (uint32_t r = 0; r < n; r++) {
-      uint32_t d = link_dof(l) + r;
       for (uint32_t c = 0; c < n; c++) D[r * JM + c] = sdot(ldS(l, r), ldU(l, c));
-      v4 dr = dof_drive(d);
-      D[r * JM + r] += dr.x;
-      float damp = dof_passive(d).x;
-      D[r * JM + r] += P.dt * damp;
-      float tau = (-damp) * art[C.A_QD + d] + art[C.A_JF + d];
-      v2 sp = dof_spring(d);
-      if (sp.x != 0.0f) tau += sp.x * (sp.y - art[C.A_Q + link_qs(l) + r]);
-      if (C.DRIVE_ROWS == 0u && (dr.y > 0.0f || dr.z > 0.0f)) {
-        float q = art[C.A_Q + link_qs(l) + r], qd = art[C.A_QD + d];
-        float err = art[C.A_TGT + d] - q;
-        float tv = art[C.A_TGTV + d];
-        float mm = fmaxf_(D[r * JM + r], 1e-9f);
-        float qdn = (mm * qd + P.dt * (dr.y * err + dr.z * tv)) / ((mm + P.dt * dr.z) + (P.dt * P.dt) * dr.y);
-        float ti = dr.y * (err - P.dt * qdn) + dr.z * (tv - qdn);
-        if (std::fabs(ti) <= dr.w || dr.w <= 0.0f) {
-          D[r * JM + r] += (P.dt * P.dt) * dr.y + P.dt * dr.z;
-          tau += (dr.y * err - (P.dt * dr.y) * qd) + dr.z * (tv - qd);
-        } else {
-          tau += clampf(ti, -dr.w, dr.w);
-        }
-      }
+      float tau = dof_tau(l, r, D[r * JM + r]);
       u[r] = tau - sdot(ldS(l, r), pA);
     }
     float Di[36];

@@ -34,7 +34,7 @@ namespace orc {
   X(WH) X(ROWS) X(PO) X(FMO) X(FMODE) X(PATCH) X(EXTRA) X(SHARED) X(FSHARED) X(REST) X(CTI) X(SLEEP)      \
   X(DRIVE_ROWS) X(VEL_DRIVE_ACTIVE) X(FUSE_VLIM) X(VLIM_ON) X(FSTART) X(VELITERS) X(AH) X(ANG) X(ANG_ART)  \
   X(JFL) X(TORS) X(TO) X(EO) X(CO) X(COMPL) X(LONGEST_FIRST) X(VLIM_FREE) X(FRICTION_COMBINE)             \
-  X(RESTITUTION_COMBINE) X(JM) X(MAXPATH) X(MAXLP)                                                        \
+  X(RESTITUTION_COMBINE) X(JM) X(MAXPATH) X(MAXLP) X(ART_F64)                                                        \
   X(SF_BODY) X(SF_SHAPE) X(SF_HAABB) X(SF_VERTS) X(SF_FPLANE) X(SF_LINK) X(SF_DOF) X(SF_PATH) X(SF_LOOP)  \
   X(SF_MIMIC) X(SF_CTRL) X(SU_HULL) X(SU_FACE) X(SU_FV) X(SU_HEDGE) X(SU_EDGE) X(SU_ART) X(SU_ACON)        \
   X(SU_FILTER) X(P_BODY) X(P_SHAPE) X(P_AABB) X(P_PREV)                                                   \
@@ -236,6 +236,9 @@ struct Oracle {
   void art_fk(uint32_t a);
   v4 link_rot(uint32_t l) const { return mk4(ld3(lo(l) + 216u), art[lo(l) + 216u + 3u]); }
   void art_factor(uint32_t a);
+  template <class T>
+  float dof_tau(uint32_t l, uint32_t r, T& Drr) const;
+  void art_back_f64(uint32_t l);
   uint32_t link_path(uint32_t l0, uint32_t* path) const;
   float dof_hinv(uint32_t l, uint32_t r) const;
   void link_response(uint32_t l, const uint32_t* split_count);

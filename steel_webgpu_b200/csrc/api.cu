@@ -159,7 +159,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
   K(SF_BODY) K(SF_SHAPE) K(SF_HAABB) K(SF_VERTS) K(SF_FPLANE) K(SF_LINK) K(SF_DOF) K(SF_PATH) K(SF_LOOP)
   K(SF_MIMIC) K(SF_CTRL) K(SU_HULL) K(SU_FACE) K(SU_FV) K(SU_HEDGE) K(SU_EDGE) K(SU_ART) K(SU_ACON)
   K(SU_FILTER) K(NB) K(NS) K(NA) K(NL) K(ND) K(NDA) K(JM) K(MAXPATH) K(MAXLP) K(NLOOP) K(NMIMIC) K(PATCH)
-  K(EXTRA) K(SHARED) K(FSHARED) K(REST) K(FSTART) K(TGT_HELD) K(CTRL_KIND) K(CTRL_A) K(CTRL_B) K(VLIM_FREE) K(VLIM_ON)
+  K(EXTRA) K(SHARED) K(FSHARED) K(REST) K(FSTART) K(TGT_HELD) K(CTRL_KIND) K(CTRL_A) K(CTRL_B) K(VLIM_FREE) K(VLIM_ON) K(ART_F64)
   K(FRICTION_COMBINE) K(RESTITUTION_COMBINE) K(NCOLW) K(NCOL) K(MAXP) K(MAXC) K(MAXU) K(WH) K(AH)
   K(MAXDENSE) K(ROWS) K(PO) K(DHDR) K(DPS)
 #undef K
@@ -401,6 +401,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   uint8_t* A = b->arena;
   std::vector<SceneDev> dev(n);
   size_t prep_smem = 0, solve_smem = 0;
+  uint32_t art_f64 = 0;
   for (uint32_t i = 0; i < n; i++) {
     SceneHost& s = b->sc[i];
     SceneDev& d = s.d;
@@ -427,6 +428,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
     if (4ull * d.NB * d.NCOLW <= STAGE_WMASK_CAP) d.stage |= STAGE_WMASK;
     prep_smem = std::max<size_t>(prep_smem, prep_smem_layout(d.stage, d.NL, d.NB, d.NCOLW, d.NCOL).total);
     solve_smem = std::max<size_t>(solve_smem, solve_smem_layout(d.stage, d.NB, d.ND, d.NCOL, d.NL).total);
+    art_f64 |= d.ART_F64;
     dev[i] = d;
     CU(cudaMemcpyAsync((void*)d.sf.p, s.statF.data(), s.statF.size() * 4, cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync((void*)d.su.p, s.statU.data(), s.statU.size() * 4, cudaMemcpyHostToDevice, st));
@@ -463,6 +465,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   bd.error = at<uint32_t>(A, b->o_err);
   bd.prep_smem = (uint32_t)prep_smem;
   bd.solve_smem = (uint32_t)solve_smem;
+  bd.art_f64 = art_f64 != 0u ? 1u : 0u;
   CU(configure_prepare(prep_smem));
   CU(configure_solve(solve_smem));
   CU(configure_prepare_solve(std::max(prep_smem, solve_smem)));

@@ -32,6 +32,32 @@ SD SVec fshift(SVec f, f3 r) { return SVec{f.a + cross(r, f.l), f.l}; }
 SD float4 qaxis(f3 axis, float angle) { return mf4(axis * fsin(0.5f * angle), fcos(0.5f * angle)); }
 SD f3 unit_axis(uint32_t c) { return c == 0 ? mf3(1, 0, 0) : (c == 1 ? mf3(0, 1, 0) : mf3(0, 0, 1)); }
 
+// Double 3-vectors and column-major 3x3 blocks for the FP64 articulated-inertia option (ART_F64),
+// evaluated in the float path's orders (no contraction: the library builds with --fmad=false).
+struct d3 { double x, y, z; };
+struct dm3 { d3 c[3]; };
+SD d3 dv(f3 v) { return d3{(double)v.x, (double)v.y, (double)v.z}; }
+SD f3 fv(d3 v) { return mf3((float)v.x, (float)v.y, (float)v.z); }
+SD d3 operator+(d3 a, d3 b) { return d3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+SD d3 operator-(d3 a, d3 b) { return d3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+SD d3 operator*(d3 a, double s) { return d3{a.x * s, a.y * s, a.z * s}; }
+SD d3 operator*(double s, d3 a) { return d3{s * a.x, s * a.y, s * a.z}; }
+SD double ddot(d3 a, d3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+SD dm3 dcols(d3 a, d3 b, d3 c) { return dm3{{a, b, c}}; }
+SD dm3 dm(const m3& m) { return dcols(dv(m.c[0]), dv(m.c[1]), dv(m.c[2])); }
+SD m3 fm(const dm3& m) { return mcols(fv(m.c[0]), fv(m.c[1]), fv(m.c[2])); }
+SD d3 dmul(const dm3& m, d3 v) { return (m.c[0] * v.x + m.c[1] * v.y) + m.c[2] * v.z; }
+SD dm3 dmul(const dm3& a, const dm3& b) { return dcols(dmul(a, b.c[0]), dmul(a, b.c[1]), dmul(a, b.c[2])); }
+SD dm3 dtr(const dm3& m) {
+  return dcols(d3{m.c[0].x, m.c[1].x, m.c[2].x}, d3{m.c[0].y, m.c[1].y, m.c[2].y}, d3{m.c[0].z, m.c[1].z, m.c[2].z});
+}
+SD dm3 dadd(const dm3& a, const dm3& b) { return dcols(a.c[0] + b.c[0], a.c[1] + b.c[1], a.c[2] + b.c[2]); }
+SD dm3 dsub(const dm3& a, const dm3& b) { return dcols(a.c[0] - b.c[0], a.c[1] - b.c[1], a.c[2] - b.c[2]); }
+SD dm3 dscl(double s, const dm3& a) { return dcols(s * a.c[0], s * a.c[1], s * a.c[2]); }
+SD dm3 douter(d3 x, d3 y) { return dcols(x * y.x, x * y.y, x * y.z); }
+SD dm3 dskew(d3 r) { return dcols(d3{0.0, r.z, -r.y}, d3{-r.z, 0.0, r.x}, d3{r.y, -r.x, 0.0}); }
+SD double dmx(double a, double b) { return b > a ? b : a; }
+
 struct Art {
   const SceneDev& S;
   float* A;   // the scene's articulation buffer
@@ -190,24 +216,26 @@ struct Art {
 
   // Diagonal terms and generalized force of dof d (the r-th of its link, joint coordinates from
   // qs): joint damping, spring, and the implicit PD drive folded into D (artwgsl.js:290-318).
-  // Drr holds D[r][r] = S_r . U_r on entry and gains the drive and damping terms.
-  __device__ float dof_tau(uint32_t d, uint32_t qs, uint32_t r, float& Drr, const Params& P) const {
+  // Drr (float, or double under ART_F64) holds D[r][r] = S_r . U_r on entry and gains the drive
+  // and damping terms; the drive's saturation test reads it rounded to float.
+  template <class T>
+  __device__ float dof_tau(uint32_t d, uint32_t qs, uint32_t r, T& Drr, const Params& P) const {
     // Every input is loaded first, so the loads overlap.
     const float4 dr = dof_drive(d), pas = dof_passive(d), spr = DR[d * 5u + 4u];
     const float qd = A[S.A_QD + d], jf = A[S.A_JF + d], q = A[S.A_Q + qs + r];
     const float tgt = A[S.A_TGT + d], tv = A[S.A_TGTV + d];
-    Drr += dr.x;
+    Drr += (T)dr.x;
     float damp = pas.x;
-    Drr += P.dt * damp;
+    Drr += (T)P.dt * (T)damp;
     float tau = (-damp) * qd + jf;
     if (spr.x != 0.0f) tau += spr.x * (spr.y - q);
     if (dr.y > 0.0f || dr.z > 0.0f) {
       float err = tgt - q;
-      float mm = fmx(Drr, 1e-9f);
+      float mm = fmx((float)Drr, 1e-9f);
       float qdn = (mm * qd + P.dt * (dr.y * err + dr.z * tv)) / ((mm + P.dt * dr.z) + (P.dt * P.dt) * dr.y);
       float ti = dr.y * (err - P.dt * qdn) + dr.z * (tv - qdn);
       if (fabsf(ti) <= dr.w || dr.w <= 0.0f) {
-        Drr += (P.dt * P.dt) * dr.y + P.dt * dr.z;
+        Drr += ((T)P.dt * (T)P.dt) * (T)dr.y + (T)P.dt * (T)dr.z;
         tau += (dr.y * err - (P.dt * dr.y) * qd) + dr.z * (tv - qd);
       } else {
         tau += clmp(ti, -dr.w, dr.w);
@@ -216,7 +244,78 @@ struct Art {
     return tau;
   }
 
+  // Backward step of link l with the articulated-inertia branch in double (ART_F64, not a
+  // reference option): U = I^A S, D = S^T U and its Gauss-Jordan inverse (artwgsl.js:192-207), the
+  // projected inertia I^A - U D^-1 U^T and its shifted sum into the parent (artwgsl.js:90-95, 342)
+  // are computed in double from the stored float blocks and rounded once on store, so the
+  // accumulation toward the root cancels in double; bias forces stay float as in the FP32 step.
+  __device__ void back_f64(uint32_t l, const Params& P) const {
+    const uint32_t JM = JMc, L = lo(l), n = lndof(l), d0 = ldof(l), qs = lqs(l);
+    const SVec pA = ldsv(L + L_PA);
+    dm3 Am = dm(ldm(L + L_IA)), Bm = dm(ldm(L + L_IA + 9u)), Cm = dm(ldm(L + L_IA + 18u));
+    d3 Ua[6], Ul[6];
+    for (uint32_t c = 0; c < n; c++) {
+      SVec s = ldS(l, c);
+      d3 sa = dv(s.a), sl = dv(s.l);
+      Ua[c] = dmul(Am, sa) + dmul(Bm, sl);
+      Ul[c] = dmul(dtr(Bm), sa) + dmul(Cm, sl);
+      stsv(L + L_U + c * 6u, SVec{fv(Ua[c]), fv(Ul[c])});
+    }
+    double D[36], Di[36];
+    float u[6];
+    for (uint32_t i = 0; i < 36u; i++) D[i] = 0.0;
+    for (uint32_t r = 0; r < n; r++) {
+      SVec s = ldS(l, r);
+      for (uint32_t c = 0; c < n; c++) D[r * JM + c] = ddot(dv(s.a), Ua[c]) + ddot(dv(s.l), Ul[c]);
+      float tau = dof_tau(d0 + r, qs, r, D[r * JM + r], P);
+      u[r] = tau - sdot(s, pA);
+    }
+    for (uint32_t i = 0; i < JM * JM; i++) Di[i] = 0.0;
+    for (uint32_t i = 0; i < n; i++) Di[i * JM + i] = 1.0;
+    for (uint32_t c = 0; c < n; c++) {
+      double pv = 1.0 / dmx(D[c * JM + c], 1e-12);
+      for (uint32_t k = 0; k < n; k++) { D[c * JM + k] *= pv; Di[c * JM + k] *= pv; }
+      for (uint32_t r = 0; r < n; r++) {
+        if (r == c) continue;
+        double f = D[r * JM + c];
+        if (f == 0.0) continue;
+        for (uint32_t k = 0; k < n; k++) { D[r * JM + k] -= f * D[c * JM + k]; Di[r * JM + k] -= f * Di[c * JM + k]; }
+      }
+    }
+    for (uint32_t i = 0; i < JM * JM; i++) LB[L + L_DI + i] = (float)Di[i];
+    for (uint32_t r = 0; r < JM; r++) LB[L + L_UU + r] = r < n ? u[r] : 0.0f;
+    int par = lparent(l);
+    if (par < 0) return;
+    SVec Duu = sv0();
+    for (uint32_t r = 0; r < n; r++) {
+      float du = 0.0f;
+      for (uint32_t c = 0; c < n; c++) {
+        double w = Di[r * JM + c];
+        Am = dsub(Am, dscl(w, douter(Ua[r], Ua[c])));
+        Bm = dsub(Bm, dscl(w, douter(Ua[r], Ul[c])));
+        Cm = dsub(Cm, dscl(w, douter(Ul[r], Ul[c])));
+        du += ldDI(l, r, c) * u[c];
+      }
+      Duu = sadd(Duu, sscl(ldU(l, r), du));
+    }
+    stm(L + L_IA, fm(Am));
+    stm(L + L_IA + 9u, fm(Bm));
+    stm(L + L_IA + 18u, fm(Cm));
+    SVec pa = sadd(sadd(pA, imul(L + L_IA, ldsv(L + L_C))), Duu);
+    uint32_t P0 = lo((uint32_t)par);
+    f3 r = link_r(l);
+    dm3 Rs = dskew(dv(r));
+    dm3 PA = dm(ldm(P0 + L_IA)), PB = dm(ldm(P0 + L_IA + 9u)), PC = dm(ldm(P0 + L_IA + 18u));
+    stm(P0 + L_IA, fm(dsub(dadd(dsub(dadd(PA, Am), dmul(Bm, Rs)), dmul(Rs, dtr(Bm))), dmul(dmul(Rs, Cm), Rs))));
+    stm(P0 + L_IA + 9u, fm(dadd(dadd(PB, Bm), dmul(Rs, Cm))));
+    stm(P0 + L_IA + 18u, fm(dadd(PC, Cm)));
+    stsv(P0 + L_PA, sadd(ldsv(P0 + L_PA), fshift(pa, r)));
+  }
+
   // Articulated inertias, U = I^A S, D^-1 with implicit drives, free velocity (artwgsl.js:210-369).
+  // F64: the backward pass's articulated-inertia branch in double (back_f64), for scenes with
+  // ART_F64; it is a separate instance so the FP32 kernels keep their registers.
+  template <bool F64>
   __device__ void factor(uint32_t a, const Params& P) const {
     uint4 ai = info(a);
     f3 g = v3(P.gravity);
@@ -276,6 +375,10 @@ struct Art {
     }
     for (uint32_t kk = 0; kk < ai.y; kk++) {
       uint32_t l = ai.x + ai.y - 1u - kk, L = lo(l);
+      if (F64) {
+        back_f64(l, P);
+        continue;
+      }
       uint32_t n = lndof(l), d0 = ldof(l), qs = lqs(l);
       SVec pA = ldsv(L + L_PA);
       float u[6] = {0, 0, 0, 0, 0, 0};

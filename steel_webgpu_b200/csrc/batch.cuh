@@ -24,6 +24,7 @@ struct BatchDev {
   uint32_t* error;            // [1] first device-side error code (0 = none)
   uint32_t prep_smem;         // dynamic shared memory of k_prepare / k_solve launches (bytes)
   uint32_t solve_smem;
+  uint32_t art_f64;           // some scene has ART_F64: launch the prepare instances that carry it
 };
 
 constexpr uint32_t BROAD_TILE = 32;

@@ -3,11 +3,19 @@
 
 namespace steel {
 
-__global__ void __launch_bounds__(PREP_THREADS, 4) k_prepare(BatchDev B) { prepare_scene(B, blockIdx.x); }
+// F64: the instance with the FP64 articulated-inertia branch, launched when a scene of the batch
+// has ART_F64 (scenes without it still run the FP32 branch in that instance).
+template <bool F64>
+__global__ void __launch_bounds__(PREP_THREADS, 4) k_prepare(BatchDev B) { prepare_scene<F64>(B, blockIdx.x); }
 
 cudaError_t configure_prepare(size_t smem_bytes) {
-  return cudaFuncSetAttribute(k_prepare, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  cudaError_t e = cudaFuncSetAttribute(k_prepare<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_prepare<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
 }
-void launch_prepare(const BatchDev& b, cudaStream_t st) { k_prepare<<<b.nscenes, PREP_THREADS, b.prep_smem, st>>>(b); }
+void launch_prepare(const BatchDev& b, cudaStream_t st) {
+  if (b.art_f64) k_prepare<true><<<b.nscenes, PREP_THREADS, b.prep_smem, st>>>(b);
+  else k_prepare<false><<<b.nscenes, PREP_THREADS, b.prep_smem, st>>>(b);
+}
 
 }  // namespace steel

@@ -503,6 +503,7 @@ struct Prep {
 };
 
 // Prepare of scene sc by the calling block (all its threads).
+template <bool F64>
 __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
   extern __shared__ float4 psm4[];  // prep_smem_layout: link blocks, coloring
   __shared__ uint32_t stmp[40];
@@ -605,7 +606,8 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
     }
     A[S.A_RLN + a] = (float)n;
     ar.fk(a);
-    ar.factor(a, P);
+    if (F64 && S.ART_F64 == 1u) ar.factor<true>(a, P);
+    else ar.factor<false>(a, P);
   }
   // Phase 1: classify the sorted contacts; units are runs of one body pair.
   const uint32_t nc = min(S.counters[1], S.MAXC);

@@ -586,6 +586,9 @@ def pack(scene: LoadedScene, opts: dict | None = None, colorWords: int | None = 
         VEL_DRIVE_ACTIVE=1 if SV.get("velocity_drive_mode") == "active" else 0,
         FUSE_VLIM=0 if SV.get("fuse_joint_velocity_limits") is False else 1,
         VLIM_ON=1 if SO.get("enable_joint_velocity_limits") else 0,
+        # Not a reference option: the articulated-inertia pass's D factor/inverse and the inertia
+        # accumulation into parents (up to the root) in FP64; off reproduces the reference's FP32.
+        ART_F64=1 if SO.get("articulation_fp64") else 0,
         FSTART=0 if fpi < 0 else iters - min(fpi, iters), VELITERS=SV["velocity_iterations"], AH=AH,
         ANG=1 if ang_on else 0, ANG_ART=1 if ang_art else 0, F_FR_MUT=fr_mut, F_FR_MUR=fr_mur,
         JFL=1 if any(d["loadCoef"] > 0 for d in dofs) else 0, TORS=1 if tors_on else 0, TO=TO, EO=EO,

@@ -147,3 +147,45 @@ def test_joint_velocity_limits_hold(oracle_lib):
     assert on == 1 and off == 0
     assert limited < 2.05
     assert free > 2.5
+
+
+def _chain_qdd_error(oracle_lib, height, n_links, ratio, fp64_option, seeds=3):
+    """Worst max |qdd - qdd64| / max |qdd64| over seeded serial revolute chains (link masses
+    log-uniform over `ratio`, random joint angles, qd = 0): the oracle's articulated-body pass (one
+    prepare) against the float64 joint-space dynamics of tests/fp64_aba.py."""
+    from steel_webgpu_b200 import synth
+    from tests.fp64_aba import qdd_fp64
+    worst = 0.0
+    for seed in range(seeds):
+        b = SceneBuilder(fps=240)
+        synth._add_chain(b, np.random.default_rng(seed), [0.0, 0.0, height], n_links, ratio_max=ratio)
+        pk = pack(b.finalize(), opts={"solver": {"articulation_fp64": fp64_option}})
+        C = pk.C
+        assert C["ART_F64"] == (1 if fp64_option else 0)
+        pk.art[C["A_Q"]:C["A_Q"] + pk.NQ] = np.random.default_rng(100 + seed).uniform(-0.6, 0.6, pk.NQ)
+        dt = float(np.float32(1.0 / (pk.params["fps"] * pk.params["substeps"])))
+        o = oracle_lib.OracleSim(pk)
+        o.stage(0)
+        o.stage(1)
+        qdd = o.read("art")[C["A_QDH"]:C["A_QDH"] + pk.ND].astype(np.float64) / dt
+        qdd64 = qdd_fp64(pk, dt)
+        worst = max(worst, float(np.abs(qdd - qdd64).max() / np.abs(qdd64).max()))
+    return worst
+
+
+@pytest.mark.parametrize("height,n_links,bound", [(0.0, 2, 1e-6), (0.0, 40, 2e-5), (5.0, 40, 2e-5)])
+def test_articulation_fp32_error_against_fp64(oracle_lib, height, n_links, bound):
+    """FP32 pass (the reference's precision) on chains with a 10^3 mass ratio. World-frame link
+    positions are FP32, so the error grows with the chain's distance from the origin; the GPU path
+    is bit-identical to the oracle here."""
+    assert _chain_qdd_error(oracle_lib, height, n_links, 1e3, False) < bound
+
+
+def test_articulation_fp64_option_error(oracle_lib):
+    """The FP64 articulated-inertia option (D = S^T I^A S, its inverse and the inertia accumulation
+    toward the root in double) on 40-link chains with a 10^5 mass ratio: at least 3x below the FP32
+    pass's error against FP64, and below 4e-6."""
+    e32 = _chain_qdd_error(oracle_lib, 0.0, 40, 1e5, False)
+    e64 = _chain_qdd_error(oracle_lib, 0.0, 40, 1e5, True)
+    assert e64 < 4e-6
+    assert e32 > 3.0 * e64

@@ -14,7 +14,10 @@ from tests import scenes
 pytestmark = pytest.mark.gpu
 
 SCENES = {"boxes": scenes.boxes, "mixed_prims": scenes.mixed_prims, "articulated": scenes.articulated,
-          "chains_and_quads": scenes.chains_and_quads, "hull_bin": scenes.hull_bin, "vel_limited": scenes.vel_limited}
+          "chains_and_quads": scenes.chains_and_quads, "hull_bin": scenes.hull_bin, "vel_limited": scenes.vel_limited,
+          "chains_and_quads_fp64": scenes.chains_and_quads}
+# Packing options per scene (the FP64 articulated-inertia option on the articulation workload).
+OPTS = {"chains_and_quads_fp64": {"solver": {"articulation_fp64": True}}}
 
 
 def _pair_set(p):
@@ -49,7 +52,7 @@ def test_pairs_and_sorted_contacts(name, steel, oracle_lib):
 
 @pytest.mark.parametrize("name", list(SCENES))
 def test_trajectory_bit_exact(name, steel, oracle_lib):
-    pk = pack(SCENES[name]())
+    pk = pack(SCENES[name](), opts=OPTS.get(name))
     o = oracle_lib.OracleSim(pk)
     g = Batch([pk])
     nb = pk.NB
@@ -108,6 +111,21 @@ def test_batch_matches_each_scene_alone(steel, oracle_lib):
     for i, (pk, o) in enumerate(zip(pks, orcs)):
         o.step(40)
         assert np.array_equal(_bits(g.poses(i)), _bits(o.read("poses")[:pk.NB * 8])), f"scene {i} differs"
+
+
+def test_fp64_and_fp32_scenes_in_one_batch(steel, oracle_lib):
+    """A batch with an ART_F64 scene runs the FP64 kernel instances; its FP32 scenes must still match
+    their oracle bit for bit, and the FP64 scene its own."""
+    pks = [pack(scenes.chains_and_quads(n_quad=2), opts={"solver": {"articulation_fp64": True}}),
+           pack(scenes.chains_and_quads(n_quad=2)), pack(scenes.articulated())]
+    assert [pk.C["ART_F64"] for pk in pks] == [1, 0, 0]
+    g = Batch(pks)
+    orcs = [oracle_lib.OracleSim(pk) for pk in pks]
+    g.step(40)
+    for i, (pk, o) in enumerate(zip(pks, orcs)):
+        o.step(40)
+        assert np.array_equal(_bits(g.poses(i)), _bits(o.read("poses")[:pk.NB * 8])), f"scene {i} differs"
+    assert not np.array_equal(_bits(g.poses(0)), _bits(g.poses(1))), "the option changed nothing"
 
 
 def test_reset_replays_identically(steel):
