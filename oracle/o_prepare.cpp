@@ -350,6 +350,80 @@ void Oracle::build_patch(uint32_t sp) {
   }
 }
 
+// sleep_islands (wgsl.js:1371-1457): islands are nodes (free bodies, articulations) joined by
+// contacts. The reference's parallel union-find hooks the larger root under the smaller until no
+// contact joins two islands, so every node ends pointing at its island's lowest node; a sequential
+// union-find that links the larger root under the smaller, then compresses, gives that same
+// state. Island flags OR onto the root: 1 supported (touches static geometry, or a fixed-base
+// articulation), 2 vetoed (moving, driven, loop or mimic owner; picking is not carried), 4 some
+// member younger than the quiet time.
+void Oracle::sleep_islands() {
+  uint32_t* sc = sched.data();
+  const uint32_t NN = C.NB + C.NA;
+  uint32_t* uf = sc + C.S_UF;
+  uint32_t* uff = sc + C.S_UFF;
+  for (uint32_t n = 0; n < NN; n++) { uf[n] = n; uff[n] = 0u; }
+  sc[C.S_META + 5u] = 0u;
+  const uint32_t nc = std::min(counters[1], C.MAXC);
+  for (uint32_t c = 0; c < nc; c++) {
+    v4 m = contacts[c * 5u + 2u];
+    int na = body_node(f2i(m.x)), nb = body_node(f2i(m.y));
+    if ((na < 0 || nb < 0) && std::max(na, nb) >= 0 && contacts[c * 5u].w <= 1e-5f)
+      uff[(uint32_t)std::max(na, nb)] |= 1u;
+  }
+  auto find = [&](uint32_t n) {
+    uint32_t r = n;
+    for (uint32_t k = 0; k < NN && uf[r] != r; k++) r = uf[r];
+    return r;
+  };
+  for (uint32_t c = 0; c < nc; c++) {
+    v4 m = contacts[c * 5u + 2u];
+    int na = body_node(f2i(m.x)), nb = body_node(f2i(m.y));
+    if (na < 0 || nb < 0) continue;
+    uint32_t ra = find((uint32_t)na), rb = find((uint32_t)nb);
+    if (ra != rb) uf[std::max(ra, rb)] = std::min(ra, rb);
+  }
+  for (uint32_t n = 0; n < NN; n++) uf[n] = find(n);
+  for (uint32_t n = 0; n < NN; n++) {
+    bool moving = false, fixed = false, veto = false;
+    if (n < C.NB) {
+      if (body_kind((int)n) != 1u) continue;
+      if (art[C.A_SLP + n * 4u + 1u] < 0.5f)
+        moving = length(xyz(vel[n * 2u])) > C.F_SLEEP_LIN || length(xyz(vel[n * 2u + 1u])) > C.F_SLEEP_ANG;
+    } else {
+      u4 ai = art_info(n - C.NB);
+      fixed = link_type(ai.x) != 4u;
+      for (uint32_t k = 0; k < ai.y; k++) {
+        SV v = ldsv(lo(ai.x + k) + L_V);
+        if (art[C.A_SLP + n * 4u + 1u] < 0.5f && (length(v.l) > C.F_SLEEP_LIN || length(v.a) > C.F_SLEEP_ANG))
+          moving = true;
+      }
+      for (uint32_t d = ai.z; d < ai.z + ai.w; d++) {
+        v4 dr = dof_drive(d);
+        if (dr.y > 0.0f || dr.z > 0.0f) veto = true;
+      }
+      if (art_has_constraint(n - C.NB)) veto = true;
+    }
+    uint32_t f = (fixed ? 1u : 0u) | ((moving || veto) ? 2u : 0u) | (uff[n] & 1u);
+    uff[uf[n]] |= f;
+  }
+  for (uint32_t n = 0; n < NN; n++) {
+    if (n < C.NB && body_kind((int)n) != 1u) continue;
+    uint32_t r = uf[n], f = uff[r];
+    float age = art[C.A_SLP + n * 4u];
+    if ((f & 2u) != 0u || (f & 1u) == 0u) age = 0.0f;
+    else age = fminf_(age + P.dt, C.F_SLEEP_TIME);
+    art[C.A_SLP + n * 4u] = age;
+    if (age < C.F_SLEEP_TIME) uff[r] |= 4u;
+  }
+  for (uint32_t n = 0; n < NN; n++) {
+    if (n < C.NB && body_kind((int)n) != 1u) continue;
+    bool s = (uff[uf[n]] & 4u) == 0u;
+    art[C.A_SLP + n * 4u + 1u] = s ? 1.0f : 0.0f;
+    if (s) sc[C.S_META + 5u]++;
+  }
+}
+
 // The prepare kernel (wgsl.js:1788-2494) on the default flag set.
 void Oracle::k_prepare() {
   const uint32_t ROWS = C.ROWS, PO = C.PO, WH = C.WH, NCOL = C.NCOL, MAXC = C.MAXC;
@@ -363,6 +437,7 @@ void Oracle::k_prepare() {
   std::fill(wmask.begin(), wmask.end(), 0u);
   std::fill(wcount.begin(), wcount.end(), 0u);
   sc[C.S_META + 3u] = 0u;
+  if (C.SLEEP == 1u) sleep_islands();
   for (uint32_t tid = 0; tid < P.driven; tid++) {
     float ramp = ((P.phase + ((float)P.substep + 0.5f) * P.dt) * 60.0f) - 0.5f;
     float frame = clampf(C.TGT_HELD == 1u ? P.phase * 60.0f : ramp, 0.0f, (float)(P.path_frames - 1u));
@@ -446,12 +521,15 @@ void Oracle::k_prepare() {
       int a = f2i(m.x), b = f2i(m.y);
       uint32_t pk = (uint32_t)(a + 1) | ((uint32_t)(b + 1) << 16u);
       uint32_t cls = 0xfffffffeu;
-      if (same_art(a, b)) {
-        cls = 0xffffffffu;
-        ndc++;
-        sc[C.S_CLOCAL + c] = 1u;
-      } else {
-        cls = (c == 0u || prev != pk) ? UNIT_HEAD : 0u;
+      if (!pair_asleep(a, b)) {
+        if (same_art(a, b)) {
+          cls = 0xffffffffu;
+          bool rows = !node_asleep(body_node(a));
+          if (rows) ndc++;
+          sc[C.S_CLOCAL + c] = rows ? 1u : 0u;
+        } else {
+          cls = (c == 0u || prev != pk) ? UNIT_HEAD : 0u;
+        }
       }
       sc[C.S_CSLOT + c] = cls;
       prev = pk;

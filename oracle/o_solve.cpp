@@ -446,6 +446,14 @@ void Oracle::k_solve() {
   wn_y = std::min(sc[C.S_META + 1u], NCOL);
   for (uint32_t i = 0; i < NCOL + 2u; i++) wcs[i] = sc[C.S_CSTART + i];
   for (uint32_t i = 0; i < C.ND; i++) aqd[i] = art[C.A_QDH + i];
+  // Sleeping articulations start the solve at rest (wgsl.js:3640-3646; the reference's loop has no
+  // barrier after the copy above, so its intent, these zeros, is what is restated).
+  if (C.SLEEP == 1u)
+    for (uint32_t a = 0; a < C.NA; a++) {
+      if (!node_asleep((int)(C.NB + a))) continue;
+      u4 ai = art_info(a);
+      for (uint32_t d = ai.z; d < ai.z + ai.w; d++) aqd[d] = 0.0f;
+    }
   for (uint32_t b = 0; b < C.NB; b++) {
     uint32_t kind = body_kind((int)b);
     imp[b * 2u] = mk4(0, 0, 0, 0);
@@ -455,7 +463,7 @@ void Oracle::k_solve() {
     tw[b * 2u + 1u] = mk4(0, 0, 0, 0);
     if (kind == 1u) {
       uint32_t fl = body_flags((int)b);
-      v3 v = xyz(vel[b * 2u]) + (fl != 0u ? splat3(0.0f) : xyz(P.gravity) * P.dt);
+      v3 v = xyz(vel[b * 2u]) + ((node_asleep((int)b) || fl != 0u) ? splat3(0.0f) : xyz(P.gravity) * P.dt);
       v3 w = xyz(vel[b * 2u + 1u]);
       uint32_t bfo = C.A_BF + b * 8u;
       if ((fl & 1u) == 0u && (any_ne0(ld3(bfo)) || any_ne0(ld3(bfo + 4u)))) {
@@ -522,6 +530,11 @@ void Oracle::k_solve() {
     float damp = (body_flags((int)b) & 1u) != 0u ? 1.0f : 1.0f - body_limits((int)b).x * P.dt;
     vel[b * 2u] = mk4(v, 0.0f);
     vel[b * 2u + 1u] = mk4(w * damp, 0.0f);
+    if (node_asleep((int)b)) {
+      vel[b * 2u] = mk4(0, 0, 0, 0);
+      vel[b * 2u + 1u] = mk4(0, 0, 0, 0);
+      continue;
+    }
     v3 c = xyz(poses[C.P_BODY + b * 2u]) + v * P.dt;
     v4 q = poses[C.P_BODY + b * 2u + 1u];
     q = normalize(q + (0.5f * P.dt) * qmul(mk4(w, 0.0f), q));

@@ -48,7 +48,8 @@ namespace orc {
 
 #define ORC_F32_CONSTS(X)                                                                                 \
   X(F_ANCHOR_BETA) X(F_CFM) X(F_OMEGA) X(F_SPEC) X(F_GAP_GATE) X(F_FGAP) X(F_FSCALE) X(F_REST_SPEED)      \
-  X(F_FR_MUT) X(F_FR_MUR) X(F_BP_CELL) X(F_VLIM_FRAC) X(F_JL_GAP) X(F_JL_SPEED)
+  X(F_FR_MUT) X(F_FR_MUR) X(F_BP_CELL) X(F_VLIM_FRAC) X(F_JL_GAP) X(F_JL_SPEED) X(F_SLEEP_LIN) X(F_SLEEP_ANG) \
+  X(F_SLEEP_TIME)
 
 struct Consts {
 #define X(n) uint32_t n = 0;
@@ -220,6 +221,12 @@ struct Oracle {
   }
   int body_node(int b) const;
   bool node_asleep(int n) const { return C.SLEEP == 1u && n >= 0 && art[C.A_SLP + (uint32_t)n * 4u + 1u] > 0.5f; }
+  // pair_asleep (wgsl.js:1732-1736): both sides asleep or static.
+  bool pair_asleep(int a, int b) const {
+    if (C.SLEEP == 0u) return false;
+    int na = body_node(a), nb = body_node(b);
+    return (na < 0 || node_asleep(na)) && (nb < 0 || node_asleep(nb));
+  }
   uint32_t lo(uint32_t l) const { return C.A_LINK + l * 268u; }
   v3 ld3(uint32_t o) const { return mk3(art[o], art[o + 1], art[o + 2]); }
   void st3(uint32_t o, v3 v) { art[o] = v.x; art[o + 1] = v.y; art[o + 2] = v.z; }
@@ -236,6 +243,7 @@ struct Oracle {
   void art_fk(uint32_t a);
   v4 link_rot(uint32_t l) const { return mk4(ld3(lo(l) + 216u), art[lo(l) + 216u + 3u]); }
   void art_factor(uint32_t a);
+  void sleep_islands();
   template <class T>
   float dof_tau(uint32_t l, uint32_t r, T& Drr) const;
   void art_back_f64(uint32_t l);

@@ -146,7 +146,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
       {"TORS", "contact torsion"}, {"COMPL", "contact_compliance"}, {"NEST", "nesterov_momentum"},
       {"CTI", "row_schedule contact_then_internal"}, {"LONGEST_FIRST", "propagation_color_order longest_first"},
       {"DRIVE_ROWS", "drive_mode rows"},
-      {"JFL", "joint friction load coefficient"}, {"SLEEP", "enable_sleeping"}, {"VELITERS", "velocity_iterations"}};
+      {"JFL", "joint friction load coefficient"}, {"VELITERS", "velocity_iterations"}};
   for (auto& u : unsupported)
     if (C.u(u[0]) != 0u) { why = std::string("unsupported solver option: ") + u[1]; return STEEL_E_UNSUPPORTED; }
   if (in.statF_floats != (uint64_t)C.u("LEN_STATF4") * 4u || in.statU_words != C.u("LEN_STATU") ||
@@ -159,13 +159,13 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
   K(SF_BODY) K(SF_SHAPE) K(SF_HAABB) K(SF_VERTS) K(SF_FPLANE) K(SF_LINK) K(SF_DOF) K(SF_PATH) K(SF_LOOP)
   K(SF_MIMIC) K(SF_CTRL) K(SU_HULL) K(SU_FACE) K(SU_FV) K(SU_HEDGE) K(SU_EDGE) K(SU_ART) K(SU_ACON)
   K(SU_FILTER) K(NB) K(NS) K(NA) K(NL) K(ND) K(NDA) K(JM) K(MAXPATH) K(MAXLP) K(NLOOP) K(NMIMIC) K(PATCH)
-  K(EXTRA) K(SHARED) K(FSHARED) K(REST) K(FSTART) K(TGT_HELD) K(CTRL_KIND) K(CTRL_A) K(CTRL_B) K(VLIM_FREE) K(VLIM_ON) K(ART_F64)
+  K(EXTRA) K(SHARED) K(FSHARED) K(REST) K(FSTART) K(TGT_HELD) K(CTRL_KIND) K(CTRL_A) K(CTRL_B) K(VLIM_FREE) K(VLIM_ON) K(ART_F64) K(SLEEP)
   K(FRICTION_COMBINE) K(RESTITUTION_COMBINE) K(NCOLW) K(NCOL) K(MAXP) K(MAXC) K(MAXU) K(WH) K(AH)
   K(MAXDENSE) K(ROWS) K(PO) K(DHDR) K(DPS)
 #undef K
 #define F(n) d.n = C.f(#n);
   F(F_ANCHOR_BETA) F(F_CFM) F(F_OMEGA) F(F_SPEC) F(F_GAP_GATE) F(F_FGAP) F(F_FSCALE) F(F_REST_SPEED) F(F_FR_MUT)
-  F(F_FR_MUR) F(F_BP_CELL) F(F_JL_GAP) F(F_JL_SPEED) F(F_VLIM_FRAC)
+  F(F_FR_MUR) F(F_BP_CELL) F(F_JL_GAP) F(F_JL_SPEED) F(F_VLIM_FRAC) F(F_SLEEP_LIN) F(F_SLEEP_ANG) F(F_SLEEP_TIME)
 #undef F
   if (d.NCOLW == 0u || d.NCOLW > 64u || d.NCOL != d.NCOLW * 32u) { why = "bad color table size"; return STEEL_E_INVALID; }
   if (d.MAXC == 0u || d.MAXP == 0u || d.WH == 0u || d.AH == 0u) { why = "zero capacity"; return STEEL_E_INVALID; }
@@ -192,7 +192,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
     auto put = [&](uint32_t& field, size_t n) { field = (uint32_t)ao; ao += n > 0 ? n : 1; };
     uint32_t tmp;
     put(d.A_Q, NQ); put(d.A_QD, ND); put(d.A_QDH, ND); put(d.A_INT, ND); put(d.A_TGT, ND); put(d.A_TGTV, ND);
-    put(d.A_LIM, 2 * ND); put(d.A_DRV, ND); put(tmp, ND); put(d.A_JF, ND); put(d.A_BF, NB * 8); put(tmp, (NB + NA) * 4);
+    put(d.A_LIM, 2 * ND); put(d.A_DRV, ND); put(tmp, ND); put(d.A_JF, ND); put(d.A_BF, NB * 8); put(d.A_SLP, (NB + NA) * 4);
     put(d.A_FRIC, ND); put(d.A_HINV, ND);
     ao = (ao + 3) & ~(size_t)3;  // link blocks start on a 16-byte boundary (bulk copies)
     put(d.A_LINK, (size_t)(NL > 0 ? NL : 1) * 268); put(tmp, NB * 8 + ND);
@@ -211,6 +211,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
     put(d.S_RUNIT, MAXC); put(d.S_RCON, MAXC); put(d.S_PCOL, MAXC); put(d.S_PORD, MAXC);
     put(d.S_CSTART, d.NCOL + 2); put(d.S_META, 8); put(d.S_WWIN, d.WH); put(d.S_WSLOT, (size_t)MAXC + d.MAXDENSE);
     put(d.S_WMASK, (size_t)NB * d.NCOLW); put(d.S_WCOUNT, d.NCOL + 2); put(d.S_LINKHIT, NB); put(d.S_JSPLIT, NL);
+    put(d.S_UF, NB + NA); put(d.S_UFF, NB + NA);
     s.sched_words = so;
   }
   s.warm_words = 10ull * d.WH + 30ull * d.AH;
@@ -792,7 +793,7 @@ int steel_layout_get(steel_batch* b, uint32_t scene, const char* key, uint64_t* 
   const SceneDev& d = s->d;
 #define L1(k) if (!std::strcmp(key, #k)) { *value = d.k; return STEEL_OK; }
   L1(A_Q) L1(A_QD) L1(A_QDH) L1(A_INT) L1(A_TGT) L1(A_TGTV) L1(A_LIM) L1(A_DRV) L1(A_JF) L1(A_BF) L1(A_FRIC)
-  L1(A_HINV) L1(A_LINK) L1(A_VLG) L1(A_LG) L1(A_RL) L1(A_RLN) L1(A_ULOAD) L1(A_DENSE) L1(ROWS) L1(PO)
+  L1(A_HINV) L1(A_LINK) L1(A_VLG) L1(A_LG) L1(A_RL) L1(A_RLN) L1(A_ULOAD) L1(A_DENSE) L1(A_SLP) L1(A_AVL) L1(ROWS) L1(PO)
   L1(S_UKEY) L1(S_USIZE) L1(S_USTART) L1(S_RUNIT) L1(S_RCON) L1(S_PCOL) L1(S_PORD) L1(S_CSTART) L1(S_META)
   L1(S_KEEP) L1(S_CORDER) L1(S_KEPT)
 #undef L1

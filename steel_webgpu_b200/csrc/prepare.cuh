@@ -51,6 +51,24 @@ struct Prep {
     return m;
   }
   __device__ uint32_t* sc(uint32_t off) const { return S.sched + off; }
+  // Sleep-island node of body b (artwgsl.js:49 node_asleep's index): a free body is its own node,
+  // a link its articulation's (NB + a); static bodies have none.
+  __device__ int bnode(int b) const {
+    if (b < 0) return -1;
+    uint32_t k = bkind(b);
+    if (k == 1u) return b;
+    if (k == 2u || k == 3u) return (int)S.NB + bart(b);
+    return -1;
+  }
+  __device__ bool node_asleep(int n) const {
+    return S.SLEEP == 1u && n >= 0 && S.art[S.A_SLP + (uint32_t)n * 4u + 1u] > 0.5f;
+  }
+  // Both sides asleep or static (wgsl.js:1732-1736): the contact makes no rows.
+  __device__ bool pair_asleep(int a, int b) const {
+    if (S.SLEEP == 0u) return false;
+    int na = bnode(a), nb = bnode(b);
+    return (na < 0 || node_asleep(na)) && (nb < 0 || node_asleep(nb));
+  }
 
   // Twist change of body b for a unit (force, torque) impulse (wgsl.js:1299-1328).
   __device__ void response(int b, f3 f, f3 t, f3 out[2], bool unsplit = false) const {
@@ -502,6 +520,106 @@ struct Prep {
   }
 };
 
+// Sleep islands (wgsl.js:1371-1457), by the whole block. Islands are nodes (free bodies,
+// articulations) joined by contacts: roots hook under the smaller root (atomicMin) and paths are
+// compressed until a round joins nothing, so each node ends pointing at its island's lowest node
+// whatever the order of the atomics. A round that changes something joins two islands, so NN + 1
+// rounds always suffice; the loop is bounded by that. Island flags OR onto the root: 1 supported
+// (touches static geometry, or a fixed-base articulation), 2 vetoed (moving, driven, loop or
+// mimic owner; picking is not carried), 4 some member younger than the quiet time. Ages and the
+// asleep flags are in A_SLP (age, asleep) per node; S_META + 5 counts the sleeping nodes.
+__device__ __forceinline__ void sleep_islands(const Prep& pr, uint32_t tid, uint32_t nt) {
+  const SceneDev& S = pr.S;
+  const Art& ar = pr.ar;
+  const uint32_t NN = S.NB + S.NA;
+  uint32_t* uf = S.sched + S.S_UF;
+  uint32_t* uff = S.sched + S.S_UFF;
+  float* A = S.art;
+  __shared__ uint32_t changed;
+  for (uint32_t n = tid; n < NN; n += nt) { uf[n] = n; uff[n] = 0u; }
+  if (tid == 0u) S.sched[S.S_META + 5u] = 0u;
+  __syncthreads();
+  const uint32_t nc = min(S.counters[1], S.MAXC);
+  for (uint32_t c = tid; c < nc; c += nt) {
+    float4 m = S.con[c * 5u + 2u];
+    int na = pr.bnode(f2i(m.x)), nb = pr.bnode(f2i(m.y));
+    if ((na < 0 || nb < 0) && max(na, nb) >= 0 && S.con[c * 5u].w <= 1e-5f) atomicOr(&uff[max(na, nb)], 1u);
+  }
+  // Parent links change under other threads' atomics: read them volatile.
+  auto find = [&](uint32_t n) {
+    const volatile uint32_t* v = uf;
+    uint32_t r = n;
+    for (uint32_t k = 0; k < NN; k++) {
+      uint32_t p = v[r];
+      if (p == r) break;
+      r = p;
+    }
+    return r;
+  };
+  for (uint32_t round = 0; round <= NN; round++) {
+    if (tid == 0u) changed = 0u;
+    __syncthreads();
+    for (uint32_t c = tid; c < nc; c += nt) {
+      float4 m = S.con[c * 5u + 2u];
+      int na = pr.bnode(f2i(m.x)), nb = pr.bnode(f2i(m.y));
+      if (na < 0 || nb < 0) continue;
+      uint32_t ra = find((uint32_t)na), rb = find((uint32_t)nb);
+      if (ra != rb) { atomicMin(&uf[max(ra, rb)], min(ra, rb)); changed = 1u; }
+    }
+    __syncthreads();
+    for (uint32_t n = tid; n < NN; n += nt) {
+      uint32_t r = find(n);
+      reinterpret_cast<volatile uint32_t*>(uf)[n] = r;
+    }
+    __syncthreads();
+    const bool more = changed != 0u;
+    __syncthreads();  // every thread has read the flag before thread 0 clears it
+    if (!more) break;
+  }
+  for (uint32_t n = tid; n < NN; n += nt) {
+    bool moving = false, fixed = false, veto = false;
+    if (n < S.NB) {
+      if (pr.bkind((int)n) != 1u) continue;
+      if (A[S.A_SLP + n * 4u + 1u] < 0.5f)
+        moving = len(v3(S.lv[n])) > S.F_SLEEP_LIN || len(v3(S.av[n])) > S.F_SLEEP_ANG;
+    } else {
+      const uint32_t a = n - S.NB;
+      uint4 ai = ar.info(a);
+      fixed = ar.ltype(ai.x) != 4u;
+      for (uint32_t k = 0; k < ai.y; k++) {
+        SVec v = ar.ldsv(ar.lo(ai.x + k) + L_V);
+        if (A[S.A_SLP + n * 4u + 1u] < 0.5f && (len(v.l) > S.F_SLEEP_LIN || len(v.a) > S.F_SLEEP_ANG)) moving = true;
+      }
+      for (uint32_t d = ai.z; d < ai.z + ai.w; d++) {
+        float4 dr = ar.dof_drive(d);
+        if (dr.y > 0.0f || dr.z > 0.0f) veto = true;
+      }
+      if (S.su[S.SU_ACON + a] != 0u) veto = true;
+    }
+    uint32_t f = (fixed ? 1u : 0u) | ((moving || veto) ? 2u : 0u) | (uff[n] & 1u);
+    atomicOr(&uff[uf[n]], f);
+  }
+  __syncthreads();
+  // Ages: reset in vetoed or unsupported islands, else grown to the quiet time.
+  for (uint32_t n = tid; n < NN; n += nt) {
+    if (n < S.NB && pr.bkind((int)n) != 1u) continue;
+    uint32_t r = uf[n];
+    uint32_t f = reinterpret_cast<volatile uint32_t*>(uff)[r];
+    float age = A[S.A_SLP + n * 4u];
+    if ((f & 2u) != 0u || (f & 1u) == 0u) age = 0.0f;
+    else age = fmn(age + pr.P.dt, S.F_SLEEP_TIME);
+    A[S.A_SLP + n * 4u] = age;
+    if (age < S.F_SLEEP_TIME) atomicOr(&uff[r], 4u);
+  }
+  __syncthreads();
+  for (uint32_t n = tid; n < NN; n += nt) {
+    if (n < S.NB && pr.bkind((int)n) != 1u) continue;
+    bool s = (uff[uf[n]] & 4u) == 0u;
+    A[S.A_SLP + n * 4u + 1u] = s ? 1.0f : 0.0f;
+    if (s) atomicAdd(&S.sched[S.S_META + 5u], 1u);
+  }
+}
+
 // Prepare of scene sc by the calling block (all its threads).
 template <bool F64>
 __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
@@ -561,6 +679,7 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
     float4 c = S.sf[S.SF_CTRL];
     A[S.A_TGTV + S.CTRL_B] = c.y * clmp(A[S.A_Q + S.CTRL_A] / c.x, 0.0f, 1.0f);
   }
+  if (S.SLEEP == 1u) sleep_islands(pr, tid, nt);
   __syncthreads();
   // Joint-limit gating, listed joint rows, FK and factorisation per articulation.
   for (uint32_t a = tid; a < S.NA; a += nt) {
@@ -623,7 +742,15 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
     int a = f2i(m.x), b = f2i(m.y);
     return a >= 0 && b >= 0 && pr.bkind(a) == 2u && pr.bkind(b) == 2u && pr.bart(a) == pr.bart(b);
   };
+  // Contacts between sleeping (or static) sides make no rows (wgsl.js:1905). A same-articulation
+  // contact is asleep exactly when its articulation is, so every dense contact left has rows.
+  auto asleep = [&](uint32_t c) {
+    if (S.SLEEP == 0u) return false;
+    float4 m = S.con[c * 5u + 2u];
+    return pr.pair_asleep(f2i(m.x), f2i(m.y));
+  };
   for (uint32_t c = c_lo; c < c_hi; c++) {
+    if (asleep(c)) continue;
     if (is_dense(c)) { dn++; continue; }
     listed++;
     if (c == 0u || pair_of(c - 1u) != pair_of(c)) heads++;
@@ -635,6 +762,11 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
   {
     uint32_t unit = ubase, pos = lbase, ds = dbase;
     for (uint32_t c = c_lo; c < c_hi; c++) {
+      if (asleep(c)) {
+        sch[S.S_UNITOF + c] = 0xffffffffu;
+        sch[S.S_DSLOT + c] = 0xffffffffu;
+        continue;
+      }
       if (is_dense(c)) {
         sch[S.S_UNITOF + c] = 0xffffffffu;
         sch[S.S_DSLOT + c] = ds++;

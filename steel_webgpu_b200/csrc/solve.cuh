@@ -591,6 +591,17 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
   float* A = S.art;
   // Prologue (wgsl.js:3635-3691).
   for (uint32_t i = tid; i < S.ND; i += nt) sv.aqd[i] = A[S.A_QDH + i];
+  auto asleep = [&](uint32_t n) { return S.SLEEP == 1u && A[S.A_SLP + n * 4u + 1u] > 0.5f; };
+  if (S.SLEEP == 1u) {
+    // Sleeping articulations start the solve at rest (wgsl.js:3640-3646). The reference zeroes
+    // them with no barrier after the copy above; the zeros are its intent and are what runs here.
+    __syncthreads();
+    for (uint32_t a = tid; a < S.NA; a += nt) {
+      if (!asleep(S.NB + a)) continue;
+      uint4 ai = sv.ar.info(a);
+      for (uint32_t d = ai.z; d < ai.z + ai.w; d++) sv.aqd[d] = 0.0f;
+    }
+  }
   for (uint32_t b = tid; b < S.NB; b += nt) {
     uint32_t kind = sv.bkind((int)b);
     sv.imp[b * 2u] = make_float4(0, 0, 0, 0);
@@ -600,7 +611,7 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     sv.tw[b * 2u + 1u] = make_float4(0, 0, 0, 0);
     if (kind != 1u) continue;
     uint32_t fl = sv.bflags((int)b);
-    f3 v = v3(S.lv[b]) + (fl != 0u ? sp3(0.0f) : v3(P.gravity) * P.dt);
+    f3 v = v3(S.lv[b]) + ((asleep(b) || fl != 0u) ? sp3(0.0f) : v3(P.gravity) * P.dt);
     f3 w = v3(S.av[b]);
     uint32_t bfo = S.A_BF + b * 8u;
     f3 bf = mf3(A[bfo], A[bfo + 1], A[bfo + 2]), bt = mf3(A[bfo + 4], A[bfo + 5], A[bfo + 6]);
@@ -671,6 +682,11 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     float damp = (sv.bflags((int)b) & 1u) != 0u ? 1.0f : 1.0f - S.sf[S.SF_BODY + b * 8u + 3u].w * P.dt;
     S.lv[b] = mf4(v, 0.0f);
     S.av[b] = mf4(w * damp, 0.0f);
+    if (asleep(b)) {  // a sleeping body stays put at rest (wgsl.js:3779)
+      S.lv[b] = make_float4(0, 0, 0, 0);
+      S.av[b] = make_float4(0, 0, 0, 0);
+      continue;
+    }
     f3 c = v3(S.pos[b]) + v * P.dt;
     float4 q = S.rot[b];
     q = nrm4(add4(q, scale4(0.5f * P.dt, qmul(mf4(w, 0.0f), q))));
@@ -777,6 +793,7 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     st[5] = S.counters[1];
     st[6] = ncol;
     st[7] = max(st[7], S.sched[S.S_META + 3u]);
+    st[8] = S.sched[S.S_META + 5u];
     S.counters[0] = 0u;
     S.counters[1] = 0u;
   }

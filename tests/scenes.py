@@ -88,3 +88,32 @@ def vel_limited(seed=17):
         parent = body
     synth._add_quadruped(b, rng, [1.5, 0.0, 0.9])
     return b.finalize(solver=dict(enable_joint_velocity_limits=True))
+
+
+def sleepers(seed=19):
+    """Sleeping on (enable_sleeping): boxes resting on the plane and a two-box stack settle and fall
+    asleep, a 4-link revolute chain hangs at rest from the world (a fixed-base island), and a box
+    dropped from 2.4 m lands on the stack after about 0.7 s and wakes its island."""
+    rng = np.random.default_rng(seed)
+    b = SceneBuilder(fps=240, box_hulls="direct")
+    b.add_ground_plane(mu=0.6)
+    for i in range(3):
+        body = b.add_body(xform=[-1.0 + 0.5 * i, 0.8, 0.101, 0, 0, 0, 1])
+        h = float(rng.uniform(0.08, 0.12))
+        b.add_shape_box(body, hx=h, hy=h, hz=0.1, mu=0.6)
+    lo = b.add_body(xform=[0.0, 0.0, 0.1, 0, 0, 0, 1])
+    b.add_shape_box(lo, hx=0.2, hy=0.2, hz=0.1, mu=0.6)
+    hi = b.add_body(xform=[0.0, 0.0, 0.3, 0, 0, 0, 1])
+    b.add_shape_box(hi, hx=0.15, hy=0.15, hz=0.1, mu=0.6)
+    drop = b.add_body(xform=[0.02, 0.01, 2.8, 0, 0, 0, 1])
+    b.add_shape_box(drop, hx=0.08, hy=0.08, hz=0.08, mu=0.6)
+    parent = -1
+    top = [1.2, -0.8, 1.5]
+    for k in range(4):
+        body = b.add_body(xform=[top[0], top[1], top[2] - 0.1 * (k + 0.5), 0, 0, 0, 1])
+        b.add_shape_capsule(body, radius=0.02, half_height=0.04, mass=0.2)
+        b.add_joint_revolute(parent, body, axis=[0, 1, 0],
+                             parent_xform=[0, 0, -0.05, 0, 0, 0, 1] if parent >= 0 else top + [0, 0, 0, 1],
+                             child_xform=[0, 0, 0.05, 0, 0, 0, 1])
+        parent = body
+    return b.finalize(solver=dict(enable_sleeping=True))

@@ -128,6 +128,33 @@ def test_fp64_and_fp32_scenes_in_one_batch(steel, oracle_lib):
     assert not np.array_equal(_bits(g.poses(0)), _bits(g.poses(1))), "the option changed nothing"
 
 
+def test_sleeping_bit_exact(steel, oracle_lib):
+    """Islands fall asleep, wake on contact and sleep again identically: poses, velocities, joint
+    state, per-node (age, asleep) words and the asleep count every 20 frames over 320 frames."""
+    pk = pack(scenes.sleepers())
+    assert pk.C["SLEEP"] == 1
+    o = oracle_lib.OracleSim(pk)
+    g = Batch([pk])
+    nn = pk.NB + pk.NA
+    counts = []
+    for k in range(16):
+        o.step(20)
+        g.step(20)
+        oa = o.read("art")
+        assert np.array_equal(_bits(g.poses()), _bits(o.read("poses")[:pk.NB * 8])), f"poses differ at {20 * (k + 1)}"
+        _, gv, gq, gqd, _ = g.raw_state()
+        assert np.array_equal(_bits(gv), _bits(o.read("vel")[:pk.NB * 8]))
+        assert np.array_equal(_bits(gq), _bits(oa[pk.C["A_Q"]:pk.C["A_Q"] + pk.NQ]))
+        gslp = g.read_words("art", g.layout("A_SLP"), nn * 4)
+        assert np.array_equal(_bits(gslp), _bits(oa[pk.C["A_SLP"]:pk.C["A_SLP"] + nn * 4])), "sleep words differ"
+        ost = o.read("stats", np.uint32)
+        assert g.stats()["asleep"] == int(ost[8])
+        counts.append(int(ost[8]))
+    # Asleep, woken by the dropped box, asleep again.
+    first = next(i for i, c in enumerate(counts) if c >= 6)
+    assert min(counts[first:]) < counts[first] and counts[-1] >= 6, counts
+
+
 def test_reset_replays_identically(steel):
     pk = pack(scenes.boxes(24))
     g = Batch([pk])
