@@ -49,7 +49,6 @@ bool Oracle::init(const char* constants, const float* statF_, size_t nF, const u
   else if (C.ANG || C.ANG_ART) unsup = "torsional/rolling friction";
   else if (C.TORS) unsup = "contact torsion";
   else if (C.COMPL) unsup = "contact_compliance";
-  else if (C.NEST) unsup = "nesterov_momentum";
   else if (C.CTI) unsup = "row_schedule contact_then_internal";
   else if (C.LONGEST_FIRST) unsup = "propagation_color_order longest_first";
   else if (C.DRIVE_ROWS) unsup = "drive_mode rows";

@@ -368,6 +368,84 @@ v3 Oracle::body_motion(int b, v3 x) const {
   return lin + cross(ang, x - 0.5f * (p0 + p1));
 }
 
+// nesterov_momentum (wgsl.js:3491-3557): MuJoCo's PGS acceleration on the contact rows. Each row's
+// impulse is extrapolated by beta along its change since the last extrapolation, and the change
+// e = y - lam reaches the twists and link impulses through the row's own response, as a sweep
+// update would. rows[o + MO] keeps lam at the last extrapolation, rows[o + MO + 1] keeps e.
+void Oracle::momentum_unit(uint32_t us, uint32_t row, float beta, bool init) {
+  const uint32_t o = row * C.ROWS, MO = C.MO;
+  v4 lam = rows[o + 6u];
+  if (init) {
+    rows[o + MO] = mk4(xyz(lam), 0.0f);
+    rows[o + MO + 1u] = mk4(0.0f, 0.0f, 0.0f, 0.0f);
+    return;
+  }
+  v3 y = xyz(lam) + beta * (xyz(lam) - xyz(rows[o + MO]));
+  v3 e = y - xyz(lam);
+  rows[o + MO] = mk4(xyz(lam), 0.0f);
+  rows[o + MO + 1u] = mk4(e, 0.0f);
+  if (e.x == 0.0f && e.y == 0.0f && e.z == 0.0f) return;
+  rows[o + 6u] = mk4(y, lam.w);
+  uint32_t key = sched[C.S_UKEY + us];
+  int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
+  v3 ta[2], tb[2];
+  load_tw(a, ta);
+  load_tw(b, tb);
+  ta[0] = ta[0] + ((xyz(rows[o + 7u]) * e.x + xyz(rows[o + 11u]) * e.y) + xyz(rows[o + 15u]) * e.z);
+  ta[1] = ta[1] + ((xyz(rows[o + 8u]) * e.x + xyz(rows[o + 12u]) * e.y) + xyz(rows[o + 16u]) * e.z);
+  tb[0] = tb[0] + ((xyz(rows[o + 9u]) * e.x + xyz(rows[o + 13u]) * e.y) + xyz(rows[o + 17u]) * e.z);
+  tb[1] = tb[1] + ((xyz(rows[o + 10u]) * e.x + xyz(rows[o + 14u]) * e.y) + xyz(rows[o + 18u]) * e.z);
+  v3 ra = xyz(rows[o + 3u]), rb = xyz(rows[o + 4u]);
+  v3 fa = ra, fb = rb;
+  if (C.EXTRA == 1u) { fa = xyz(rows[o + C.PO]); fb = xyz(rows[o + C.PO + 1u]); }
+  v3 fn = xyz(rows[o]) * e.x;
+  v3 ft = xyz(rows[o + 1u]) * e.y + xyz(rows[o + 2u]) * e.z;
+  add_imp(a, (-fn) - ft, (-cross(ra, fn)) - cross(fa, ft));
+  add_imp(b, fn + ft, cross(rb, fn) + cross(fb, ft));
+  if (a >= 0) { tw[(uint32_t)a * 2u] = mk4(ta[0], 0.0f); tw[(uint32_t)a * 2u + 1u] = mk4(ta[1], 0.0f); }
+  if (b >= 0) { tw[(uint32_t)b * 2u] = mk4(tb[0], 0.0f); tw[(uint32_t)b * 2u + 1u] = mk4(tb[1], 0.0f); }
+}
+
+// One momentum step before a position sweep (wgsl.js:3528-3557), with the O'Donoghue-Candes
+// restart when the last sweep's correction opposed its extrapolation or friction switches on.
+// The restart test sums per-invocation partials of the 256-invocation solve workgroup
+// (wgsl.js:2503), each over rows tid, tid + 256, ..., then the partials in invocation order.
+void Oracle::momentum_step(uint32_t ncol, uint32_t it) {
+  const uint32_t NCOL = C.NCOL, WGS = 256u;
+  const uint32_t nrows = wcs[NCOL + 1u];
+  if (it > 0u) {
+    float total = 0.0f;
+    for (uint32_t t = 0; t < WGS; t++) {
+      float part = 0.0f;
+      for (uint32_t u = t; u < nrows; u += WGS) {
+        uint32_t o = sched[C.S_PORD + u] * C.ROWS;
+        v3 e = xyz(rows[o + C.MO + 1u]);
+        part += dot((xyz(rows[o + 6u]) - xyz(rows[o + C.MO])) - e, e);
+      }
+      total += part;
+    }
+    float k = (total < 0.0f || it == C.FSTART) ? 0.0f : wmom_k + 1.0f;
+    wmom_k = k;
+    wmom_beta = k > 1.0f ? (k - 1.0f) / (k + 2.0f) : 0.0f;
+  } else {
+    wmom_k = 0.0f;
+    wmom_beta = 0.0f;
+  }
+  const float beta = wmom_beta;
+  for (uint32_t c = 0; c < NCOL; c++) {
+    if (c >= ncol) break;
+    for (uint32_t u = wcs[c]; u < wcs[c + 1u]; u++) {
+      uint32_t row = sched[C.S_PORD + u];
+      momentum_unit(sched[C.S_RUNIT + row], row, beta, it == 0u);
+    }
+  }
+  for (uint32_t u = wcs[NCOL]; u < wcs[NCOL + 1u]; u++) {
+    uint32_t row = sched[C.S_PORD + u];
+    momentum_unit(sched[C.S_RUNIT + row], row, beta, it == 0u);
+  }
+  for (uint32_t a = 0; a < C.NA; a++) { art_contact_impulses(a); art_propagate(a, true, false); }
+}
+
 void Oracle::sweep(uint32_t mode, uint32_t ncol0, uint32_t it, uint32_t ph) {
   const uint32_t NCOL = C.NCOL;
   uint32_t ncol = ph == 2u ? 0u : ncol0;
@@ -492,7 +570,10 @@ void Oracle::k_solve() {
   for (uint32_t a = 0; a < C.NA; a++) art_twists(a);
   dense_phase(0u, 0u, 0u);
   sweep(0u, wn_y, 0u, 0u);
-  for (uint32_t it = 0; it < P.iterations; it++) sweep(1u, wn_y, it, 0u);
+  for (uint32_t it = 0; it < P.iterations; it++) {
+    if (C.NEST == 1u) momentum_step(wn_y, it);
+    sweep(1u, wn_y, it, 0u);
+  }
   // Warm-start table store (wgsl.js:3737-3767).
   uint32_t nc = sc[C.S_USTART + wn_x];
   uint32_t ndense = std::min(sc[C.S_META + 3u], C.MAXDENSE);

@@ -486,6 +486,98 @@ struct Solver {
     }
     __syncthreads();
   }
+  // nesterov_momentum (wgsl.js:3491-3557): MuJoCo's PGS acceleration on the contact rows. Each
+  // row's impulse is extrapolated by beta along its change since the last extrapolation, and the
+  // change e = y - lam reaches the twists and link impulses through the row's own response, as a
+  // sweep update would. rows[o + MO] keeps lam at the last extrapolation, rows[o + MO + 1] keeps e.
+  __device__ void momentum_unit(uint32_t us, uint32_t row, float beta, bool init) const {
+    float4* R = S.rows + (size_t)row * S.ROWS;
+    const uint32_t MO = S.MO;
+    const float4 lam = R[6];
+    if (init) {
+      R[MO] = mf4(v3(lam), 0.0f);
+      R[MO + 1u] = make_float4(0, 0, 0, 0);
+      return;
+    }
+    f3 y = v3(lam) + beta * (v3(lam) - v3(R[MO]));
+    f3 e = y - v3(lam);
+    R[MO] = mf4(v3(lam), 0.0f);
+    R[MO + 1u] = mf4(e, 0.0f);
+    if (e.x == 0.0f && e.y == 0.0f && e.z == 0.0f) return;
+    R[6] = mf4(y, lam.w);
+    uint32_t key = S.sched[S.S_UKEY + us];
+    int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
+    f3 ta[2], tb[2];
+    load_tw(a, ta);
+    load_tw(b, tb);
+    ta[0] = ta[0] + ((v3(R[7]) * e.x + v3(R[11]) * e.y) + v3(R[15]) * e.z);
+    ta[1] = ta[1] + ((v3(R[8]) * e.x + v3(R[12]) * e.y) + v3(R[16]) * e.z);
+    tb[0] = tb[0] + ((v3(R[9]) * e.x + v3(R[13]) * e.y) + v3(R[17]) * e.z);
+    tb[1] = tb[1] + ((v3(R[10]) * e.x + v3(R[14]) * e.y) + v3(R[18]) * e.z);
+    f3 ra = v3(R[3]), rb = v3(R[4]);
+    f3 fa = ra, fb = rb;
+    if (S.EXTRA == 1u) { fa = v3(R[S.PO]); fb = v3(R[S.PO + 1u]); }
+    f3 fn = v3(R[0]) * e.x;
+    f3 ft = v3(R[1]) * e.y + v3(R[2]) * e.z;
+    add_imp(a, (-fn) - ft, (-cross(ra, fn)) - cross(fa, ft));
+    add_imp(b, fn + ft, cross(rb, fn) + cross(fb, ft));
+    if (a >= 0) { tw[(uint32_t)a * 2u] = mf4(ta[0], 0.0f); tw[(uint32_t)a * 2u + 1u] = mf4(ta[1], 0.0f); }
+    if (b >= 0) { tw[(uint32_t)b * 2u] = mf4(tb[0], 0.0f); tw[(uint32_t)b * 2u + 1u] = mf4(tb[1], 0.0f); }
+  }
+  // One momentum step before a position sweep (wgsl.js:3528-3557), with the O'Donoghue-Candes
+  // restart when the last sweep's correction opposed its extrapolation or friction switches on.
+  // The restart test keeps the reference's sum: partials of its 256-invocation solve workgroup
+  // (wgsl.js:2503), each over rows t, t + 256, ..., added in invocation order by one thread; each
+  // thread of this block computes the partials of invocations tid and tid + 128.
+  __device__ void momentum_step(uint32_t ncol, uint32_t it, const uint32_t* wcs) const {
+    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    constexpr uint32_t WGS = 256u;
+    __shared__ float wred[WGS];
+    __shared__ float wmom[2];  // (k, beta), carried across the iterations of one solve
+    if (it > 0u) {
+      const uint32_t nrows = wcs[S.NCOL + 1u];
+      for (uint32_t t = tid; t < WGS; t += nt) {
+        float part = 0.0f;
+        for (uint32_t u = t; u < nrows; u += WGS) {
+          const float4* R = S.rows + (size_t)S.sched[S.S_PORD + u] * S.ROWS;
+          f3 e = v3(R[S.MO + 1u]);
+          part += dot((v3(R[6]) - v3(R[S.MO])) - e, e);
+        }
+        wred[t] = part;
+      }
+      __syncthreads();
+      if (tid == 0u) {
+        float total = 0.0f;
+        for (uint32_t i = 0; i < WGS; i++) total += wred[i];
+        float k = (total < 0.0f || it == S.FSTART) ? 0.0f : wmom[0] + 1.0f;
+        wmom[0] = k;
+        wmom[1] = k > 1.0f ? (k - 1.0f) / (k + 2.0f) : 0.0f;
+      }
+    } else if (tid == 0u) {
+      wmom[0] = 0.0f;
+      wmom[1] = 0.0f;
+    }
+    __syncthreads();
+    const float beta = wmom[1];
+    for (uint32_t c = 0; c < ncol; c++) {
+      for (uint32_t u = wcs[c] + tid; u < wcs[c + 1u]; u += nt) {
+        uint32_t row = S.sched[S.S_PORD + u];
+        momentum_unit(S.sched[S.S_RUNIT + row], row, beta, it == 0u);
+      }
+      __syncthreads();
+    }
+    if (tid == 0u)
+      for (uint32_t u = wcs[S.NCOL]; u < wcs[S.NCOL + 1u]; u++) {
+        uint32_t row = S.sched[S.S_PORD + u];
+        momentum_unit(S.sched[S.S_RUNIT + row], row, beta, it == 0u);
+      }
+    __syncthreads();
+    for (uint32_t a = tid; a < S.NA; a += nt) {
+      contact_impulses(a);
+      if (S.VLIM_ON == 1u) vlim_rows(a);
+    }
+    __syncthreads();
+  }
   // One sweep (wgsl.js:3559-3611).
   __device__ void sweep(uint32_t mode, uint32_t ncol, uint32_t it, const uint32_t* wcs, uint32_t nu) const {
     const uint32_t tid = threadIdx.x, nt = blockDim.x;
@@ -642,7 +734,10 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
   __syncthreads();
   sv.dense_phase(0u, 0u, 0u);
   sv.sweep(0u, ncol, 0u, wcs, nu);
-  for (uint32_t it = 0; it < P.iterations; it++) sv.sweep(1u, ncol, it, wcs, nu);
+  for (uint32_t it = 0; it < P.iterations; it++) {
+    if (S.NEST == 1u) sv.momentum_step(ncol, it, wcs);
+    sv.sweep(1u, ncol, it, wcs, nu);
+  }
   // Warm-start table (wgsl.js:3737-3767): rows sharing a key keep the largest normal impulse.
   const uint32_t nc = S.sched[S.S_USTART + nu];
   const uint32_t ndense = min(S.sched[S.S_META + 3u], S.MAXDENSE);

@@ -117,3 +117,18 @@ def sleepers(seed=19):
                              child_xform=[0, 0, 0.05, 0, 0, 0, 1])
         parent = body
     return b.finalize(solver=dict(enable_sleeping=True))
+
+
+def momentum_stack(seed=23):
+    """nesterov_momentum on: a five-box stack whose masses grow 10^0.75 per box (a 10^3 ratio,
+    heavy on light) and a PD-held quadruped standing on the plane (contact impulses on links);
+    friction joins at iteration 8 (contact_friction_position_iterations=4), so the restart at
+    that iteration runs too."""
+    rng = np.random.default_rng(seed)
+    b = SceneBuilder(fps=240, box_hulls="direct")
+    b.add_ground_plane(mu=0.7)
+    for k in range(5):
+        body = b.add_body(xform=[0.0, 0.0, 0.1 + 0.2 * k + 0.002 * k, 0, 0, 0, 1])
+        b.add_shape_box(body, hx=0.15, hy=0.15, hz=0.1, mu=0.7, mass=float(0.2 * 10.0 ** (0.75 * k)))
+    synth._add_quadruped(b, rng, [1.2, 0.0, 0.9])
+    return b.finalize(solver=dict(nesterov_momentum=True, contact_friction_position_iterations=4))
