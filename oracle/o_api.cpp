@@ -47,7 +47,6 @@ bool Oracle::init(const char* constants, const float* statF_, size_t nF, const u
   const char* unsup = nullptr;
   if (C.FMODE) unsup = "friction_mode";
   else if (C.ANG || C.ANG_ART) unsup = "torsional/rolling friction";
-  else if (C.TORS) unsup = "contact torsion";
   else if (C.COMPL) unsup = "contact_compliance";
   else if (C.CTI) unsup = "row_schedule contact_then_internal";
   else if (C.LONGEST_FIRST) unsup = "propagation_color_order longest_first";

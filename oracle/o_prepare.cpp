@@ -176,6 +176,47 @@ uint32_t Oracle::unit_of(uint32_t p, uint32_t nu) const {
 
 static inline uint32_t anchor_hash(uint32_t pair, uint32_t k) { return std::max(hash_u32(pair * 2u + k), 1u); }
 
+// build_torsion (wgsl.js:1526-1557): contact torsion (min_torsional_patch_radius), one spin row
+// per articulated unit about the normal of its touching coplanar cluster. The cluster is the
+// unit's rows within 0.995 of the deepest row's normal and 2 mm of its plane; its radius is the
+// members' largest torsion radius. The header lives in the unit's first row: (Ma lin, mu),
+// (Ma ang, 1/K), (Mb lin, spin impulse), (Mb ang, r), (n, member).
+void Oracle::build_torsion(uint32_t sp) {
+  const uint32_t* sc = sched.data();
+  const uint32_t ROWS = C.ROWS, TO = C.TO;
+  uint32_t st = sc[C.S_USTART + sp];
+  uint32_t n = std::min(sc[C.S_USIZE + sp], C.MAXC - std::min(st, C.MAXC));
+  if (n == 0u) return;
+  uint32_t pair = sc[C.S_UKEY + sp];
+  int a = (int)(pair & 0xffffu) - 1, b = (int)(pair >> 16u) - 1;
+  uint32_t L = st * ROWS;
+  bool art_u = (a >= 0 && body_kind(a) >= 2u) || (b >= 0 && body_kind(b) >= 2u);
+  uint32_t seed = st;
+  for (uint32_t i = st; i < st + n; i++)
+    if (rows[i * ROWS + 1u].w < rows[seed * ROWS + 1u].w) seed = i;
+  v3 ns = xyz(rows[seed * ROWS]), ps = xyz(rows[seed * ROWS + TO + 4u]);
+  float r = 0.0f;
+  for (uint32_t i = st; i < st + n; i++) {
+    uint32_t o = i * ROWS;
+    bool member = art_u && rows[o + 6u].w <= 0.0f && dot(xyz(rows[o]), ns) >= 0.995f &&
+                  std::fabs(dot(xyz(rows[o + TO + 4u]) - ps, ns)) <= 0.002f;
+    if (member) r = fmaxf_(r, rows[o + TO + 3u].w);
+    rows[o + TO + 4u].w = member ? 1.0f : 0.0f;
+  }
+  float mu = rows[seed * ROWS + 2u].w;
+  if (r <= 0.0f || mu <= 0.0f) { rows[L + TO] = mk4(0.0f, 0.0f, 0.0f, 0.0f); return; }
+  v3 Ma[2], Mb[2];
+  body_response(a, splat3(0.0f), -ns, Ma);
+  body_response(b, splat3(0.0f), ns, Mb);
+  float k = dot(-ns, Ma[1]) + dot(ns, Mb[1]);
+  float lead = rows[L + TO + 4u].w;
+  rows[L + TO] = mk4(Ma[0], mu);
+  rows[L + TO + 1u] = mk4(Ma[1], k > 1e-12f ? 1.0f / (k + C.F_CFM) : 0.0f);
+  rows[L + TO + 2u] = mk4(Mb[0], 0.0f);
+  rows[L + TO + 3u] = mk4(Mb[1], r);
+  rows[L + TO + 4u] = mk4(ns, lead);
+}
+
 // build_patch (wgsl.js:1562-1725)
 void Oracle::build_patch(uint32_t sp) {
   const uint32_t ROWS = C.ROWS, PO = C.PO;
@@ -709,6 +750,10 @@ void Oracle::k_prepare() {
       rows[o + PO + 1u] = mk4(fb, 0.0f);
       rows[o + PO + 2u] = mk4(p, 0.0f);
     }
+    if (C.TORS == 1u) {
+      rows[o + C.TO + 3u] = mk4(0.0f, 0.0f, 0.0f, contacts[c * 5u + 3u].w);
+      rows[o + C.TO + 4u] = mk4(p, 0.0f);
+    }
     float kscale = fmaxf_((K[0] + K[4]) + K[8], 1e-30f);
     float effn = 0.0f;
     if (K[0] > 1e-6f * kscale && K[0] > 1e-12f) effn = 1.0f / (K[0] + C.F_CFM);
@@ -761,7 +806,8 @@ void Oracle::k_prepare() {
     rows[o + 5u] = mk4(k11 / det, -k01 / det, k00 / det, bounce ? 1.0f : wrow);
     rows[o + 6u] = mk4(ln, lt.x, lt.y, bounce ? 1e30f : phi);
   }
-  // Phase 6b: friction patches.
+  // Phase 6b: contact torsion headers, then friction patches.
+  if (C.TORS == 1u) for (uint32_t sp = 0; sp < nu; sp++) build_torsion(sp);
   if (C.PATCH == 1u) for (uint32_t sp = 0; sp < nu; sp++) build_patch(sp);
   // Phase 6c: coloring in walk order.
   uint32_t totp = std::min(sc[C.S_USTART + nu], MAXC);

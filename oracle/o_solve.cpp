@@ -122,7 +122,7 @@ void Oracle::solve_slot(uint32_t u, uint32_t mode, uint32_t it) {
 }
 
 // solve_unit (wgsl.js:3033-3231), fixed_normal friction with anchors.
-void Oracle::solve_unit(uint32_t us, uint32_t row, int a, int b, uint32_t /*s0*/, uint32_t /*s1*/, uint32_t mode,
+void Oracle::solve_unit(uint32_t us, uint32_t row, int a, int b, uint32_t s0, uint32_t s1, uint32_t mode,
                         uint32_t it) {
   const uint32_t ROWS = C.ROWS, PO = C.PO;
   v3 ta[2], tb[2];
@@ -195,6 +195,58 @@ void Oracle::solve_unit(uint32_t us, uint32_t row, int a, int b, uint32_t /*s0*/
       add_imp(b, f, cross(frb, f));
     }
     rows[o + 6u] = lam;
+  }
+  // Contact torsion (wgsl.js:3185-3228) on the unit's last-colored row: sliding and spin share
+  // the cluster's Coulomb budget mu * N.
+  const uint32_t TO = C.TO;
+  if (C.TORS == 1u && mode == 1u && row == sched[C.S_UTP + us] && rows[s0 * ROWS + TO].w > 0.0f) {
+    uint32_t L = s0 * ROWS;
+    float mu = rows[L + TO].w;
+    float load = 0.0f, slide = 0.0f;
+    for (uint32_t m = s0; m < s1; m++) {
+      uint32_t om = m * ROWS;
+      if (rows[om + TO + 4u].w < 0.5f) continue;
+      v4 lm = rows[om + 6u];
+      load += fmaxf_(lm.x, 0.0f);
+      if (C.EXTRA == 0u || rows[om + PO].w != 0.0f) slide += length(mk2(lm.y, lm.z));
+    }
+    float budget = mu * load;
+    if (slide > budget && slide > 0.0f) {
+      // Later normals lowered the load: the members' tangent pairs are projected onto it.
+      float scale = budget / slide;
+      for (uint32_t m = s0; m < s1; m++) {
+        uint32_t om = m * ROWS;
+        if (rows[om + TO + 4u].w < 0.5f || (C.EXTRA == 1u && rows[om + PO].w == 0.0f)) continue;
+        v4 lm = rows[om + 6u];
+        float d1 = lm.y * (scale - 1.0f), d2 = lm.z * (scale - 1.0f);
+        ta[0] += xyz(rows[om + 11u]) * d1 + xyz(rows[om + 15u]) * d2;
+        ta[1] += xyz(rows[om + 12u]) * d1 + xyz(rows[om + 16u]) * d2;
+        tb[0] += xyz(rows[om + 13u]) * d1 + xyz(rows[om + 17u]) * d2;
+        tb[1] += xyz(rows[om + 14u]) * d1 + xyz(rows[om + 18u]) * d2;
+        v3 fa = xyz(rows[om + 3u]), fb = xyz(rows[om + 4u]);
+        if (C.EXTRA == 1u) { fa = xyz(rows[om + PO]); fb = xyz(rows[om + PO + 1u]); }
+        v3 f = xyz(rows[om + 1u]) * d1 + xyz(rows[om + 2u]) * d2;
+        add_imp(a, -f, -cross(fa, f));
+        add_imp(b, f, cross(fb, f));
+        rows[om + 6u] = mk4(lm.x, lm.y * scale, lm.z * scale, lm.w);
+      }
+      slide = budget;
+    }
+    float bound = rows[L + TO + 3u].w * fmaxf_(budget - slide, 0.0f);
+    if (it < C.FSTART) bound = 0.0f;
+    v3 ng = xyz(rows[L + TO + 4u]);
+    float ls = rows[L + TO + 2u].w;
+    float nls = clampf(ls - (C.F_OMEGA * dot(ng, tb[1] - ta[1])) * rows[L + TO + 1u].w, -bound, bound);
+    float ds = nls - ls;
+    if (ds != 0.0f) {
+      ta[0] += xyz(rows[L + TO]) * ds;
+      ta[1] += xyz(rows[L + TO + 1u]) * ds;
+      tb[0] += xyz(rows[L + TO + 2u]) * ds;
+      tb[1] += xyz(rows[L + TO + 3u]) * ds;
+      rows[L + TO + 2u].w = nls;
+      add_imp(a, splat3(0.0f), (-ng) * ds);
+      add_imp(b, splat3(0.0f), ng * ds);
+    }
   }
   if (a >= 0) { tw[(uint32_t)a * 2u] = mk4(ta[0], 0.0f); tw[(uint32_t)a * 2u + 1u] = mk4(ta[1], 0.0f); }
   if (b >= 0) { tw[(uint32_t)b * 2u] = mk4(tb[0], 0.0f); tw[(uint32_t)b * 2u + 1u] = mk4(tb[1], 0.0f); }

@@ -244,6 +244,7 @@ struct Oracle {
   v4 link_rot(uint32_t l) const { return mk4(ld3(lo(l) + 216u), art[lo(l) + 216u + 3u]); }
   void art_factor(uint32_t a);
   void sleep_islands();
+  void build_torsion(uint32_t sp);
   template <class T>
   float dof_tau(uint32_t l, uint32_t r, T& Drr) const;
   void art_back_f64(uint32_t l);

@@ -143,7 +143,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
   if (!C.parse(in.constants)) { why = "malformed constants text"; return STEEL_E_INVALID; }
   static const char* unsupported[][2] = {
       {"FMODE", "friction_mode"}, {"ANG", "torsional/rolling friction"}, {"ANG_ART", "torsional/rolling friction"},
-      {"TORS", "contact torsion"}, {"COMPL", "contact_compliance"},
+      {"COMPL", "contact_compliance"},
       {"CTI", "row_schedule contact_then_internal"}, {"LONGEST_FIRST", "propagation_color_order longest_first"},
       {"DRIVE_ROWS", "drive_mode rows"},
       {"JFL", "joint friction load coefficient"}, {"VELITERS", "velocity_iterations"}};
@@ -159,7 +159,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
   K(SF_BODY) K(SF_SHAPE) K(SF_HAABB) K(SF_VERTS) K(SF_FPLANE) K(SF_LINK) K(SF_DOF) K(SF_PATH) K(SF_LOOP)
   K(SF_MIMIC) K(SF_CTRL) K(SU_HULL) K(SU_FACE) K(SU_FV) K(SU_HEDGE) K(SU_EDGE) K(SU_ART) K(SU_ACON)
   K(SU_FILTER) K(NB) K(NS) K(NA) K(NL) K(ND) K(NDA) K(JM) K(MAXPATH) K(MAXLP) K(NLOOP) K(NMIMIC) K(PATCH)
-  K(EXTRA) K(SHARED) K(FSHARED) K(REST) K(FSTART) K(TGT_HELD) K(CTRL_KIND) K(CTRL_A) K(CTRL_B) K(VLIM_FREE) K(VLIM_ON) K(ART_F64) K(SLEEP) K(NEST) K(MO)
+  K(EXTRA) K(SHARED) K(FSHARED) K(REST) K(FSTART) K(TGT_HELD) K(CTRL_KIND) K(CTRL_A) K(CTRL_B) K(VLIM_FREE) K(VLIM_ON) K(ART_F64) K(SLEEP) K(NEST) K(MO) K(TORS) K(TO)
   K(FRICTION_COMBINE) K(RESTITUTION_COMBINE) K(NCOLW) K(NCOL) K(MAXP) K(MAXC) K(MAXU) K(WH) K(AH)
   K(MAXDENSE) K(ROWS) K(PO) K(DHDR) K(DPS)
 #undef K
@@ -211,7 +211,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
     put(d.S_RUNIT, MAXC); put(d.S_RCON, MAXC); put(d.S_PCOL, MAXC); put(d.S_PORD, MAXC);
     put(d.S_CSTART, d.NCOL + 2); put(d.S_META, 8); put(d.S_WWIN, d.WH); put(d.S_WSLOT, (size_t)MAXC + d.MAXDENSE);
     put(d.S_WMASK, (size_t)NB * d.NCOLW); put(d.S_WCOUNT, d.NCOL + 2); put(d.S_LINKHIT, NB); put(d.S_JSPLIT, NL);
-    put(d.S_UF, NB + NA); put(d.S_UFF, NB + NA);
+    put(d.S_UF, NB + NA); put(d.S_UFF, NB + NA); put(d.S_UTP, MAXC);
     s.sched_words = so;
   }
   s.warm_words = 10ull * d.WH + 30ull * d.AH;

@@ -195,7 +195,7 @@ struct SceneDev {
   // counts
   uint32_t NB, NS, NA, NL, ND, NQ, NDA, JM, MAXPATH, MAXLP, NLOOP, NMIMIC;
   // solver flags and constants
-  uint32_t PATCH, EXTRA, SHARED, FSHARED, REST, FSTART, TGT_HELD, CTRL_KIND, CTRL_A, CTRL_B, VLIM_FREE, VLIM_ON, ART_F64, SLEEP, NEST, MO;
+  uint32_t PATCH, EXTRA, SHARED, FSHARED, REST, FSTART, TGT_HELD, CTRL_KIND, CTRL_A, CTRL_B, VLIM_FREE, VLIM_ON, ART_F64, SLEEP, NEST, MO, TORS, TO;
   uint32_t FRICTION_COMBINE, RESTITUTION_COMBINE, NCOLW, NCOL;
   float F_ANCHOR_BETA, F_CFM, F_OMEGA, F_SPEC, F_GAP_GATE, F_FGAP, F_FSCALE, F_REST_SPEED, F_FR_MUT, F_FR_MUR;
   float F_BP_CELL, F_JL_GAP, F_JL_SPEED, F_VLIM_FRAC, F_SLEEP_LIN, F_SLEEP_ANG, F_SLEEP_TIME;
@@ -224,7 +224,7 @@ struct SceneDev {
   uint32_t* sched;                   // scheduling arrays, offsets below
   uint32_t S_UNITOF, S_DSLOT, S_CORDER, S_UKEY, S_USTART0, S_USIZE, S_USTART, S_RK0, S_RK1, S_RK2, S_BPC, S_LEAD,
       S_KEEP, S_SLOT, S_KEPT, S_ROWOF, S_RUNIT, S_RCON, S_PCOL, S_PORD, S_CSTART, S_META, S_WWIN, S_WSLOT, S_WMASK,
-      S_WCOUNT, S_LINKHIT, S_JSPLIT, S_UF, S_UFF;
+      S_WCOUNT, S_LINKHIT, S_JSPLIT, S_UF, S_UFF, S_UTP;
   float* tscr;                       // per-thread scratch slices (path temporaries), TSCR floats each
   uint32_t TSCR;
   float4 *tw, *imp;                  // solve: body twists and link impulses [NB * 2]

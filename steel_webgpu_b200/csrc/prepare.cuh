@@ -343,6 +343,47 @@ struct Prep {
   }
 
   // Contact row idx for contact c (wgsl.js:2106-2269).
+  // Contact torsion header of unit sp (wgsl.js:1526-1557; min_torsional_patch_radius): one spin
+  // row per articulated unit about the normal of its touching coplanar cluster, the unit's rows
+  // within 0.995 of the deepest row's normal and 2 mm of its plane; the radius is the members'
+  // largest torsion radius. The header lives in the unit's first row: (Ma lin, mu),
+  // (Ma ang, 1/K), (Mb lin, spin impulse), (Mb ang, r), (n, member).
+  __device__ void build_torsion(uint32_t sp) const {
+    const uint32_t ROWS = S.ROWS, TO = S.TO;
+    float4* rows = S.rows;
+    const uint32_t st = S.sched[S.S_USTART + sp];
+    const uint32_t n = min(S.sched[S.S_USIZE + sp], S.MAXC - min(st, S.MAXC));
+    if (n == 0u) return;
+    const uint32_t pair = S.sched[S.S_UKEY + sp];
+    const int a = (int)(pair & 0xffffu) - 1, b = (int)(pair >> 16u) - 1;
+    const uint32_t L = st * ROWS;
+    const bool art_u = (a >= 0 && bkind(a) >= 2u) || (b >= 0 && bkind(b) >= 2u);
+    uint32_t seed = st;
+    for (uint32_t i = st; i < st + n; i++)
+      if (rows[i * ROWS + 1u].w < rows[seed * ROWS + 1u].w) seed = i;
+    const f3 ns = v3(rows[seed * ROWS]), ps = v3(rows[seed * ROWS + TO + 4u]);
+    float r = 0.0f;
+    for (uint32_t i = st; i < st + n; i++) {
+      const uint32_t o = i * ROWS;
+      const bool member = art_u && rows[o + 6u].w <= 0.0f && dot(v3(rows[o]), ns) >= 0.995f &&
+                          fabsf(dot(v3(rows[o + TO + 4u]) - ps, ns)) <= 0.002f;
+      if (member) r = fmx(r, rows[o + TO + 3u].w);
+      rows[o + TO + 4u].w = member ? 1.0f : 0.0f;
+    }
+    const float mu = rows[seed * ROWS + 2u].w;
+    if (r <= 0.0f || mu <= 0.0f) { rows[L + TO] = make_float4(0, 0, 0, 0); return; }
+    f3 Ma[2], Mb[2];
+    response(a, sp3(0.0f), -ns, Ma);
+    response(b, sp3(0.0f), ns, Mb);
+    const float k = dot(-ns, Ma[1]) + dot(ns, Mb[1]);
+    const float lead = rows[L + TO + 4u].w;
+    rows[L + TO] = mf4(Ma[0], mu);
+    rows[L + TO + 1u] = mf4(Ma[1], k > 1e-12f ? 1.0f / (k + S.F_CFM) : 0.0f);
+    rows[L + TO + 2u] = mf4(Mb[0], 0.0f);
+    rows[L + TO + 3u] = mf4(Mb[1], r);
+    rows[L + TO + 4u] = mf4(ns, lead);
+  }
+
   __device__ void build_row(uint32_t idx, uint32_t c) const {
     const uint32_t ROWS = S.ROWS, PO = S.PO;
     float4* rows = S.rows;
@@ -387,6 +428,10 @@ struct Prep {
       rows[o + PO] = mf4(fa, 1.0f);
       rows[o + PO + 1u] = mf4(fb, 0.0f);
       rows[o + PO + 2u] = mf4(p, 0.0f);
+    }
+    if (S.TORS == 1u) {
+      rows[o + S.TO + 3u] = make_float4(0.0f, 0.0f, 0.0f, S.con[c * 5u + 3u].w);
+      rows[o + S.TO + 4u] = mf4(p, 0.0f);
     }
     float kscale = fmx((K[0] + K[4]) + K[8], 1e-30f);
     float effn = 0.0f;
@@ -893,6 +938,10 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
   // Phase 6: rows, then friction patches.
   for (uint32_t idx = tid; idx < total; idx += nt) pr.build_row(idx, sch[S.S_RCON + idx]);
   __syncthreads();
+  if (S.TORS == 1u) {
+    for (uint32_t u = tid; u < nu; u += nt) pr.build_torsion(u);
+    __syncthreads();
+  }
   if (S.PATCH == 1u)
     for (uint32_t u = tid; u < nu; u += nt) pr.build_patch(u);
   __syncthreads();
@@ -949,6 +998,20 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
       sch[S.S_META + 0u] = nu;
       sch[S.S_META + 1u] = ncol;
       sch[S.S_META + 2u] = nc;
+    }
+    if (S.TORS == 1u) {
+      // Each unit's torsion row is its row of the highest color, the latest contact among equals:
+      // (color + 1, contact) packed as the reference packs it, 16 bits of contact index
+      // (wgsl.js:2288-2325).
+      for (uint32_t u = tid; u < nu; u += nt) sch[S.S_UTP + u] = 0u;
+      __syncthreads();
+      for (uint32_t row = tid; row < total; row += nt)
+        atomicMax(&sch[S.S_UTP + sch[S.S_RUNIT + row]], ((sch[S.S_PCOL + row] + 1u) << 16u) | sch[S.S_RCON + row]);
+      __syncthreads();
+      for (uint32_t u = tid; u < nu; u += nt) {
+        uint32_t packed = sch[S.S_UTP + u];
+        sch[S.S_UTP + u] = packed != 0u ? sch[S.S_ROWOF + (packed & 0xffffu)] : 0xffffffffu;
+      }
     }
     __syncthreads();
     if (tid < 32u) {

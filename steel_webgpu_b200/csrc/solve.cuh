@@ -139,6 +139,61 @@ struct Solver {
 
   // One contact row of unit us (wgsl.js:3033-3231, default option set). mode 0 applies the warm
   // impulses, mode 1 solves.
+  // Contact torsion (wgsl.js:3185-3228), run by a unit's last-colored row in position sweeps:
+  // sliding and spin share the cluster's Coulomb budget mu * N.
+  __device__ void torsion(uint32_t us, int a, int b, uint32_t it, f3 ta[2], f3 tb[2]) const {
+    const uint32_t ROWS = S.ROWS, PO = S.PO, TO = S.TO;
+    float4* rows = S.rows;
+    const uint32_t s0 = S.sched[S.S_USTART + us], s1 = s0 + S.sched[S.S_USIZE + us];
+    const uint32_t L = s0 * ROWS;
+    if (!(rows[L + TO].w > 0.0f)) return;
+    const float mu = rows[L + TO].w;
+    float load = 0.0f, slide = 0.0f;
+    for (uint32_t m = s0; m < s1; m++) {
+      const uint32_t om = m * ROWS;
+      if (rows[om + TO + 4u].w < 0.5f) continue;
+      const float4 lm = rows[om + 6u];
+      load += fmx(lm.x, 0.0f);
+      if (S.EXTRA == 0u || rows[om + PO].w != 0.0f) slide += len(mf2(lm.y, lm.z));
+    }
+    const float budget = mu * load;
+    if (slide > budget && slide > 0.0f) {
+      // Later normals lowered the load: the members' tangent pairs are projected onto it.
+      const float scale = budget / slide;
+      for (uint32_t m = s0; m < s1; m++) {
+        const uint32_t om = m * ROWS;
+        if (rows[om + TO + 4u].w < 0.5f || (S.EXTRA == 1u && rows[om + PO].w == 0.0f)) continue;
+        const float4 lm = rows[om + 6u];
+        const float d1 = lm.y * (scale - 1.0f), d2 = lm.z * (scale - 1.0f);
+        ta[0] += v3(rows[om + 11u]) * d1 + v3(rows[om + 15u]) * d2;
+        ta[1] += v3(rows[om + 12u]) * d1 + v3(rows[om + 16u]) * d2;
+        tb[0] += v3(rows[om + 13u]) * d1 + v3(rows[om + 17u]) * d2;
+        tb[1] += v3(rows[om + 14u]) * d1 + v3(rows[om + 18u]) * d2;
+        f3 fa = v3(rows[om + 3u]), fb = v3(rows[om + 4u]);
+        if (S.EXTRA == 1u) { fa = v3(rows[om + PO]); fb = v3(rows[om + PO + 1u]); }
+        const f3 f = v3(rows[om + 1u]) * d1 + v3(rows[om + 2u]) * d2;
+        add_imp(a, -f, -cross(fa, f));
+        add_imp(b, f, cross(fb, f));
+        rows[om + 6u] = make_float4(lm.x, lm.y * scale, lm.z * scale, lm.w);
+      }
+      slide = budget;
+    }
+    float bound = rows[L + TO + 3u].w * fmx(budget - slide, 0.0f);
+    if (it < S.FSTART) bound = 0.0f;
+    const f3 ng = v3(rows[L + TO + 4u]);
+    const float ls = rows[L + TO + 2u].w;
+    const float nls = clmp(ls - (S.F_OMEGA * dot(ng, tb[1] - ta[1])) * rows[L + TO + 1u].w, -bound, bound);
+    const float ds = nls - ls;
+    if (ds != 0.0f) {
+      ta[0] += v3(rows[L + TO]) * ds;
+      ta[1] += v3(rows[L + TO + 1u]) * ds;
+      tb[0] += v3(rows[L + TO + 2u]) * ds;
+      tb[1] += v3(rows[L + TO + 3u]) * ds;
+      rows[L + TO + 2u].w = nls;
+      add_imp(a, sp3(0.0f), (-ng) * ds);
+      add_imp(b, sp3(0.0f), ng * ds);
+    }
+  }
   __device__ void solve_row(uint32_t us, uint32_t row, int a, int b, uint32_t mode, uint32_t it) const {
     const uint32_t ROWS = S.ROWS, PO = S.PO;
     float4* rows = S.rows;
@@ -210,6 +265,7 @@ struct Solver {
         add_imp(b, f, cross(frb, f));
       }
       rows[o + 6u] = lam;
+      if (S.TORS == 1u && row == S.sched[S.S_UTP + us]) torsion(us, a, b, it, ta, tb);
     }
     if (a >= 0) { tw[(uint32_t)a * 2u] = mf4(ta[0], 0.0f); tw[(uint32_t)a * 2u + 1u] = mf4(ta[1], 0.0f); }
     if (b >= 0) { tw[(uint32_t)b * 2u] = mf4(tb[0], 0.0f); tw[(uint32_t)b * 2u + 1u] = mf4(tb[1], 0.0f); }

@@ -132,3 +132,35 @@ def momentum_stack(seed=23):
         b.add_shape_box(body, hx=0.15, hy=0.15, hz=0.1, mu=0.7, mass=float(0.2 * 10.0 ** (0.75 * k)))
     synth._add_quadruped(b, rng, [1.2, 0.0, 0.9])
     return b.finalize(solver=dict(nesterov_momentum=True, contact_friction_position_iterations=4))
+
+
+def spinners(seed=29):
+    """Contact torsion: articulated plates spinning flat on the plane whose shapes have a torsion
+    radius (min_torsional_patch_radius), so each plate's coplanar contact cluster gets a spin row
+    that shares the Coulomb budget with sliding: a plate with a hinged tab, a sliding plate with a
+    hinged flap, and a free-body plate (no spin row: torsion rows are articulated-only)."""
+    rng = np.random.default_rng(seed)
+    b = SceneBuilder(fps=240, box_hulls="direct")
+    b.add_ground_plane(mu=0.8)
+    spun = []
+    p0 = b.add_body(xform=[0.0, 0.0, 0.05, 0, 0, 0, 1], twist=[0.0, 0.0, 0.0, 0.0, 0.0, 6.0])
+    spun.append(b.add_shape_box(p0, hx=0.2, hy=0.15, hz=0.05, mu=0.8))
+    b.add_joint_free(p0)
+    tab = b.add_body(xform=[0.0, 0.2, 0.05, 0, 0, 0, 1])
+    b.add_shape_box(tab, hx=0.05, hy=0.05, hz=0.02, mu=0.8)
+    b.add_joint_revolute(p0, tab, axis=[1, 0, 0], parent_xform=[0.0, 0.15, 0.0, 0, 0, 0, 1],
+                         child_xform=[0.0, -0.05, 0.0, 0, 0, 0, 1])
+    p1 = b.add_body(xform=[1.0, 0.0, 0.04, 0, 0, 0, 1], twist=[0.3, 0.0, 0.0, 0.0, 0.0, -4.0])
+    spun.append(b.add_shape_box(p1, hx=0.15, hy=0.15, hz=0.04, mu=0.8))
+    b.add_joint_free(p1)
+    flap = b.add_body(xform=[1.25, 0.0, 0.02, 0, 0, 0, 1])
+    spun.append(b.add_shape_box(flap, hx=0.1, hy=0.12, hz=0.02, mu=0.8))
+    b.add_joint_revolute(p1, flap, axis=[0, 1, 0], parent_xform=[0.15, 0.0, -0.02, 0, 0, 0, 1],
+                         child_xform=[-0.1, 0.0, 0.0, 0, 0, 0, 1])
+    f = b.add_body(xform=[-1.0, 0.0, 0.05, 0, 0, 0, 1], twist=[0.0, 0.0, 0.0, 0.0, 0.0, 5.0])
+    spun.append(b.add_shape_box(f, hx=0.2, hy=0.15, hz=0.05, mu=0.8))
+    sc = b.finalize()
+    for s in sc.json["shapes"]:
+        if s["sid"] in spun:
+            s["torsion_radius"] = float(rng.uniform(0.08, 0.12))
+    return sc
