@@ -283,104 +283,141 @@ struct Solver {
   }
   // Dense same-articulation rows of articulation a (wgsl.js:3306-3364), one warp: lane l owns
   // dofs l, l + 32, ... (so lanes never touch each other's qd entries) and its partial sums
-  // are combined with lane_sum. Each lane first loads its slice of the row (J and Y rows of its
-  // dofs, up to DENSE_REG of them) into registers. Called by all 32 lanes; returns whether a
-  // row belongs to a.
+  // are combined with lane_sum. The lanes keep their qd entries in registers for the whole pass
+  // (no other warp touches a's dofs meanwhile) and store them back at the end. The rows are
+  // Gauss-Seidel, one after another, but their data are not: a's rows are found 32 at a time
+  // with one ballot, and each lane holds its slice of a row (J and Y rows of its dofs, up to
+  // DENSE_REG of them) and the row's header in registers, the next row's loaded while this one
+  // is solved. Called by all 32 lanes; returns whether a row belongs to a.
   static constexpr uint32_t DENSE_REG = 2u;  // articulations of up to 64 dofs keep rows in registers
+  struct DenseRow {
+    float J[3][DENSE_REG], Y[3][DENSE_REG];
+    float m3_, m4, m5, m6, m7, m8, nbil, m22, m23, m24;
+    f3 lam;
+  };
+  __device__ void dense_load(uint32_t o, uint32_t lane, uint32_t nw, DenseRow& d) const {
+    const float* A = S.art;
+    const uint32_t NDA = S.NDA, jo = o + S.DHDR, yo = o + S.DHDR + 3u * NDA;
+#pragma unroll
+    for (uint32_t j = 0; j < DENSE_REG; j++) {
+      uint32_t k = lane + 32u * j;
+      bool v = k < nw;
+#pragma unroll
+      for (uint32_t r = 0; r < 3u; r++) {
+        d.J[r][j] = v ? A[jo + r * NDA + k] : 0.0f;
+        d.Y[r][j] = v ? A[yo + r * NDA + k] : 0.0f;
+      }
+    }
+    d.m3_ = A[o + 3u]; d.m4 = A[o + 4u]; d.m5 = A[o + 5u]; d.m6 = A[o + 6u]; d.m7 = A[o + 7u]; d.m8 = A[o + 8u];
+    d.nbil = A[o + 21u]; d.m22 = A[o + 22u]; d.m23 = A[o + 23u]; d.m24 = A[o + 24u];
+    d.lam = mf3(A[o + 9u], A[o + 10u], A[o + 11u]);
+  }
   __device__ bool dense(uint32_t a, uint32_t mode, uint32_t it, uint32_t ph, uint32_t lane) const {
-    const uint32_t NDA = S.NDA, DHDR = S.DHDR, DPS = S.DPS;
-    float* A = S.art;
-    uint32_t nd = min(S.sched[S.S_META + 3u], S.MAXDENSE);
-    uint4 ai = ar.info(a);
+    const uint32_t DPS = S.DPS, base0 = S.A_DENSE;
+    const uint32_t nd = min(S.sched[S.S_META + 3u], S.MAXDENSE);
+    const uint4 ai = ar.info(a);
     if (ai.w > 32u * DENSE_REG) return dense_wide(a, mode, it, ph, lane, nd, ai);
-    float* q = aqd + ai.z;
     bool touched = false;
-    for (uint32_t i = 0; i < nd; i++) {
-      uint32_t o = S.A_DENSE + i * DPS;
-      if (f2u(A[o]) != a) continue;
+    float* qg = aqd + ai.z;
+    float q[DENSE_REG];
+#pragma unroll
+    for (uint32_t j = 0; j < DENSE_REG; j++) q[j] = lane + 32u * j < ai.w ? qg[lane + 32u * j] : 0.0f;
+    for (uint32_t base = 0; base < nd; base += 32u) {
+      const uint32_t i = base + lane;
+      uint32_t mask = __ballot_sync(0xffffffffu, i < nd && f2u(S.art[base0 + i * DPS]) == a);
+      if (mask == 0u) continue;
       touched = true;
-      uint32_t jo = o + DHDR, yo = o + DHDR + 3u * NDA;
-      float J[3][DENSE_REG], Y[3][DENSE_REG];
-#pragma unroll
-      for (uint32_t j = 0; j < DENSE_REG; j++) {
-        uint32_t k = lane + 32u * j;
-        bool v = k < ai.w;
-#pragma unroll
-        for (uint32_t r = 0; r < 3u; r++) {
-          J[r][j] = v ? A[jo + r * NDA + k] : 0.0f;
-          Y[r][j] = v ? A[yo + r * NDA + k] : 0.0f;
-        }
+      uint32_t row = base + (uint32_t)__ffs(mask) - 1u;
+      mask &= mask - 1u;
+      DenseRow cur;
+      dense_load(base0 + row * DPS, lane, ai.w, cur);
+      while (true) {
+        const bool more = mask != 0u;
+        const uint32_t nrow = more ? base + (uint32_t)__ffs(mask) - 1u : row;
+        DenseRow nxt;
+        if (more) dense_load(base0 + nrow * DPS, lane, ai.w, nxt);
+        dense_row(cur, base0 + row * DPS, ai, mode, it, ph, lane, q);
+        if (!more) break;
+        mask &= mask - 1u;
+        cur = nxt;
+        row = nrow;
       }
-      const float m3_ = A[o + 3u], m4 = A[o + 4u], m5 = A[o + 5u], m6 = A[o + 6u], m7 = A[o + 7u], m8 = A[o + 8u];
-      const float nbil = A[o + 21u], m22 = A[o + 22u], m23 = A[o + 23u], m24 = A[o + 24u];
-      f3 lam = mf3(A[o + 9u], A[o + 10u], A[o + 11u]);
-      if ((nbil > 0.5f) == (ph == 1u) && ph != 0u) continue;
-      if (nbil > 0.5f) {
-        if (mode == 0u) continue;
-        f3 nlam = lam;
-        const uint32_t nr = f2u(nbil);
+    }
 #pragma unroll
-        for (uint32_t r = 0; r < 3u; r++) {
-          if (r >= nr) break;
-          float part = 0.0f;
+    for (uint32_t j = 0; j < DENSE_REG; j++)
+      if (lane + 32u * j < ai.w) qg[lane + 32u * j] = q[j];
+    return touched;
+  }
+  // One dense row (wgsl.js:3320-3362) from its registers; lane 0 stores the new impulses.
+  __device__ void dense_row(const DenseRow& d, uint32_t o, uint4 ai, uint32_t mode, uint32_t it, uint32_t ph,
+                            uint32_t lane, float (&q)[DENSE_REG]) const {
+    float* A = S.art;
+    const f3 lam = d.lam;
+    if ((d.nbil > 0.5f) == (ph == 1u) && ph != 0u) return;
+    if (d.nbil > 0.5f) {
+      if (mode == 0u) return;
+      f3 nlam = lam;
+      const uint32_t nr = f2u(d.nbil);
 #pragma unroll
-          for (uint32_t j = 0; j < DENSE_REG; j++) {
-            uint32_t k = lane + 32u * j;
-            if (k < ai.w) part += J[r][j] * q[k];
-          }
-          float jv = lane_sum(part);
-          float rhs = r == 0u ? m4 : (r == 1u ? m22 : m23);
-          float dl = ((-S.F_OMEGA) * (jv + rhs)) * A[o + 5u + r];
-          setc(nlam, (int)r, comp(nlam, (int)r) + dl);
-#pragma unroll
-          for (uint32_t j = 0; j < DENSE_REG; j++) {
-            uint32_t k = lane + 32u * j;
-            if (k < ai.w) q[k] += Y[r][j] * dl;
-          }
-        }
-        if (lane == 0u) { A[o + 9u] = nlam.x; A[o + 10u] = nlam.y; A[o + 11u] = nlam.z; }
-        continue;
-      }
-      if (mode == 0u) {
+      for (uint32_t r = 0; r < 3u; r++) {
+        if (r >= nr) break;
+        float part = 0.0f;
 #pragma unroll
         for (uint32_t j = 0; j < DENSE_REG; j++) {
           uint32_t k = lane + 32u * j;
-          if (k < ai.w) q[k] += (Y[0][j] * lam.x + Y[1][j] * lam.y) + Y[2][j] * lam.z;
+          if (k < ai.w) part += d.J[r][j] * q[j];
         }
-        continue;
-      }
-      float part = 0.0f;
+        float jv = lane_sum(part);
+        float rhs = r == 0u ? d.m4 : (r == 1u ? d.m22 : d.m23);
+        float dl = ((-S.F_OMEGA) * (jv + rhs)) * A[o + 5u + r];
+        setc(nlam, (int)r, comp(nlam, (int)r) + dl);
 #pragma unroll
-      for (uint32_t j = 0; j < DENSE_REG; j++) {
-        uint32_t k = lane + 32u * j;
-        if (k < ai.w) part += J[0][j] * q[k];
-      }
-      float jv = lane_sum(part);
-      float nl = fmx(lam.x + S.F_OMEGA * ((((-(jv + m4)) * m5) * m24) - (1.0f - m24) * lam.x), 0.0f);
-      float dn = nl - lam.x;
-      float p1 = 0.0f, p2 = 0.0f;
-#pragma unroll
-      for (uint32_t j = 0; j < DENSE_REG; j++) {
-        uint32_t k = lane + 32u * j;
-        if (k < ai.w) {
-          q[k] += Y[0][j] * dn;
-          p1 += J[1][j] * q[k];
-          p2 += J[2][j] * q[k];
+        for (uint32_t j = 0; j < DENSE_REG; j++) {
+          uint32_t k = lane + 32u * j;
+          if (k < ai.w) q[j] += d.Y[r][j] * dl;
         }
       }
-      float s1 = lane_sum(p1), s2 = lane_sum(p2);
-      float lim = it < S.FSTART ? 0.0f : m3_ * nl;
-      float kd = m6 * m8 - m7 * m7;
-      f2 lt = friction_pair(m8 / kd, -m7 / kd, m6 / kd, s1, s2, lam.y, lam.z, lim, S.F_OMEGA);
-      float d1 = lt.x - lam.y, d2 = lt.y - lam.z;
-#pragma unroll
-      for (uint32_t j = 0; j < DENSE_REG; j++) {
-        uint32_t k = lane + 32u * j;
-        if (k < ai.w) q[k] += Y[1][j] * d1 + Y[2][j] * d2;
-      }
-      if (lane == 0u) { A[o + 9u] = nl; A[o + 10u] = lt.x; A[o + 11u] = lt.y; }
+      if (lane == 0u) { A[o + 9u] = nlam.x; A[o + 10u] = nlam.y; A[o + 11u] = nlam.z; }
+      return;
     }
-    return touched;
+    if (mode == 0u) {
+#pragma unroll
+      for (uint32_t j = 0; j < DENSE_REG; j++) {
+        uint32_t k = lane + 32u * j;
+        if (k < ai.w) q[j] += (d.Y[0][j] * lam.x + d.Y[1][j] * lam.y) + d.Y[2][j] * lam.z;
+      }
+      return;
+    }
+    float part = 0.0f;
+#pragma unroll
+    for (uint32_t j = 0; j < DENSE_REG; j++) {
+      uint32_t k = lane + 32u * j;
+      if (k < ai.w) part += d.J[0][j] * q[j];
+    }
+    float jv = lane_sum(part);
+    float nl = fmx(lam.x + S.F_OMEGA * ((((-(jv + d.m4)) * d.m5) * d.m24) - (1.0f - d.m24) * lam.x), 0.0f);
+    float dn = nl - lam.x;
+    float p1 = 0.0f, p2 = 0.0f;
+#pragma unroll
+    for (uint32_t j = 0; j < DENSE_REG; j++) {
+      uint32_t k = lane + 32u * j;
+      if (k < ai.w) {
+        q[j] += d.Y[0][j] * dn;
+        p1 += d.J[1][j] * q[j];
+        p2 += d.J[2][j] * q[j];
+      }
+    }
+    float s1 = lane_sum(p1), s2 = lane_sum(p2);
+    float lim = it < S.FSTART ? 0.0f : d.m3_ * nl;
+    float kd = d.m6 * d.m8 - d.m7 * d.m7;
+    f2 lt = friction_pair(d.m8 / kd, -d.m7 / kd, d.m6 / kd, s1, s2, lam.y, lam.z, lim, S.F_OMEGA);
+    float d1 = lt.x - lam.y, d2 = lt.y - lam.z;
+#pragma unroll
+    for (uint32_t j = 0; j < DENSE_REG; j++) {
+      uint32_t k = lane + 32u * j;
+      if (k < ai.w) q[j] += d.Y[1][j] * d1 + d.Y[2][j] * d2;
+    }
+    if (lane == 0u) { A[o + 9u] = nl; A[o + 10u] = lt.x; A[o + 11u] = lt.y; }
   }
   // The same for articulations of more than 32 * DENSE_REG dofs, reading rows as it goes.
   __device__ bool dense_wide(uint32_t a, uint32_t mode, uint32_t it, uint32_t ph, uint32_t lane, uint32_t nd,
