@@ -850,6 +850,53 @@ struct Art {
       set_twist(l, v, tw);
     }
   }
+  // twists() by one warp (all 32 lanes call it). The per-link inputs that do not depend on the
+  // recursion -- the parent, the COM offset to it and, for a one-dof link, S qd -- are computed
+  // by lane k for link k of each 32-link chunk and broadcast with shuffles; every lane then runs
+  // the recursion with the same operations in the same order as twists(), and lane 0 stores.
+  // A chain link's parent twist is the previous link's, kept in registers.
+  __device__ void twists_warp(uint32_t a, const float* aqd, float4* tw, uint32_t lane) const {
+    const uint4 ai = info(a);
+    const uint32_t full = 0xffffffffu;
+    SVec vprev = sv0();
+    for (uint32_t c0 = 0; c0 < ai.y; c0 += 32u) {
+      const uint32_t nl = min(32u, ai.y - c0);
+      int par = -1;
+      uint32_t nd = 0u;
+      f3 r = sp3(0.0f);
+      SVec prod = sv0();
+      if (lane < nl) {
+        const uint32_t l = ai.x + c0 + lane;
+        par = lparent(l);
+        nd = lndof(l);
+        if (par >= 0) r = link_r(l);
+        if (nd == 1u) prod = sscl(ldS(l, 0u), aqd[ldof(l)]);
+      }
+      for (uint32_t k = 0; k < nl; k++) {
+        const uint32_t l = ai.x + c0 + k;
+        const int p = __shfl_sync(full, par, (int)k);
+        const uint32_t n = __shfl_sync(full, nd, (int)k);
+        const f3 rr = mf3(__shfl_sync(full, r.x, (int)k), __shfl_sync(full, r.y, (int)k), __shfl_sync(full, r.z, (int)k));
+        const SVec pr = SVec{mf3(__shfl_sync(full, prod.a.x, (int)k), __shfl_sync(full, prod.a.y, (int)k),
+                                 __shfl_sync(full, prod.a.z, (int)k)),
+                             mf3(__shfl_sync(full, prod.l.x, (int)k), __shfl_sync(full, prod.l.y, (int)k),
+                                 __shfl_sync(full, prod.l.z, (int)k))};
+        SVec v = sv0();
+        if (p >= 0) v = mshift((uint32_t)p + 1u == l ? vprev : ldsv(lo((uint32_t)p) + L_V), rr);
+        if (n == 1u) {
+          v = sadd(v, pr);
+        } else {
+          for (uint32_t q = 0; q < n; q++) v = sadd(v, sscl(ldS(l, q), aqd[ldof(l) + q]));
+        }
+        if (lane == 0u) {
+          stsv(lo(l) + L_V, v);
+          set_twist(l, v, tw);
+        }
+        __syncwarp();
+        vprev = v;
+      }
+    }
+  }
   __device__ void apply(uint32_t a, float* aqd, float4* tw) const {
     uint4 ai = info(a);
     for (uint32_t kk = 0; kk < ai.y; kk++) {

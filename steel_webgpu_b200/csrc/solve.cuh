@@ -574,7 +574,7 @@ struct Solver {
     for (uint32_t a = warp; a < S.NA; a += nw) {
       bool touched = dense(a, mode, it, ph, lane);
       __syncwarp();
-      if (lane == 0u && touched) ar.twists(a, aqd, tw);
+      if (touched) ar.twists_warp(a, aqd, tw, lane);
       __syncwarp();
     }
     __syncthreads();
@@ -823,7 +823,7 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     S.slots[2u * u] = make_float4((float)row, (float)us, (float)((int)(key & 0xffffu) - 1), (float)((int)(key >> 16u) - 1));
   }
   __syncthreads();
-  for (uint32_t a = tid; a < S.NA; a += nt) sv.ar.twists(a, sv.aqd, sv.tw);
+  for (uint32_t a = tid >> 5u; a < S.NA; a += nt >> 5u) sv.ar.twists_warp(a, sv.aqd, sv.tw, tid & 31u);
   __syncthreads();
   sv.dense_phase(0u, 0u, 0u);
   sv.sweep(0u, ncol, 0u, wcs, nu);
