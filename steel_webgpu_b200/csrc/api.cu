@@ -131,7 +131,7 @@ struct steel_batch {
   std::vector<uint32_t> serve_mask;            // host copy of the device activity mask
   std::vector<Done> serve_done;
   uint32_t serve_admitted = 0, serve_max_active = 0;
-  std::vector<uint32_t> order_host;  // block order of the fused prepare + solve kernel
+  std::vector<uint32_t> order_host;  // block order of the prepare and solve kernels
   uint64_t serve_next_id = 1;
   bool serve_on = false;
 };
@@ -294,7 +294,8 @@ void enqueue_substeps(steel_batch* b, cudaStream_t st) {
     launch_broad(bd, st);
     launch_narrow(bd, b->narrow_blocks, st);
     launch_csort(bd, b->sort_keys, st);
-    launch_prepare_solve(bd, st);
+    launch_prepare(bd, st);
+    launch_solve(bd, st);
   }
   launch_frame_end(bd, st);
 }
@@ -451,7 +452,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   bd.active = at<uint32_t>(A, b->o_active);
   bd.order = at<uint32_t>(A, b->o_order);
   {
-    // Fused prepare + solve blocks take the scenes longest first (chain length, then bodies), so
+    // Prepare and solve blocks take the scenes longest first (chain length, then bodies), so
     // short scenes fill the end of the launch.
     std::vector<uint32_t> order(n);
     for (uint32_t i = 0; i < n; i++) order[i] = i;
@@ -469,7 +470,6 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   bd.art_f64 = art_f64 != 0u ? 1u : 0u;
   CU(configure_prepare(prep_smem));
   CU(configure_solve(solve_smem));
-  CU(configure_prepare_solve(std::max(prep_smem, solve_smem)));
   CU(cudaMemcpyAsync(bd.scenes, dev.data(), sizeof(SceneDev) * n, cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync((void*)bd.shape_scene, b->shape_scene.data(), 4 * b->shape_scene.size(), cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync((void*)bd.shape_local, b->shape_local.data(), 4 * b->shape_local.size(), cudaMemcpyHostToDevice, st));

@@ -19,6 +19,15 @@ enum : uint32_t {
 };
 
 struct SVec { f3 a, l; };
+// A thread's scratch interleaved with the other threads of its block: element i at p[i * s]
+// (p = scratch + thread index, s = block size). Threads that walk the same articulation in step
+// then touch consecutive words instead of one cache line each.
+struct Lane {
+  float* p;
+  uint32_t s;
+  __device__ float& operator[](uint32_t i) const { return p[(size_t)i * s]; }
+  __device__ Lane operator+(uint32_t i) const { return Lane{p + (size_t)i * s, s}; }
+};
 SD SVec sv0() { return SVec{sp3(0.0f), sp3(0.0f)}; }
 SD SVec sadd(SVec x, SVec y) { return SVec{x.a + y.a, x.l + y.l}; }
 SD SVec sscl(SVec x, float s) { return SVec{x.a * s, x.l * s}; }
@@ -117,84 +126,160 @@ struct Art {
   }
   __device__ float4 link_rot(uint32_t l) const { return mf4(ld3(lo(l) + L_ROT), LB[lo(l) + L_ROT + 3u]); }
 
-  // Link poses, COMs and world motion subspaces (artwgsl.js:98-187).
-  __device__ void fk(uint32_t a) const {
-    uint4 ai = info(a);
+  // Link poses, COMs and world motion subspaces (artwgsl.js:98-187), in three parts per link:
+  // the joint's own motion from its coordinates (fk_joint), the pose chain from the parent's pose
+  // (fk_pose), and the COM, motion subspace and joint offset from the link's pose (fk_out).
+  struct FkJoint {
+    float4 mq;
+    f3 mp;
+    f3 ang[3];
+    uint32_t nlin, nang;
+  };
+  __device__ FkJoint fk_joint(uint32_t l) const {
     const float* Q = A + S.A_Q;
+    const float4 r0 = lrec(l, 0), r1 = lrec(l, 1), r3 = lrec(l, 3), r5 = lrec(l, 5);
+    FkJoint j;
+    j.mq = make_float4(0, 0, 0, 1);
+    j.mp = sp3(0.0f);
+    j.ang[0] = sp3(0.0f); j.ang[1] = sp3(0.0f); j.ang[2] = sp3(0.0f);
+    const f3 axis = v3(r5);
+    const uint32_t t = f2u(r0.x), qs = f2u(r3.w), d0 = f2u(r0.z);
+    if (t == 1u) j.mq = qaxis(axis, Q[qs]);
+    if (t == 0u) j.mp = axis * Q[qs];
+    if (t == 2u) j.mq = nrm4(make_float4(Q[qs], Q[qs + 1], Q[qs + 2], Q[qs + 3]));
+    j.nlin = f2u(r5.w);
+    j.nang = f2u(r1.w) - j.nlin;
+    if (t == 6u) {
+      for (uint32_t c = 0; c < j.nlin; c++) j.mp += dof_axis(d0 + c) * Q[qs + c];
+      uint32_t iq = qs + j.nlin;
+      if (j.nang == 1u) { j.ang[0] = dof_axis(d0 + j.nlin); j.mq = qaxis(j.ang[0], Q[iq]); }
+      if (j.nang == 2u) {
+        f3 x0 = nrm(dof_axis(d0 + j.nlin));
+        f3 x2 = nrm(cross(x0, dof_axis(d0 + j.nlin + 1u)));
+        j.ang[0] = x0;
+        float4 q0 = qaxis(x0, Q[iq]);
+        j.ang[1] = qrot(q0, cross(x2, x0));
+        j.mq = qmul(qaxis(j.ang[1], Q[iq + 1u]), q0);
+      }
+      if (j.nang == 3u) {
+        j.ang[0] = dof_axis(d0 + j.nlin);
+        float4 q0 = qaxis(j.ang[0], Q[iq]);
+        j.ang[1] = qrot(q0, dof_axis(d0 + j.nlin + 1u));
+        float4 q1 = qaxis(j.ang[1], Q[iq + 1u]);
+        j.ang[2] = qrot(qmul(q1, q0), dof_axis(d0 + j.nlin + 2u));
+        j.mq = qmul(qaxis(j.ang[2], Q[iq + 2u]), qmul(q1, q0));
+      }
+    }
+    if (t == 4u) {
+      j.mp = mf3(Q[qs], Q[qs + 1], Q[qs + 2]);
+      j.mq = nrm4(make_float4(Q[qs + 3], Q[qs + 4], Q[qs + 5], Q[qs + 6]));
+    }
+    return j;
+  }
+  // Joint frame (jp, jq), child frame (cp, cq) and link pose (lp, lq) from the parent's pose.
+  __device__ void fk_pose(uint32_t l, f3 pp, float4 pq, float4 mq, f3 mp, f3& jp, float4& jq, f3& cp, f3& lp,
+                          float4& lq) const {
+    const float4 r1 = lrec(l, 1), r2 = lrec(l, 2), r3 = lrec(l, 3), r4 = lrec(l, 4);
+    jp = pp + qrot(pq, v3(r1));
+    jq = qmul(pq, r2);
+    const float4 cq = qmul(jq, mq);
+    cp = jp + qrot(jq, mp);
+    const float4 iq = qconj(r4);
+    lq = nrm4(qmul(cq, iq));
+    lp = cp + qrot(cq, -qrot(iq, v3(r3)));
+  }
+  __device__ void fk_store_pose(uint32_t l, f3 lp, float4 lq) const {
+    const uint32_t L = lo(l);
+    st3(L + L_POS, lp);
+    st3(L + L_ROT, v3(lq));
+    LB[L + L_ROT + 3u] = lq.w;
+  }
+  __device__ void fk_out(uint32_t l, const FkJoint& j, f3 jp, float4 jq, f3 cp, f3 lp, float4 lq) const {
+    const float4 r0 = lrec(l, 0), r5 = lrec(l, 5);
+    const uint32_t t = f2u(r0.x), d0 = f2u(r0.z), L = lo(l);
+    const f3 axis = v3(r5);
+    f3 com = lp + qrot(lq, v3(BR[(uint32_t)f2i(r0.w) * 8u + 1u]));
+    st3(L + L_COM, com);
+    f3 aw = qrot(jq, axis);
+    f3 rj = com - jp;
+    for (uint32_t c = 0; c < S.JM; c++) stsv(L + L_S + c * 6u, sv0());
+    if (t == 1u) stsv(L + L_S, SVec{aw, cross(aw, rj)});
+    if (t == 0u) stsv(L + L_S, SVec{sp3(0.0f), aw});
+    if (t == 2u)
+      for (uint32_t c = 0; c < 3u; c++) { f3 ew = qrot(jq, unit_axis(c)); stsv(L + L_S + c * 6u, SVec{ew, cross(ew, rj)}); }
+    f3 rf = com - cp;
+    st3(L + L_JR, rf);
+    if (t == 6u) {
+      for (uint32_t c = 0; c < j.nlin; c++) stsv(L + L_S + c * 6u, SVec{sp3(0.0f), qrot(jq, dof_axis(d0 + c))});
+      for (uint32_t c = 0; c < j.nang; c++) {
+        f3 ew = qrot(jq, j.ang[c]);
+        stsv(L + L_S + (j.nlin + c) * 6u, SVec{ew, cross(ew, rf)});
+      }
+    }
+    if (t == 4u) {
+      for (uint32_t c = 0; c < 3u; c++) {
+        f3 ew = qrot(jq, unit_axis(c));
+        stsv(L + L_S + c * 6u, SVec{sp3(0.0f), ew});
+        stsv(L + L_S + (c + 3u) * 6u, SVec{ew, cross(ew, rf)});
+      }
+    }
+  }
+  __device__ void fk(uint32_t a) const {
+    const uint4 ai = info(a);
     for (uint32_t k = 0; k < ai.y; k++) {
-      uint32_t l = ai.x + k;
-      float4 r0 = lrec(l, 0), r1 = lrec(l, 1), r2 = lrec(l, 2), r3 = lrec(l, 3), r4 = lrec(l, 4), r5 = lrec(l, 5);
+      const uint32_t l = ai.x + k;
       f3 pp = sp3(0.0f);
       float4 pq = make_float4(0, 0, 0, 1);
-      int par = f2i(r0.y);
+      const int par = lparent(l);
       if (par >= 0) { pp = ld3(lo((uint32_t)par) + L_POS); pq = link_rot((uint32_t)par); }
-      f3 jp = pp + qrot(pq, v3(r1));
-      float4 jq = qmul(pq, r2);
-      f3 axis = v3(r5);
-      float4 mq = make_float4(0, 0, 0, 1);
-      f3 mp = sp3(0.0f);
-      uint32_t t = f2u(r0.x), qs = f2u(r3.w), d0 = f2u(r0.z);
-      if (t == 1u) mq = qaxis(axis, Q[qs]);
-      if (t == 0u) mp = axis * Q[qs];
-      if (t == 2u) mq = nrm4(make_float4(Q[qs], Q[qs + 1], Q[qs + 2], Q[qs + 3]));
-      uint32_t nlin = f2u(r5.w), nang = f2u(r1.w) - nlin;
-      f3 ang[3] = {sp3(0.0f), sp3(0.0f), sp3(0.0f)};
-      if (t == 6u) {
-        for (uint32_t c = 0; c < nlin; c++) mp += dof_axis(d0 + c) * Q[qs + c];
-        uint32_t iq = qs + nlin;
-        if (nang == 1u) { ang[0] = dof_axis(d0 + nlin); mq = qaxis(ang[0], Q[iq]); }
-        if (nang == 2u) {
-          f3 x0 = nrm(dof_axis(d0 + nlin));
-          f3 x2 = nrm(cross(x0, dof_axis(d0 + nlin + 1u)));
-          ang[0] = x0;
-          float4 q0 = qaxis(x0, Q[iq]);
-          ang[1] = qrot(q0, cross(x2, x0));
-          mq = qmul(qaxis(ang[1], Q[iq + 1u]), q0);
+      const FkJoint j = fk_joint(l);
+      f3 jp, cp, lp;
+      float4 jq, lq;
+      fk_pose(l, pp, pq, j.mq, j.mp, jp, jq, cp, lp, lq);
+      fk_store_pose(l, lp, lq);
+      fk_out(l, j, jp, jq, cp, lp, lq);
+    }
+  }
+  // fk() by one warp (all 32 lanes call it): lane k evaluates the joint motion of link k of each
+  // 32-link chunk (the trigonometry) and afterwards its COM and motion subspace; between the two,
+  // every lane runs the pose chain with the broadcast joint motions (same operations as fk()),
+  // lane 0 stores the poses and each link's owner keeps its frames. A chain link's parent pose is
+  // the previous link's, kept in registers.
+  __device__ void fk_warp(uint32_t a, uint32_t lane) const {
+    const uint4 ai = info(a);
+    const uint32_t full = 0xffffffffu;
+    f3 pprev = sp3(0.0f);
+    float4 qprev = make_float4(0, 0, 0, 1);
+    for (uint32_t c0 = 0; c0 < ai.y; c0 += 32u) {
+      const uint32_t nl = min(32u, ai.y - c0);
+      FkJoint j{};
+      if (lane < nl) j = fk_joint(ai.x + c0 + lane);
+      f3 ojp = sp3(0.0f), ocp = sp3(0.0f), olp = sp3(0.0f);
+      float4 ojq = make_float4(0, 0, 0, 1), olq = make_float4(0, 0, 0, 1);
+      for (uint32_t k = 0; k < nl; k++) {
+        const uint32_t l = ai.x + c0 + k;
+        const float4 mq = make_float4(__shfl_sync(full, j.mq.x, (int)k), __shfl_sync(full, j.mq.y, (int)k),
+                                      __shfl_sync(full, j.mq.z, (int)k), __shfl_sync(full, j.mq.w, (int)k));
+        const f3 mp = mf3(__shfl_sync(full, j.mp.x, (int)k), __shfl_sync(full, j.mp.y, (int)k),
+                          __shfl_sync(full, j.mp.z, (int)k));
+        f3 pp = sp3(0.0f);
+        float4 pq = make_float4(0, 0, 0, 1);
+        const int par = lparent(l);
+        if (par >= 0) {
+          if ((uint32_t)par + 1u == l) { pp = pprev; pq = qprev; }
+          else { pp = ld3(lo((uint32_t)par) + L_POS); pq = link_rot((uint32_t)par); }
         }
-        if (nang == 3u) {
-          ang[0] = dof_axis(d0 + nlin);
-          float4 q0 = qaxis(ang[0], Q[iq]);
-          ang[1] = qrot(q0, dof_axis(d0 + nlin + 1u));
-          float4 q1 = qaxis(ang[1], Q[iq + 1u]);
-          ang[2] = qrot(qmul(q1, q0), dof_axis(d0 + nlin + 2u));
-          mq = qmul(qaxis(ang[2], Q[iq + 2u]), qmul(q1, q0));
-        }
+        f3 jp, cp, lp;
+        float4 jq, lq;
+        fk_pose(l, pp, pq, mq, mp, jp, jq, cp, lp, lq);
+        if (lane == 0u) fk_store_pose(l, lp, lq);
+        __syncwarp();
+        if (lane == k) { ojp = jp; ojq = jq; ocp = cp; olp = lp; olq = lq; }
+        pprev = lp;
+        qprev = lq;
       }
-      if (t == 4u) {
-        mp = mf3(Q[qs], Q[qs + 1], Q[qs + 2]);
-        mq = nrm4(make_float4(Q[qs + 3], Q[qs + 4], Q[qs + 5], Q[qs + 6]));
-      }
-      float4 cq = qmul(jq, mq);
-      f3 cp = jp + qrot(jq, mp);
-      float4 iq = qconj(r4);
-      float4 lq = nrm4(qmul(cq, iq));
-      f3 lp = cp + qrot(cq, -qrot(iq, v3(r3)));
-      uint32_t L = lo(l);
-      st3(L + L_POS, lp);
-      st3(L + L_ROT, v3(lq));
-      LB[L + L_ROT + 3u] = lq.w;
-      f3 com = lp + qrot(lq, v3(BR[(uint32_t)f2i(r0.w) * 8u + 1u]));
-      st3(L + L_COM, com);
-      f3 aw = qrot(jq, axis);
-      f3 rj = com - jp;
-      for (uint32_t c = 0; c < S.JM; c++) stsv(L + L_S + c * 6u, sv0());
-      if (t == 1u) stsv(L + L_S, SVec{aw, cross(aw, rj)});
-      if (t == 0u) stsv(L + L_S, SVec{sp3(0.0f), aw});
-      if (t == 2u)
-        for (uint32_t c = 0; c < 3u; c++) { f3 ew = qrot(jq, unit_axis(c)); stsv(L + L_S + c * 6u, SVec{ew, cross(ew, rj)}); }
-      f3 rf = com - cp;
-      st3(L + L_JR, rf);
-      if (t == 6u) {
-        for (uint32_t c = 0; c < nlin; c++) stsv(L + L_S + c * 6u, SVec{sp3(0.0f), qrot(jq, dof_axis(d0 + c))});
-        for (uint32_t c = 0; c < nang; c++) { f3 ew = qrot(jq, ang[c]); stsv(L + L_S + (nlin + c) * 6u, SVec{ew, cross(ew, rf)}); }
-      }
-      if (t == 4u) {
-        for (uint32_t c = 0; c < 3u; c++) {
-          f3 ew = qrot(jq, unit_axis(c));
-          stsv(L + L_S + c * 6u, SVec{sp3(0.0f), ew});
-          stsv(L + L_S + (c + 3u) * 6u, SVec{ew, cross(ew, rf)});
-        }
-      }
+      if (lane < nl) fk_out(ai.x + c0 + lane, j, ojp, ojq, ocp, olp, olq);
+      __syncwarp();
     }
   }
 
@@ -573,7 +658,8 @@ struct Art {
   }
 
   // Generalized Jacobians (artwgsl.js:525-554).
-  __device__ void gen_jac(uint32_t x, f3 p, float sgn, f3 d0, f3 d1, f3 d2, uint32_t ds, float* J) const {
+  template <class PJ>
+  __device__ void gen_jac(uint32_t x, f3 p, float sgn, f3 d0, f3 d1, f3 d2, uint32_t ds, PJ J) const {
     int l = (int)x;
     while (l >= 0) {
       uint32_t k = (uint32_t)l;
@@ -672,8 +758,8 @@ struct Art {
   }
 
   // solve_gen3 on a serial chain: p and dv carried in registers, u staged in uu (18 per link).
-  __device__ void solve_gen3_chain(uint4 ai, const float* __restrict__ J, float* __restrict__ Y,
-                                   float* __restrict__ uu) const {
+  template <class PF>
+  __device__ void solve_gen3_chain(uint4 ai, PF J, PF Y, PF uu) const {
     const uint32_t NDA = S.NDA;
     SVec pc[3] = {sv0(), sv0(), sv0()};  // p of the link being visited (its child's contribution)
     for (uint32_t kk = 0; kk < ai.y; kk++) {
@@ -683,7 +769,7 @@ struct Art {
       uint32_t dl = ldof(l) - ai.z;
 #pragma unroll
       for (uint32_t rs = 0; rs < 3u; rs++) {
-        const float* tau = J + rs * NDA;
+        const PF tau = J + rs * NDA;
         float u[6] = {0, 0, 0, 0, 0, 0};
         SVec pk = pc[rs];
 #pragma unroll
@@ -692,7 +778,10 @@ struct Art {
           u[r] = tau[dl + r] - sdot(ldS(l, r), pk);
         }
 #pragma unroll
-        for (uint32_t r = 0; r < 6u; r++) uu[(k * 3u + rs) * 6u + r] = u[r];
+        for (uint32_t r = 0; r < 6u; r++) {
+          if (r >= n) break;
+          uu[(k * 3u + rs) * 6u + r] = u[r];
+        }
         if (has_parent) {
           SVec pp = pk;
 #pragma unroll
@@ -746,7 +835,8 @@ struct Art {
   // floats, zero beyond the articulation's dofs) is the generalized impulse of right-hand side r,
   // row r of Y receives its qd change. Each right-hand side goes through exactly the operations of
   // solve_gen. scratch: 54 * MAXLP floats.
-  __device__ void solve_gen3(uint32_t a, const float* __restrict__ J, float* __restrict__ Y, float* __restrict__ scr) const {
+  template <class PF>
+  __device__ void solve_gen3(uint32_t a, PF J, PF Y, PF scr) const {
     uint4 ai = info(a);
     const uint32_t NDA = S.NDA, M = S.MAXLP;
     // A serial chain (every link's parent is the previous link) has one child per link, so the
@@ -755,14 +845,14 @@ struct Art {
     bool chain = true;
     for (uint32_t k = 1; k < ai.y; k++) chain = chain && lparent(ai.x + k) == (int)(ai.x + k - 1u);
     if (chain) { solve_gen3_chain(ai, J, Y, scr + 18u * M); return; }
-    float* p = scr;                 // per link, 3 x 6
-    float* uu = scr + 18u * M;      // per link, 3 x 6
-    float* dvs = scr + 36u * M;     // per link, 3 x 6
+    PF p = scr;                     // per link, 3 x 6
+    PF uu = scr + 18u * M;          // per link, 3 x 6
+    PF dvs = scr + 36u * M;         // per link, 3 x 6
     for (uint32_t k = 0; k < 18u * ai.y; k++) p[k] = 0.0f;
-    auto ldp = [&](const float* base, uint32_t k) {
+    auto ldp = [&](PF base, uint32_t k) {
       return SVec{mf3(base[k * 6], base[k * 6 + 1], base[k * 6 + 2]), mf3(base[k * 6 + 3], base[k * 6 + 4], base[k * 6 + 5])};
     };
-    auto stp = [&](float* base, uint32_t k, SVec v) {
+    auto stp = [&](PF base, uint32_t k, SVec v) {
       base[k * 6] = v.a.x; base[k * 6 + 1] = v.a.y; base[k * 6 + 2] = v.a.z;
       base[k * 6 + 3] = v.l.x; base[k * 6 + 4] = v.l.y; base[k * 6 + 5] = v.l.z;
     };
@@ -773,7 +863,7 @@ struct Art {
       uint32_t dl = ldof(l) - ai.z;
 #pragma unroll
       for (uint32_t rs = 0; rs < 3u; rs++) {
-        const float* tau = J + rs * NDA;
+        const PF tau = J + rs * NDA;
         float u[6] = {0, 0, 0, 0, 0, 0};
         SVec pk = ldp(p, k * 3u + rs);
 #pragma unroll
@@ -782,7 +872,10 @@ struct Art {
           u[r] = tau[dl + r] - sdot(ldS(l, r), pk);
         }
 #pragma unroll
-        for (uint32_t r = 0; r < 6u; r++) uu[(k * 3u + rs) * 6u + r] = u[r];
+        for (uint32_t r = 0; r < 6u; r++) {
+          if (r >= n) break;
+          uu[(k * 3u + rs) * 6u + r] = u[r];
+        }
         if (par >= 0) {
           SVec pp = pk;
 #pragma unroll

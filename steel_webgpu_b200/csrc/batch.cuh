@@ -20,7 +20,7 @@ struct BatchDev {
   double* phase;              // per-scene clock (sim.js:674-678)
   unsigned long long* substep_count;  // [nscenes] substeps each scene has run (warm-table parity)
   const uint32_t* active;     // [nscenes] nonzero: the scene steps in this frame (serving loop mask)
-  const uint32_t* order;      // [nscenes] scenes in the fused kernel's block order (longest first)
+  const uint32_t* order;      // [nscenes] scenes in the prepare and solve kernels' block order (longest first)
   uint32_t* error;            // [1] first device-side error code (0 = none)
   uint32_t prep_smem;         // dynamic shared memory of k_prepare / k_solve launches (bytes)
   uint32_t solve_smem;
@@ -105,8 +105,6 @@ cudaError_t configure_prepare(size_t smem_bytes);
 cudaError_t configure_solve(size_t smem_bytes);
 void launch_prepare(const BatchDev& b, cudaStream_t st);
 void launch_solve(const BatchDev& b, cudaStream_t st);
-cudaError_t configure_prepare_solve(size_t smem_bytes);
-void launch_prepare_solve(const BatchDev& b, cudaStream_t st);
 void launch_frame_end(const BatchDev& b, cudaStream_t st);
 // Host-I/O staging: scatter packed joint targets into each scene, gather packed body poses.
 void launch_scatter_targets(const BatchDev& b, const float* packed, const uint64_t* offsets, cudaStream_t st);

@@ -6,7 +6,7 @@ namespace steel {
 // F64: the instance with the FP64 articulated-inertia branch, launched when a scene of the batch
 // has ART_F64 (scenes without it still run the FP32 branch in that instance).
 template <bool F64>
-__global__ void __launch_bounds__(PREP_THREADS, 4) k_prepare(BatchDev B) { prepare_scene<F64>(B, blockIdx.x); }
+__global__ void __launch_bounds__(PREP_THREADS, 4) k_prepare(BatchDev B) { prepare_scene<F64>(B, B.order[blockIdx.x]); }
 
 cudaError_t configure_prepare(size_t smem_bytes) {
   cudaError_t e = cudaFuncSetAttribute(k_prepare<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);

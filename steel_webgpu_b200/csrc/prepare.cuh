@@ -1,5 +1,5 @@
 #pragma once
-// Prepare of one scene by one block (the body of k_prepare and of the fused k_prepare_solve).
+// Prepare of one scene by one block (the body of k_prepare).
 //
 // Follows the reference's prepare pass (packages/steel-webgpu/src/wgsl.js:1222-2494) on its
 // default option set: drive targets (wgsl.js:1800-1825), joint-limit gating and the
@@ -474,7 +474,7 @@ struct Prep {
   }
 
   // Dense row of a same-articulation contact (wgsl.js:2370-2444). scr: JDIM + 2 NDA + 18 MAXLP floats.
-  __device__ void dense_row(uint32_t slot, uint32_t c, float* scr) const {
+  __device__ void dense_row(uint32_t slot, uint32_t c, Lane scr) const {
     const uint32_t NDA = S.NDA, DHDR = S.DHDR, DPS = S.DPS;
     float* A = S.art;
     float4 c0 = S.con[c * 5u], c1 = S.con[c * 5u + 1u], cmeta = S.con[c * 5u + 2u];
@@ -489,9 +489,9 @@ struct Prep {
     f3 t2 = cross(n, t1);
     uint32_t art_id = (uint32_t)bart(a);
     uint4 ai = ar.info(art_id);
-    float* J = scr;
-    float* Y = scr + 3u * NDA;
-    float* gs = Y + 3u * NDA;
+    Lane J = scr;
+    Lane Y = scr + 3u * NDA;
+    Lane gs = Y + 3u * NDA;
     for (uint32_t k = 0; k < 3u * NDA; k++) { J[k] = 0.0f; Y[k] = 0.0f; }
     ar.gen_jac((uint32_t)blink(b), p, 1.0f, n, t1, t2, ai.z, J);
     ar.gen_jac((uint32_t)blink(a), p, -1.0f, n, t1, t2, ai.z, J);
@@ -500,7 +500,7 @@ struct Prep {
     // Row r's right-hand side is J row r (zero beyond the articulation's dofs, as gen_jac leaves it).
     ar.solve_gen3(art_id, J, Y, gs);
     for (uint32_t r = 0; r < 3u; r++) {
-      const float* y = Y + r * NDA;
+      const Lane y = Y + r * NDA;
       for (uint32_t k = 0; k < ai.w; k++) {
         A[o + DHDR + r * NDA + k] = J[r * NDA + k];
         A[o + DHDR + 3u * NDA + r * NDA + k] = y[k];
@@ -727,7 +727,7 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
   if (S.SLEEP == 1u) sleep_islands(pr, tid, nt);
   __syncthreads();
   // Joint-limit gating, listed joint rows, FK and factorisation per articulation.
-  for (uint32_t a = tid; a < S.NA; a += nt) {
+  auto gate = [&](uint32_t a) {
     uint4 ai = ar.info(a);
     // Joint velocity limits (wgsl.js:1829-1854): scale the articulation's scalar dof speeds so the
     // most exceeded limit is met, then mark the dofs near their limit (rows exist only there).
@@ -769,9 +769,28 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
       if (row && ar.scalar_dof(d)) { A[S.A_RL + ai.z + n] = (float)d; n++; }
     }
     A[S.A_RLN + a] = (float)n;
-    ar.fk(a);
+  };
+  auto factor = [&](uint32_t a) {
     if (F64 && S.ART_F64 == 1u) ar.factor<true>(a, P);
     else ar.factor<false>(a, P);
+  };
+  if (S.NA <= (nt >> 5u)) {
+    // Few articulations: a warp each, so the FK's per-link trigonometry and outputs run across
+    // lanes and only the pose chain is serial.
+    const uint32_t lane = tid & 31u;
+    for (uint32_t a = tid >> 5u; a < S.NA; a += nt >> 5u) {
+      if (lane == 0u) gate(a);
+      __syncwarp();
+      ar.fk_warp(a, lane);
+      if (lane == 0u) factor(a);
+      __syncwarp();
+    }
+  } else {
+    for (uint32_t a = tid; a < S.NA; a += nt) {
+      gate(a);
+      ar.fk(a);
+      factor(a);
+    }
   }
   // Phase 1: classify the sorted contacts; units are runs of one body pair.
   const uint32_t nc = min(S.counters[1], S.MAXC);
@@ -1037,8 +1056,9 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
   for (uint32_t c = tid; c < nc; c += nt) {
     uint32_t slot = sch[S.S_DSLOT + c];
     if (slot == 0xffffffffu || slot >= S.MAXDENSE) continue;
-    pr.dense_row(slot, c, tscr);
+    pr.dense_row(slot, c, Lane{S.tscr + tid, nt});
   }
+  __syncthreads();  // the loop and mimic rows below use per-thread contiguous scratch slices
   const uint32_t JDIM = 3u * S.NDA;
   for (uint32_t i = tid; i < S.NLOOP; i += nt) {
     float4 L0 = S.sf[S.SF_LOOP + i * 5u];

@@ -1,5 +1,5 @@
 #pragma once
-// Solve of one scene by one block (the body of k_solve and of the fused k_prepare_solve).
+// Solve of one scene by one block (the body of k_solve).
 //
 // Follows the reference's solve pass (packages/steel-webgpu/src/wgsl.js:2501-3891) on its
 // default option set: free-body gravity, wrench and gyroscopic prologue (wgsl.js:3647-3675),
@@ -823,7 +823,12 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     S.slots[2u * u] = make_float4((float)row, (float)us, (float)((int)(key & 0xffffu) - 1), (float)((int)(key >> 16u) - 1));
   }
   __syncthreads();
-  for (uint32_t a = tid >> 5u; a < S.NA; a += nt >> 5u) sv.ar.twists_warp(a, sv.aqd, sv.tw, tid & 31u);
+  // Few articulations: a warp each (the chain recursion shortened); many: a thread each.
+  if (S.NA <= (nt >> 5u)) {
+    for (uint32_t a = tid >> 5u; a < S.NA; a += nt >> 5u) sv.ar.twists_warp(a, sv.aqd, sv.tw, tid & 31u);
+  } else {
+    for (uint32_t a = tid; a < S.NA; a += nt) sv.ar.twists(a, sv.aqd, sv.tw);
+  }
   __syncthreads();
   sv.dense_phase(0u, 0u, 0u);
   sv.sweep(0u, ncol, 0u, wcs, nu);
@@ -890,34 +895,50 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     A[S.A_QD + d + 3u] *= k; A[S.A_QD + d + 4u] *= k; A[S.A_QD + d + 5u] *= k;
   }
   __syncthreads();
-  for (uint32_t a = tid; a < S.NA; a += nt) {
-    uint4 ai = sv.ar.info(a);
+  // Joint integration of link l (wgsl.js:3797-3826).
+  auto integrate_link = [&](uint32_t l) {
     float* Q = A + S.A_Q;
     const float* aqd = sv.aqd;
-    for (uint32_t k = 0; k < ai.y; k++) {
-      uint32_t l = ai.x + k, qs = sv.ar.lqs(l), d = sv.ar.ldof(l), t = sv.ar.ltype(l);
-      if (t == 1u || t == 0u || t == 6u)
-        for (uint32_t r = 0; r < sv.ar.lndof(l); r++) Q[qs + r] += aqd[d + r] * P.dt;
-      if (t == 2u) {
-        f3 w = mf3(aqd[d], aqd[d + 1u], aqd[d + 2u]);
-        float4 q = make_float4(Q[qs], Q[qs + 1], Q[qs + 2], Q[qs + 3]);
-        q = nrm4(add4(q, scale4(0.5f * P.dt, qmul(mf4(w, 0.0f), q))));
-        Q[qs] = q.x; Q[qs + 1] = q.y; Q[qs + 2] = q.z; Q[qs + 3] = q.w;
-      }
-      if (t == 4u) {
-        for (uint32_t c = 0; c < 3u; c++) Q[qs + c] += aqd[d + c] * P.dt;
-        f3 w = mf3(aqd[d + 3u], aqd[d + 4u], aqd[d + 5u]);
-        float4 q = make_float4(Q[qs + 3], Q[qs + 4], Q[qs + 5], Q[qs + 6]);
-        q = nrm4(add4(q, scale4(0.5f * P.dt, qmul(mf4(w, 0.0f), q))));
-        Q[qs + 3] = q.x; Q[qs + 4] = q.y; Q[qs + 5] = q.z; Q[qs + 6] = q.w;
-      }
+    uint32_t qs = sv.ar.lqs(l), d = sv.ar.ldof(l), t = sv.ar.ltype(l);
+    if (t == 1u || t == 0u || t == 6u)
+      for (uint32_t r = 0; r < sv.ar.lndof(l); r++) Q[qs + r] += aqd[d + r] * P.dt;
+    if (t == 2u) {
+      f3 w = mf3(aqd[d], aqd[d + 1u], aqd[d + 2u]);
+      float4 q = make_float4(Q[qs], Q[qs + 1], Q[qs + 2], Q[qs + 3]);
+      q = nrm4(add4(q, scale4(0.5f * P.dt, qmul(mf4(w, 0.0f), q))));
+      Q[qs] = q.x; Q[qs + 1] = q.y; Q[qs + 2] = q.z; Q[qs + 3] = q.w;
     }
-    sv.ar.fk(a);
-    for (uint32_t k = 0; k < ai.y; k++) {
-      uint32_t l = ai.x + k;
-      uint32_t b = (uint32_t)sv.ar.lbody(l);
-      S.pos[b] = mf4(sv.ar.ld3(sv.ar.lo(l) + L_COM), 0.0f);
-      S.rot[b] = sv.ar.link_rot(l);
+    if (t == 4u) {
+      for (uint32_t c = 0; c < 3u; c++) Q[qs + c] += aqd[d + c] * P.dt;
+      f3 w = mf3(aqd[d + 3u], aqd[d + 4u], aqd[d + 5u]);
+      float4 q = make_float4(Q[qs + 3], Q[qs + 4], Q[qs + 5], Q[qs + 6]);
+      q = nrm4(add4(q, scale4(0.5f * P.dt, qmul(mf4(w, 0.0f), q))));
+      Q[qs + 3] = q.x; Q[qs + 4] = q.y; Q[qs + 5] = q.z; Q[qs + 6] = q.w;
+    }
+  };
+  auto store_link_pose = [&](uint32_t l) {
+    uint32_t b = (uint32_t)sv.ar.lbody(l);
+    S.pos[b] = mf4(sv.ar.ld3(sv.ar.lo(l) + L_COM), 0.0f);
+    S.rot[b] = sv.ar.link_rot(l);
+  };
+  if (S.NA <= (nt >> 5u)) {
+    // Few articulations: a warp each; the links' joint updates and body poses are independent,
+    // the FK runs across lanes (fk_warp).
+    const uint32_t lane = tid & 31u;
+    for (uint32_t a = tid >> 5u; a < S.NA; a += nt >> 5u) {
+      uint4 ai = sv.ar.info(a);
+      for (uint32_t k = lane; k < ai.y; k += 32u) integrate_link(ai.x + k);
+      __syncwarp();
+      sv.ar.fk_warp(a, lane);
+      for (uint32_t k = lane; k < ai.y; k += 32u) store_link_pose(ai.x + k);
+      __syncwarp();
+    }
+  } else {
+    for (uint32_t a = tid; a < S.NA; a += nt) {
+      uint4 ai = sv.ar.info(a);
+      for (uint32_t k = 0; k < ai.y; k++) integrate_link(ai.x + k);
+      sv.ar.fk(a);
+      for (uint32_t k = 0; k < ai.y; k++) store_link_pose(ai.x + k);
     }
   }
   // Friction anchors: advance and store for the next substep (wgsl.js:3832-3878).
