@@ -1220,7 +1220,7 @@ struct Narrow {
   }
 };
 
-__global__ void __launch_bounds__(NARROW_WARPS * 32, 2) k_narrow(BatchDev B) {
+__global__ void __launch_bounds__(NARROW_WARPS * 32, 3) k_narrow(BatchDev B) {
   uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5u;
   uint32_t nwarps = (gridDim.x * blockDim.x) >> 5u;
   uint32_t total = *B.pair_count;
@@ -1232,14 +1232,40 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, 2) k_narrow(BatchDev B) {
   }
 }
 
-// The jobs k_narrow deferred, one per thread (grid-stride).
+// The jobs k_narrow deferred, one per thread (grid-stride over blocks of NARROW_JOB_THREADS
+// jobs). Each block first orders its jobs by kind (a counting sort in shared memory), so a warp's
+// threads mostly run the same routine. The order within a kind follows shared-memory atomics;
+// jobs only append contacts, whose order the canonical sort fixes.
 __global__ void __launch_bounds__(NARROW_JOB_THREADS, 4) k_narrow_jobs(BatchDev B) {
+  constexpr uint32_t KINDS = 8u;  // job kinds are 1..7
+  __shared__ uint32_t start[KINDS];
+  __shared__ uint32_t order[NARROW_JOB_THREADS];
   const uint32_t total = min(B.pair_count[1], B.pair_cap);
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
-    JobR r(B.jobs + (size_t)j * (NJOB_WORDS / 4u));
-    const uint32_t scene = r.w[1];
-    Narrow N(B.scenes[scene], &B, scene);
-    N.run_job(r);
+  const uint32_t tid = threadIdx.x;
+  for (uint32_t base = blockIdx.x * NARROW_JOB_THREADS; base < total; base += gridDim.x * NARROW_JOB_THREADS) {
+    const uint32_t j = base + tid;
+    if (tid < KINDS) start[tid] = 0u;
+    __syncthreads();
+    uint32_t kind = 0u, pos = 0u;
+    if (j < total) {
+      kind = min(B.jobs[(size_t)j * (NJOB_WORDS / 4u)].x, KINDS - 1u);
+      pos = atomicAdd(&start[kind], 1u);
+    }
+    __syncthreads();
+    if (tid == 0u) {
+      uint32_t acc = 0u;
+      for (uint32_t k = 0; k < KINDS; k++) { uint32_t c = start[k]; start[k] = acc; acc += c; }
+    }
+    __syncthreads();
+    if (j < total) order[start[kind] + pos] = j;
+    __syncthreads();
+    if (tid < min(NARROW_JOB_THREADS, total - base)) {
+      JobR r(B.jobs + (size_t)order[tid] * (NJOB_WORDS / 4u));
+      const uint32_t scene = r.w[1];
+      Narrow N(B.scenes[scene], &B, scene);
+      N.run_job(r);
+    }
+    __syncthreads();
   }
 }
 
