@@ -790,8 +790,25 @@ void Oracle::k_prepare() {
     float lim = mu * ln;
     float lm = length(lt);
     if (lm > lim) lt = lt * (lim / fmaxf_(lm, 1e-12f));
-    rows[o + 0u] = mk4(n, effn);
-    rows[o + 1u] = mk4(t1, rhs);
+    float effc = effn, rhsc = rhs;
+    if (C.COMPL == 1u) {
+      // contact_compliance (wgsl.js:2194-2206): a spring-damper normal row; the pair's series
+      // stiffness and summed damping are split over the unit's kept points.
+      v4 kc4 = contacts[c * 5u + 4u];
+      float nk = (float)std::max(sc[C.S_USIZE + sp], 1u);
+      v2 kc = mk2(kc4.x / nk, kc4.y / nk);
+      float gam = 0.0f;
+      if (kc.x > 0.0f) {
+        float ce = phi <= 0.0f ? kc.y : 0.0f;
+        float den = P.dt * kc.x + ce;
+        gam = 1.0f / (P.dt * den);
+        rhsc = (kc.x * phi) / den;
+        if (effn > 0.0f) effc = 1.0f / (1.0f / effn + gam);
+      }
+      rows[o + C.CO] = mk4(gam, 0.0f, 0.0f, 0.0f);
+    }
+    rows[o + 0u] = mk4(n, effc);
+    rows[o + 1u] = mk4(t1, rhsc);
     rows[o + 2u] = mk4(t2, mu);
     rows[o + 3u] = mk4(ra, (float)(key & 0xffffu));
     rows[o + 4u] = mk4(rb, (float)(key >> 16u));

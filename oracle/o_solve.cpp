@@ -104,6 +104,13 @@ v2 Oracle::friction_pair_solve(float a0, float c0, float d0, float r0, float r1,
   return m > radius ? relaxed * (radius / m) : relaxed;
 }
 
+// snap_tw (wgsl.js:2930-2934): a body's twist at the end of the position iterations.
+void Oracle::snap_tw(int b, v3 out[2]) const {
+  if (b < 0) { out[0] = splat3(0.0f); out[1] = splat3(0.0f); return; }
+  uint32_t o = C.A_SNAP + (uint32_t)b * 8u;
+  out[0] = ld3(o);
+  out[1] = ld3(o + 4u);
+}
 void Oracle::load_tw(int b, v3 out[2]) const {
   if (b < 0) { out[0] = splat3(0.0f); out[1] = splat3(0.0f); return; }
   out[0] = xyz(tw[(uint32_t)b * 2u]);
@@ -149,8 +156,9 @@ void Oracle::solve_unit(uint32_t us, uint32_t row, int a, int b, uint32_t s0, ui
   } else {
     v3 vrel = (tb[0] + cross(tb[1], rb)) - (ta[0] + cross(ta[1], ra));
     float jv = dot(n, vrel);
-    float w = rows[o + 5u].w;
+    float w = vpass ? 1.0f : rows[o + 5u].w;
     float res = jv + r1.w;
+    if (C.COMPL == 1u) res += rows[o + C.CO].x * lam.x;
     float nl = fmaxf_(lam.x + C.F_OMEGA * ((((-res) * r0.w) * w) - (1.0f - w) * lam.x), 0.0f);
     dn = nl - lam.x;
     lam.x = nl;
@@ -171,7 +179,7 @@ void Oracle::solve_unit(uint32_t us, uint32_t row, int a, int b, uint32_t s0, ui
         float load = art[C.A_ULOAD + us];
         lim = r2.w * load;
         v3 e = xyz(rows[o + PO + 2u]);
-        bias = (C.F_ANCHOR_BETA * mk2(dot(t1, e), dot(t2, e))) / P.dt;
+        bias = vpass ? mk2(0.0f, 0.0f) : (C.F_ANCHOR_BETA * mk2(dot(t1, e), dot(t2, e))) / P.dt;
         rows[o + PO + 2u].w = lim;
       }
     }
@@ -288,7 +296,7 @@ bool Oracle::art_dense(uint32_t a, uint32_t mode, uint32_t it, uint32_t ph) {
         for (uint32_t l = 0; l < 32u; l++) part[l] = 0.0f;
         for (uint32_t k = 0; k < ai.w; k++) part[k % 32u] += art[jo + r * NDA + k] * aqd[ai.z + k];
         float jv = lane_sum32(part);
-        float rhs = r == 0u ? art[o + 4u] : (r == 1u ? art[o + 22u] : art[o + 23u]);
+        float rhs = vpass ? 0.0f : (r == 0u ? art[o + 4u] : (r == 1u ? art[o + 22u] : art[o + 23u]));
         float dl = ((-C.F_OMEGA) * (jv + rhs)) * art[o + 5u + r];
         setat(nlam, (int)r, at(nlam, (int)r) + dl);
         for (uint32_t k = 0; k < ai.w; k++) aqd[ai.z + k] += art[yo + r * NDA + k] * dl;
@@ -304,7 +312,7 @@ bool Oracle::art_dense(uint32_t a, uint32_t mode, uint32_t it, uint32_t ph) {
     for (uint32_t l = 0; l < 32u; l++) part[l] = 0.0f;
     for (uint32_t k = 0; k < ai.w; k++) part[k % 32u] += art[jo + k] * aqd[ai.z + k];
     float jv = lane_sum32(part);
-    float w = art[o + 24u];
+    float w = vpass ? 1.0f : art[o + 24u];
     float nl = fmaxf_(lam.x + C.F_OMEGA * ((((-(jv + art[o + 4u])) * art[o + 5u]) * w) - (1.0f - w) * lam.x), 0.0f);
     float dn = nl - lam.x;
     for (uint32_t l = 0; l < 32u; l++) { p1[l] = 0.0f; p2[l] = 0.0f; }
@@ -384,7 +392,7 @@ void Oracle::art_dof_rows(uint32_t a, uint32_t l, uint32_t r, uint32_t d, bool v
       float gap = side == 0u ? q - lim.x : lim.y - q;
       float lam = art[C.A_LIM + 2u * d + side];
       float rhs = gap / P.dt;
-      if (gap < 0.0f) rhs = fmaxf_((P.beta * gap) / P.dt, -P.max_depen);
+      if (gap < 0.0f) rhs = vpass ? 0.0f : fmaxf_((P.beta * gap) / P.dt, -P.max_depen);
       float nl = fmaxf_(lam - (C.F_OMEGA * (sg * aqd[d] + rhs)) / hinv, 0.0f);
       if (nl == lam) continue;
       art[C.A_LIM + 2u * d + side] = nl;
@@ -626,6 +634,45 @@ void Oracle::k_solve() {
     if (C.NEST == 1u) momentum_step(wn_y, it);
     sweep(1u, wn_y, it, 0u);
   }
+  // Velocity pass (velocity_iterations, wgsl.js:3700-3736): positions integrate with the velocities
+  // reached here; further bias-free sweeps from the accumulated impulses set the output velocities.
+  if (C.VELITERS > 0u) {
+    for (uint32_t b = 0; b < C.NB; b++) {
+      st3(C.A_SNAP + b * 8u, xyz(tw[b * 2u]));
+      st3(C.A_SNAP + b * 8u + 4u, xyz(tw[b * 2u + 1u]));
+    }
+    for (uint32_t i = 0; i < C.ND; i++) art[C.A_SNAP + C.NB * 8u + i] = aqd[i];
+    // Contact rhs without bias: 0, or a speculative gap still open at the snapshot velocity.
+    for (uint32_t us = 0; us < wn_x; us++) {
+      uint32_t key = sc[C.S_UKEY + us];
+      int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
+      v3 ta[2], tb[2];
+      load_tw(a, ta);
+      load_tw(b, tb);
+      uint32_t s0 = sc[C.S_USTART + us];
+      for (uint32_t i = s0; i < s0 + sc[C.S_USIZE + us]; i++) {
+        uint32_t o = i * ROWS;
+        float phi = rows[o + 6u].w;
+        if (phi >= 1e29f) continue;
+        v3 n = xyz(rows[o]);
+        float jv = dot(n, (tb[0] + cross(tb[1], xyz(rows[o + 4u]))) - (ta[0] + cross(ta[1], xyz(rows[o + 3u]))));
+        rows[o + 1u].w = (phi > 0.0f && phi + P.dt * jv > 1e-6f) ? phi / P.dt : 0.0f;
+      }
+    }
+    uint32_t nd = std::min(sc[C.S_META + 3u], C.MAXDENSE);
+    for (uint32_t i = 0; i < nd; i++) {
+      uint32_t o = C.A_DENSE + i * C.DPS;
+      if (art[o + 21u] > 0.5f || art[o + 22u] >= 1e29f) continue;
+      u4 ai = art_info(f2u(art[o]));
+      float jv = 0.0f;
+      for (uint32_t k = 0; k < ai.w; k++) jv += art[o + C.DHDR + k] * aqd[ai.z + k];
+      float phi = art[o + 22u];
+      art[o + 4u] = (phi > 0.0f && phi + P.dt * jv > 1e-6f) ? phi / P.dt : 0.0f;
+    }
+    vpass = true;
+    for (uint32_t it = 0; it < C.VELITERS; it++) sweep(1u, wn_y, P.iterations + it, 0u);
+    vpass = false;
+  }
   // Warm-start table store (wgsl.js:3737-3767).
   uint32_t nc = sc[C.S_USTART + wn_x];
   uint32_t ndense = std::min(sc[C.S_META + 3u], C.MAXDENSE);
@@ -663,6 +710,12 @@ void Oracle::k_solve() {
     float damp = (body_flags((int)b) & 1u) != 0u ? 1.0f : 1.0f - body_limits((int)b).x * P.dt;
     vel[b * 2u] = mk4(v, 0.0f);
     vel[b * 2u + 1u] = mk4(w * damp, 0.0f);
+    if (C.VELITERS > 0u) {
+      v3 s2[2];
+      snap_tw((int)b, s2);
+      v = s2[0];
+      w = s2[1];
+    }
     if (node_asleep((int)b)) {
       vel[b * 2u] = mk4(0, 0, 0, 0);
       vel[b * 2u + 1u] = mk4(0, 0, 0, 0);
@@ -674,7 +727,10 @@ void Oracle::k_solve() {
     poses[C.P_BODY + b * 2u] = mk4(c, 0.0f);
     poses[C.P_BODY + b * 2u + 1u] = q;
   }
-  for (uint32_t i = 0; i < C.ND; i++) art[C.A_QD + i] = aqd[i];
+  for (uint32_t i = 0; i < C.ND; i++) {
+    art[C.A_QD + i] = aqd[i];
+    if (C.VELITERS > 0u) aqd[i] = art[C.A_SNAP + C.NB * 8u + i];
+  }
   for (uint32_t l = 0; l < C.NL; l++) {
     if (link_type(l) != 4u || link_parent(l) >= 0) continue;
     float k = 1.0f - body_limits(link_body(l)).x * P.dt;
@@ -728,6 +784,7 @@ void Oracle::k_solve() {
       v3 ta[2], tb[2];
       load_tw(a, ta);
       load_tw(b, tb);
+      if (C.VELITERS > 0u) { snap_tw(a, ta); snap_tw(b, tb); }
       v3 vrel = (tb[0] + cross(tb[1], frb)) - (ta[0] + cross(ta[1], fra));
       v4 lam = rows[o + 6u];
       v3 lt = t1 * lam.y + t2 * lam.z;

@@ -294,6 +294,8 @@ struct Oracle {
   void momentum_unit(uint32_t us, uint32_t row, float beta, bool init);
   void momentum_step(uint32_t ncol, uint32_t it);
   float wmom_k = 0.0f, wmom_beta = 0.0f;  // the solve's momentum state (k, beta)
+  bool vpass = false;  // velocity pass (wgsl.js:2928): rows without position bias or regularization
+  void snap_tw(int b, v3 out[2]) const;
   void art_dof_impulse(uint32_t a, uint32_t l, uint32_t r, float dl);
   void art_propagate(uint32_t a, bool vlim, bool rowsOn);
   void art_dof_rows(uint32_t a, uint32_t l, uint32_t r, uint32_t d, bool vlim, bool rowsOn);

@@ -456,8 +456,25 @@ struct Prep {
     float lim = mu * ln;
     float lm = len(lt);
     if (lm > lim) lt = lt * (lim / fmx(lm, 1e-12f));
-    rows[o + 0u] = mf4(n, effn);
-    rows[o + 1u] = mf4(t1, rhs);
+    float effc = effn, rhsc = rhs;
+    if (S.COMPL == 1u) {
+      // contact_compliance (wgsl.js:2194-2206): a spring-damper normal row; the pair's series
+      // stiffness and summed damping are split over the unit's kept points.
+      const float4 kc4 = S.con[c * 5u + 4u];
+      const float nk = (float)max(S.sched[S.S_USIZE + S.sched[S.S_RUNIT + idx]], 1u);
+      const f2 kc = mf2(kc4.x / nk, kc4.y / nk);
+      float gam = 0.0f;
+      if (kc.x > 0.0f) {
+        float ce = phi <= 0.0f ? kc.y : 0.0f;
+        float den = P.dt * kc.x + ce;
+        gam = 1.0f / (P.dt * den);
+        rhsc = (kc.x * phi) / den;
+        if (effn > 0.0f) effc = 1.0f / (1.0f / effn + gam);
+      }
+      rows[o + S.CO] = make_float4(gam, 0.0f, 0.0f, 0.0f);
+    }
+    rows[o + 0u] = mf4(n, effc);
+    rows[o + 1u] = mf4(t1, rhsc);
     rows[o + 2u] = mf4(t2, mu);
     rows[o + 3u] = mf4(ra, (float)(key & 0xffffu));
     rows[o + 4u] = mf4(rb, (float)(key >> 16u));
@@ -930,7 +947,7 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
       Prep::bp_value(__uint_as_float(bpc[0]), __uint_as_float(bpc[1]), __uint_as_float(bpc[2]), bpc[3], q, &s_, &id);
       if (id != 0u && s_ == sl[q * 2u] && id == sl[q * 2u + 1u]) win = true;
     }
-    sch[S.S_KEEP + p] = win ? 1u : 0u;
+    sch[S.S_KEEP + p] = (win || S.COMPL == 1u) ? 1u : 0u;  // compliant contacts stay whole
   }
   __syncthreads();
   for (uint32_t u = tid; u < nu; u += nt) {

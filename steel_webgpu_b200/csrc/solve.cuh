@@ -26,6 +26,7 @@ struct Solver {
   float4* tw;
   float4* imp;
   float* aqd;
+  bool vpass = false;  // velocity pass (wgsl.js:2928): rows without position bias or regularization
   __device__ Solver(const SceneDev& s, const Params& p, float* lb, float4* tw_, float4* imp_, float* aqd_)
       : S(s), P(p), ar(s, lb), tw(tw_), imp(imp_), aqd(aqd_) {}
 
@@ -35,6 +36,13 @@ struct Solver {
   __device__ m3 binv_inertia(int b) const {
     RO<float4> o = S.sf + S.SF_BODY + (uint32_t)b * 8u;
     return tr(mcols(v3(o[5]), v3(o[6]), v3(o[7])));
+  }
+  // A body's twist at the end of the position iterations (wgsl.js:2930-2934).
+  __device__ void snap_tw(int b, f3 out[2]) const {
+    if (b < 0) { out[0] = sp3(0.0f); out[1] = sp3(0.0f); return; }
+    const uint32_t o = S.A_SNAP + (uint32_t)b * 8u;
+    out[0] = ar.ald3(o);
+    out[1] = ar.ald3(o + 4u);
   }
   __device__ void load_tw(int b, f3 out[2]) const {
     if (b < 0) { out[0] = sp3(0.0f); out[1] = sp3(0.0f); return; }
@@ -220,8 +228,9 @@ struct Solver {
     } else {
       f3 vrel = (tb[0] + cross(tb[1], rb)) - (ta[0] + cross(ta[1], ra));
       float jv = dot(n, vrel);
-      float w = rows[o + 5u].w;
+      float w = vpass ? 1.0f : rows[o + 5u].w;
       float res = jv + r1.w;
+      if (S.COMPL == 1u) res += rows[o + S.CO].x * lam.x;
       float nl = fmx(lam.x + S.F_OMEGA * ((((-res) * r0.w) * w) - (1.0f - w) * lam.x), 0.0f);
       float dn = nl - lam.x;
       lam.x = nl;
@@ -242,7 +251,7 @@ struct Solver {
           float load = S.art[S.A_ULOAD + us];
           lim = r2.w * load;
           f3 e = v3(rows[o + PO + 2u]);
-          bias = (S.F_ANCHOR_BETA * mf2(dot(t1, e), dot(t2, e))) / P.dt;
+          bias = vpass ? mf2(0.0f, 0.0f) : (S.F_ANCHOR_BETA * mf2(dot(t1, e), dot(t2, e))) / P.dt;
           rows[o + PO + 2u].w = lim;
         }
       }
@@ -368,7 +377,7 @@ struct Solver {
           if (k < ai.w) part += d.J[r][j] * q[j];
         }
         float jv = lane_sum(part);
-        float rhs = r == 0u ? d.m4 : (r == 1u ? d.m22 : d.m23);
+        float rhs = vpass ? 0.0f : (r == 0u ? d.m4 : (r == 1u ? d.m22 : d.m23));
         float dl = ((-S.F_OMEGA) * (jv + rhs)) * A[o + 5u + r];
         setc(nlam, (int)r, comp(nlam, (int)r) + dl);
 #pragma unroll
@@ -395,7 +404,8 @@ struct Solver {
       if (k < ai.w) part += d.J[0][j] * q[j];
     }
     float jv = lane_sum(part);
-    float nl = fmx(lam.x + S.F_OMEGA * ((((-(jv + d.m4)) * d.m5) * d.m24) - (1.0f - d.m24) * lam.x), 0.0f);
+    const float w = vpass ? 1.0f : d.m24;
+    float nl = fmx(lam.x + S.F_OMEGA * ((((-(jv + d.m4)) * d.m5) * w) - (1.0f - w) * lam.x), 0.0f);
     float dn = nl - lam.x;
     float p1 = 0.0f, p2 = 0.0f;
 #pragma unroll
@@ -439,7 +449,7 @@ struct Solver {
           float part = 0.0f;
           for (uint32_t k = lane; k < ai.w; k += 32u) part += A[jo + r * NDA + k] * aqd[ai.z + k];
           float jv = lane_sum(part);
-          float rhs = r == 0u ? A[o + 4u] : (r == 1u ? A[o + 22u] : A[o + 23u]);
+          float rhs = vpass ? 0.0f : (r == 0u ? A[o + 4u] : (r == 1u ? A[o + 22u] : A[o + 23u]));
           float dl = ((-S.F_OMEGA) * (jv + rhs)) * A[o + 5u + r];
           setc(nlam, (int)r, comp(nlam, (int)r) + dl);
           for (uint32_t k = lane; k < ai.w; k += 32u) aqd[ai.z + k] += A[yo + r * NDA + k] * dl;
@@ -455,7 +465,7 @@ struct Solver {
       float part = 0.0f;
       for (uint32_t k = lane; k < ai.w; k += 32u) part += A[jo + k] * aqd[ai.z + k];
       float jv = lane_sum(part);
-      float w = A[o + 24u];
+      float w = vpass ? 1.0f : A[o + 24u];
       float nl = fmx(lam.x + S.F_OMEGA * ((((-(jv + A[o + 4u])) * A[o + 5u]) * w) - (1.0f - w) * lam.x), 0.0f);
       float dn = nl - lam.x;
       float p1 = 0.0f, p2 = 0.0f;
@@ -515,7 +525,7 @@ struct Solver {
           float gap = side == 0u ? q - lim.x : lim.y - q;
           float lam = A[S.A_LIM + 2u * d + side];
           float rhs = gap / P.dt;
-          if (gap < 0.0f) rhs = fmx((P.beta * gap) / P.dt, -P.max_depen);
+          if (gap < 0.0f) rhs = vpass ? 0.0f : fmx((P.beta * gap) / P.dt, -P.max_depen);
           float nl = fmx(lam - (S.F_OMEGA * (sg * aqd[d] + rhs)) / hinv, 0.0f);
           if (nl == lam) continue;
           A[S.A_LIM + 2u * d + side] = nl;
@@ -836,6 +846,46 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     if (S.NEST == 1u) sv.momentum_step(ncol, it, wcs);
     sv.sweep(1u, ncol, it, wcs, nu);
   }
+  // Velocity pass (velocity_iterations, wgsl.js:3700-3736): positions integrate with the velocities
+  // reached here; further bias-free sweeps from the accumulated impulses set the output velocities.
+  if (S.VELITERS > 0u) {
+    for (uint32_t b = tid; b < S.NB; b += nt) {
+      sv.ar.ast3(S.A_SNAP + b * 8u, v3(sv.tw[b * 2u]));
+      sv.ar.ast3(S.A_SNAP + b * 8u + 4u, v3(sv.tw[b * 2u + 1u]));
+    }
+    for (uint32_t i = tid; i < S.ND; i += nt) A[S.A_SNAP + S.NB * 8u + i] = sv.aqd[i];
+    // Contact rhs without bias: 0, or a speculative gap still open at the snapshot velocity.
+    for (uint32_t us = tid; us < nu; us += nt) {
+      const uint32_t key = S.sched[S.S_UKEY + us];
+      const int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
+      f3 ta[2], tb[2];
+      sv.load_tw(a, ta);
+      sv.load_tw(b, tb);
+      const uint32_t s0 = S.sched[S.S_USTART + us];
+      for (uint32_t i = s0; i < s0 + S.sched[S.S_USIZE + us]; i++) {
+        float4* R = S.rows + (size_t)i * S.ROWS;
+        const float phi = R[6].w;
+        if (phi >= 1e29f) continue;
+        const f3 n = v3(R[0]);
+        const float jv = dot(n, (tb[0] + cross(tb[1], v3(R[4]))) - (ta[0] + cross(ta[1], v3(R[3]))));
+        R[1].w = (phi > 0.0f && phi + P.dt * jv > 1e-6f) ? phi / P.dt : 0.0f;
+      }
+    }
+    const uint32_t ndv = min(S.sched[S.S_META + 3u], S.MAXDENSE);
+    for (uint32_t i = tid; i < ndv; i += nt) {
+      const uint32_t o = S.A_DENSE + i * S.DPS;
+      if (A[o + 21u] > 0.5f || A[o + 22u] >= 1e29f) continue;
+      const uint4 ai = sv.ar.info(f2u(A[o]));
+      float jv = 0.0f;
+      for (uint32_t k = 0; k < ai.w; k++) jv += A[o + S.DHDR + k] * sv.aqd[ai.z + k];
+      const float phi = A[o + 22u];
+      A[o + 4u] = (phi > 0.0f && phi + P.dt * jv > 1e-6f) ? phi / P.dt : 0.0f;
+    }
+    __syncthreads();
+    sv.vpass = true;
+    for (uint32_t it = 0; it < S.VELITERS; it++) sv.sweep(1u, ncol, P.iterations + it, wcs, nu);
+    sv.vpass = false;
+  }
   // Warm-start table (wgsl.js:3737-3767): rows sharing a key keep the largest normal impulse.
   const uint32_t nc = S.sched[S.S_USTART + nu];
   const uint32_t ndense = min(S.sched[S.S_META + 3u], S.MAXDENSE);
@@ -875,6 +925,12 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     float damp = (sv.bflags((int)b) & 1u) != 0u ? 1.0f : 1.0f - S.sf[S.SF_BODY + b * 8u + 3u].w * P.dt;
     S.lv[b] = mf4(v, 0.0f);
     S.av[b] = mf4(w * damp, 0.0f);
+    if (S.VELITERS > 0u) {
+      f3 s2[2];
+      sv.snap_tw((int)b, s2);
+      v = s2[0];
+      w = s2[1];
+    }
     if (asleep(b)) {  // a sleeping body stays put at rest (wgsl.js:3779)
       S.lv[b] = make_float4(0, 0, 0, 0);
       S.av[b] = make_float4(0, 0, 0, 0);
@@ -886,7 +942,10 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     S.pos[b] = mf4(c, 0.0f);
     S.rot[b] = q;
   }
-  for (uint32_t i = tid; i < S.ND; i += nt) A[S.A_QD + i] = sv.aqd[i];
+  for (uint32_t i = tid; i < S.ND; i += nt) {
+    A[S.A_QD + i] = sv.aqd[i];
+    if (S.VELITERS > 0u) sv.aqd[i] = A[S.A_SNAP + S.NB * 8u + i];
+  }
   __syncthreads();
   for (uint32_t l = tid; l < S.NL; l += nt) {
     if (sv.ar.ltype(l) != 4u || sv.ar.lparent(l) >= 0) continue;
@@ -962,6 +1021,7 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
       f3 ta[2], tb[2];
       sv.load_tw(a, ta);
       sv.load_tw(b, tb);
+      if (S.VELITERS > 0u) { sv.snap_tw(a, ta); sv.snap_tw(b, tb); }
       f3 vrel = (tb[0] + cross(tb[1], frb)) - (ta[0] + cross(ta[1], fra));
       float4 lam = rows[o + 6u];
       f3 lt = t1 * lam.y + t2 * lam.z;

@@ -164,3 +164,40 @@ def spinners(seed=29):
         if s["sid"] in spun:
             s["torsion_radius"] = float(rng.uniform(0.08, 0.12))
     return sc
+
+
+def compliant(seed=31):
+    """contact_compliance on: boxes of three stiffnesses (ke 1e3, 1e4, 1e5 with damping kd) dropped
+    on a stiff plane; their normal rows are spring-dampers, and the body-pair reduction keeps every
+    point."""
+    rng = np.random.default_rng(seed)
+    b = SceneBuilder(fps=240, box_hulls="direct")
+    b.add_ground_plane(mu=0.6, ke=1e7, kd=0.0)
+    for i, (ke, kd) in enumerate(((1e3, 20.0), (1e4, 60.0), (1e5, 200.0), (1e4, 60.0))):
+        body = b.add_body(xform=[-0.9 + 0.6 * i, 0.0, 0.3 + 0.2 * i] + synth._rand_quat(rng))
+        b.add_shape_box(body, hx=0.1, hy=0.08, hz=0.06, mu=0.6, ke=ke, kd=kd)
+    return b.finalize(solver=dict(contact_compliance=True, enable_restitution=False))
+
+
+def velocity_pass(seed=37):
+    """velocity_iterations=4: a stack of boxes that starts 3 mm interpenetrated (a depenetration the
+    position sweeps push out, the velocity sweeps then clear of bias), friction anchors on, and a
+    6-link revolute chain with +-0.4 rad joint limits released from 1 rad, whose links hit each
+    other (dense rows) and their limits (limit rows) while the velocity pass runs without bias."""
+    rng = np.random.default_rng(seed)
+    b = SceneBuilder(fps=240, box_hulls="direct")
+    b.add_ground_plane(mu=0.7)
+    for k in range(4):
+        body = b.add_body(xform=[0.01 * float(rng.uniform(-1, 1)), 0.0, 0.097 + 0.197 * k, 0, 0, 0, 1])
+        b.add_shape_box(body, hx=0.15, hy=0.12, hz=0.1, mu=0.7)
+    parent = -1
+    top = [1.0, 0.0, 1.2]
+    for k in range(6):
+        body = b.add_body(xform=[top[0], top[1], top[2] - 0.1 * (k + 0.5), 0, 0, 0, 1])
+        b.add_shape_capsule(body, radius=0.03, half_height=0.04, mass=0.3)
+        b.add_joint_revolute(parent, body, axis=[0, 1, 0],
+                             parent_xform=[0, 0, -0.05, 0, 0, 0, 1] if parent >= 0 else top + [0, 0, 0, 1],
+                             child_xform=[0, 0, 0.05, 0, 0, 0, 1], q=[1.0] if k == 0 else [0.3],
+                             limitLower=-0.4 if k else -2.0, limitUpper=0.4 if k else 2.0)
+        parent = body
+    return b.finalize(solver=dict(velocity_iterations=4))
