@@ -397,6 +397,16 @@ void Oracle::art_factor(uint32_t a) {
       acc = sadd(acc, sscale(ldS(l, r), qdd));
     }
     stsv(L + L_A, acc);
+    if (C.JFL == 1u) {
+      // joint_friction_load_coefficient (artwgsl.js:361-367): the joint's transmitted force and
+      // torque under the free dynamics (I^A a + p^A at the child COM) raise its friction bound.
+      SV f = sadd(imul(L + L_IA, acc), ldsv(L + L_PA));
+      float fm = length(f.l) + length(f.a);
+      for (uint32_t r = 0; r < n; r++) {
+        uint32_t d = link_dof(l) + r;
+        art[C.A_JFL + d] = statF[C.SF_DOF + d * 5u + 3u].w * fm;
+      }
+    }
   }
 }
 

@@ -379,6 +379,7 @@ void Oracle::art_dof_rows(uint32_t a, uint32_t l, uint32_t r, uint32_t d, bool v
   float hinv = fmaxf_(art[C.A_HINV + d], 1e-12f);
   v4 pv = dof_passive(d);
   float fr = pv.y;
+  if (C.JFL == 1u) fr += art[C.A_JFL + d];
   if (rowsOn && fr > 0.0f) {
     float lam = art[C.A_FRIC + d];
     float nl = clampf(lam - (C.F_OMEGA * aqd[d]) / hinv, -fr * P.dt, fr * P.dt);

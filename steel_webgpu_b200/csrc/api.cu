@@ -144,8 +144,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
   static const char* unsupported[][2] = {
       {"FMODE", "friction_mode"}, {"ANG", "torsional/rolling friction"}, {"ANG_ART", "torsional/rolling friction"},
       {"CTI", "row_schedule contact_then_internal"}, {"LONGEST_FIRST", "propagation_color_order longest_first"},
-      {"DRIVE_ROWS", "drive_mode rows"},
-      {"JFL", "joint friction load coefficient"}};
+      {"DRIVE_ROWS", "drive_mode rows"}};
   for (auto& u : unsupported)
     if (C.u(u[0]) != 0u) { why = std::string("unsupported solver option: ") + u[1]; return STEEL_E_UNSUPPORTED; }
   if (in.statF_floats != (uint64_t)C.u("LEN_STATF4") * 4u || in.statU_words != C.u("LEN_STATU") ||
@@ -158,7 +157,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
   K(SF_BODY) K(SF_SHAPE) K(SF_HAABB) K(SF_VERTS) K(SF_FPLANE) K(SF_LINK) K(SF_DOF) K(SF_PATH) K(SF_LOOP)
   K(SF_MIMIC) K(SF_CTRL) K(SU_HULL) K(SU_FACE) K(SU_FV) K(SU_HEDGE) K(SU_EDGE) K(SU_ART) K(SU_ACON)
   K(SU_FILTER) K(NB) K(NS) K(NA) K(NL) K(ND) K(NDA) K(JM) K(MAXPATH) K(MAXLP) K(NLOOP) K(NMIMIC) K(PATCH)
-  K(EXTRA) K(SHARED) K(FSHARED) K(REST) K(FSTART) K(TGT_HELD) K(CTRL_KIND) K(CTRL_A) K(CTRL_B) K(VLIM_FREE) K(VLIM_ON) K(ART_F64) K(SLEEP) K(NEST) K(MO) K(TORS) K(TO) K(COMPL) K(CO) K(VELITERS)
+  K(EXTRA) K(SHARED) K(FSHARED) K(REST) K(FSTART) K(TGT_HELD) K(CTRL_KIND) K(CTRL_A) K(CTRL_B) K(VLIM_FREE) K(VLIM_ON) K(ART_F64) K(SLEEP) K(NEST) K(MO) K(TORS) K(TO) K(COMPL) K(CO) K(VELITERS) K(JFL)
   K(FRICTION_COMBINE) K(RESTITUTION_COMBINE) K(NCOLW) K(NCOL) K(MAXP) K(MAXC) K(MAXU) K(WH) K(AH)
   K(MAXDENSE) K(ROWS) K(PO) K(DHDR) K(DPS)
 #undef K
@@ -189,9 +188,8 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
   {
     size_t ao = 0;
     auto put = [&](uint32_t& field, size_t n) { field = (uint32_t)ao; ao += n > 0 ? n : 1; };
-    uint32_t tmp;
     put(d.A_Q, NQ); put(d.A_QD, ND); put(d.A_QDH, ND); put(d.A_INT, ND); put(d.A_TGT, ND); put(d.A_TGTV, ND);
-    put(d.A_LIM, 2 * ND); put(d.A_DRV, ND); put(tmp, ND); put(d.A_JF, ND); put(d.A_BF, NB * 8); put(d.A_SLP, (NB + NA) * 4);
+    put(d.A_LIM, 2 * ND); put(d.A_DRV, ND); put(d.A_JFL, ND); put(d.A_JF, ND); put(d.A_BF, NB * 8); put(d.A_SLP, (NB + NA) * 4);
     put(d.A_FRIC, ND); put(d.A_HINV, ND);
     ao = (ao + 3) & ~(size_t)3;  // link blocks start on a 16-byte boundary (bulk copies)
     put(d.A_LINK, (size_t)(NL > 0 ? NL : 1) * 268); put(d.A_SNAP, NB * 8 + ND);

@@ -539,6 +539,13 @@ struct Art {
         acc = sadd(acc, sscl(ldS(l, r), qdd));
       }
       stsv(L + L_A, acc);
+      if (S.JFL == 1u) {
+        // joint_friction_load_coefficient (artwgsl.js:361-367): the joint's transmitted force and
+        // torque under the free dynamics (I^A a + p^A at the child COM) raise its friction bound.
+        const SVec f = sadd(imul(L + L_IA, acc), ldsv(L + L_PA));
+        const float fm = len(f.l) + len(f.a);
+        for (uint32_t r = 0; r < n; r++) A[S.A_JFL + d0 + r] = DR[(d0 + r) * 5u + 3u].w * fm;
+      }
     }
   }
 

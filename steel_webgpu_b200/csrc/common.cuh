@@ -195,7 +195,7 @@ struct SceneDev {
   // counts
   uint32_t NB, NS, NA, NL, ND, NQ, NDA, JM, MAXPATH, MAXLP, NLOOP, NMIMIC;
   // solver flags and constants
-  uint32_t PATCH, EXTRA, SHARED, FSHARED, REST, FSTART, TGT_HELD, CTRL_KIND, CTRL_A, CTRL_B, VLIM_FREE, VLIM_ON, ART_F64, SLEEP, NEST, MO, TORS, TO, COMPL, CO, VELITERS;
+  uint32_t PATCH, EXTRA, SHARED, FSHARED, REST, FSTART, TGT_HELD, CTRL_KIND, CTRL_A, CTRL_B, VLIM_FREE, VLIM_ON, ART_F64, SLEEP, NEST, MO, TORS, TO, COMPL, CO, VELITERS, JFL;
   uint32_t FRICTION_COMBINE, RESTITUTION_COMBINE, NCOLW, NCOL;
   float F_ANCHOR_BETA, F_CFM, F_OMEGA, F_SPEC, F_GAP_GATE, F_FGAP, F_FSCALE, F_REST_SPEED, F_FR_MUT, F_FR_MUR;
   float F_BP_CELL, F_JL_GAP, F_JL_SPEED, F_VLIM_FRAC, F_SLEEP_LIN, F_SLEEP_ANG, F_SLEEP_TIME;
@@ -211,7 +211,7 @@ struct SceneDev {
   float4 *spos, *srot, *alo, *ahi;   // shape pose and AABB [NS]
   float* art;                        // articulation buffer (A_* layout)
   uint32_t A_Q, A_QD, A_QDH, A_INT, A_TGT, A_TGTV, A_LIM, A_DRV, A_JF, A_BF, A_FRIC, A_HINV, A_LINK, A_VLG, A_AVL, A_LG,
-      A_RL, A_RLN, A_ULOAD, A_DENSE, A_SLP, A_SNAP;
+      A_RL, A_RLN, A_ULOAD, A_DENSE, A_SLP, A_SNAP, A_JFL;
   uint32_t* counters;                // [0] pairs, [1] contacts
   uint32_t* stats;                   // SimStats words (sim.js:822-834)
   Params* params;                    // this substep's parameters

@@ -782,7 +782,7 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
         on = q <= lim.x + g || q >= lim.y - g;
       }
       A[S.A_LG + d] = on ? 1.0f : 0.0f;
-      bool row = on || ar.dof_passive(d).y > 0.0f;
+      bool row = on || ar.dof_passive(d).y > 0.0f || S.JFL == 1u;
       if (row && ar.scalar_dof(d)) { A[S.A_RL + ai.z + n] = (float)d; n++; }
     }
     A[S.A_RLN + a] = (float)n;

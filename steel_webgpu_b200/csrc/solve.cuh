@@ -512,6 +512,7 @@ struct Solver {
       uint32_t r = d - ar.ldof(l);
       float hinv = fmx(A[S.A_HINV + d], 1e-12f);
       float fr = ar.dof_passive(d).y;
+      if (S.JFL == 1u) fr += A[S.A_JFL + d];
       if (fr > 0.0f) {
         float lam = A[S.A_FRIC + d];
         float nl = clmp(lam - (S.F_OMEGA * aqd[d]) / hinv, -fr * P.dt, fr * P.dt);

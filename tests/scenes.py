@@ -201,3 +201,19 @@ def velocity_pass(seed=37):
                              limitLower=-0.4 if k else -2.0, limitUpper=0.4 if k else 2.0)
         parent = body
     return b.finalize(solver=dict(velocity_iterations=4))
+
+
+def load_friction(seed=41):
+    """Joint friction with a load coefficient (enable_joint_friction, friction_load_coefficient): two
+    pendulums released from 1.2 rad, one whose friction bound grows with the force its joint
+    transmits (0.3 per newton) and holds it, one with plain friction that swings."""
+    b = SceneBuilder(fps=240)
+    for i in range(2):
+        top = [0.8 * i, 0.0, 1.5]
+        body = b.add_body(xform=[top[0], 0.0, top[2] - 0.3, 0, 0, 0, 1])
+        b.add_shape_box(body, hx=0.04, hy=0.04, hz=0.25, mass=1.0)
+        b.add_joint_revolute(-1, body, axis=[0, 1, 0], parent_xform=top + [0, 0, 0, 1],
+                             child_xform=[0, 0, 0.3, 0, 0, 0, 1], q=[1.2], friction=0.2)
+    sc = b.finalize(solver=dict(enable_joint_friction=True))
+    sc.json["joints"]["friction_load_coefficient"] = [0.3, 0.0]
+    return sc
