@@ -49,7 +49,6 @@ bool Oracle::init(const char* constants, const float* statF_, size_t nF, const u
   else if (C.ANG || C.ANG_ART) unsup = "torsional/rolling friction";
   else if (C.CTI) unsup = "row_schedule contact_then_internal";
   else if (C.LONGEST_FIRST) unsup = "propagation_color_order longest_first";
-  else if (C.DRIVE_ROWS) unsup = "drive_mode rows";
   if (unsup) { error = std::string("unsupported solver option: ") + unsup; return false; }
   if (nF != (size_t)C.LEN_STATF4 * 4u || nU != C.LEN_STATU || nArt != C.LEN_ART) { error = "buffer size mismatch"; return false; }
   statF.resize(C.LEN_STATF4);

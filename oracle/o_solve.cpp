@@ -378,6 +378,22 @@ void Oracle::art_propagate(uint32_t a, bool vlim, bool rowsOn) {
 void Oracle::art_dof_rows(uint32_t a, uint32_t l, uint32_t r, uint32_t d, bool vlim, bool rowsOn) {
   float hinv = fmaxf_(art[C.A_HINV + d], 1e-12f);
   v4 pv = dof_passive(d);
+  v4 dr = dof_drive(d);
+  // drive_mode="rows" (wgsl.js:3425-3438): a PhysX-style drive row, cold-started each substep, no
+  // relaxation; in the velocity pass only when velocity drives are active, against the snapshot.
+  bool driven = rowsOn && C.DRIVE_ROWS == 1u && (dr.y > 0.0f || dr.z > 0.0f);
+  if (driven && !(vpass && C.VEL_DRIVE_ACTIVE == 0u)) {
+    float q = art[C.A_Q + link_qs(l) + r];
+    float pd = 0.0f;
+    if (vpass) pd = P.dt * art[C.A_SNAP + C.NB * 8u + d];
+    float ca = P.dt * (P.dt * dr.y + dr.z);
+    float x = 1.0f / (1.0f + ca * hinv);
+    float bias = ((x * P.dt) * dr.z) * art[C.A_TGTV + d] + ((dr.y * x) * P.dt) * (((art[C.A_TGT + d] - q) - pd));
+    float mx = dr.w > 0.0f ? dr.w * P.dt : 1e20f;
+    float lam = art[C.A_DRV + d];
+    float nl = clampf((lam * (1.0f - x) - (x * ca) * aqd[d]) + bias, -mx, mx);
+    if (nl != lam) { art[C.A_DRV + d] = nl; art_dof_impulse(a, l, r, nl - lam); }
+  }
   float fr = pv.y;
   if (C.JFL == 1u) fr += art[C.A_JFL + d];
   if (rowsOn && fr > 0.0f) {

@@ -314,7 +314,7 @@ struct Art {
     Drr += (T)P.dt * (T)damp;
     float tau = (-damp) * qd + jf;
     if (spr.x != 0.0f) tau += spr.x * (spr.y - q);
-    if (dr.y > 0.0f || dr.z > 0.0f) {
+    if (S.DRIVE_ROWS == 0u && (dr.y > 0.0f || dr.z > 0.0f)) {
       float err = tgt - q;
       float mm = fmx((float)Drr, 1e-9f);
       float qdn = (mm * qd + P.dt * (dr.y * err + dr.z * tv)) / ((mm + P.dt * dr.z) + (P.dt * P.dt) * dr.y);

@@ -748,19 +748,23 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
     uint4 ai = ar.info(a);
     // Joint velocity limits (wgsl.js:1829-1854): scale the articulation's scalar dof speeds so the
     // most exceeded limit is met, then mark the dofs near their limit (rows exist only there).
-    // Drive rows are unsupported, so no dof has the fused drive clamp.
+    // A driven dof under drive rows with the fused clamp is not scaled (artwgsl.js:54).
+    auto fused = [&](uint32_t d) {
+      const float4 dr = ar.dof_drive(d);
+      return S.DRIVE_ROWS == 1u && S.FUSE_VLIM == 1u && (dr.y > 0.0f || dr.z > 0.0f);
+    };
     if (S.VLIM_ON == 1u) {
       float ratio = 1.0f;
       for (uint32_t k = 0; k < ai.w; k++) {
         uint32_t d = ai.z + k;
         float vl = ar.dof_passive(d).z;
-        if (vl < 0.0f) continue;
+        if (vl < 0.0f || fused(d)) continue;
         float sp = fabsf(A[S.A_QD + d]);
         if (sp > vl) ratio = fmn(ratio, vl / sp);
       }
       if (ratio < 1.0f)
         for (uint32_t k = 0; k < ai.w; k++)
-          if (ar.scalar_dof(ai.z + k)) A[S.A_QD + ai.z + k] *= ratio;
+          if (ar.scalar_dof(ai.z + k) && !fused(ai.z + k)) A[S.A_QD + ai.z + k] *= ratio;
       bool any = false;
       for (uint32_t k = 0; k < ai.w; k++) {
         uint32_t d = ai.z + k;
@@ -782,7 +786,8 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
         on = q <= lim.x + g || q >= lim.y - g;
       }
       A[S.A_LG + d] = on ? 1.0f : 0.0f;
-      bool row = on || ar.dof_passive(d).y > 0.0f || S.JFL == 1u;
+      const float4 drv = ar.dof_drive(d);
+      bool row = on || ar.dof_passive(d).y > 0.0f || S.JFL == 1u || (S.DRIVE_ROWS == 1u && (drv.y > 0.0f || drv.z > 0.0f));
       if (row && ar.scalar_dof(d)) { A[S.A_RL + ai.z + n] = (float)d; n++; }
     }
     A[S.A_RLN + a] = (float)n;
@@ -891,8 +896,9 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
     }
     for (uint32_t d = tid; d < S.ND; d += nt) {
       float4 lim = ar.dof_limit(d);
+      const float4 drv = ar.dof_drive(d);
       if (lim.z > 0.5f || ar.dof_passive(d).y > 0.0f || ar.dof_passive(d).z >= 0.0f ||
-          S.sf[S.SF_DOF + d * 5u + 3u].w > 0.0f) {
+          S.sf[S.SF_DOF + d * 5u + 3u].w > 0.0f || (S.DRIVE_ROWS == 1u && (drv.y > 0.0f || drv.z > 0.0f))) {
         uint32_t l = f2u(lim.w);
         A[S.A_HINV + d] = ar.dof_hinv(l, d - ar.ldof(l), pth, ub);
       }

@@ -511,6 +511,21 @@ struct Solver {
       uint32_t l = f2u(ar.dof_limit(d).w);
       uint32_t r = d - ar.ldof(l);
       float hinv = fmx(A[S.A_HINV + d], 1e-12f);
+      const float4 dr = ar.dof_drive(d);
+      // drive_mode="rows" (wgsl.js:3425-3438): a PhysX-style drive row, cold-started each substep,
+      // no relaxation; in the velocity pass only when velocity drives are active.
+      if (S.DRIVE_ROWS == 1u && (dr.y > 0.0f || dr.z > 0.0f) && !(vpass && S.VEL_DRIVE_ACTIVE == 0u)) {
+        float q = A[S.A_Q + ar.lqs(l) + r];
+        float pd = 0.0f;
+        if (vpass) pd = P.dt * A[S.A_SNAP + S.NB * 8u + d];
+        float ca = P.dt * (P.dt * dr.y + dr.z);
+        float x = 1.0f / (1.0f + ca * hinv);
+        float bias = ((x * P.dt) * dr.z) * A[S.A_TGTV + d] + ((dr.y * x) * P.dt) * ((A[S.A_TGT + d] - q) - pd);
+        float mx = dr.w > 0.0f ? dr.w * P.dt : 1e20f;
+        float lam = A[S.A_DRV + d];
+        float nl = clmp((lam * (1.0f - x) - (x * ca) * aqd[d]) + bias, -mx, mx);
+        if (nl != lam) { A[S.A_DRV + d] = nl; ar.LB[ar.lo(l) + L_TAU + r] = nl - lam; ar.apply(a, aqd, tw); }
+      }
       float fr = ar.dof_passive(d).y;
       if (S.JFL == 1u) fr += A[S.A_JFL + d];
       if (fr > 0.0f) {

@@ -17,9 +17,13 @@ SCENES = {"boxes": scenes.boxes, "mixed_prims": scenes.mixed_prims, "articulated
           "chains_and_quads": scenes.chains_and_quads, "hull_bin": scenes.hull_bin, "vel_limited": scenes.vel_limited,
           "chains_and_quads_fp64": scenes.chains_and_quads, "momentum_stack": scenes.momentum_stack,
           "spinners": scenes.spinners, "compliant": scenes.compliant,
-          "velocity_pass": scenes.velocity_pass, "load_friction": scenes.load_friction}
-# Packing options per scene (the FP64 articulated-inertia option on the articulation workload).
-OPTS = {"chains_and_quads_fp64": {"solver": {"articulation_fp64": True}}}
+          "velocity_pass": scenes.velocity_pass, "load_friction": scenes.load_friction,
+          "articulated_drive_rows": scenes.articulated, "vel_limited_drive_rows": scenes.vel_limited}
+# Packing options per scene: the FP64 articulated-inertia option on the articulation workload, and
+# PD drives as solver rows (drive_mode "rows"; with velocity limits, the fused drive clamp).
+OPTS = {"chains_and_quads_fp64": {"solver": {"articulation_fp64": True}},
+        "articulated_drive_rows": {"solver": {"drive_mode": "rows"}},
+        "vel_limited_drive_rows": {"solver": {"drive_mode": "rows"}}}
 
 
 def _pair_set(p):
