@@ -754,6 +754,10 @@ void Oracle::k_prepare() {
       rows[o + C.TO + 3u] = mk4(0.0f, 0.0f, 0.0f, contacts[c * 5u + 3u].w);
       rows[o + C.TO + 4u] = mk4(p, 0.0f);
     }
+    if (C.FMODE > 0u) {
+      rows[o + C.FMO] = mk4(K[0], 0.5f * (K[1] + K[3]), 0.5f * (K[2] + K[6]), 0.0f);
+      rows[o + C.FMO + 1u] = mk4(K[4], 0.5f * (K[5] + K[7]), K[8], 0.0f);
+    }
     float kscale = fmaxf_((K[0] + K[4]) + K[8], 1e-30f);
     float effn = 0.0f;
     if (K[0] > 1e-6f * kscale && K[0] > 1e-12f) effn = 1.0f / (K[0] + C.F_CFM);

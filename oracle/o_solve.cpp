@@ -40,6 +40,102 @@ v3 Oracle::gyroscopic_velocity(const m3& inertia, v3 u0, float dt) const {
   return w;
 }
 
+// Friction modes (friction_mode, wgsl.js:2567-2652): the (normal, t1, t2) impulses of a contact
+// point re-solved together on its 3x3 block, g0 = (G_nn, G_nt) and g1 = (G_tt: xx, xy, yy).
+// Mode 1 and 2 bisect the normal impulse with the tangent pair re-solved and clipped at each
+// trial (2 adds mu |u_t| to the normal target); mode 3 is the Coulomb-Newton root search.
+static v2 tangent_step(v2 ut, v4 g1) {
+  float det = g1.x * g1.z - g1.y * g1.y;
+  if (std::fabs(det) <= 1e-20f) return mk2(0.0f, 0.0f);
+  return mk2((-ut.x) * g1.z + ut.y * g1.y, ut.x * g1.y - ut.y * g1.x) / det;
+}
+static v2 clip_cone(v2 t, float lim) {
+  float m = length(t);
+  if (m > lim && m > 1e-20f) return t * (lim / m);
+  return t;
+}
+// A singular block (fewer than two tangential mobilities) keeps the normal impulse and takes the
+// fixed-normal pair on its disk.
+v3 Oracle::fixed_normal_pair(v2 ut0, v4 g1, float mu, v3 lam) const {
+  v2 t = friction_pair_solve(g1.x, g1.y, g1.z, ut0.x, ut0.y, lam.y, lam.z, fmaxf_(mu * lam.x, 0.0f), 1.0f);
+  return mk3(lam.x, t.x, t.y);
+}
+v3 Oracle::contact_block(uint32_t mode, float un, v2 ut0, v4 g0, v4 g1, float vtarget0, float mu,
+                          v3 lam) const {
+  const float gnn = g0.x;
+  const v2 gnt = mk2(g0.y, g0.z);
+  const float trace = g1.x + g1.z;
+  if (g1.x * g1.z - g1.y * g1.y <= (1e-6f * trace) * trace) return fixed_normal_pair(ut0, g1, mu, lam);
+  if (gnn < 1e-20f) return lam;
+  const v2 lt = mk2(lam.y, lam.z);
+  float vt_n = vtarget0;
+  if (mode == 2u) vt_n += mu * length(ut0);
+  if (mode == 3u) {
+    const float un_f = un - (gnn * lam.x + dot(gnt, lt));
+    const v2 ut_f = ut0 - mk2((gnt.x * lam.x + g1.x * lt.x) + g1.y * lt.y, (gnt.y * lam.x + g1.y * lt.x) + g1.z * lt.y);
+    if (un_f >= vt_n) return mk3(0.0f, 0.0f, 0.0f);
+    const float bN = un_f - vt_n;
+    const float A00 = g1.x - (gnt.x * gnt.x) / gnn, A01 = g1.y - (gnt.x * gnt.y) / gnn;
+    const float A11 = g1.z - (gnt.y * gnt.y) / gnn;
+    if (A00 * A11 - A01 * A01 <= (1e-6f * trace) * trace) return fixed_normal_pair(ut0, g1, mu, lam);
+    const v2 c = ut_f - (bN / gnn) * gnt;
+    const float id0 = 1.0f / (A00 * A11 - A01 * A01);
+    v2 s = mk2(A11 * c.x - A01 * c.y, A00 * c.y - A01 * c.x) * id0;
+    const float phi0 = length(s) - (mu * (dot(gnt, s) - bN)) / gnn;
+    if (phi0 > 0.0f) {
+      float hi = 1.0f;
+      for (uint32_t e = 0; e < 30u; e++) {
+        const float a = A00 + hi, d = A11 + hi, idt = 1.0f / (a * d - A01 * A01);
+        const v2 sh = mk2(d * c.x - A01 * c.y, a * c.y - A01 * c.x) * idt;
+        if (length(sh) - (mu * (dot(gnt, sh) - bN)) / gnn < 0.0f) break;
+        hi *= 2.0f;
+      }
+      float lo = 0.0f, x = 0.5f * hi;
+      const float tol = 1e-6f + 1e-6f * phi0;
+      for (uint32_t k = 0; k < 50u; k++) {
+        const float a = A00 + x, d = A11 + x, idt = 1.0f / (a * d - A01 * A01);
+        const v2 sx = mk2(d * c.x - A01 * c.y, a * c.y - A01 * c.x) * idt;
+        const v2 tx = mk2(d * sx.x - A01 * sx.y, a * sx.y - A01 * sx.x) * idt;
+        const float ns = length(sx);
+        const float fx = ns - (mu * (dot(gnt, sx) - bN)) / gnn;
+        const float dfx = (-dot(sx, tx)) / ns + (mu * dot(gnt, tx)) / gnn;
+        s = sx;
+        if (std::fabs(fx) < tol || std::fabs(hi - lo) < 1e-6f * (1.0f + hi)) break;
+        if (fx > 0.0f) lo = x; else hi = x;
+        float xn = 0.5f * (lo + hi);
+        if (dfx != 0.0f) {
+          const float xt = x - fx / dfx;
+          if (xt > lo && xt < hi) xn = xt;
+        }
+        x = xn;
+      }
+    }
+    const v2 rt = mk2(-s.x, -s.y);
+    // The finite search can end just below zero load; the exact root is non-negative.
+    const float ln = fmaxf_((-(dot(gnt, rt) + bN)) / gnn, 0.0f);
+    const float lim = fmaxf_(mu * ln, 0.0f);
+    const float m = length(rt);
+    const v2 t = m > lim ? rt * (lim / m) : rt;
+    return mk3(ln, t.x, t.y);
+  }
+  const float u0 = (un - gnn * lam.x) - dot(gnt, lt);
+  if (u0 >= vt_n) return mk3(0.0f, 0.0f, 0.0f);
+  float lo = 0.0f;
+  float hi = fmaxf_(fmaxf_(2.0f * lam.x, (vt_n - un) / gnn + lam.x), 1.0f);
+  float flo = u0 - vt_n, fhi = -1.0f;
+  for (uint32_t k = 0; k < 20u; k++) {
+    const float mid = 0.5f * (lo + hi);
+    const float dn = mid - lam.x;
+    const v2 tr = clip_cone(lt + tangent_step(ut0 + gnt * dn, g1), mu * mid);
+    const float u = (un + gnn * dn) + dot(gnt, tr - lt);
+    if (u < vt_n) { lo = mid; flo = u - vt_n; } else { hi = mid; fhi = u - vt_n; }
+  }
+  float ln = 0.5f * (lo + hi);
+  if (fhi >= 0.0f) ln = lo - (flo * (hi - lo)) / (fhi - flo);
+  const v2 tf = clip_cone(lt + tangent_step(ut0 + gnt * (ln - lam.x), g1), mu * ln);
+  return mk3(ln, tf.x, tf.y);
+}
+
 // friction_pair_solve (wgsl.js:2952-3011)
 v2 Oracle::friction_pair_solve(float a0, float c0, float d0, float r0, float r1, float old0, float old1, float radius,
                                float omega) const {
@@ -184,7 +280,23 @@ void Oracle::solve_unit(uint32_t us, uint32_t row, int a, int b, uint32_t s0, ui
       }
     }
     if (it < C.FSTART) { lam.y = 0.0f; lam.z = 0.0f; }
-    if (role != 0.0f && it >= C.FSTART) {
+    if (C.FMODE > 0u && it >= C.FSTART) {
+      // Coupled (normal, t1, t2) re-solve (wgsl.js:3081-3095); overwrites all three impulses.
+      v3 vn = (tb[0] + cross(tb[1], rb)) - (ta[0] + cross(ta[1], ra));
+      v3 vt = (tb[0] + cross(tb[1], frb)) - (ta[0] + cross(ta[1], fra));
+      v3 nlam = contact_block(C.FMODE, dot(n, vn), mk2(dot(t1, vt), dot(t2, vt)), rows[o + C.FMO], rows[o + C.FMO + 1u],
+                              -r1.w, r2.w, xyz(lam));
+      v3 d = nlam - xyz(lam);
+      if (C.PATCH == 1u && role != 1.0f) art[C.A_ULOAD + us] += d.x;
+      ta[0] += (xyz(rows[o + 7u]) * d.x + xyz(rows[o + 11u]) * d.y) + xyz(rows[o + 15u]) * d.z;
+      ta[1] += (xyz(rows[o + 8u]) * d.x + xyz(rows[o + 12u]) * d.y) + xyz(rows[o + 16u]) * d.z;
+      tb[0] += (xyz(rows[o + 9u]) * d.x + xyz(rows[o + 13u]) * d.y) + xyz(rows[o + 17u]) * d.z;
+      tb[1] += (xyz(rows[o + 10u]) * d.x + xyz(rows[o + 14u]) * d.y) + xyz(rows[o + 18u]) * d.z;
+      v3 fn2 = n * d.x, ft = t1 * d.y + t2 * d.z;
+      add_imp(a, (-fn2) - ft, (-cross(ra, fn2)) - cross(fra, ft));
+      add_imp(b, fn2 + ft, cross(rb, fn2) + cross(frb, ft));
+      lam = mk4(nlam, lam.w);
+    } else if (role != 0.0f && it >= C.FSTART) {
       v3 vr2 = (tb[0] + cross(tb[1], frb)) - (ta[0] + cross(ta[1], fra));
       v4 ki = rows[o + 5u];
       float v1 = dot(t1, vr2) + bias.x, v2_ = dot(t2, vr2) + bias.y;

@@ -281,6 +281,8 @@ struct Oracle {
   v3 twv(int b) const { return xyz(tw[(uint32_t)b * 2u]); }
   void load_tw(int b, v3 out[2]) const;
   void add_imp(int b, v3 f, v3 t);
+  v3 fixed_normal_pair(v2 ut0, v4 g1, float mu, v3 lam) const;
+  v3 contact_block(uint32_t mode, float un, v2 ut0, v4 g0, v4 g1, float vtarget0, float mu, v3 lam) const;
   v2 friction_pair_solve(float a0, float c0, float d0, float r0, float r1, float old0, float old1, float radius,
                          float omega) const;
   void solve_slot(uint32_t u, uint32_t mode, uint32_t it);

@@ -433,6 +433,10 @@ struct Prep {
       rows[o + S.TO + 3u] = make_float4(0.0f, 0.0f, 0.0f, S.con[c * 5u + 3u].w);
       rows[o + S.TO + 4u] = mf4(p, 0.0f);
     }
+    if (S.FMODE > 0u) {
+      rows[o + S.FMO] = make_float4(K[0], 0.5f * (K[1] + K[3]), 0.5f * (K[2] + K[6]), 0.0f);
+      rows[o + S.FMO + 1u] = make_float4(K[4], 0.5f * (K[5] + K[7]), K[8], 0.0f);
+    }
     float kscale = fmx((K[0] + K[4]) + K[8], 1e-30f);
     float effn = 0.0f;
     if (K[0] > 1e-6f * kscale && K[0] > 1e-12f) effn = 1.0f / (K[0] + S.F_CFM);

@@ -81,6 +81,101 @@ struct Solver {
     }
     return w;
   }
+  // Friction modes (friction_mode, wgsl.js:2567-2652): the (normal, t1, t2) impulses of a contact
+  // point re-solved together on its 3x3 block, g0 = (G_nn, G_nt) and g1 = (G_tt: xx, xy, yy).
+  // Mode 1 and 2 bisect the normal impulse with the tangent pair re-solved and clipped at each
+  // trial (2 adds mu |u_t| to the normal target); mode 3 is the Coulomb-Newton root search.
+  static __device__ f2 tangent_step(f2 ut, float4 g1) {
+    float det = g1.x * g1.z - g1.y * g1.y;
+    if (fabsf(det) <= 1e-20f) return mf2(0.0f, 0.0f);
+    return mf2((-ut.x) * g1.z + ut.y * g1.y, ut.x * g1.y - ut.y * g1.x) / det;
+  }
+  static __device__ f2 clip_cone(f2 t, float lim) {
+    float m = len(t);
+    if (m > lim && m > 1e-20f) return t * (lim / m);
+    return t;
+  }
+  // A singular block (fewer than two tangential mobilities) keeps the normal impulse and takes the
+  // fixed-normal pair on its disk.
+  static __device__ f3 fixed_normal_pair(f2 ut0, float4 g1, float mu, f3 lam) {
+    f2 t = friction_pair(g1.x, g1.y, g1.z, ut0.x, ut0.y, lam.y, lam.z, fmx(mu * lam.x, 0.0f), 1.0f);
+    return mf3(lam.x, t.x, t.y);
+  }
+  static __device__ f3 contact_block(uint32_t mode, float un, f2 ut0, float4 g0, float4 g1, float vtarget0, float mu,
+                          f3 lam) {
+    const float gnn = g0.x;
+    const f2 gnt = mf2(g0.y, g0.z);
+    const float trace = g1.x + g1.z;
+    if (g1.x * g1.z - g1.y * g1.y <= (1e-6f * trace) * trace) return fixed_normal_pair(ut0, g1, mu, lam);
+    if (gnn < 1e-20f) return lam;
+    const f2 lt = mf2(lam.y, lam.z);
+    float vt_n = vtarget0;
+    if (mode == 2u) vt_n += mu * len(ut0);
+    if (mode == 3u) {
+      const float un_f = un - (gnn * lam.x + dot(gnt, lt));
+      const f2 ut_f = ut0 - mf2((gnt.x * lam.x + g1.x * lt.x) + g1.y * lt.y, (gnt.y * lam.x + g1.y * lt.x) + g1.z * lt.y);
+      if (un_f >= vt_n) return mf3(0.0f, 0.0f, 0.0f);
+      const float bN = un_f - vt_n;
+      const float A00 = g1.x - (gnt.x * gnt.x) / gnn, A01 = g1.y - (gnt.x * gnt.y) / gnn;
+      const float A11 = g1.z - (gnt.y * gnt.y) / gnn;
+      if (A00 * A11 - A01 * A01 <= (1e-6f * trace) * trace) return fixed_normal_pair(ut0, g1, mu, lam);
+      const f2 c = ut_f - (bN / gnn) * gnt;
+      const float id0 = 1.0f / (A00 * A11 - A01 * A01);
+      f2 s = mf2(A11 * c.x - A01 * c.y, A00 * c.y - A01 * c.x) * id0;
+      const float phi0 = len(s) - (mu * (dot(gnt, s) - bN)) / gnn;
+      if (phi0 > 0.0f) {
+        float hi = 1.0f;
+        for (uint32_t e = 0; e < 30u; e++) {
+          const float a = A00 + hi, d = A11 + hi, idt = 1.0f / (a * d - A01 * A01);
+          const f2 sh = mf2(d * c.x - A01 * c.y, a * c.y - A01 * c.x) * idt;
+          if (len(sh) - (mu * (dot(gnt, sh) - bN)) / gnn < 0.0f) break;
+          hi *= 2.0f;
+        }
+        float lo = 0.0f, x = 0.5f * hi;
+        const float tol = 1e-6f + 1e-6f * phi0;
+        for (uint32_t k = 0; k < 50u; k++) {
+          const float a = A00 + x, d = A11 + x, idt = 1.0f / (a * d - A01 * A01);
+          const f2 sx = mf2(d * c.x - A01 * c.y, a * c.y - A01 * c.x) * idt;
+          const f2 tx = mf2(d * sx.x - A01 * sx.y, a * sx.y - A01 * sx.x) * idt;
+          const float ns = len(sx);
+          const float fx = ns - (mu * (dot(gnt, sx) - bN)) / gnn;
+          const float dfx = (-dot(sx, tx)) / ns + (mu * dot(gnt, tx)) / gnn;
+          s = sx;
+          if (fabsf(fx) < tol || fabsf(hi - lo) < 1e-6f * (1.0f + hi)) break;
+          if (fx > 0.0f) lo = x; else hi = x;
+          float xn = 0.5f * (lo + hi);
+          if (dfx != 0.0f) {
+            const float xt = x - fx / dfx;
+            if (xt > lo && xt < hi) xn = xt;
+          }
+          x = xn;
+        }
+      }
+      const f2 rt = mf2(-s.x, -s.y);
+      // The finite search can end just below zero load; the exact root is non-negative.
+      const float ln = fmx((-(dot(gnt, rt) + bN)) / gnn, 0.0f);
+      const float lim = fmx(mu * ln, 0.0f);
+      const float m = len(rt);
+      const f2 t = m > lim ? rt * (lim / m) : rt;
+      return mf3(ln, t.x, t.y);
+    }
+    const float u0 = (un - gnn * lam.x) - dot(gnt, lt);
+    if (u0 >= vt_n) return mf3(0.0f, 0.0f, 0.0f);
+    float lo = 0.0f;
+    float hi = fmx(fmx(2.0f * lam.x, (vt_n - un) / gnn + lam.x), 1.0f);
+    float flo = u0 - vt_n, fhi = -1.0f;
+    for (uint32_t k = 0; k < 20u; k++) {
+      const float mid = 0.5f * (lo + hi);
+      const float dn = mid - lam.x;
+      const f2 tr = clip_cone(lt + tangent_step(ut0 + gnt * dn, g1), mu * mid);
+      const float u = (un + gnn * dn) + dot(gnt, tr - lt);
+      if (u < vt_n) { lo = mid; flo = u - vt_n; } else { hi = mid; fhi = u - vt_n; }
+    }
+    float ln = 0.5f * (lo + hi);
+    if (fhi >= 0.0f) ln = lo - (flo * (hi - lo)) / (fhi - flo);
+    const f2 tf = clip_cone(lt + tangent_step(ut0 + gnt * (ln - lam.x), g1), mu * ln);
+    return mf3(ln, tf.x, tf.y);
+  }
   // Friction pair update on its 2x2 block with a disk bound (wgsl.js:2952-3011).
   static __device__ f2 friction_pair(float a0, float c0, float d0, float r0, float r1, float old0, float old1,
                                      float radius, float omega) {
@@ -256,7 +351,23 @@ struct Solver {
         }
       }
       if (it < S.FSTART) { lam.y = 0.0f; lam.z = 0.0f; }
-      if (role != 0.0f && it >= S.FSTART) {
+      if (S.FMODE > 0u && it >= S.FSTART) {
+        // Coupled (normal, t1, t2) re-solve (wgsl.js:3081-3095); overwrites all three impulses.
+        const f3 vn = (tb[0] + cross(tb[1], rb)) - (ta[0] + cross(ta[1], ra));
+        const f3 vt = (tb[0] + cross(tb[1], frb)) - (ta[0] + cross(ta[1], fra));
+        const f3 nlam = contact_block(S.FMODE, dot(n, vn), mf2(dot(t1, vt), dot(t2, vt)), rows[o + S.FMO],
+                                      rows[o + S.FMO + 1u], -r1.w, r2.w, v3(lam));
+        const f3 d = nlam - v3(lam);
+        if (S.PATCH == 1u && role != 1.0f) S.art[S.A_ULOAD + us] += d.x;
+        ta[0] += (v3(rows[o + 7u]) * d.x + v3(rows[o + 11u]) * d.y) + v3(rows[o + 15u]) * d.z;
+        ta[1] += (v3(rows[o + 8u]) * d.x + v3(rows[o + 12u]) * d.y) + v3(rows[o + 16u]) * d.z;
+        tb[0] += (v3(rows[o + 9u]) * d.x + v3(rows[o + 13u]) * d.y) + v3(rows[o + 17u]) * d.z;
+        tb[1] += (v3(rows[o + 10u]) * d.x + v3(rows[o + 14u]) * d.y) + v3(rows[o + 18u]) * d.z;
+        const f3 fn2 = n * d.x, ft = t1 * d.y + t2 * d.z;
+        add_imp(a, (-fn2) - ft, (-cross(ra, fn2)) - cross(fra, ft));
+        add_imp(b, fn2 + ft, cross(rb, fn2) + cross(frb, ft));
+        lam = mf4(nlam, lam.w);
+      } else if (role != 0.0f && it >= S.FSTART) {
         f3 vr2 = (tb[0] + cross(tb[1], frb)) - (ta[0] + cross(ta[1], fra));
         float4 ki = rows[o + 5u];
         float v1 = dot(t1, vr2) + bias.x, v2_ = dot(t2, vr2) + bias.y;

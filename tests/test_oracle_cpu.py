@@ -15,7 +15,7 @@ from tests import scenes
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "oracle_fixtures.npz")
 REF_SCENES = "/root/reference/assets/scenes"
-UNSUPPORTED = ("FMODE", "ANG", "ANG_ART", "CTI", "LONGEST_FIRST")
+UNSUPPORTED = ("ANG", "ANG_ART", "CTI", "LONGEST_FIRST")
 
 
 def test_trig_accuracy(oracle_lib):
@@ -107,8 +107,8 @@ def test_oracle_matches_committed_fixtures(oracle_lib):
 
 def test_oracle_refuses_unsupported_options(oracle_lib):
     sc = scenes.boxes(n=4, seed=2)
-    pk = pack(sc, opts={"solver": {"friction_mode": "bisection"}})
-    if pk.C.get("FMODE", 0) == 0:
+    pk = pack(sc, opts={"solver": {"row_schedule": "contact_then_internal"}})
+    if pk.C.get("CTI", 0) == 0:
         pytest.skip("option not carried by the packer")
     with pytest.raises(ValueError):
         oracle_lib.OracleSim(pk)

@@ -18,12 +18,18 @@ SCENES = {"boxes": scenes.boxes, "mixed_prims": scenes.mixed_prims, "articulated
           "chains_and_quads_fp64": scenes.chains_and_quads, "momentum_stack": scenes.momentum_stack,
           "spinners": scenes.spinners, "compliant": scenes.compliant,
           "velocity_pass": scenes.velocity_pass, "load_friction": scenes.load_friction,
-          "articulated_drive_rows": scenes.articulated, "vel_limited_drive_rows": scenes.vel_limited}
-# Packing options per scene: the FP64 articulated-inertia option on the articulation workload, and
-# PD drives as solver rows (drive_mode "rows"; with velocity limits, the fused drive clamp).
+          "articulated_drive_rows": scenes.articulated, "vel_limited_drive_rows": scenes.vel_limited,
+          "boxes_bisection": scenes.boxes, "mixed_desaxce": scenes.mixed_prims,
+          "articulated_coulomb_newton": scenes.articulated}
+# Packing options per scene: the FP64 articulated-inertia option on the articulation workload, PD
+# drives as solver rows (drive_mode "rows"; with velocity limits, the fused drive clamp), and the
+# three coupled friction modes.
 OPTS = {"chains_and_quads_fp64": {"solver": {"articulation_fp64": True}},
         "articulated_drive_rows": {"solver": {"drive_mode": "rows"}},
-        "vel_limited_drive_rows": {"solver": {"drive_mode": "rows"}}}
+        "vel_limited_drive_rows": {"solver": {"drive_mode": "rows"}},
+        "boxes_bisection": {"solver": {"friction_mode": "bisection"}},
+        "mixed_desaxce": {"solver": {"friction_mode": "bisection_desaxce"}},
+        "articulated_coulomb_newton": {"solver": {"friction_mode": "coulomb_newton"}}}
 
 
 def _pair_set(p):
