@@ -826,6 +826,30 @@ void Oracle::k_prepare() {
     }
     rows[o + 5u] = mk4(k11 / det, -k01 / det, k00 / det, bounce ? 1.0f : wrow);
     rows[o + 6u] = mk4(ln, lt.x, lt.y, bounce ? 1e30f : phi);
+    if (C.ANG == 1u) {
+      // Torsional (about n) and rolling (about t1, t2) rows of free bodies (wgsl.js:2223-2243):
+      // angular-only Jacobians, the spin row's 1 / K and the rolling pair's inverse 2x2 block.
+      const v4 mat = contacts[c * 5u + 3u];
+      v3 MA[3][2], MB[3][2];
+      for (uint32_t r = 0; r < 3u; r++) {
+        const v3 d = dirs[r];
+        body_response(a, splat3(0.0f), -d, MA[r]);
+        body_response(b, splat3(0.0f), d, MB[r]);
+        rows[o + 22u + r * 4u] = mk4(MA[r][0], 0.0f);
+        rows[o + 23u + r * 4u] = mk4(MA[r][1], 0.0f);
+        rows[o + 24u + r * 4u] = mk4(MB[r][0], 0.0f);
+        rows[o + 25u + r * 4u] = mk4(MB[r][1], 0.0f);
+      }
+      float KA[9];
+      for (uint32_t r = 0; r < 3u; r++)
+        for (uint32_t s3 = 0; s3 < 3u; s3++) KA[r * 3u + s3] = dot(-dirs[r], MA[s3][1]) + dot(dirs[r], MB[s3][1]);
+      const float ks = fmaxf_(KA[0], 1e-12f);
+      const float r00 = KA[4] + 1e-9f, r01 = 0.5f * (KA[5] + KA[7]), r11 = KA[8] + 1e-9f;
+      const float rd = r00 * r11 - r01 * r01;
+      rows[o + 19u] = mk4(mat.y, mat.z, KA[0] > 1e-12f ? 1.0f / ks : 0.0f, 0.0f);
+      rows[o + 20u] = mk4(r11 / rd, -r01 / rd, r00 / rd, 0.0f);
+      rows[o + 21u] = mk4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
   }
   // Phase 6b: contact torsion headers, then friction patches.
   if (C.TORS == 1u) for (uint32_t sp = 0; sp < nu; sp++) build_torsion(sp);

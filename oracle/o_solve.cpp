@@ -264,6 +264,7 @@ void Oracle::solve_unit(uint32_t us, uint32_t row, int a, int b, uint32_t s0, ui
     add_imp(b, n * dn, cross(rb, n * dn));
     v3 fra = ra, frb = rb;
     float lim = r2.w * nl;
+    float pooled = nl;
     v2 bias = mk2(0.0f, 0.0f);
     float role = 1.0f;
     if (C.EXTRA == 1u) {
@@ -274,6 +275,7 @@ void Oracle::solve_unit(uint32_t us, uint32_t row, int a, int b, uint32_t s0, ui
       if (C.PATCH == 1u && role == 2.0f) {
         float load = art[C.A_ULOAD + us];
         lim = r2.w * load;
+        pooled = load;
         v3 e = xyz(rows[o + PO + 2u]);
         bias = vpass ? mk2(0.0f, 0.0f) : (C.F_ANCHOR_BETA * mk2(dot(t1, e), dot(t2, e))) / P.dt;
         rows[o + PO + 2u].w = lim;
@@ -315,6 +317,36 @@ void Oracle::solve_unit(uint32_t us, uint32_t row, int a, int b, uint32_t s0, ui
       add_imp(b, f, cross(frb, f));
     }
     rows[o + 6u] = lam;
+    if (C.ANG == 1u) {
+      // Spin within mu_t * N, rolling within a disk of mu_r * N (wgsl.js:3144-3170); under
+      // friction patches only the region's first anchor carries them, with the pooled load.
+      const v4 g = rows[o + 19u];
+      const bool aon = C.PATCH == 0u || role == 1.0f || (role == 2.0f && rows[o + PO + 1u].w == 0.0f);
+      const float nl2 = pooled;
+      if (aon && (g.x > 0.0f || g.y > 0.0f)) {
+        const v4 la = rows[o + 21u];
+        const v3 wrel = tb[1] - ta[1];
+        const float ns = clampf(la.x - dot(n, wrel) * g.z, (-g.x) * nl2, g.x * nl2);
+        const float ds = ns - la.x;
+        ta[0] += xyz(rows[o + 22u]) * ds; ta[1] += xyz(rows[o + 23u]) * ds;
+        tb[0] += xyz(rows[o + 24u]) * ds; tb[1] += xyz(rows[o + 25u]) * ds;
+        const v3 w2 = tb[1] - ta[1];
+        const v4 ri = rows[o + 20u];
+        const float u1 = dot(t1, w2), u2 = dot(t2, w2);
+        v2 lr = mk2(la.y, la.z) - mk2(ri.x * u1 + ri.y * u2, ri.y * u1 + ri.z * u2);
+        const float rl = g.y * nl2;
+        if (length(lr) > rl) lr = lr * (rl / fmaxf_(length(lr), 1e-12f));
+        const float d1 = lr.x - la.y, d2 = lr.y - la.z;
+        ta[0] += xyz(rows[o + 26u]) * d1 + xyz(rows[o + 30u]) * d2;
+        ta[1] += xyz(rows[o + 27u]) * d1 + xyz(rows[o + 31u]) * d2;
+        tb[0] += xyz(rows[o + 28u]) * d1 + xyz(rows[o + 32u]) * d2;
+        tb[1] += xyz(rows[o + 29u]) * d1 + xyz(rows[o + 33u]) * d2;
+        rows[o + 21u] = mk4(ns, lr.x, lr.y, 0.0f);
+        const v3 tq = (n * ds + t1 * d1) + t2 * d2;
+        add_imp(a, splat3(0.0f), -tq);
+        add_imp(b, splat3(0.0f), tq);
+      }
+    }
   }
   // Contact torsion (wgsl.js:3185-3228) on the unit's last-colored row: sliding and spin share
   // the cluster's Coulomb budget mu * N.

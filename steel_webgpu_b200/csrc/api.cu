@@ -142,7 +142,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
   Consts& C = s.C;
   if (!C.parse(in.constants)) { why = "malformed constants text"; return STEEL_E_INVALID; }
   static const char* unsupported[][2] = {
-      {"ANG", "torsional/rolling friction"}, {"ANG_ART", "torsional/rolling friction"},
+      {"ANG_ART", "torsional/rolling friction of articulated contacts"},
       {"CTI", "row_schedule contact_then_internal"}, {"LONGEST_FIRST", "propagation_color_order longest_first"}};
   for (auto& u : unsupported)
     if (C.u(u[0]) != 0u) { why = std::string("unsupported solver option: ") + u[1]; return STEEL_E_UNSUPPORTED; }
@@ -157,7 +157,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
   K(SF_MIMIC) K(SF_CTRL) K(SU_HULL) K(SU_FACE) K(SU_FV) K(SU_HEDGE) K(SU_EDGE) K(SU_ART) K(SU_ACON)
   K(SU_FILTER) K(NB) K(NS) K(NA) K(NL) K(ND) K(NDA) K(JM) K(MAXPATH) K(MAXLP) K(NLOOP) K(NMIMIC) K(PATCH)
   K(EXTRA) K(SHARED) K(FSHARED) K(REST) K(FSTART) K(TGT_HELD) K(CTRL_KIND) K(CTRL_A) K(CTRL_B) K(VLIM_FREE) K(VLIM_ON) K(ART_F64) K(SLEEP) K(NEST) K(MO) K(TORS) K(TO) K(COMPL) K(CO) K(VELITERS) K(JFL) K(DRIVE_ROWS) K(FUSE_VLIM)
-  K(VEL_DRIVE_ACTIVE) K(FMODE) K(FMO)
+  K(VEL_DRIVE_ACTIVE) K(FMODE) K(FMO) K(ANG)
   K(FRICTION_COMBINE) K(RESTITUTION_COMBINE) K(NCOLW) K(NCOL) K(MAXP) K(MAXC) K(MAXU) K(WH) K(AH)
   K(MAXDENSE) K(ROWS) K(PO) K(DHDR) K(DPS)
 #undef K

@@ -492,6 +492,30 @@ struct Prep {
     }
     rows[o + 5u] = make_float4(k11 / det, -k01 / det, k00 / det, bounce ? 1.0f : wrow);
     rows[o + 6u] = make_float4(ln, lt.x, lt.y, bounce ? 1e30f : phi);
+    if (S.ANG == 1u) {
+      // Torsional (about n) and rolling (about t1, t2) rows of free bodies (wgsl.js:2223-2243):
+      // angular-only Jacobians, the spin row's 1 / K and the rolling pair's inverse 2x2 block.
+      const float4 mat = S.con[c * 5u + 3u];
+      f3 MA[3][2], MB[3][2];
+      for (uint32_t r = 0; r < 3u; r++) {
+        const f3 d = dirs[r];
+        response(a, sp3(0.0f), -d, MA[r]);
+        response(b, sp3(0.0f), d, MB[r]);
+        rows[o + 22u + r * 4u] = mf4(MA[r][0], 0.0f);
+        rows[o + 23u + r * 4u] = mf4(MA[r][1], 0.0f);
+        rows[o + 24u + r * 4u] = mf4(MB[r][0], 0.0f);
+        rows[o + 25u + r * 4u] = mf4(MB[r][1], 0.0f);
+      }
+      float KA[9];
+      for (uint32_t r = 0; r < 3u; r++)
+        for (uint32_t s3 = 0; s3 < 3u; s3++) KA[r * 3u + s3] = dot(-dirs[r], MA[s3][1]) + dot(dirs[r], MB[s3][1]);
+      const float ks = fmx(KA[0], 1e-12f);
+      const float r00 = KA[4] + 1e-9f, r01 = 0.5f * (KA[5] + KA[7]), r11 = KA[8] + 1e-9f;
+      const float rd = r00 * r11 - r01 * r01;
+      rows[o + 19u] = make_float4(mat.y, mat.z, KA[0] > 1e-12f ? 1.0f / ks : 0.0f, 0.0f);
+      rows[o + 20u] = make_float4(r11 / rd, -r01 / rd, r00 / rd, 0.0f);
+      rows[o + 21u] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
   }
 
   // Dense row of a same-articulation contact (wgsl.js:2370-2444). scr: JDIM + 2 NDA + 18 MAXLP floats.

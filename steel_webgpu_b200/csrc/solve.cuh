@@ -335,6 +335,7 @@ struct Solver {
       add_imp(b, n * dn, cross(rb, n * dn));
       f3 fra = ra, frb = rb;
       float lim = r2.w * nl;
+      float pooled = nl;
       f2 bias = mf2(0.0f, 0.0f);
       float role = 1.0f;
       if (S.EXTRA == 1u) {
@@ -345,6 +346,7 @@ struct Solver {
         if (S.PATCH == 1u && role == 2.0f) {
           float load = S.art[S.A_ULOAD + us];
           lim = r2.w * load;
+          pooled = load;
           f3 e = v3(rows[o + PO + 2u]);
           bias = vpass ? mf2(0.0f, 0.0f) : (S.F_ANCHOR_BETA * mf2(dot(t1, e), dot(t2, e))) / P.dt;
           rows[o + PO + 2u].w = lim;
@@ -385,6 +387,36 @@ struct Solver {
         add_imp(b, f, cross(frb, f));
       }
       rows[o + 6u] = lam;
+      if (S.ANG == 1u) {
+        // Spin within mu_t * N, rolling within a disk of mu_r * N (wgsl.js:3144-3170); under
+        // friction patches only the region's first anchor carries them, with the pooled load.
+        const float4 g = rows[o + 19u];
+        const bool aon = S.PATCH == 0u || role == 1.0f || (role == 2.0f && rows[o + PO + 1u].w == 0.0f);
+        const float nl2 = pooled;
+        if (aon && (g.x > 0.0f || g.y > 0.0f)) {
+          const float4 la = rows[o + 21u];
+          const f3 wrel = tb[1] - ta[1];
+          const float ns = clmp(la.x - dot(n, wrel) * g.z, (-g.x) * nl2, g.x * nl2);
+          const float ds = ns - la.x;
+          ta[0] += v3(rows[o + 22u]) * ds; ta[1] += v3(rows[o + 23u]) * ds;
+          tb[0] += v3(rows[o + 24u]) * ds; tb[1] += v3(rows[o + 25u]) * ds;
+          const f3 w2 = tb[1] - ta[1];
+          const float4 ri = rows[o + 20u];
+          const float u1 = dot(t1, w2), u2 = dot(t2, w2);
+          f2 lr = mf2(la.y, la.z) - mf2(ri.x * u1 + ri.y * u2, ri.y * u1 + ri.z * u2);
+          const float rl = g.y * nl2;
+          if (len(lr) > rl) lr = lr * (rl / fmx(len(lr), 1e-12f));
+          const float d1 = lr.x - la.y, d2 = lr.y - la.z;
+          ta[0] += v3(rows[o + 26u]) * d1 + v3(rows[o + 30u]) * d2;
+          ta[1] += v3(rows[o + 27u]) * d1 + v3(rows[o + 31u]) * d2;
+          tb[0] += v3(rows[o + 28u]) * d1 + v3(rows[o + 32u]) * d2;
+          tb[1] += v3(rows[o + 29u]) * d1 + v3(rows[o + 33u]) * d2;
+          rows[o + 21u] = make_float4(ns, lr.x, lr.y, 0.0f);
+          const f3 tq = (n * ds + t1 * d1) + t2 * d2;
+          add_imp(a, sp3(0.0f), -tq);
+          add_imp(b, sp3(0.0f), tq);
+        }
+      }
       if (S.TORS == 1u && row == S.sched[S.S_UTP + us]) torsion(us, a, b, it, ta, tb);
     }
     if (a >= 0) { tw[(uint32_t)a * 2u] = mf4(ta[0], 0.0f); tw[(uint32_t)a * 2u + 1u] = mf4(ta[1], 0.0f); }

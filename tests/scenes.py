@@ -217,3 +217,18 @@ def load_friction(seed=41):
     sc = b.finalize(solver=dict(enable_joint_friction=True))
     sc.json["joints"]["friction_load_coefficient"] = [0.3, 0.0]
     return sc
+
+
+def spin_roll(seed=43):
+    """Torsional and rolling friction of free bodies (free_rigid_torsional_friction 0.05,
+    free_rigid_rolling_friction 0.01): a box spinning flat on the plane and spheres rolling on it
+    come to rest through the spin row and the rolling pair of each contact."""
+    b = SceneBuilder(fps=240, box_hulls="direct")
+    b.add_ground_plane(mu=0.6)
+    box = b.add_body(xform=[0.0, 0.0, 0.05, 0, 0, 0, 1], twist=[0.0, 0.0, 0.0, 0.0, 0.0, 8.0])
+    b.add_shape_box(box, hx=0.15, hy=0.1, hz=0.05, mu=0.6)
+    for i, v in enumerate((1.0, 2.0)):
+        r = 0.08
+        ball = b.add_body(xform=[-0.6, 0.4 * i - 0.2, r, 0, 0, 0, 1], twist=[v, 0.0, 0.0, 0.0, v / r, 0.0])
+        b.add_shape_sphere(ball, radius=r, mu=0.6)
+    return b.finalize(solver=dict(free_rigid_torsional_friction=0.05, free_rigid_rolling_friction=0.01))

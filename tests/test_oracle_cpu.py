@@ -15,7 +15,7 @@ from tests import scenes
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "oracle_fixtures.npz")
 REF_SCENES = "/root/reference/assets/scenes"
-UNSUPPORTED = ("ANG", "ANG_ART", "CTI", "LONGEST_FIRST")
+UNSUPPORTED = ("ANG_ART", "CTI", "LONGEST_FIRST")
 
 
 def test_trig_accuracy(oracle_lib):

@@ -20,7 +20,7 @@ SCENES = {"boxes": scenes.boxes, "mixed_prims": scenes.mixed_prims, "articulated
           "velocity_pass": scenes.velocity_pass, "load_friction": scenes.load_friction,
           "articulated_drive_rows": scenes.articulated, "vel_limited_drive_rows": scenes.vel_limited,
           "boxes_bisection": scenes.boxes, "mixed_desaxce": scenes.mixed_prims,
-          "articulated_coulomb_newton": scenes.articulated}
+          "articulated_coulomb_newton": scenes.articulated, "spin_roll": scenes.spin_roll}
 # Packing options per scene: the FP64 articulated-inertia option on the articulation workload, PD
 # drives as solver rows (drive_mode "rows"; with velocity limits, the fused drive clamp), and the
 # three coupled friction modes.
