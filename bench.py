@@ -33,7 +33,24 @@ WORKLOADS = {
     "uneven_batch_256": dict(n_scenes=256),
     "uneven_batch_512": dict(n_scenes=512),  # loaded case (several blocks per SM) for profiler captures
     "uneven_batch_64": dict(n_scenes=64),  # small case for profiler captures
+    # Single large scenes (the plain method at scale): one block runs each scene's prepare and solve.
+    "convex_pour_8192": dict(n_scenes=1, single="convex_pour"),  # 8192 hulls, boxes, capsules in a bin
+    "quadrupeds_1024": dict(n_scenes=1, single="quadrupeds"),  # 1024 quadrupeds + 64 x 40-link chains
+    "boxes_64": dict(n_scenes=1, single="boxes"),  # 64 boxes on a plane
 }
+
+
+def _build_single(kind: str, seed: int):
+    from steel_webgpu_b200 import pack, synth
+    from steel_webgpu_b200.sim import auto_caps
+    if kind == "convex_pour":
+        sc = synth.convex_pour(n=8192, seed=seed)
+        caps = auto_caps(sc)  # the settled pour needs more than the uneven batch's 8 pairs per shape
+        caps.update(MAXP=1 << 18, MAXC=1 << 18, MAXU=1 << 18, UH=1 << 18, WH=1 << 19, AH=1 << 18)
+        return [pack(sc, caps=caps)]
+    sc = synth.quadrupeds(n_quad=1024, n_chains=64, chain_links=40, seed=seed) if kind == "quadrupeds" \
+        else synth.boxes_on_plane(64, seed=seed)
+    return [pack(sc, caps=auto_caps(sc))]
 
 
 def _build_chunk(args):
@@ -49,6 +66,8 @@ def _build_chunk(args):
 
 
 def build_workload(name: str, seed: int, caps_mode: str = "auto", nproc: int | None = None, limit: int | None = None):
+    if "single" in WORKLOADS[name]:
+        return _build_single(WORKLOADS[name]["single"], seed)
     n = WORKLOADS[name]["n_scenes"]
     if limit is not None:
         n = min(n, limit)
@@ -298,7 +317,7 @@ def run_reference(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": args.workload, "sample_scenes": len(sample), "sample_bodies": nb,
-                       "fps": 240, "substeps": 4, "iterations": 12},
+                       "fps": sample[0].params["fps"], "substeps": sample[0].params["substeps"], "iterations": sample[0].params["iterations"]},
             "cpu_baseline": {"value": value, "unit": "body-steps/s", "cores": nproc, "kind": "port",
                              "sample": f"{len(sample)} scenes ({nb} bodies) of {args.workload}, 1 frame per step"},
             "e2e": {"value": value, "unit": "body-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -364,7 +383,7 @@ def run_steel(args):
         "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes, no dataset)",
         "config": {"workload": args.workload, "scenes_per_gpu": len(pks), "bodies_per_gpu": nbodies,
-                   "fps": 240, "substeps": substeps, "iterations": iterations, "parallelism": f"replicas x{world}",
+                   "fps": pks[0].params["fps"], "substeps": substeps, "iterations": iterations, "parallelism": f"replicas x{world}",
                    "graph": True, "l2": "per-scene state is resident and re-read every substep; no L2 flush",
                    "contact_steps_per_s": world * counts["contacts"] * substeps * args.steps / (ms / 1000.0),
                    "build_s": round(build_s, 1), "overflow_scenes": overflow_scenes,

@@ -209,6 +209,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
     put(d.S_CSTART, d.NCOL + 2); put(d.S_META, 8); put(d.S_WWIN, d.WH); put(d.S_WSLOT, (size_t)MAXC + d.MAXDENSE);
     put(d.S_WMASK, (size_t)NB * d.NCOLW); put(d.S_WCOUNT, d.NCOL + 2); put(d.S_LINKHIT, NB); put(d.S_JSPLIT, NL);
     put(d.S_UF, NB + NA); put(d.S_UFF, NB + NA); put(d.S_UTP, MAXC);
+    put(d.S_DSTART, NA + 1); put(d.S_DOFF, NA); put(d.S_DLIST, d.MAXDENSE);
     s.sched_words = so;
   }
   s.warm_words = 10ull * d.WH + 30ull * d.AH;

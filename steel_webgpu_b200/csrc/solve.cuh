@@ -13,6 +13,7 @@
 // with one barrier per color; the overflow color runs serially in contact order.
 #include "art.cuh"
 #include "batch.cuh"
+#include "block.cuh"
 #include "bulk.cuh"
 
 namespace steel {
@@ -433,12 +434,45 @@ struct Solver {
     for (uint32_t off = 16u; off > 0u; off >>= 1u) x += __shfl_xor_sync(0xffffffffu, x, off);
     return x;
   }
+  // Each articulation's dense rows in slot order (S_DSTART / S_DLIST), by a stable counting sort
+  // once per solve, so the dense passes walk their own rows instead of filtering all of them (the
+  // order within an articulation, the one the Gauss-Seidel pass needs, is kept). All threads call
+  // it.
+  __device__ void dense_lists(uint32_t* tmp) const {
+    const uint32_t tid = threadIdx.x, nt = blockDim.x, lane = tid & 31u, warp = tid >> 5u, nw = nt >> 5u;
+    const uint32_t nd = min(S.sched[S.S_META + 3u], S.MAXDENSE);
+    uint32_t* start = S.sched + S.S_DSTART;
+    uint32_t* off = S.sched + S.S_DOFF;
+    uint32_t* list = S.sched + S.S_DLIST;
+    const float* A = S.art;
+    for (uint32_t a = tid; a <= S.NA; a += nt) start[a] = 0u;
+    __syncthreads();
+    for (uint32_t i = tid; i < nd; i += nt) atomicAdd(&start[f2u(A[S.A_DENSE + i * S.DPS])], 1u);
+    __syncthreads();
+    block_scan_array(start, S.NA + 1u, tmp);
+    for (uint32_t a = tid; a < S.NA; a += nt) off[a] = start[a];
+    __syncthreads();
+    // Blocks of nt rows in order; inside one, warps in order and lanes ranked among equal ids.
+    for (uint32_t c0 = 0; c0 < nd; c0 += nt) {
+      const uint32_t i = c0 + tid;
+      const bool v = i < nd;
+      const uint32_t art = v ? f2u(A[S.A_DENSE + i * S.DPS]) : 0xffffffffu;
+      const uint32_t peers = __match_any_sync(0xffffffffu, art);
+      const uint32_t rank = (uint32_t)__popc(peers & ((1u << lane) - 1u));
+      for (uint32_t w = 0; w < nw; w++) {
+        if (warp == w && v) list[off[art] + rank] = i;
+        __syncthreads();
+        if (warp == w && v && lane == 31u - (uint32_t)__clz(peers)) off[art] += (uint32_t)__popc(peers);
+        __syncthreads();
+      }
+    }
+  }
   // Dense same-articulation rows of articulation a (wgsl.js:3306-3364), one warp: lane l owns
   // dofs l, l + 32, ... (so lanes never touch each other's qd entries) and its partial sums
   // are combined with lane_sum. The lanes keep their qd entries in registers for the whole pass
   // (no other warp touches a's dofs meanwhile) and store them back at the end. The rows are
-  // Gauss-Seidel, one after another, but their data are not: a's rows are found 32 at a time
-  // with one ballot, and each lane holds its slice of a row (J and Y rows of its dofs, up to
+  // Gauss-Seidel, one after another, but their data are not: a's rows come from its slot-ordered
+  // list (dense_lists), and each lane holds its slice of a row (J and Y rows of its dofs, up to
   // DENSE_REG of them) and the row's header in registers, the next row's loaded while this one
   // is solved. Called by all 32 lanes; returns whether a row belongs to a.
   static constexpr uint32_t DENSE_REG = 2u;  // articulations of up to 64 dofs keep rows in registers
@@ -469,36 +503,30 @@ struct Solver {
     const uint32_t nd = min(S.sched[S.S_META + 3u], S.MAXDENSE);
     const uint4 ai = ar.info(a);
     if (ai.w > 32u * DENSE_REG) return dense_wide(a, mode, it, ph, lane, nd, ai);
-    bool touched = false;
+    const uint32_t* dl = S.sched + S.S_DLIST;
+    const uint32_t k0 = S.sched[S.S_DSTART + a], k1 = S.sched[S.S_DSTART + a + 1u];
+    if (k0 >= k1) return false;
     float* qg = aqd + ai.z;
     float q[DENSE_REG];
 #pragma unroll
     for (uint32_t j = 0; j < DENSE_REG; j++) q[j] = lane + 32u * j < ai.w ? qg[lane + 32u * j] : 0.0f;
-    for (uint32_t base = 0; base < nd; base += 32u) {
-      const uint32_t i = base + lane;
-      uint32_t mask = __ballot_sync(0xffffffffu, i < nd && f2u(S.art[base0 + i * DPS]) == a);
-      if (mask == 0u) continue;
-      touched = true;
-      uint32_t row = base + (uint32_t)__ffs(mask) - 1u;
-      mask &= mask - 1u;
-      DenseRow cur;
-      dense_load(base0 + row * DPS, lane, ai.w, cur);
-      while (true) {
-        const bool more = mask != 0u;
-        const uint32_t nrow = more ? base + (uint32_t)__ffs(mask) - 1u : row;
-        DenseRow nxt;
-        if (more) dense_load(base0 + nrow * DPS, lane, ai.w, nxt);
-        dense_row(cur, base0 + row * DPS, ai, mode, it, ph, lane, q);
-        if (!more) break;
-        mask &= mask - 1u;
-        cur = nxt;
-        row = nrow;
-      }
+    uint32_t row = dl[k0];
+    DenseRow cur;
+    dense_load(base0 + row * DPS, lane, ai.w, cur);
+    for (uint32_t k = k0; k < k1; k++) {
+      const bool more = k + 1u < k1;
+      const uint32_t nrow = more ? dl[k + 1u] : row;
+      DenseRow nxt;
+      if (more) dense_load(base0 + nrow * DPS, lane, ai.w, nxt);
+      dense_row(cur, base0 + row * DPS, ai, mode, it, ph, lane, q);
+      cur = nxt;
+      row = nrow;
     }
+    (void)nd;
 #pragma unroll
     for (uint32_t j = 0; j < DENSE_REG; j++)
       if (lane + 32u * j < ai.w) qg[lane + 32u * j] = q[j];
-    return touched;
+    return true;
   }
   // One dense row (wgsl.js:3320-3362) from its registers; lane 0 stores the new impulses.
   __device__ void dense_row(const DenseRow& d, uint32_t o, uint4 ai, uint32_t mode, uint32_t it, uint32_t ph,
@@ -999,6 +1027,10 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     for (uint32_t a = tid; a < S.NA; a += nt) sv.ar.twists(a, sv.aqd, sv.tw);
   }
   __syncthreads();
+  {
+    __shared__ uint32_t dtmp[33];
+    sv.dense_lists(dtmp);
+  }
   sv.dense_phase(0u, 0u, 0u);
   sv.sweep(0u, ncol, 0u, wcs, nu);
   for (uint32_t it = 0; it < P.iterations; it++) {

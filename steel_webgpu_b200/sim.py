@@ -26,11 +26,13 @@ def auto_caps(scene: LoadedScene) -> dict:
     # Piles of the uneven batch peak near 4 pairs and 2.5 contacts per shape; these leave 2-5x room.
     maxp = int(min(max(256, 8 * ns), 1 << 22))
     maxc = int(min(max(512, 12 * ns), 1 << 24))
+    # Same-articulation contacts: a 40-link chain keeps about 3 per link (links two apart touch).
+    maxdense = int(min(max(512, 4 * int(scene.json["joints"].get("count", 0))), 1 << 20))
 
     def p2(x):
         return 1 << max(int(x) - 1, 1).bit_length()
 
-    return dict(MAXP=maxp, MAXC=maxc, MAXU=maxc, UH=p2(maxc), WH=p2(2 * maxc), AH=p2(maxc), MAXDENSE=512)
+    return dict(MAXP=maxp, MAXC=maxc, MAXU=maxc, UH=p2(maxc), WH=p2(2 * maxc), AH=p2(maxc), MAXDENSE=maxdense)
 
 
 class _Context:
