@@ -138,7 +138,7 @@ struct steel_batch {
 
 namespace {
 
-int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string& why) {
+int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, uint32_t threads, std::string& why) {
   Consts& C = s.C;
   if (!C.parse(in.constants)) { why = "malformed constants text"; return STEEL_E_INVALID; }
   static const char* unsupported[][2] = {
@@ -257,7 +257,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, std::string
   s.o_sched = L.take(s.sched_words * 4);
   s.o_tw = L.take((size_t)NB * 32); s.o_imp = L.take((size_t)NB * 32);
   s.o_aqd = L.take((size_t)(ND > 0 ? ND : 1) * 4);
-  s.o_tscr = L.take((size_t)PREP_THREADS * s.tscr_floats * 4);
+  s.o_tscr = L.take((size_t)threads * s.tscr_floats * 4);
   return STEEL_OK;
 }
 
@@ -350,9 +350,10 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   b->ctx = ctx;
   b->sc.resize(n);
   Layout L;
+  const bool big = n <= (uint32_t)ctx->sms;
   for (uint32_t i = 0; i < n; i++) {
     std::string why;
-    int rc = build_scene(b->sc[i], scenes[i], L, why);
+    int rc = build_scene(b->sc[i], scenes[i], L, big ? BIG_THREADS : PREP_THREADS, why);
     if (rc) return fail(rc, "scene " + std::to_string(i) + ": " + why);
     if (i > 0 && b->sc[i].d.substeps != b->sc[0].d.substeps)
       return fail(STEEL_E_INVALID, "scenes of one batch must share the substep count");
@@ -466,6 +467,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   bd.prep_smem = (uint32_t)prep_smem;
   bd.solve_smem = (uint32_t)solve_smem;
   bd.art_f64 = art_f64 != 0u ? 1u : 0u;
+  bd.big = big ? 1u : 0u;
   CU(configure_prepare(prep_smem));
   CU(configure_solve(solve_smem));
   CU(cudaMemcpyAsync(bd.scenes, dev.data(), sizeof(SceneDev) * n, cudaMemcpyHostToDevice, st));

@@ -25,6 +25,7 @@ struct BatchDev {
   uint32_t prep_smem;         // dynamic shared memory of k_prepare / k_solve launches (bytes)
   uint32_t solve_smem;
   uint32_t art_f64;           // some scene has ART_F64: launch the prepare instances that carry it
+  uint32_t big;               // prepare and solve run BIG_THREADS blocks (few scenes)
 };
 
 constexpr uint32_t BROAD_TILE = 32;
@@ -34,6 +35,10 @@ constexpr uint32_t NJOB_WORDS = 44;     // words per narrowphase job record
 constexpr int SORT_THREADS = 512;
 constexpr int PREP_THREADS = 128;
 constexpr int SOLVE_THREADS = 128;
+// Batches of no more scenes than SMs run prepare and solve with one BIG_THREADS block per scene
+// (one per SM, the same 128 registers per thread): large scenes get four times the threads for
+// their parallel phases. Results do not depend on the block size.
+constexpr int BIG_THREADS = 512;
 
 // Device error codes written to BatchDev::error.
 enum : uint32_t { ERR_NONE = 0, ERR_SORT_CAPACITY = 1, ERR_JOB_CAPACITY = 2, ERR_STAGE_TIMEOUT = 3 };

@@ -167,6 +167,19 @@ def test_sleeping_bit_exact(steel, oracle_lib):
     assert min(counts[first:]) < counts[first] and counts[-1] >= 6, counts
 
 
+def test_block_size_does_not_change_results(steel):
+    """A batch of no more scenes than SMs runs prepare and solve with 512-thread blocks, a larger
+    batch with 128-thread blocks; the same scene gives the same bits either way."""
+    pk = pack(scenes.chains_and_quads(n_quad=2))
+    small = Batch([pk])
+    large = Batch([pk] * 160)
+    small.step(20)
+    large.step(20)
+    for i in (0, 159):
+        assert np.array_equal(_bits(small.poses()), _bits(large.poses(i)))
+        assert np.array_equal(_bits(small.raw_state()[2]), _bits(large.raw_state(i)[2]))
+
+
 def test_reset_replays_identically(steel):
     pk = pack(scenes.boxes(24))
     g = Batch([pk])
