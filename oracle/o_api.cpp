@@ -45,8 +45,7 @@ bool Oracle::init(const char* constants, const float* statF_, size_t nF, const u
   C.reg = get("PARAM_reg", 0);
   // The oracle restates the default-flag path (and the small features that ride on it).
   const char* unsup = nullptr;
-  if (C.ANG_ART) unsup = "torsional/rolling friction of articulated contacts";
-  else if (C.CTI) unsup = "row_schedule contact_then_internal";
+  if (C.CTI) unsup = "row_schedule contact_then_internal";
   else if (C.LONGEST_FIRST) unsup = "propagation_color_order longest_first";
   if (unsup) { error = std::string("unsupported solver option: ") + unsup; return false; }
   if (nF != (size_t)C.LEN_STATF4 * 4u || nU != C.LEN_STATU || nArt != C.LEN_ART) { error = "buffer size mismatch"; return false; }

@@ -849,6 +849,32 @@ void Oracle::k_prepare() {
       rows[o + 19u] = mk4(mat.y, mat.z, KA[0] > 1e-12f ? 1.0f / ks : 0.0f, 0.0f);
       rows[o + 20u] = mk4(r11 / rd, -r01 / rd, r00 / rd, 0.0f);
       rows[o + 21u] = mk4(0.0f, 0.0f, 0.0f, 0.0f);
+      if (C.ANG_ART == 1u) {
+        // The raw 5x5 response of (t1, t2, spin, roll1, roll2), upper triangle row by row, for the
+        // articulated angular block (wgsl.js:2244-2267).
+        v3 JA[5][2], JB[5][2], RA[5][2], RB[5][2];
+        for (uint32_t q = 0; q < 2u; q++) {
+          const v3 d = dirs[q + 1u];
+          JA[q][0] = -d; JA[q][1] = -cross(fa, d);
+          JB[q][0] = d; JB[q][1] = cross(fb, d);
+          RA[q][0] = Ma[q + 1u][0]; RA[q][1] = Ma[q + 1u][1];
+          RB[q][0] = Mb[q + 1u][0]; RB[q][1] = Mb[q + 1u][1];
+        }
+        for (uint32_t q = 0; q < 3u; q++) {
+          JA[q + 2u][0] = splat3(0.0f); JA[q + 2u][1] = -dirs[q];
+          JB[q + 2u][0] = splat3(0.0f); JB[q + 2u][1] = dirs[q];
+          RA[q + 2u][0] = MA[q][0]; RA[q + 2u][1] = MA[q][1];
+          RB[q + 2u][0] = MB[q][0]; RB[q + 2u][1] = MB[q][1];
+        }
+        float Hu[16];
+        uint32_t idx = 0;
+        for (uint32_t x = 0; x < 5u; x++)
+          for (uint32_t y = x; y < 5u; y++)
+            Hu[idx++] = ((dot(JA[x][0], RA[y][0]) + dot(JA[x][1], RA[y][1])) + dot(JB[x][0], RB[y][0])) +
+                        dot(JB[x][1], RB[y][1]);
+        Hu[15] = 0.0f;
+        for (uint32_t q = 0; q < 4u; q++) rows[o + C.EO + q] = v4{Hu[q * 4u], Hu[q * 4u + 1u], Hu[q * 4u + 2u], Hu[q * 4u + 3u]};
+      }
     }
   }
   // Phase 6b: contact torsion headers, then friction patches.

@@ -4,6 +4,7 @@
 
 #include "oracle.h"
 #include "smath_o.h"
+#include "o_cone5.h"
 
 namespace orc {
 
@@ -316,12 +317,48 @@ void Oracle::solve_unit(uint32_t us, uint32_t row, int a, int b, uint32_t s0, ui
       add_imp(a, -f, -cross(fra, f));
       add_imp(b, f, cross(frb, f));
     }
+    // Articulated torsional/rolling (wgsl.js:3080, 3112-3140): after the sliding pair, the block
+    // over sliding, spin and rolling of a contact that touches an articulation.
+    const bool art_u = (a >= 0 && body_kind(a) >= 2u) || (b >= 0 && body_kind(b) >= 2u);
+    const bool ell = C.ANG_ART == 1u && C.ANG == 1u && art_u && (rows[o + 19u].x > 0.0f || rows[o + 19u].y > 0.0f);
+    if (ell && it >= C.FSTART) {
+      float H[25];
+      uint32_t idx = 0;
+      for (uint32_t x = 0; x < 5u; x++)
+        for (uint32_t y = x; y < 5u; y++) {
+          const v4 q = rows[o + C.EO + idx / 4u];
+          const float hv = (&q.x)[idx % 4u];
+          H[x * 5u + y] = hv;
+          H[y * 5u + x] = hv;
+          idx++;
+        }
+      const v3 vt = (tb[0] + cross(tb[1], frb)) - (ta[0] + cross(ta[1], fra));
+      const v3 wr = tb[1] - ta[1];
+      const v4 la0 = rows[o + 21u], g19 = rows[o + 19u];
+      const float g[5] = {dot(t1, vt), dot(t2, vt), dot(n, wr), dot(t1, wr), dot(t2, wr)};
+      const float mu5[5] = {r2.w, r2.w, g19.x, g19.y, g19.y};
+      const float l5[5] = {lam.y, lam.z, la0.x, la0.y, la0.z};
+      float nl5[5], d[5];
+      ell_block5(H, g, mu5, l5, pooled, C.PYRAMID == 1u, C.F_CREEP, C.F_OMEGA, nl5);
+      for (uint32_t k = 0; k < 5u; k++) d[k] = nl5[k] - l5[k];
+      ta[0] += (((xyz(rows[o + 11u]) * d[0] + xyz(rows[o + 15u]) * d[1]) + xyz(rows[o + 22u]) * d[2]) + xyz(rows[o + 26u]) * d[3]) + xyz(rows[o + 30u]) * d[4];
+      ta[1] += (((xyz(rows[o + 12u]) * d[0] + xyz(rows[o + 16u]) * d[1]) + xyz(rows[o + 23u]) * d[2]) + xyz(rows[o + 27u]) * d[3]) + xyz(rows[o + 31u]) * d[4];
+      tb[0] += (((xyz(rows[o + 13u]) * d[0] + xyz(rows[o + 17u]) * d[1]) + xyz(rows[o + 24u]) * d[2]) + xyz(rows[o + 28u]) * d[3]) + xyz(rows[o + 32u]) * d[4];
+      tb[1] += (((xyz(rows[o + 14u]) * d[0] + xyz(rows[o + 18u]) * d[1]) + xyz(rows[o + 25u]) * d[2]) + xyz(rows[o + 29u]) * d[3]) + xyz(rows[o + 33u]) * d[4];
+      const v3 f = t1 * d[0] + t2 * d[1];
+      const v3 tq = (n * d[2] + t1 * d[3]) + t2 * d[4];
+      add_imp(a, -f, (-cross(fra, f)) - tq);
+      add_imp(b, f, cross(frb, f) + tq);
+      lam.y = nl5[0];
+      lam.z = nl5[1];
+      rows[o + 21u] = mk4(nl5[2], nl5[3], nl5[4], 0.0f);
+    }
     rows[o + 6u] = lam;
     if (C.ANG == 1u) {
       // Spin within mu_t * N, rolling within a disk of mu_r * N (wgsl.js:3144-3170); under
       // friction patches only the region's first anchor carries them, with the pooled load.
       const v4 g = rows[o + 19u];
-      const bool aon = C.PATCH == 0u || role == 1.0f || (role == 2.0f && rows[o + PO + 1u].w == 0.0f);
+      const bool aon = !ell && (C.PATCH == 0u || role == 1.0f || (role == 2.0f && rows[o + PO + 1u].w == 0.0f));
       const float nl2 = pooled;
       if (aon && (g.x > 0.0f || g.y > 0.0f)) {
         const v4 la = rows[o + 21u];

@@ -33,7 +33,7 @@ namespace orc {
   X(CTRL_KIND) X(CTRL_A) X(CTRL_B) X(NDA) X(JDIM) X(MAXDENSE) X(DHDR) X(DPS) X(MAXP) X(MAXC) X(MAXU) X(UH) \
   X(WH) X(ROWS) X(PO) X(FMO) X(FMODE) X(PATCH) X(EXTRA) X(SHARED) X(FSHARED) X(REST) X(CTI) X(SLEEP)      \
   X(DRIVE_ROWS) X(VEL_DRIVE_ACTIVE) X(FUSE_VLIM) X(VLIM_ON) X(FSTART) X(VELITERS) X(AH) X(ANG) X(ANG_ART)  \
-  X(JFL) X(TORS) X(TO) X(EO) X(CO) X(COMPL) X(LONGEST_FIRST) X(VLIM_FREE) X(FRICTION_COMBINE)             \
+  X(JFL) X(TORS) X(TO) X(EO) X(PYRAMID) X(CO) X(COMPL) X(LONGEST_FIRST) X(VLIM_FREE) X(FRICTION_COMBINE)             \
   X(RESTITUTION_COMBINE) X(JM) X(MAXPATH) X(MAXLP) X(ART_F64)                                                        \
   X(SF_BODY) X(SF_SHAPE) X(SF_HAABB) X(SF_VERTS) X(SF_FPLANE) X(SF_LINK) X(SF_DOF) X(SF_PATH) X(SF_LOOP)  \
   X(SF_MIMIC) X(SF_CTRL) X(SU_HULL) X(SU_FACE) X(SU_FV) X(SU_HEDGE) X(SU_EDGE) X(SU_ART) X(SU_ACON)        \
@@ -49,7 +49,7 @@ namespace orc {
 #define ORC_F32_CONSTS(X)                                                                                 \
   X(F_ANCHOR_BETA) X(F_CFM) X(F_OMEGA) X(F_SPEC) X(F_GAP_GATE) X(F_FGAP) X(F_FSCALE) X(F_REST_SPEED)      \
   X(F_FR_MUT) X(F_FR_MUR) X(F_BP_CELL) X(F_VLIM_FRAC) X(F_JL_GAP) X(F_JL_SPEED) X(F_SLEEP_LIN) X(F_SLEEP_ANG) \
-  X(F_SLEEP_TIME)
+  X(F_SLEEP_TIME) X(F_CREEP)
 
 struct Consts {
 #define X(n) uint32_t n = 0;

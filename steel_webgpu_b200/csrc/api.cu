@@ -142,7 +142,6 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, uint32_t th
   Consts& C = s.C;
   if (!C.parse(in.constants)) { why = "malformed constants text"; return STEEL_E_INVALID; }
   static const char* unsupported[][2] = {
-      {"ANG_ART", "torsional/rolling friction of articulated contacts"},
       {"CTI", "row_schedule contact_then_internal"}, {"LONGEST_FIRST", "propagation_color_order longest_first"}};
   for (auto& u : unsupported)
     if (C.u(u[0]) != 0u) { why = std::string("unsupported solver option: ") + u[1]; return STEEL_E_UNSUPPORTED; }
@@ -157,13 +156,13 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, uint32_t th
   K(SF_MIMIC) K(SF_CTRL) K(SU_HULL) K(SU_FACE) K(SU_FV) K(SU_HEDGE) K(SU_EDGE) K(SU_ART) K(SU_ACON)
   K(SU_FILTER) K(NB) K(NS) K(NA) K(NL) K(ND) K(NDA) K(JM) K(MAXPATH) K(MAXLP) K(NLOOP) K(NMIMIC) K(PATCH)
   K(EXTRA) K(SHARED) K(FSHARED) K(REST) K(FSTART) K(TGT_HELD) K(CTRL_KIND) K(CTRL_A) K(CTRL_B) K(VLIM_FREE) K(VLIM_ON) K(ART_F64) K(SLEEP) K(NEST) K(MO) K(TORS) K(TO) K(COMPL) K(CO) K(VELITERS) K(JFL) K(DRIVE_ROWS) K(FUSE_VLIM)
-  K(VEL_DRIVE_ACTIVE) K(FMODE) K(FMO) K(ANG)
+  K(VEL_DRIVE_ACTIVE) K(FMODE) K(FMO) K(ANG) K(ANG_ART) K(EO) K(PYRAMID)
   K(FRICTION_COMBINE) K(RESTITUTION_COMBINE) K(NCOLW) K(NCOL) K(MAXP) K(MAXC) K(MAXU) K(WH) K(AH)
   K(MAXDENSE) K(ROWS) K(PO) K(DHDR) K(DPS)
 #undef K
 #define F(n) d.n = C.f(#n);
   F(F_ANCHOR_BETA) F(F_CFM) F(F_OMEGA) F(F_SPEC) F(F_GAP_GATE) F(F_FGAP) F(F_FSCALE) F(F_REST_SPEED) F(F_FR_MUT)
-  F(F_FR_MUR) F(F_BP_CELL) F(F_JL_GAP) F(F_JL_SPEED) F(F_VLIM_FRAC) F(F_SLEEP_LIN) F(F_SLEEP_ANG) F(F_SLEEP_TIME)
+  F(F_FR_MUR) F(F_BP_CELL) F(F_JL_GAP) F(F_JL_SPEED) F(F_VLIM_FRAC) F(F_SLEEP_LIN) F(F_SLEEP_ANG) F(F_SLEEP_TIME) F(F_CREEP)
 #undef F
   if (d.NCOLW == 0u || d.NCOLW > 64u || d.NCOL != d.NCOLW * 32u) { why = "bad color table size"; return STEEL_E_INVALID; }
   if (d.MAXC == 0u || d.MAXP == 0u || d.WH == 0u || d.AH == 0u) { why = "zero capacity"; return STEEL_E_INVALID; }
@@ -402,7 +401,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   uint8_t* A = b->arena;
   std::vector<SceneDev> dev(n);
   size_t prep_smem = 0, solve_smem = 0;
-  uint32_t art_f64 = 0;
+  uint32_t art_f64 = 0, ang_art = 0;
   for (uint32_t i = 0; i < n; i++) {
     SceneHost& s = b->sc[i];
     SceneDev& d = s.d;
@@ -430,6 +429,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
     prep_smem = std::max<size_t>(prep_smem, prep_smem_layout(d.stage, d.NL, d.NB, d.NCOLW, d.NCOL).total);
     solve_smem = std::max<size_t>(solve_smem, solve_smem_layout(d.stage, d.NB, d.ND, d.NCOL, d.NL).total);
     art_f64 |= d.ART_F64;
+    ang_art |= d.ANG_ART;
     dev[i] = d;
     CU(cudaMemcpyAsync((void*)d.sf.p, s.statF.data(), s.statF.size() * 4, cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync((void*)d.su.p, s.statU.data(), s.statU.size() * 4, cudaMemcpyHostToDevice, st));
@@ -467,6 +467,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   bd.prep_smem = (uint32_t)prep_smem;
   bd.solve_smem = (uint32_t)solve_smem;
   bd.art_f64 = art_f64 != 0u ? 1u : 0u;
+  bd.ang_art = ang_art != 0u ? 1u : 0u;
   bd.big = big ? 1u : 0u;
   CU(configure_prepare(prep_smem));
   CU(configure_solve(solve_smem));

@@ -526,7 +526,12 @@ struct Narrow {
     float mu = combine(A0.z, B0.z, S.FRICTION_COMBINE);
     bool art_c = (ba >= 0 && body_kind(ba) >= 2u) || (bb >= 0 && body_kind(bb) >= 2u);
     float mt = 0.0f, mr = 0.0f;
-    if (!art_c) {
+    if (art_c) {
+      if (S.ANG_ART == 1u) {
+        mt = combine(ma.y, mb.y, S.FRICTION_COMBINE);
+        mr = combine(ma.z, mb.z, S.FRICTION_COMBINE);
+      }
+    } else {
       mt = fmx(ma.w >= 4.0f ? ma.y : 0.0f, mb.w >= 4.0f ? mb.y : 0.0f);
       mr = fmx(ma.w >= 6.0f ? ma.z : 0.0f, mb.w >= 6.0f ? mb.z : 0.0f);
       if (S.F_FR_MUT >= 0.0f) mt = S.F_FR_MUT;

@@ -15,6 +15,7 @@
 #include "batch.cuh"
 #include "block.cuh"
 #include "bulk.cuh"
+#include "cone5.cuh"
 
 namespace steel {
 
@@ -298,6 +299,51 @@ struct Solver {
       add_imp(b, sp3(0.0f), ng * ds);
     }
   }
+  // The articulated angular block of one contact row: H unpacked from the row's upper triangle, the
+  // rows' velocity residual, the cone solve, then the impulse change applied to both bodies. Twists
+  // and impulses go in and out by value, so the contact loop's own stay in registers.
+  struct AngOut {
+    f3 ta0, ta1, tb0, tb1;
+    float l1, l2;
+  };
+  __device__ __noinline__ AngOut ang_block(uint32_t o, int a, int b, f3 n, f3 t1, f3 t2, f3 fra, f3 frb, float mu,
+                                           float pooled, float ly, float lz, f3 ta0, f3 ta1, f3 tb0, f3 tb1) const {
+    float4* rows = S.rows;
+    f3 ta[2] = {ta0, ta1}, tb[2] = {tb0, tb1};
+    float H[25];
+    uint32_t idx = 0;
+    for (uint32_t x = 0; x < 5u; x++)
+      for (uint32_t y = x; y < 5u; y++) {
+        const float4 q = rows[o + S.EO + idx / 4u];
+        const uint32_t m = idx % 4u;
+        const float hv = m == 0u ? q.x : (m == 1u ? q.y : (m == 2u ? q.z : q.w));
+        H[x * 5u + y] = hv;
+        H[y * 5u + x] = hv;
+        idx++;
+      }
+    const f3 vt = (tb[0] + cross(tb[1], frb)) - (ta[0] + cross(ta[1], fra));
+    const f3 wr = tb[1] - ta[1];
+    const float4 la0 = rows[o + 21u], g19 = rows[o + 19u];
+    const float g[5] = {dot(t1, vt), dot(t2, vt), dot(n, wr), dot(t1, wr), dot(t2, wr)};
+    const float mu5[5] = {mu, mu, g19.x, g19.y, g19.y};
+    const float l5[5] = {ly, lz, la0.x, la0.y, la0.z};
+    float nl5[5], d[5];
+    ell_block5(H, g, mu5, l5, pooled, S.PYRAMID == 1u, S.F_CREEP, S.F_OMEGA, nl5);
+    for (uint32_t k = 0; k < 5u; k++) d[k] = nl5[k] - l5[k];
+    ta[0] += (((v3(rows[o + 11u]) * d[0] + v3(rows[o + 15u]) * d[1]) + v3(rows[o + 22u]) * d[2]) + v3(rows[o + 26u]) * d[3]) + v3(rows[o + 30u]) * d[4];
+    ta[1] += (((v3(rows[o + 12u]) * d[0] + v3(rows[o + 16u]) * d[1]) + v3(rows[o + 23u]) * d[2]) + v3(rows[o + 27u]) * d[3]) + v3(rows[o + 31u]) * d[4];
+    tb[0] += (((v3(rows[o + 13u]) * d[0] + v3(rows[o + 17u]) * d[1]) + v3(rows[o + 24u]) * d[2]) + v3(rows[o + 28u]) * d[3]) + v3(rows[o + 32u]) * d[4];
+    tb[1] += (((v3(rows[o + 14u]) * d[0] + v3(rows[o + 18u]) * d[1]) + v3(rows[o + 25u]) * d[2]) + v3(rows[o + 29u]) * d[3]) + v3(rows[o + 33u]) * d[4];
+    const f3 f = t1 * d[0] + t2 * d[1];
+    const f3 tq = (n * d[2] + t1 * d[3]) + t2 * d[4];
+    add_imp(a, -f, (-cross(fra, f)) - tq);
+    add_imp(b, f, cross(frb, f) + tq);
+    rows[o + 21u] = make_float4(nl5[2], nl5[3], nl5[4], 0.0f);
+    return AngOut{ta[0], ta[1], tb[0], tb[1], nl5[0], nl5[1]};
+  }
+  // ELL compiles the articulated angular block in (the solve kernel's ELL instance, launched for
+  // batches with a scene that has it); the ELL = false kernel is the plain contact loop.
+  template <bool ELL>
   __device__ void solve_row(uint32_t us, uint32_t row, int a, int b, uint32_t mode, uint32_t it) const {
     const uint32_t ROWS = S.ROWS, PO = S.PO;
     float4* rows = S.rows;
@@ -387,12 +433,22 @@ struct Solver {
         add_imp(a, -f, -cross(fra, f));
         add_imp(b, f, cross(frb, f));
       }
+      // Articulated torsional/rolling (wgsl.js:3080, 3112-3140): after the sliding pair, the block
+      // over sliding, spin and rolling of a contact that touches an articulation.
+      const bool art_u = (a >= 0 && bkind(a) >= 2u) || (b >= 0 && bkind(b) >= 2u);
+      const bool ell = ELL && S.ANG_ART == 1u && S.ANG == 1u && art_u && (rows[o + 19u].x > 0.0f || rows[o + 19u].y > 0.0f);
+      if (ell && it >= S.FSTART) {
+        const AngOut r = ang_block(o, a, b, n, t1, t2, fra, frb, r2.w, pooled, lam.y, lam.z, ta[0], ta[1], tb[0], tb[1]);
+        ta[0] = r.ta0; ta[1] = r.ta1; tb[0] = r.tb0; tb[1] = r.tb1;
+        lam.y = r.l1;
+        lam.z = r.l2;
+      }
       rows[o + 6u] = lam;
       if (S.ANG == 1u) {
         // Spin within mu_t * N, rolling within a disk of mu_r * N (wgsl.js:3144-3170); under
         // friction patches only the region's first anchor carries them, with the pooled load.
         const float4 g = rows[o + 19u];
-        const bool aon = S.PATCH == 0u || role == 1.0f || (role == 2.0f && rows[o + PO + 1u].w == 0.0f);
+        const bool aon = !ell && (S.PATCH == 0u || role == 1.0f || (role == 2.0f && rows[o + PO + 1u].w == 0.0f));
         const float nl2 = pooled;
         if (aon && (g.x > 0.0f || g.y > 0.0f)) {
           const float4 la = rows[o + 21u];
@@ -423,10 +479,12 @@ struct Solver {
     if (a >= 0) { tw[(uint32_t)a * 2u] = mf4(ta[0], 0.0f); tw[(uint32_t)a * 2u + 1u] = mf4(ta[1], 0.0f); }
     if (b >= 0) { tw[(uint32_t)b * 2u] = mf4(tb[0], 0.0f); tw[(uint32_t)b * 2u + 1u] = mf4(tb[1], 0.0f); }
   }
+  template <bool ELL>
   __device__ void solve_slot(uint32_t u, uint32_t mode, uint32_t it) const {
     float4 sl = S.slots[2u * u];
-    solve_row(f2u(sl.y), f2u(sl.x), f2i(sl.z), f2i(sl.w), mode, it);
+    solve_row<ELL>(f2u(sl.y), f2u(sl.x), f2i(sl.z), f2i(sl.w), mode, it);
   }
+
 
   // subgroupAdd over the warp (wgsl.js:3305, subgroups on), pinned to an xor butterfly over lane
   // offsets 16, 8, 4, 2, 1. IEEE addition commutes, so every lane ends with the same bits.
@@ -869,6 +927,7 @@ struct Solver {
     __syncthreads();
   }
   // One sweep (wgsl.js:3559-3611).
+  template <bool ELL>
   __device__ void sweep(uint32_t mode, uint32_t ncol, uint32_t it, const uint32_t* wcs, uint32_t nu) const {
     const uint32_t tid = threadIdx.x, nt = blockDim.x;
     for (uint32_t a = tid; a < S.NA; a += nt) joint_rows(a);
@@ -884,11 +943,11 @@ struct Solver {
     __syncthreads();
     dense_phase(1u, it, 0u);
     for (uint32_t c = 0; c < ncol; c++) {
-      for (uint32_t u = wcs[c] + tid; u < wcs[c + 1u]; u += nt) solve_slot(u, mode, it);
+      for (uint32_t u = wcs[c] + tid; u < wcs[c + 1u]; u += nt) solve_slot<ELL>(u, mode, it);
       __syncthreads();
     }
     if (tid == 0u)
-      for (uint32_t u = wcs[S.NCOL]; u < wcs[S.NCOL + 1u]; u++) solve_slot(u, mode, it);
+      for (uint32_t u = wcs[S.NCOL]; u < wcs[S.NCOL + 1u]; u++) solve_slot<ELL>(u, mode, it);
     __syncthreads();
     for (uint32_t a = tid; a < S.NA; a += nt) {
       contact_impulses(a);
@@ -944,6 +1003,7 @@ struct Solver {
 };
 
 // Solve of scene sc by the calling block (all its threads).
+template <bool ELL>
 __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
   extern __shared__ float4 ssm4[];  // solve_smem_layout: [tw | imp], qd, color starts, link blocks
   __shared__ Params Ps;
@@ -1032,10 +1092,10 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     sv.dense_lists(dtmp);
   }
   sv.dense_phase(0u, 0u, 0u);
-  sv.sweep(0u, ncol, 0u, wcs, nu);
+  sv.sweep<ELL>(0u, ncol, 0u, wcs, nu);
   for (uint32_t it = 0; it < P.iterations; it++) {
     if (S.NEST == 1u) sv.momentum_step(ncol, it, wcs);
-    sv.sweep(1u, ncol, it, wcs, nu);
+    sv.sweep<ELL>(1u, ncol, it, wcs, nu);
   }
   // Velocity pass (velocity_iterations, wgsl.js:3700-3736): positions integrate with the velocities
   // reached here; further bias-free sweeps from the accumulated impulses set the output velocities.
@@ -1074,7 +1134,7 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     }
     __syncthreads();
     sv.vpass = true;
-    for (uint32_t it = 0; it < S.VELITERS; it++) sv.sweep(1u, ncol, P.iterations + it, wcs, nu);
+    for (uint32_t it = 0; it < S.VELITERS; it++) sv.sweep<ELL>(1u, ncol, P.iterations + it, wcs, nu);
     sv.vpass = false;
   }
   // Warm-start table (wgsl.js:3737-3767): rows sharing a key keep the largest normal impulse.

@@ -232,3 +232,29 @@ def spin_roll(seed=43):
         ball = b.add_body(xform=[-0.6, 0.4 * i - 0.2, r, 0, 0, 0, 1], twist=[v, 0.0, 0.0, 0.0, v / r, 0.0])
         b.add_shape_sphere(ball, radius=r, mu=0.6)
     return b.finalize(solver=dict(free_rigid_torsional_friction=0.05, free_rigid_rolling_friction=0.01))
+
+
+def ang_art(seed=47, cone="elliptic", creep=0.0, relaxation=1.0):
+    """Torsional and rolling friction of articulated contacts (enable_torsional_rolling_friction,
+    friction_anchor_beta 0): two free-floating dumbbells (two spheres on a fixed joint), one spinning
+    flat about the vertical and one rolling across its bar, and a quadruped dropped on its feet. Every contact that
+    touches a link runs the 5-row angular block (t1, t2, spin, roll1, roll2) on the chosen cone."""
+    rng = np.random.default_rng(seed)
+    b = SceneBuilder(fps=240)
+    mat = dict(muTorsional=0.05, muRolling=0.02)
+    b.add_ground_plane(mu=0.7, **mat)
+    r = 0.08
+    for i, tw in enumerate(([0.0, 0.0, 0.0, 0.0, 0.0, 6.0], [0.0, 1.0, 0.0, -1.0 / r, 0.0, 0.0])):
+        y = 0.6 * i
+        left = b.add_body(xform=[-0.15, y, r, 0, 0, 0, 1], twist=tw)
+        b.add_shape_sphere(left, radius=r, mu=0.6, **mat)
+        b.add_joint_free(left)
+        right = b.add_body(xform=[0.15, y, r, 0, 0, 0, 1])
+        b.add_shape_sphere(right, radius=r, mu=0.6, **mat)
+        b.add_shape_capsule(right, radius=0.02, half_height=0.1, mu=0.6,
+                            xform=[-0.15, 0, 0, 0, math.sin(math.pi / 4), 0, math.cos(math.pi / 4)], **mat)
+        b.add_joint_fixed(left, right, parent_xform=[0.3, 0, 0, 0, 0, 0, 1])
+    synth._add_quadruped(b, rng, [0.0, 1.6, 0.9])
+    return b.finalize(solver=dict(enable_torsional_rolling_friction=True, friction_anchor_beta=0.0,
+                                  torsional_rolling_friction_cone=cone,
+                                  torsional_rolling_friction_creep_speed=creep, relaxation=relaxation))

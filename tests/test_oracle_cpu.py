@@ -15,7 +15,7 @@ from tests import scenes
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "oracle_fixtures.npz")
 REF_SCENES = "/root/reference/assets/scenes"
-UNSUPPORTED = ("ANG_ART", "CTI", "LONGEST_FIRST")
+UNSUPPORTED = ("CTI", "LONGEST_FIRST")
 
 
 def test_trig_accuracy(oracle_lib):
@@ -188,3 +188,29 @@ def test_articulation_fp64_option_error(oracle_lib):
     e64 = _chain_qdd_error(oracle_lib, 0.0, 40, 1e5, True)
     assert e64 < 4e-6
     assert e32 > 3.0 * e64
+
+
+@pytest.mark.parametrize("opts", [dict(), dict(cone="pyramidal", creep=0.01)])
+def test_articulated_rolling_and_spin_friction(oracle_lib, opts):
+    """enable_torsional_rolling_friction: a dumbbell rolling across its bar at 1 m/s slows down and
+    one spinning flat at 6 rad/s stops, while without the option the rolling one keeps its speed."""
+    from tests import scenes
+
+    def run(on):
+        sc = scenes.ang_art(**opts)
+        sc.json["solver"]["enable_torsional_rolling_friction"] = on
+        pk = pack(sc)
+        o = oracle_lib.OracleSim(pk)
+        o.step(60)
+        qd60 = o.read("art")[pk.C["A_QD"]:pk.C["A_QD"] + pk.ND].copy()
+        o.step(90)
+        qd150 = o.read("art")[pk.C["A_QD"]:pk.C["A_QD"] + pk.ND].copy()
+        return qd60, qd150, o.body_poses()
+
+    on60, on150, p_on = run(True)
+    off60, off150, _ = run(False)
+    assert np.isfinite(p_on).all()
+    assert abs(off60[7]) > 0.99                     # rolling dumbbell, no angular friction: ~1 m/s
+    assert 0.2 < abs(on60[7]) < 0.8                 # rolling resistance mu_r N over 0.25 s
+    assert np.linalg.norm(off150[3:6]) > 3.0        # the spinning one keeps spinning without it
+    assert np.linalg.norm(on150[3:6]) < 0.1         # and stops with it

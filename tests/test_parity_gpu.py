@@ -4,6 +4,8 @@ Integer and order outputs (pair sets, the canonical contact order, colors) must 
 the float pipeline is pinned to IEEE operations in a fixed order on both sides (no FMA), so
 contact records, rows, poses and velocities are compared bit for bit as well.
 """
+import functools
+
 import numpy as np
 import pytest
 
@@ -20,10 +22,14 @@ SCENES = {"boxes": scenes.boxes, "mixed_prims": scenes.mixed_prims, "articulated
           "velocity_pass": scenes.velocity_pass, "load_friction": scenes.load_friction,
           "articulated_drive_rows": scenes.articulated, "vel_limited_drive_rows": scenes.vel_limited,
           "boxes_bisection": scenes.boxes, "mixed_desaxce": scenes.mixed_prims,
-          "articulated_coulomb_newton": scenes.articulated, "spin_roll": scenes.spin_roll}
+          "articulated_coulomb_newton": scenes.articulated, "spin_roll": scenes.spin_roll,
+          "ang_art_elliptic": scenes.ang_art,
+          "ang_art_pyramid_creep": functools.partial(scenes.ang_art, cone="pyramidal", creep=0.01),
+          "ang_art_relaxed": functools.partial(scenes.ang_art, relaxation=0.8)}
 # Packing options per scene: the FP64 articulated-inertia option on the articulation workload, PD
 # drives as solver rows (drive_mode "rows"; with velocity limits, the fused drive clamp), and the
-# three coupled friction modes.
+# three coupled friction modes. The articulated torsional/rolling scenes carry their options in the
+# scene: the elliptic cone, the pyramidal cone with creep compliance, and relaxation 0.8.
 OPTS = {"chains_and_quads_fp64": {"solver": {"articulation_fp64": True}},
         "articulated_drive_rows": {"solver": {"drive_mode": "rows"}},
         "vel_limited_drive_rows": {"solver": {"drive_mode": "rows"}},
