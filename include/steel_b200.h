@@ -20,7 +20,8 @@ extern "C" {
 
 #define STEEL_OK 0
 #define STEEL_E_INVALID 1     /* bad argument or malformed scene; Sim's throw new Error(...) */
-#define STEEL_E_UNSUPPORTED 2 /* solver option outside the supported set (sim.js:412-420) */
+#define STEEL_E_UNSUPPORTED 2 /* reserved for a solver option outside the supported set; every option of the
+                                 reference constant table (sim.js:412-477) is supported, so none returns it */
 #define STEEL_E_CAPACITY 3    /* a device capacity was exceeded and work was dropped */
 #define STEEL_E_CUDA 4        /* CUDA runtime error */
 #define STEEL_E_NOMEM 5       /* device allocation failed */

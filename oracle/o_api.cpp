@@ -43,11 +43,7 @@ bool Oracle::init(const char* constants, const float* statF_, size_t nF, const u
   C.driven = (uint32_t)get("PARAM_driven", 0);
   C.integral_count = (uint32_t)get("PARAM_integral_count", 0);
   C.reg = get("PARAM_reg", 0);
-  // The oracle restates the default-flag path (and the small features that ride on it).
-  const char* unsup = nullptr;
-  if (C.CTI) unsup = "row_schedule contact_then_internal";
-  else if (C.LONGEST_FIRST) unsup = "propagation_color_order longest_first";
-  if (unsup) { error = std::string("unsupported solver option: ") + unsup; return false; }
+  // The oracle restates every solver option of the path.
   if (nF != (size_t)C.LEN_STATF4 * 4u || nU != C.LEN_STATU || nArt != C.LEN_ART) { error = "buffer size mismatch"; return false; }
   statF.resize(C.LEN_STATF4);
   std::memcpy(statF.data(), statF_, nF * 4);

@@ -165,6 +165,16 @@ static void bp_value(const BPC& g, uint32_t q, uint32_t out[2]) {
   out[1] = g.pk;
 }
 
+// row_count (wgsl.js:1507-1514): the rows a contact point solves (normal, a friction pair unless it
+// is a patch member, the angular three), for the longest-first color order.
+uint32_t Oracle::row_count(uint32_t row) const {
+  const uint32_t o = row * C.ROWS;
+  uint32_t n = 1u;
+  const bool member = C.EXTRA == 1u && rows[o + C.PO].w == 0.0f;
+  if (rows[o + 2u].w > 0.0f && !member) n += 2u;
+  if (C.ANG == 1u && (rows[o + 19u].x > 0.0f || rows[o + 19u].y > 0.0f)) n += 3u;
+  return std::min(n, 7u);
+}
 uint32_t Oracle::unit_of(uint32_t p, uint32_t nu) const {
   uint32_t lo_ = 0u, hi = nu;
   for (uint32_t it = 0; it < 32u && hi - lo_ > 1u; it++) {
@@ -885,7 +895,10 @@ void Oracle::k_prepare() {
   for (uint32_t c = 0; c < nc; c++) sc[C.S_ROWOF + c] = 0xffffffffu;
   std::fill(wmask.begin(), wmask.end(), 0u);
   std::fill(wcount.begin(), wcount.end(), 0u);
-  for (uint32_t sp = 0; sp < nu; sp++) { sc[C.S_UTC + sp] = 0u; sc[C.S_UTP + sp] = 0u; }
+  for (uint32_t sp = 0; sp < nu; sp++) {
+    sc[C.S_UTC + sp] = 0u;
+    sc[C.S_UTP + sp] = C.LONGEST_FIRST == 0u ? 0u : 0xffffffffu;
+  }
   for (uint32_t row = 0; row < totp; row++) {
     uint32_t sp = unit_of(row, nu);
     uint32_t c = sc[C.S_KEPT + sc[C.S_OSTART + sp] + row - sc[C.S_USTART + sp]];
@@ -893,7 +906,7 @@ void Oracle::k_prepare() {
     sc[C.S_RCON + row] = c;
     if (c < nc) sc[C.S_ROWOF + c] = row;
   }
-  uint32_t ncu = std::min(wnwalk, MAXC);
+  uint32_t ncu = C.LONGEST_FIRST == 0u ? std::min(wnwalk, MAXC) : 0u;
   for (uint32_t i = 0; i < ncu; i++) {
     uint32_t wc = sc[C.S_WALK + i];
     uint32_t row = wc < MAXC ? sc[C.S_ROWOF + std::min(wc, MAXC - 1u)] : 0xffffffffu;
@@ -905,10 +918,31 @@ void Oracle::k_prepare() {
     uint32_t& utp = sc[C.S_UTP + sc[C.S_RUNIT + row]];
     utp = std::max(utp, ((col + 1u) << 16u) | wc);
   }
-  for (uint32_t sp = 0; sp < nu; sp++) {
-    uint32_t packed = sc[C.S_UTP + sp];
-    sc[C.S_UTC + sp] = packed >> 16u;
-    sc[C.S_UTP + sp] = packed != 0u ? sc[C.S_ROWOF + (packed & 0xffffu)] : 0xffffffffu;
+  if (C.LONGEST_FIRST == 0u) {
+    for (uint32_t sp = 0; sp < nu; sp++) {
+      uint32_t packed = sc[C.S_UTP + sp];
+      sc[C.S_UTC + sp] = packed >> 16u;
+      sc[C.S_UTP + sp] = packed != 0u ? sc[C.S_ROWOF + (packed & 0xffffu)] : 0xffffffffu;
+    }
+  } else {
+    // propagation_color_order "longest_first" (wgsl.js:2331-2346): first-fit by row count first
+    // (7 rows down to 1), then contact index; a unit's last row of its highest color carries its
+    // torsion row.
+    for (uint32_t lp = 0; lp < 8u; lp++)
+      for (uint32_t c = 0; c < nc; c++) {
+        uint32_t row = sc[C.S_ROWOF + c];
+        if (row >= totp) continue;
+        if (row_count(row) != 7u - lp) continue;
+        uint32_t sp = sc[C.S_RUNIT + row];
+        uint32_t key = sc[C.S_UKEY + sp];
+        uint32_t col = first_free_color((int)(key & 0xffffu) - 1, (int)(key >> 16u) - 1);
+        sc[C.S_PCOL + row] = col;
+        wcount[col]++;
+        if (col + 1u >= sc[C.S_UTC + sp]) {
+          sc[C.S_UTC + sp] = col + 1u;
+          sc[C.S_UTP + sp] = row;
+        }
+      }
   }
   {
     uint32_t acc = 0u, ncol = 0u;

@@ -828,9 +828,19 @@ void Oracle::k_solve() {
   for (uint32_t a = 0; a < C.NA; a++) art_twists(a);
   dense_phase(0u, 0u, 0u);
   sweep(0u, wn_y, 0u, 0u);
-  for (uint32_t it = 0; it < P.iterations; it++) {
-    if (C.NEST == 1u) momentum_step(wn_y, it);
-    sweep(1u, wn_y, it, 0u);
+  if (C.CTI == 1u) {
+    // row_schedule "contact_then_internal" (wgsl.js:3693-3696): all contact iterations, then the
+    // joint-internal rows.
+    for (uint32_t it = 0; it < P.iterations; it++) {
+      if (C.NEST == 1u) momentum_step(wn_y, it);
+      sweep(1u, wn_y, it, 1u);
+    }
+    for (uint32_t it = 0; it < P.iterations; it++) sweep(1u, wn_y, it, 2u);
+  } else {
+    for (uint32_t it = 0; it < P.iterations; it++) {
+      if (C.NEST == 1u) momentum_step(wn_y, it);
+      sweep(1u, wn_y, it, 0u);
+    }
   }
   // Velocity pass (velocity_iterations, wgsl.js:3700-3736): positions integrate with the velocities
   // reached here; further bias-free sweeps from the accumulated impulses set the output velocities.

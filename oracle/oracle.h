@@ -259,6 +259,7 @@ struct Oracle {
   // --- prepare (wgsl.js:1222-2494) ---
   std::vector<uint32_t> wkey, wcol, wmask, wcount, wlinkhit, wjsplit;
   uint32_t first_free_color(int a, int b);
+  uint32_t row_count(uint32_t row) const;
   void body_response(int b, v3 f, v3 t, v3 out[2]) const;
   void body_response_unsplit(int b, v3 f, v3 t, v3 out[2]) const;
   bool restitution_fires(float e, float phi, float vn) const;

@@ -141,10 +141,6 @@ namespace {
 int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, uint32_t threads, std::string& why) {
   Consts& C = s.C;
   if (!C.parse(in.constants)) { why = "malformed constants text"; return STEEL_E_INVALID; }
-  static const char* unsupported[][2] = {
-      {"CTI", "row_schedule contact_then_internal"}, {"LONGEST_FIRST", "propagation_color_order longest_first"}};
-  for (auto& u : unsupported)
-    if (C.u(u[0]) != 0u) { why = std::string("unsupported solver option: ") + u[1]; return STEEL_E_UNSUPPORTED; }
   if (in.statF_floats != (uint64_t)C.u("LEN_STATF4") * 4u || in.statU_words != C.u("LEN_STATU") ||
       in.art_floats != C.u("LEN_ART")) {
     why = "statF/statU/art sizes do not match the constants";
@@ -156,7 +152,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, uint32_t th
   K(SF_MIMIC) K(SF_CTRL) K(SU_HULL) K(SU_FACE) K(SU_FV) K(SU_HEDGE) K(SU_EDGE) K(SU_ART) K(SU_ACON)
   K(SU_FILTER) K(NB) K(NS) K(NA) K(NL) K(ND) K(NDA) K(JM) K(MAXPATH) K(MAXLP) K(NLOOP) K(NMIMIC) K(PATCH)
   K(EXTRA) K(SHARED) K(FSHARED) K(REST) K(FSTART) K(TGT_HELD) K(CTRL_KIND) K(CTRL_A) K(CTRL_B) K(VLIM_FREE) K(VLIM_ON) K(ART_F64) K(SLEEP) K(NEST) K(MO) K(TORS) K(TO) K(COMPL) K(CO) K(VELITERS) K(JFL) K(DRIVE_ROWS) K(FUSE_VLIM)
-  K(VEL_DRIVE_ACTIVE) K(FMODE) K(FMO) K(ANG) K(ANG_ART) K(EO) K(PYRAMID)
+  K(VEL_DRIVE_ACTIVE) K(FMODE) K(FMO) K(ANG) K(ANG_ART) K(EO) K(PYRAMID) K(CTI) K(LONGEST_FIRST)
   K(FRICTION_COMBINE) K(RESTITUTION_COMBINE) K(NCOLW) K(NCOL) K(MAXP) K(MAXC) K(MAXU) K(WH) K(AH)
   K(MAXDENSE) K(ROWS) K(PO) K(DHDR) K(DPS)
 #undef K
@@ -401,7 +397,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   uint8_t* A = b->arena;
   std::vector<SceneDev> dev(n);
   size_t prep_smem = 0, solve_smem = 0;
-  uint32_t art_f64 = 0, ang_art = 0;
+  uint32_t art_f64 = 0, solve_ext = 0;
   for (uint32_t i = 0; i < n; i++) {
     SceneHost& s = b->sc[i];
     SceneDev& d = s.d;
@@ -429,7 +425,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
     prep_smem = std::max<size_t>(prep_smem, prep_smem_layout(d.stage, d.NL, d.NB, d.NCOLW, d.NCOL).total);
     solve_smem = std::max<size_t>(solve_smem, solve_smem_layout(d.stage, d.NB, d.ND, d.NCOL, d.NL).total);
     art_f64 |= d.ART_F64;
-    ang_art |= d.ANG_ART;
+    solve_ext |= d.ANG_ART | d.CTI;
     dev[i] = d;
     CU(cudaMemcpyAsync((void*)d.sf.p, s.statF.data(), s.statF.size() * 4, cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync((void*)d.su.p, s.statU.data(), s.statU.size() * 4, cudaMemcpyHostToDevice, st));
@@ -467,7 +463,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   bd.prep_smem = (uint32_t)prep_smem;
   bd.solve_smem = (uint32_t)solve_smem;
   bd.art_f64 = art_f64 != 0u ? 1u : 0u;
-  bd.ang_art = ang_art != 0u ? 1u : 0u;
+  bd.solve_ext = solve_ext != 0u ? 1u : 0u;
   bd.big = big ? 1u : 0u;
   CU(configure_prepare(prep_smem));
   CU(configure_solve(solve_smem));

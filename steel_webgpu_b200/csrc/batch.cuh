@@ -25,7 +25,7 @@ struct BatchDev {
   uint32_t prep_smem;         // dynamic shared memory of k_prepare / k_solve launches (bytes)
   uint32_t solve_smem;
   uint32_t art_f64;           // some scene has ART_F64: launch the prepare instances that carry it
-  uint32_t ang_art;           // some scene has ANG_ART: launch the solve instances that carry it
+  uint32_t solve_ext;         // some scene has ANG_ART or CTI: launch the solve instances that carry them
   uint32_t big;               // prepare and solve run BIG_THREADS blocks (few scenes)
 };
 

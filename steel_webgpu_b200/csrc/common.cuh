@@ -196,7 +196,7 @@ struct SceneDev {
   uint32_t NB, NS, NA, NL, ND, NQ, NDA, JM, MAXPATH, MAXLP, NLOOP, NMIMIC;
   // solver flags and constants
   uint32_t PATCH, EXTRA, SHARED, FSHARED, REST, FSTART, TGT_HELD, CTRL_KIND, CTRL_A, CTRL_B, VLIM_FREE, VLIM_ON, ART_F64, SLEEP, NEST, MO, TORS, TO, COMPL, CO, VELITERS, JFL,
-      DRIVE_ROWS, FUSE_VLIM, VEL_DRIVE_ACTIVE, FMODE, FMO, ANG, ANG_ART, EO, PYRAMID;
+      DRIVE_ROWS, FUSE_VLIM, VEL_DRIVE_ACTIVE, FMODE, FMO, ANG, ANG_ART, EO, PYRAMID, CTI, LONGEST_FIRST;
   uint32_t FRICTION_COMBINE, RESTITUTION_COMBINE, NCOLW, NCOL;
   float F_ANCHOR_BETA, F_CFM, F_OMEGA, F_SPEC, F_GAP_GATE, F_FGAP, F_FSCALE, F_REST_SPEED, F_FR_MUT, F_FR_MUR;
   float F_BP_CELL, F_JL_GAP, F_JL_SPEED, F_VLIM_FRAC, F_SLEEP_LIN, F_SLEEP_ANG, F_SLEEP_TIME, F_CREEP;

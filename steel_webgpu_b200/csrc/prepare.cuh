@@ -384,6 +384,17 @@ struct Prep {
     rows[L + TO + 4u] = mf4(ns, lead);
   }
 
+  // row_count (wgsl.js:1507-1514): the rows a contact point solves (normal, a friction pair unless
+  // it is a patch member, the angular three), for the longest-first color order.
+  __device__ uint32_t row_count(uint32_t row) const {
+    const float4* rows = S.rows;
+    const uint32_t o = row * S.ROWS;
+    uint32_t n = 1u;
+    const bool member = S.EXTRA == 1u && rows[o + S.PO].w == 0.0f;
+    if (rows[o + 2u].w > 0.0f && !member) n += 2u;
+    if (S.ANG == 1u && (rows[o + 19u].x > 0.0f || rows[o + 19u].y > 0.0f)) n += 3u;
+    return min(n, 7u);
+  }
   __device__ void build_row(uint32_t idx, uint32_t c) const {
     const uint32_t ROWS = S.ROWS, PO = S.PO;
     float4* rows = S.rows;
@@ -1054,7 +1065,7 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
     for (uint32_t i = tid; i < S.NCOL + 2u; i += nt) wcount[i] = 0u;
     if (S.stage & STAGE_WMASK)
       for (uint32_t i = tid; i < S.NB * NCOLW; i += nt) wmask[i] = 0u;
-    for (uint32_t r0 = 0; r0 < total; r0 += COLOR_CHUNK) {
+    for (uint32_t r0 = 0; r0 < (S.LONGEST_FIRST == 0u ? total : 0u); r0 += COLOR_CHUNK) {
       const uint32_t nrow = min(COLOR_CHUNK, total - r0);
       __syncthreads();
       for (uint32_t i = tid; i < nrow; i += nt) ckey[i] = sch[S.S_UKEY + sch[S.S_RUNIT + r0 + i]];
@@ -1082,6 +1093,39 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
       }
     }
     __syncthreads();
+    if (S.LONGEST_FIRST == 1u && tid == 0u) {
+      // propagation_color_order "longest_first" (wgsl.js:2331-2346): first-fit by row count first
+      // (7 rows down to 1), then contact index. A unit's torsion row is its last row of its highest
+      // color; that color + 1 is kept as PCOL of the unit's current pick, so it needs no array.
+      for (uint32_t u = 0; u < nu; u++) sch[S.S_UTP + u] = 0xffffffffu;
+      for (uint32_t lp = 0; lp < 8u; lp++)
+        for (uint32_t c = 0; c < nc; c++) {
+          const uint32_t row = sch[S.S_ROWOF + c];
+          if (row >= total || pr.row_count(row) != 7u - lp) continue;
+          const uint32_t u = sch[S.S_RUNIT + row];
+          const uint32_t key = sch[S.S_UKEY + u];
+          const int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
+          uint32_t col = S.NCOL;
+          for (uint32_t w = 0; w < NCOLW; w++) {
+            uint32_t used = 0u;
+            if (a >= 0) used |= wmask[(uint32_t)a * NCOLW + w];
+            if (b >= 0) used |= wmask[(uint32_t)b * NCOLW + w];
+            if (used != 0xffffffffu) {
+              uint32_t k = (uint32_t)__ffs(~used) - 1u;
+              if (a >= 0) wmask[(uint32_t)a * NCOLW + w] |= 1u << k;
+              if (b >= 0) wmask[(uint32_t)b * NCOLW + w] |= 1u << k;
+              col = w * 32u + k;
+              break;
+            }
+          }
+          sch[S.S_PCOL + row] = col;
+          wcount[col]++;
+          const uint32_t utp = sch[S.S_UTP + u];
+          const uint32_t utc = utp == 0xffffffffu ? 0u : sch[S.S_PCOL + utp] + 1u;
+          if (col + 1u >= utc) sch[S.S_UTP + u] = row;
+        }
+    }
+    __syncthreads();
     if (tid == 0u) {
       uint32_t acc = 0u, ncol = 0u;
       for (uint32_t c = 0; c <= S.NCOL; c++) {
@@ -1096,7 +1140,7 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
       sch[S.S_META + 1u] = ncol;
       sch[S.S_META + 2u] = nc;
     }
-    if (S.TORS == 1u) {
+    if (S.TORS == 1u && S.LONGEST_FIRST == 0u) {
       // Each unit's torsion row is its row of the highest color, the latest contact among equals:
       // (color + 1, contact) packed as the reference packs it, 16 bits of contact index
       // (wgsl.js:2288-2325).

@@ -341,9 +341,10 @@ struct Solver {
     rows[o + 21u] = make_float4(nl5[2], nl5[3], nl5[4], 0.0f);
     return AngOut{ta[0], ta[1], tb[0], tb[1], nl5[0], nl5[1]};
   }
-  // ELL compiles the articulated angular block in (the solve kernel's ELL instance, launched for
-  // batches with a scene that has it); the ELL = false kernel is the plain contact loop.
-  template <bool ELL>
+  // EXT compiles the articulated angular block in (the solve kernel's EXT instance, launched for
+  // batches with a scene that has it or the contact-then-internal schedule); the EXT = false kernel
+  // is the plain contact loop.
+  template <bool EXT>
   __device__ void solve_row(uint32_t us, uint32_t row, int a, int b, uint32_t mode, uint32_t it) const {
     const uint32_t ROWS = S.ROWS, PO = S.PO;
     float4* rows = S.rows;
@@ -436,7 +437,7 @@ struct Solver {
       // Articulated torsional/rolling (wgsl.js:3080, 3112-3140): after the sliding pair, the block
       // over sliding, spin and rolling of a contact that touches an articulation.
       const bool art_u = (a >= 0 && bkind(a) >= 2u) || (b >= 0 && bkind(b) >= 2u);
-      const bool ell = ELL && S.ANG_ART == 1u && S.ANG == 1u && art_u && (rows[o + 19u].x > 0.0f || rows[o + 19u].y > 0.0f);
+      const bool ell = EXT && S.ANG_ART == 1u && S.ANG == 1u && art_u && (rows[o + 19u].x > 0.0f || rows[o + 19u].y > 0.0f);
       if (ell && it >= S.FSTART) {
         const AngOut r = ang_block(o, a, b, n, t1, t2, fra, frb, r2.w, pooled, lam.y, lam.z, ta[0], ta[1], tb[0], tb[1]);
         ta[0] = r.ta0; ta[1] = r.ta1; tb[0] = r.tb0; tb[1] = r.tb1;
@@ -479,10 +480,10 @@ struct Solver {
     if (a >= 0) { tw[(uint32_t)a * 2u] = mf4(ta[0], 0.0f); tw[(uint32_t)a * 2u + 1u] = mf4(ta[1], 0.0f); }
     if (b >= 0) { tw[(uint32_t)b * 2u] = mf4(tb[0], 0.0f); tw[(uint32_t)b * 2u + 1u] = mf4(tb[1], 0.0f); }
   }
-  template <bool ELL>
+  template <bool EXT>
   __device__ void solve_slot(uint32_t u, uint32_t mode, uint32_t it) const {
     float4 sl = S.slots[2u * u];
-    solve_row<ELL>(f2u(sl.y), f2u(sl.x), f2i(sl.z), f2i(sl.w), mode, it);
+    solve_row<EXT>(f2u(sl.y), f2u(sl.x), f2i(sl.z), f2i(sl.w), mode, it);
   }
 
 
@@ -927,10 +928,15 @@ struct Solver {
     __syncthreads();
   }
   // One sweep (wgsl.js:3559-3611).
-  template <bool ELL>
-  __device__ void sweep(uint32_t mode, uint32_t ncol, uint32_t it, const uint32_t* wcs, uint32_t nu) const {
+  template <bool EXT>
+  // ph: 0 every row; 1 contacts only (no joint-internal rows, no velocity-limit rows, no internal
+  // dense rows); 2 joint-internal rows only (no contact slots, no contact dense rows). The two
+  // partial sweeps serve row_schedule "contact_then_internal" (wgsl.js:3559-3590).
+  __device__ void sweep(uint32_t mode, uint32_t ncol0, uint32_t it, const uint32_t* wcs, uint32_t nu, uint32_t ph) const {
     const uint32_t tid = threadIdx.x, nt = blockDim.x;
-    for (uint32_t a = tid; a < S.NA; a += nt) joint_rows(a);
+    const uint32_t ncol = ph == 2u ? 0u : ncol0;
+    if (ph != 1u)
+      for (uint32_t a = tid; a < S.NA; a += nt) joint_rows(a);
     if (S.PATCH == 1u && mode == 1u) {
       for (uint32_t us = tid; us < nu; us += nt) {
         uint32_t s0 = S.sched[S.S_USTART + us];
@@ -941,17 +947,17 @@ struct Solver {
       }
     }
     __syncthreads();
-    dense_phase(1u, it, 0u);
+    dense_phase(1u, it, ph);
     for (uint32_t c = 0; c < ncol; c++) {
-      for (uint32_t u = wcs[c] + tid; u < wcs[c + 1u]; u += nt) solve_slot<ELL>(u, mode, it);
+      for (uint32_t u = wcs[c] + tid; u < wcs[c + 1u]; u += nt) solve_slot<EXT>(u, mode, it);
       __syncthreads();
     }
-    if (tid == 0u)
-      for (uint32_t u = wcs[S.NCOL]; u < wcs[S.NCOL + 1u]; u++) solve_slot<ELL>(u, mode, it);
+    if (tid == 0u && ph != 2u)
+      for (uint32_t u = wcs[S.NCOL]; u < wcs[S.NCOL + 1u]; u++) solve_slot<EXT>(u, mode, it);
     __syncthreads();
     for (uint32_t a = tid; a < S.NA; a += nt) {
       contact_impulses(a);
-      if (S.VLIM_ON == 1u) vlim_rows(a);
+      if (S.VLIM_ON == 1u && ph != 1u) vlim_rows(a);
     }
     __syncthreads();
     if (S.VLIM_FREE == 1u) {
@@ -1003,7 +1009,7 @@ struct Solver {
 };
 
 // Solve of scene sc by the calling block (all its threads).
-template <bool ELL>
+template <bool EXT>
 __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
   extern __shared__ float4 ssm4[];  // solve_smem_layout: [tw | imp], qd, color starts, link blocks
   __shared__ Params Ps;
@@ -1092,11 +1098,17 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     sv.dense_lists(dtmp);
   }
   sv.dense_phase(0u, 0u, 0u);
-  sv.sweep<ELL>(0u, ncol, 0u, wcs, nu);
-  for (uint32_t it = 0; it < P.iterations; it++) {
-    if (S.NEST == 1u) sv.momentum_step(ncol, it, wcs);
-    sv.sweep<ELL>(1u, ncol, it, wcs, nu);
-  }
+  sv.sweep<EXT>(0u, ncol, 0u, wcs, nu, 0u);
+  // row_schedule "contact_then_internal" (wgsl.js:3693-3696): all contact iterations (phase 1),
+  // then the joint-internal rows (phase 2); otherwise one pass of full sweeps (phase 0).
+  // Only the EXT instance carries it.
+  const bool cti = EXT && S.CTI == 1u;
+  const uint32_t npass = cti ? 2u : 1u;
+  for (uint32_t pass = 0; pass < npass; pass++)
+    for (uint32_t it = 0; it < P.iterations; it++) {
+      if (S.NEST == 1u && pass == 0u) sv.momentum_step(ncol, it, wcs);
+      sv.sweep<EXT>(1u, ncol, it, wcs, nu, cti ? pass + 1u : 0u);
+    }
   // Velocity pass (velocity_iterations, wgsl.js:3700-3736): positions integrate with the velocities
   // reached here; further bias-free sweeps from the accumulated impulses set the output velocities.
   if (S.VELITERS > 0u) {
@@ -1134,7 +1146,7 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     }
     __syncthreads();
     sv.vpass = true;
-    for (uint32_t it = 0; it < S.VELITERS; it++) sv.sweep<ELL>(1u, ncol, P.iterations + it, wcs, nu);
+    for (uint32_t it = 0; it < S.VELITERS; it++) sv.sweep<EXT>(1u, ncol, P.iterations + it, wcs, nu, 0u);
     sv.vpass = false;
   }
   // Warm-start table (wgsl.js:3737-3767): rows sharing a key keep the largest normal impulse.

@@ -258,3 +258,33 @@ def ang_art(seed=47, cone="elliptic", creep=0.0, relaxation=1.0):
     return b.finalize(solver=dict(enable_torsional_rolling_friction=True, friction_anchor_beta=0.0,
                                   torsional_rolling_friction_cone=cone,
                                   torsional_rolling_friction_creep_speed=creep, relaxation=relaxation))
+
+
+def four_bar(seed=53):
+    """A parallelogram four-bar linkage (crank, coupler and rocker on revolute joints, closed by a
+    loop joint from the world to the rocker), released at 0.5 rad so that the pendulum hung from its coupler swings into the ground, beside a
+    quadruped with PD drives and limits: loop-closure dense rows, joint rows and contacts in one scene."""
+    rng = np.random.default_rng(seed)
+    b = SceneBuilder(fps=240)
+    b.add_ground_plane(mu=0.8)
+    y = [0, 1, 0]
+    crank = b.add_body(xform=[0.0, 0.0, 0.32, 0, 0, 0, 1])
+    b.add_shape_box(crank, hx=0.02, hy=0.02, hz=0.1, mass=0.5)
+    b.add_joint_revolute(-1, crank, axis=y, parent_xform=[0.0, 0.0, 0.42, 0, 0, 0, 1],
+                         child_xform=[0, 0, 0.1, 0, 0, 0, 1], q=[0.5])
+    coupler = b.add_body(xform=[0.3, 0.0, 0.22, 0, 0, 0, 1])
+    b.add_shape_box(coupler, hx=0.3, hy=0.02, hz=0.02, mass=0.5)
+    b.add_joint_revolute(crank, coupler, axis=y, parent_xform=[0, 0, -0.1, 0, 0, 0, 1],
+                         child_xform=[-0.3, 0, 0, 0, 0, 0, 1], q=[-0.5])
+    rocker = b.add_body(xform=[0.6, 0.0, 0.32, 0, 0, 0, 1])
+    b.add_shape_box(rocker, hx=0.02, hy=0.02, hz=0.1, mass=0.5)
+    b.add_joint_revolute(coupler, rocker, axis=y, parent_xform=[0.3, 0, 0, 0, 0, 0, 1],
+                         child_xform=[0, 0, -0.1, 0, 0, 0, 1], q=[0.5])
+    b.add_joint_revolute(-1, rocker, axis=y, parent_xform=[0.6, 0.0, 0.42, 0, 0, 0, 1],
+                         child_xform=[0, 0, 0.1, 0, 0, 0, 1])
+    tip = b.add_body(xform=[0.3, 0.0, 0.07, 0, 0, 0, 1])
+    b.add_shape_sphere(tip, radius=0.05, mass=2.0)
+    b.add_joint_revolute(coupler, tip, axis=[1, 0, 0], parent_xform=[0, 0, -0.05, 0, 0, 0, 1],
+                         child_xform=[0, 0, 0.15, 0, 0, 0, 1], q=[0.4])
+    synth._add_quadruped(b, rng, [1.5, 0.0, 0.9])
+    return b.finalize()

@@ -15,7 +15,6 @@ from tests import scenes
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "oracle_fixtures.npz")
 REF_SCENES = "/root/reference/assets/scenes"
-UNSUPPORTED = ("CTI", "LONGEST_FIRST")
 
 
 def test_trig_accuracy(oracle_lib):
@@ -105,13 +104,20 @@ def test_oracle_matches_committed_fixtures(oracle_lib):
         assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), f"fixture {k} changed"
 
 
-def test_oracle_refuses_unsupported_options(oracle_lib):
-    sc = scenes.boxes(n=4, seed=2)
-    pk = pack(sc, opts={"solver": {"row_schedule": "contact_then_internal"}})
-    if pk.C.get("CTI", 0) == 0:
-        pytest.skip("option not carried by the packer")
-    with pytest.raises(ValueError):
-        oracle_lib.OracleSim(pk)
+def test_longest_first_color_order(oracle_lib):
+    """propagation_color_order "longest_first": rows are colored by row count first, so a scene
+    whose points carry 1, 3 and 6 rows steps to a different (finite) state than in contact order."""
+    def run(opts):
+        pk = pack(scenes.spin_roll(), opts=opts)
+        o = oracle_lib.OracleSim(pk)
+        o.step(30)
+        return pk, o.body_poses()
+
+    pk, p_lf = run({"solver": {"propagation_color_order": "longest_first"}})
+    _, p_co = run(None)
+    assert pk.C["LONGEST_FIRST"] == 1
+    assert np.isfinite(p_lf).all()
+    assert not np.array_equal(p_lf, p_co)
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_SCENES), reason="reference scene folders not on disk")
@@ -119,14 +125,12 @@ def test_reference_scenes_load_and_pack(oracle_lib):
     from steel_webgpu_b200.builder import load_scene
     names = sorted(d for d in os.listdir(REF_SCENES) if os.path.exists(os.path.join(REF_SCENES, d, "scene.json")))
     assert len(names) >= 40
-    supported = []
+    packed = []
     for name in names:
         pk = pack(load_scene(os.path.join(REF_SCENES, name)))
         assert pk.statF.size == pk.C["LEN_STATF4"] * 4 and pk.statU.size == pk.C["LEN_STATU"]
-        if not any(pk.C.get(k, 0) for k in UNSUPPORTED):
-            supported.append((name, pk))
-    assert len(supported) >= 15
-    for name, pk in supported:
+        packed.append((name, pk))
+    for name, pk in packed:
         o = oracle_lib.OracleSim(pk)
         o.step(5)
         assert np.isfinite(o.body_poses()).all(), name

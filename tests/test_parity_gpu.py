@@ -25,17 +25,30 @@ SCENES = {"boxes": scenes.boxes, "mixed_prims": scenes.mixed_prims, "articulated
           "articulated_coulomb_newton": scenes.articulated, "spin_roll": scenes.spin_roll,
           "ang_art_elliptic": scenes.ang_art,
           "ang_art_pyramid_creep": functools.partial(scenes.ang_art, cone="pyramidal", creep=0.01),
-          "ang_art_relaxed": functools.partial(scenes.ang_art, relaxation=0.8)}
+          "ang_art_relaxed": functools.partial(scenes.ang_art, relaxation=0.8),
+          "four_bar": scenes.four_bar, "four_bar_cti": scenes.four_bar, "articulated_cti": scenes.articulated,
+          "vel_limited_cti": scenes.vel_limited, "spin_roll_longest_first": scenes.spin_roll,
+          "spinners_longest_first": scenes.spinners, "articulated_longest_first": scenes.articulated}
 # Packing options per scene: the FP64 articulated-inertia option on the articulation workload, PD
-# drives as solver rows (drive_mode "rows"; with velocity limits, the fused drive clamp), and the
-# three coupled friction modes. The articulated torsional/rolling scenes carry their options in the
-# scene: the elliptic cone, the pyramidal cone with creep compliance, and relaxation 0.8.
+# drives as solver rows (drive_mode "rows"; with velocity limits, the fused drive clamp), the three
+# coupled friction modes, and row_schedule "contact_then_internal" (all contact iterations, then
+# the joint-internal ones) on scenes with a loop closure, limits and velocity limits, and
+# propagation_color_order "longest_first" (rows colored by row count first; with contact torsion
+# on `spinners`). The
+# articulated torsional/rolling scenes carry their options in the scene: the elliptic cone, the
+# pyramidal cone with creep compliance, and relaxation 0.8.
 OPTS = {"chains_and_quads_fp64": {"solver": {"articulation_fp64": True}},
         "articulated_drive_rows": {"solver": {"drive_mode": "rows"}},
         "vel_limited_drive_rows": {"solver": {"drive_mode": "rows"}},
         "boxes_bisection": {"solver": {"friction_mode": "bisection"}},
         "mixed_desaxce": {"solver": {"friction_mode": "bisection_desaxce"}},
-        "articulated_coulomb_newton": {"solver": {"friction_mode": "coulomb_newton"}}}
+        "articulated_coulomb_newton": {"solver": {"friction_mode": "coulomb_newton"}},
+        "four_bar_cti": {"solver": {"row_schedule": "contact_then_internal"}},
+        "articulated_cti": {"solver": {"row_schedule": "contact_then_internal"}},
+        "vel_limited_cti": {"solver": {"row_schedule": "contact_then_internal"}},
+        "spin_roll_longest_first": {"solver": {"propagation_color_order": "longest_first"}},
+        "spinners_longest_first": {"solver": {"propagation_color_order": "longest_first"}},
+        "articulated_longest_first": {"solver": {"propagation_color_order": "longest_first"}}}
 
 
 def _pair_set(p):
