@@ -344,7 +344,11 @@ def run_steel(args):
     torch.cuda.synchronize(local)
     ms = max_over_ranks(ms, world, local)
     value = whole_job_rate(world, nbodies, args.steps, ms / 1000.0)
-    # End to end through the C ABI with pinned host buffers: joint targets in, body poses out.
+    # End to end through the C ABI with pinned host buffers: joint targets in, body poses out. The
+    # batch restarts from its initial state and takes the same warm-up, so these K frames are the
+    # frames the device-timed region covered (the piles grow denser as a run goes on).
+    batch.reset()
+    batch.step(max(args.warmup, 3) - 1)
     nd = sum(pk.ND for pk in pks)
     npose = sum(pk.NB * 8 for pk in pks)
     h_tgt = torch.zeros(max(nd, 1), dtype=torch.float32, pin_memory=True).numpy()[:nd]
@@ -361,7 +365,10 @@ def run_steel(args):
         frame_ms.append((time.perf_counter() - f0) * 1000.0)
     e2e_s = max_over_ranks(time.perf_counter() - t0, world, local)
     e2e = whole_job_rate(world, nbodies, args.steps, e2e_s)
-    # Roofline of the dominant kernel: per-launch device time from CUDA events around each launch.
+    # Roofline of the dominant kernel: per-launch device time from CUDA events around each launch,
+    # over the first frames of the timed region (restart and warm-up as above).
+    batch.reset()
+    batch.step(max(args.warmup, 3))
     prof = batch.profile_kernels(max(2, min(args.steps, 8)))
     counts = scene_counts(batch, pks)
     # Capacities change results only when a buffer overflows; count the scenes where one did.
