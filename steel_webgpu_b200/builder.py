@@ -519,6 +519,15 @@ class SceneBuilder:
         return self.add_joint(JT["FREE"], -1, child,
                               axes=[[1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 0, 0], [0, 1, 0], [0, 0, 1]], linear=3, **o)
 
+    def set_joint_dof_config(self, joint, axis_index, **cfg):
+        """Change dof settings of an existing joint, e.g. drive gains (builder.js:308-309)."""
+        self.joints[joint]["dofs"][axis_index].update(cfg)
+
+    def set_joint_mimic(self, joint, reference, coeffs=(0.0, 1.0)):
+        """Newton's set_joint_mimic (builder.js:310-313): the joint's coordinates follow
+        coeffs[0] + coeffs[1] * the reference joint's; reference None clears it."""
+        self.joints[joint]["mimic"] = None if reference is None else dict(reference=reference, coeffs=list(coeffs))
+
     def joint_dof(self, joint):
         return self.dofOf[joint]
 

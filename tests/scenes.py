@@ -288,3 +288,36 @@ def four_bar(seed=53):
                          child_xform=[0, 0, 0.15, 0, 0, 0, 1], q=[0.4])
     synth._add_quadruped(b, rng, [1.5, 0.0, 0.9])
     return b.finalize()
+
+
+def mimic_arms(seed=59):
+    """Mimic joints (set_joint_mimic): a fixed base with a PD-driven arm and a second arm that
+    follows it at q2 = 0.1 - q1, and a two-finger gripper whose second finger mirrors the first on
+    prismatic joints; the arms sweep through boxes resting on the ground."""
+    b = SceneBuilder(fps=240)
+    b.add_ground_plane(mu=0.8)
+    base = b.add_body(xform=[0.0, 0.0, 0.45, 0, 0, 0, 1])
+    b.add_shape_box(base, hx=0.05, hy=0.05, hz=0.05, mass=2.0)
+    b.add_joint_fixed(-1, base, parent_xform=[0.0, 0.0, 0.45, 0, 0, 0, 1])
+    arms = []
+    for side in (-1, 1):
+        arm = b.add_body(xform=[0.0, 0.12 * side, 0.25, 0, 0, 0, 1])
+        b.add_shape_capsule(arm, radius=0.03, half_height=0.17, mass=0.6)
+        arms.append(b.add_joint_revolute(base, arm, axis=[0, 1, 0], parent_xform=[0, 0.12 * side, 0, 0, 0, 0, 1],
+                                         child_xform=[0, 0, 0.2, 0, 0, 0, 1], targetKe=40.0, targetKd=2.0,
+                                         targetPos=0.9 if side < 0 else 0.0, limitLower=-1.5, limitUpper=1.5))
+    b.set_joint_mimic(arms[1], arms[0], coeffs=(0.1, -1.0))
+    fingers = []
+    for side in (-1, 1):
+        f = b.add_body(xform=[0.0, 0.04 * side, 0.36, 0, 0, 0, 1])
+        b.add_shape_box(f, hx=0.01, hy=0.01, hz=0.03, mass=0.1)
+        fingers.append(b.add_joint_prismatic(base, f, axis=[0, 1, 0], parent_xform=[0, 0.04 * side, -0.09, 0, 0, 0, 1],
+                                             targetKe=20.0, targetKd=1.0, targetPos=-0.02 * side, limitLower=-0.03,
+                                             limitUpper=0.03))
+    b.set_joint_mimic(fingers[1], fingers[0], coeffs=(0.0, -1.0))
+    rng = np.random.default_rng(seed)
+    for i in range(6):
+        bx = b.add_body(xform=[float(rng.uniform(-0.35, 0.35)), float(rng.uniform(-0.2, 0.2)), 0.05 + 0.11 * (i % 2),
+                               0, 0, 0, 1])
+        b.add_shape_box(bx, hx=0.05, hy=0.05, hz=0.05, mass=0.3)
+    return b.finalize()

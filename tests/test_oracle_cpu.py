@@ -218,3 +218,17 @@ def test_articulated_rolling_and_spin_friction(oracle_lib, opts):
     assert 0.2 < abs(on60[7]) < 0.8                 # rolling resistance mu_r N over 0.25 s
     assert np.linalg.norm(off150[3:6]) > 3.0        # the spinning one keeps spinning without it
     assert np.linalg.norm(on150[3:6]) < 0.1         # and stops with it
+
+
+def test_mimic_joints_follow_their_reference(oracle_lib):
+    """set_joint_mimic: the second arm holds q2 = 0.1 - q1 and the second finger q4 = -q3 while the
+    driven joints move (mimic rows in the dense pass)."""
+    from tests import scenes
+    pk = pack(scenes.mimic_arms())
+    assert pk.C["NMIMIC"] == 2
+    o = oracle_lib.OracleSim(pk)
+    o.step(60)
+    q = o.read("art")[pk.C["A_Q"]:pk.C["A_Q"] + pk.NQ]
+    assert q[0] > 0.2                       # the driven arm has moved toward its target
+    assert abs(q[1] - (0.1 - q[0])) < 2e-3
+    assert abs(q[2]) > 0.01 and abs(q[3] + q[2]) < 2e-3

@@ -28,7 +28,8 @@ SCENES = {"boxes": scenes.boxes, "mixed_prims": scenes.mixed_prims, "articulated
           "ang_art_relaxed": functools.partial(scenes.ang_art, relaxation=0.8),
           "four_bar": scenes.four_bar, "four_bar_cti": scenes.four_bar, "articulated_cti": scenes.articulated,
           "vel_limited_cti": scenes.vel_limited, "spin_roll_longest_first": scenes.spin_roll,
-          "spinners_longest_first": scenes.spinners, "articulated_longest_first": scenes.articulated}
+          "spinners_longest_first": scenes.spinners, "articulated_longest_first": scenes.articulated,
+          "mimic_arms": scenes.mimic_arms, "mimic_arms_cti": scenes.mimic_arms}
 # Packing options per scene: the FP64 articulated-inertia option on the articulation workload, PD
 # drives as solver rows (drive_mode "rows"; with velocity limits, the fused drive clamp), the three
 # coupled friction modes, and row_schedule "contact_then_internal" (all contact iterations, then
@@ -48,7 +49,8 @@ OPTS = {"chains_and_quads_fp64": {"solver": {"articulation_fp64": True}},
         "vel_limited_cti": {"solver": {"row_schedule": "contact_then_internal"}},
         "spin_roll_longest_first": {"solver": {"propagation_color_order": "longest_first"}},
         "spinners_longest_first": {"solver": {"propagation_color_order": "longest_first"}},
-        "articulated_longest_first": {"solver": {"propagation_color_order": "longest_first"}}}
+        "articulated_longest_first": {"solver": {"propagation_color_order": "longest_first"}},
+        "mimic_arms_cti": {"solver": {"row_schedule": "contact_then_internal"}}}
 
 
 def _pair_set(p):
