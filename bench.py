@@ -158,10 +158,11 @@ def scene_counts(batch, pks):
     return tot
 
 
-# DRAM bytes (read + write) per body and launch, from one ncu capture of the 64-scene uneven batch
-# (cold cache; profiles/narrow_prepare_solve_uneven_batch_64.md). Scaled by a batch's body count
-# for the bench line's roofline traffic; the narrow stage is k_narrow + k_narrow_jobs.
-NCU_TRAFFIC_PER_BODY = {"narrow": 1660.0, "prepare": 1264.0, "solve": 1346.0}
+# DRAM bytes (read + write) per body and launch, from one ncu capture of the 512-scene uneven batch
+# (80,090 bodies, the 128-thread kernel instances at the bench batch's blocks per SM; cold cache;
+# profiles/traffic_uneven_batch_512.md). Scaled by a batch's body count for the bench line's
+# roofline traffic; the narrow stage is k_narrow + k_narrow_jobs.
+NCU_TRAFFIC_PER_BODY = {"narrow": 2013.0, "prepare": 2180.0, "solve": 1646.0}
 
 
 def kernel_bytes(k: str, c: dict, rows_vec4: int, iterations: int) -> float:
@@ -405,7 +406,7 @@ def run_steel(args):
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": NCU_TRAFFIC_PER_BODY[dom] * nbodies if dom in NCU_TRAFFIC_PER_BODY else None,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of uneven_batch_64, "
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of uneven_batch_512, "
                                        "per body, scaled to this batch",
                      "algorithmic_bytes_per_launch": bytes_dom, "ms_per_launch": prof[dom],
                      "kernel_share": {k: round(v / total_ms, 4) for k, v in prof.items()}},
