@@ -161,6 +161,26 @@ def test_fp64_and_fp32_scenes_in_one_batch(steel, oracle_lib):
     assert not np.array_equal(_bits(g.poses(0)), _bits(g.poses(1))), "the option changed nothing"
 
 
+def test_extended_solve_instance_in_a_mixed_batch(steel, oracle_lib):
+    """A batch with an articulated torsional/rolling scene or a contact-then-internal scene runs the
+    extended solve instance for all its scenes; the plain scenes in it (and a longest-first one)
+    must still match their oracle bit for bit."""
+    pks = [pack(scenes.ang_art()), pack(scenes.four_bar(), opts={"solver": {"row_schedule": "contact_then_internal"}}),
+           pack(scenes.articulated()), pack(scenes.spin_roll(), opts={"solver": {"propagation_color_order": "longest_first"}}),
+           pack(scenes.mimic_arms())]
+    assert (pks[0].C["ANG_ART"], pks[1].C["CTI"], pks[3].C["LONGEST_FIRST"]) == (1, 1, 1)
+    g = Batch(pks)
+    orcs = [oracle_lib.OracleSim(pk) for pk in pks]
+    g.step(40)
+    for i, (pk, o) in enumerate(zip(pks, orcs)):
+        o.step(40)
+        assert np.array_equal(_bits(g.poses(i)), _bits(o.read("poses")[:pk.NB * 8])), f"scene {i} differs"
+        if pk.NQ:
+            _, _, gq, gqd, _ = g.raw_state(i)
+            oa = o.read("art")
+            assert np.array_equal(_bits(gqd), _bits(oa[pk.C["A_QD"]:pk.C["A_QD"] + pk.ND])), f"scene {i} qd differs"
+
+
 def test_sleeping_bit_exact(steel, oracle_lib):
     """Islands fall asleep, wake on contact and sleep again identically: poses, velocities, joint
     state, per-node (age, asleep) words and the asleep count every 20 frames over 320 frames."""
