@@ -159,9 +159,9 @@ def scene_counts(batch, pks):
 
 
 # DRAM bytes (read + write) per body and launch, from one ncu capture of the 512-scene uneven batch
-# (80,090 bodies, the 128-thread kernel instances at the bench batch's blocks per SM; cold cache;
-# profiles/traffic_uneven_batch_512.md). Scaled by a batch's body count for the bench line's
-# roofline traffic; the narrow stage is k_narrow + k_narrow_jobs.
+# (80,090 bodies, the 128-thread kernel instances at the bench batch's blocks per SM; cold cache).
+# Scaled by a batch's body count for the bench line's roofline traffic; the narrow stage is
+# k_narrow + k_narrow_jobs.
 NCU_TRAFFIC_PER_BODY = {"narrow": 2013.0, "prepare": 2180.0, "solve": 1646.0}
 
 

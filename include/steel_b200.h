@@ -26,6 +26,8 @@ extern "C" {
 #define STEEL_E_CUDA 4        /* CUDA runtime error */
 #define STEEL_E_NOMEM 5       /* device allocation failed */
 #define STEEL_E_NODEVICE 6    /* no CUDA device; the reference's UnsupportedError (device.js:2-9) */
+#define STEEL_E_TIMEOUT 7     /* a bounded device-side wait ran out (a shared-memory bulk copy); the scene's
+                                 work of that substep was skipped, so reset before trusting its state */
 
 typedef struct steel_ctx steel_ctx;
 typedef struct steel_batch steel_batch;
@@ -116,6 +118,14 @@ int steel_step_io(steel_batch* b, uint32_t frames, const float* targets, uint64_
 int steel_profile_kernels(steel_batch* b, uint32_t frames, float* ms_per_launch);
 /* Device time of the last steel_step_timed call's frames, in milliseconds (CUDA events). */
 int steel_step_timed(steel_batch* b, uint32_t frames, float* ms);
+/* Failure-path testing: the number of try_wait rounds the prepare and solve kernels give a
+   shared-memory bulk copy before they record STEEL_E_TIMEOUT. steel_batch_create sets
+   STEEL_WAIT_LIMIT_DEFAULT; 0 makes every staged scene's wait run out at once. After a timeout the
+   kernel still waits, with the default limit, for its copy in flight, skips the scene and
+   returns, so the context stays usable. No counterpart in the reference (WebGPU has no bounded
+   waits). */
+#define STEEL_WAIT_LIMIT_DEFAULT 16777216u
+int steel_debug_set_wait_limit(steel_batch* b, uint32_t rounds);
 
 /* Serving loop: continuous batching over the batch's scenes as resident instances. No direct
    counterpart in the reference; the closest is Sim.run (sim.js:705-712), which keeps up to four
@@ -145,8 +155,10 @@ int steel_serve_end(steel_batch* b);
    device (NULL: the default stream); the call only enqueues the work.
    The key scratch is a static device array of STEEL_NOALLOC_MAX_CONTACTS keys (1 MiB) that every
    GPU which loads this library holds until exit; n above that maximum fails with
-   STEEL_E_CAPACITY before anything is launched. The first call on a device looks up the array's
-   device address (set-up); make that first call before any stream capture. All calls on a device
+   STEEL_E_CAPACITY before anything is launched. The first call in each CUDA context (a device's
+   primary context, and again after cudaDeviceReset) looks up the array's device address (set-up)
+   and caches it with the context's id; make that first call before any stream capture. Up to 2048
+   padded keys sort in the kernel's static shared memory instead of the array. All calls on a device
    share the array: calls whose kernels overlap on the GPU race and corrupt each other's results,
    so order them (for example on one stream). */
 #define STEEL_NOALLOC_MAX_CONTACTS 65536

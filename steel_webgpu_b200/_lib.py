@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsteel_b200.so")
 
 STEEL_OK = 0
-ERRORS = {1: "invalid", 2: "unsupported", 3: "capacity", 4: "cuda", 5: "nomem", 6: "nodevice"}
+ERRORS = {1: "invalid", 2: "unsupported", 3: "capacity", 4: "cuda", 5: "nomem", 6: "nodevice", 7: "timeout"}
 
 
 class SteelError(RuntimeError):
@@ -68,6 +68,7 @@ SIGNATURES = {
     "steel_read_words": [_VP, _U32, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint64, _VP],
     "steel_layout_get": [_VP, _U32, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64)],
     "steel_step_timed": [_VP, _U32, ctypes.POINTER(_F32)],
+    "steel_debug_set_wait_limit": [_VP, _U32],
     "steel_step_io": [_VP, _U32, _VP, ctypes.c_uint64, _VP, ctypes.c_uint64],
     "steel_profile_kernels": [_VP, _U32, _VP],
     "steel_sort_contacts_noalloc": [_VP, _U32, _VP, _VP],

@@ -15,6 +15,7 @@
 
 #include "../../include/steel_b200.h"
 #include "batch.cuh"
+#include "bulk.cuh"
 
 using namespace steel;
 
@@ -299,9 +300,16 @@ int check_device_error(steel_batch* b) {
   CU(cudaStreamSynchronize(b->ctx->stream));
   if (e == ERR_SORT_CAPACITY) return fail(STEEL_E_CAPACITY, "contact sort capacity exceeded");
   if (e == ERR_JOB_CAPACITY) return fail(STEEL_E_CAPACITY, "narrowphase job capacity exceeded");
-  if (e == ERR_STAGE_TIMEOUT) return fail(STEEL_E_CUDA, "a shared-memory bulk copy did not complete");
+  if (e == ERR_STAGE_TIMEOUT)
+    return fail(STEEL_E_TIMEOUT, "a shared-memory bulk copy did not complete within its wait limit; the scene's "
+                                 "substep was skipped");
   if (e != 0) return fail(STEEL_E_CUDA, "device error " + std::to_string(e));
   return STEEL_OK;
+}
+
+void drop_graph(steel_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
 }
 
 SceneHost* scene_of(steel_batch* b, uint32_t s) { return (b && s < b->sc.size()) ? &b->sc[s] : nullptr; }
@@ -465,6 +473,8 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   bd.art_f64 = art_f64 != 0u ? 1u : 0u;
   bd.solve_ext = solve_ext != 0u ? 1u : 0u;
   bd.big = big ? 1u : 0u;
+  bd.wait_limit = STEEL_WAIT_LIMIT_DEFAULT;
+  static_assert(STEEL_WAIT_LIMIT_DEFAULT == BULK_WAIT_LIMIT, "one default wait limit");
   CU(configure_prepare(prep_smem));
   CU(configure_solve(solve_smem));
   CU(cudaMemcpyAsync(bd.scenes, dev.data(), sizeof(SceneDev) * n, cudaMemcpyHostToDevice, st));
@@ -511,6 +521,15 @@ int steel_reset(steel_batch* b) {
   int rc = upload_state(b);
   if (rc) return rc;
   CU(cudaStreamSynchronize(b->ctx->stream));
+  return STEEL_OK;
+}
+
+int steel_debug_set_wait_limit(steel_batch* b, uint32_t rounds) {
+  if (!b) return fail(STEEL_E_INVALID, "null batch");
+  CU(cudaSetDevice(b->ctx->device));
+  CU(cudaStreamSynchronize(b->ctx->stream));
+  b->bd.wait_limit = rounds;
+  drop_graph(b);  // the limit is a launch argument: capture again
   return STEEL_OK;
 }
 
@@ -573,8 +592,8 @@ int steel_step_io(steel_batch* b, uint32_t frames, const float* targets, uint64_
     launch_gather_poses(b->bd, (float*)(A + b->o_pose_buf), (const uint64_t*)(A + b->o_pose_off), st);
     CU(cudaMemcpyAsync(poses, A + b->o_pose_buf, 4ull * b->n_poses, cudaMemcpyDeviceToHost, st));
   }
-  CU(cudaStreamSynchronize(st));
-  return STEEL_OK;
+  CU(cudaGetLastError());
+  return check_device_error(b);  // synchronizes; reports a capacity or wait error raised by these frames
 }
 
 int steel_profile_kernels(steel_batch* b, uint32_t frames, float* ms_per_launch) {

@@ -27,6 +27,8 @@ struct BatchDev {
   uint32_t art_f64;           // some scene has ART_F64: launch the prepare instances that carry it
   uint32_t solve_ext;         // some scene has ANG_ART or CTI: launch the solve instances that carry them
   uint32_t big;               // prepare and solve run BIG_THREADS blocks (few scenes)
+  uint32_t wait_limit;        // try_wait rounds of a shared-memory bulk copy (BULK_WAIT_LIMIT unless a test
+                              // lowers it to make the bounded wait run out)
 };
 
 constexpr uint32_t BROAD_TILE = 32;

@@ -1285,12 +1285,9 @@ __global__ void __launch_bounds__(SORT_THREADS) k_csort(BatchDev B, uint32_t sme
   if (nc == 0u) return;
   uint32_t n2 = 1u;
   while (n2 < nc) n2 <<= 1u;
-  // Scenes whose keys do not fit the shared array sort in their global scratch.
+  // Scenes whose keys do not fit the shared array sort in their global scratch, which holds
+  // next_pow2(MAXC) >= n2 keys (nc <= MAXC).
   uint4* keys = n2 <= smem_keys ? sk : S.ckeys;
-  if (n2 > smem_keys && n2 > S.MAXC) {
-    if (threadIdx.x == 0) atomicCAS(B.error, 0u, (uint32_t)ERR_SORT_CAPACITY);
-    return;
-  }
   for (uint32_t q = threadIdx.x; q < n2; q += blockDim.x)
     keys[q] = q < nc ? contact_key(S.craw, q) : make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu);
   __syncthreads();

@@ -766,8 +766,10 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
   float* lb = staged ? reinterpret_cast<float*>(pb + lay.links) : S.art + S.A_LINK;
   // Link blocks into shared memory with one bulk copy (A_LINK is 16-byte aligned).
   __shared__ __align__(8) uint64_t stage_bar;
-  if (staged && !stage_to_shared(lb, S.art + S.A_LINK, 4u * S.NL * LBLK, &stage_bar) && tid == 0u)
-    atomicCAS(B.error, 0u, (uint32_t)ERR_STAGE_TIMEOUT);
+  if (staged && !stage_to_shared(lb, S.art + S.A_LINK, 4u * S.NL * LBLK, &stage_bar, B.wait_limit)) {
+    if (tid == 0u) atomicCAS(B.error, 0u, (uint32_t)ERR_STAGE_TIMEOUT);
+    return;  // the whole block: the result above is the same in every thread
+  }
   __syncthreads();
   const Params& P = Ps;
   Prep pr(S, P, lb);

@@ -8,13 +8,22 @@
 // for a library to allocate. Such a caller owns its input and output buffers and only needs the
 // sort. steel_sort_contacts_noalloc gives it that sort with its key scratch in a file-scope
 // __device__ array of fixed size (STEEL_NOALLOC_MAX_CONTACTS keys of 16 bytes, 1 MiB), which every
-// GPU that loads this library holds until the process exits. The call allocates nothing.
+// GPU that loads this library holds until the process exits. The call allocates nothing. Up to
+// NOALLOC_SMEM_KEYS padded keys sort in the kernel's static shared memory instead.
 //
 // The array is shared by every call on a device and keeps the last call's keys. Each launch
 // writes every key slot it later reads (real keys, then padding up to the next power of two)
 // before the sort reads any, so nothing has to start at zero. Calls whose kernels overlap on the
 // GPU (different streams, or several host threads) race on the array and corrupt each other's
 // output; the caller must order them, for example on one stream.
+//
+// The array's device address is looked up with cudaGetSymbolAddress once per CUDA context: the
+// first call made in a context (a device's primary context, again after cudaDeviceReset) does the
+// look-up, so make that first call before any stream capture. Later calls compare the current
+// context's id with the cached one (cuCtxGetId through the runtime's driver entry points) and reuse
+// the address.
+#include <cuda.h>
+
 #include <mutex>
 #include <string>
 
@@ -28,17 +37,21 @@ int set_last_error(int code, const std::string& msg);
 namespace {
 
 constexpr uint32_t NOALLOC_THREADS = 1024;
+constexpr uint32_t NOALLOC_SMEM_KEYS = 2048;  // 32 KiB of static shared memory
 constexpr int MAX_DEVICES = 64;
 
 static __device__ __align__(256) uint4 g_sort_scratch[STEEL_NOALLOC_MAX_CONTACTS];
 
 // Same order as k_csort: keys of the n raw records (record c at raw[5c..5c+4], its shape-mu vec4
 // at raw[5n + c]), bitonic sort of the power-of-two padded key array, then a gather of the
-// records in key order. One block; `keys` is the device address of g_sort_scratch.
+// records in key order. One block; `gkeys` is the device address of g_sort_scratch, used when the
+// padded keys do not fit the block's shared array.
 __global__ void __launch_bounds__(NOALLOC_THREADS)
-    k_csort_noalloc(const float4* __restrict__ raw, uint32_t nc, float4* __restrict__ out, uint4* keys) {
+    k_csort_noalloc(const float4* __restrict__ raw, uint32_t nc, float4* __restrict__ out, uint4* gkeys) {
+  __shared__ uint4 sk[NOALLOC_SMEM_KEYS];
   uint32_t n2 = 1u;
   while (n2 < nc) n2 <<= 1u;
+  uint4* keys = n2 <= NOALLOC_SMEM_KEYS ? sk : gkeys;
   for (uint32_t q = threadIdx.x; q < n2; q += blockDim.x)
     keys[q] = q < nc ? contact_key(raw, q) : make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu);
   __syncthreads();
@@ -61,21 +74,56 @@ __global__ void __launch_bounds__(NOALLOC_THREADS)
 }
 
 std::mutex g_setup_mu;
-uint4* g_scratch_ptr[MAX_DEVICES] = {};
+struct ScratchSlot {
+  unsigned long long ctx_id = 0;  // cuCtxGetId of the context the address belongs to (ids start at 1)
+  uint4* ptr = nullptr;
+};
+ScratchSlot g_scratch[MAX_DEVICES];
 
-// Device address of g_sort_scratch on `dev`, which must be the current device. Looked up once per
-// device (the first call on that device) and cached.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Id of the calling thread's current context (0 when it cannot be read).
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+    (void)cudaGetLastError();
+  });
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Device address of g_sort_scratch on `dev`, which must be the current device. Looked up in the
+// first call of each context and cached with the context's id; a new context (after
+// cudaDeviceReset, or a primary context released and retained again) looks it up again. When the
+// id cannot be read the address is looked up on every call.
 int scratch_address(int dev, uint4** out) {
   std::lock_guard<std::mutex> lock(g_setup_mu);
-  if (!g_scratch_ptr[dev]) {
+  const unsigned long long id = current_context_id();
+  ScratchSlot& slot = g_scratch[dev];
+  if (!slot.ptr || id == 0 || slot.ctx_id != id) {
     uint4* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress((void**)&p, g_sort_scratch);
     if (e != cudaSuccess)
       return set_last_error(STEEL_E_CUDA, std::string("steel_sort_contacts_noalloc: scratch address: ") +
                                                cudaGetErrorString(e));
-    g_scratch_ptr[dev] = p;
+    slot.ptr = p;
+    slot.ctx_id = id;
   }
-  *out = g_scratch_ptr[dev];
+  *out = slot.ptr;
   return STEEL_OK;
 }
 

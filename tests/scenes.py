@@ -321,3 +321,21 @@ def mimic_arms(seed=59):
                                0, 0, 0, 1])
         b.add_shape_box(bx, hx=0.05, hy=0.05, hz=0.05, mass=0.3)
     return b.finalize()
+
+
+def controlled(seed=61):
+    """The user-control surface: two PD-driven quadrupeds and a hanging revolute chain (joint
+    targets and forces), plus free boxes on the plane and one in the air (body wrench, pose and
+    twist)."""
+    rng = np.random.default_rng(seed)
+    b = SceneBuilder(fps=240, box_hulls="direct")
+    b.add_ground_plane(mu=0.7)
+    synth._add_quadruped(b, rng, [0.0, 0.0, 0.9])
+    synth._add_quadruped(b, rng, [1.5, 0.0, 0.9])
+    synth._add_chain(b, rng, [3.0, 0.0, 2.2], 6, ratio_max=10.0)
+    for i in range(3):
+        body = b.add_body(xform=[-1.0 - 0.5 * i, 0.5, 0.101, 0, 0, 0, 1])
+        b.add_shape_box(body, hx=0.1, hy=0.1, hz=0.1, mu=0.6)
+    body = b.add_body(xform=[-2.0, -1.0, 1.5, 0, 0, 0, 1])
+    b.add_shape_box(body, hx=0.08, hy=0.12, hz=0.1, mu=0.6)
+    return b.finalize()

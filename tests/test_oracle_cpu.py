@@ -14,7 +14,9 @@ from steel_webgpu_b200 import SceneBuilder, pack
 from tests import scenes
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "oracle_fixtures.npz")
-REF_SCENES = "/root/reference/assets/scenes"
+# The reference's assets/scenes folder when it is checked out (STEEL_REFERENCE_SCENES); otherwise
+# the packed copies that tests/golden/make_reference_scenes.py wrote.
+REF_SCENES = os.environ.get("STEEL_REFERENCE_SCENES", "")
 
 
 def test_trig_accuracy(oracle_lib):
@@ -120,16 +122,23 @@ def test_longest_first_color_order(oracle_lib):
     assert not np.array_equal(p_lf, p_co)
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_SCENES), reason="reference scene folders not on disk")
+def _reference_scenes_packed():
+    from tests import refscenes
+    if REF_SCENES and os.path.isdir(REF_SCENES):
+        from steel_webgpu_b200.builder import load_scene
+        names = sorted(d for d in os.listdir(REF_SCENES) if os.path.exists(os.path.join(REF_SCENES, d, "scene.json")))
+        return [(n, pack(load_scene(os.path.join(REF_SCENES, n)))) for n in names]
+    return [(n, refscenes.load(n)) for n in refscenes.names()]
+
+
+@pytest.mark.skipif(not (REF_SCENES and os.path.isdir(REF_SCENES)) and not os.path.isdir(
+    os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "_ref")),
+                    reason="neither the reference scene folders nor their packed copies are on disk")
 def test_reference_scenes_load_and_pack(oracle_lib):
-    from steel_webgpu_b200.builder import load_scene
-    names = sorted(d for d in os.listdir(REF_SCENES) if os.path.exists(os.path.join(REF_SCENES, d, "scene.json")))
-    assert len(names) >= 40
-    packed = []
-    for name in names:
-        pk = pack(load_scene(os.path.join(REF_SCENES, name)))
-        assert pk.statF.size == pk.C["LEN_STATF4"] * 4 and pk.statU.size == pk.C["LEN_STATU"]
-        packed.append((name, pk))
+    packed = _reference_scenes_packed()
+    assert len(packed) >= 40
+    for name, pk in packed:
+        assert pk.statF.size == pk.C["LEN_STATF4"] * 4 and pk.statU.size == pk.C["LEN_STATU"], name
     for name, pk in packed:
         o = oracle_lib.OracleSim(pk)
         o.step(5)
