@@ -88,6 +88,10 @@ struct SceneHost {
   // arena offsets
   size_t o_sf, o_su, o_pos, o_rot, o_ppos, o_prot, o_lv, o_av, o_spos, o_srot, o_alo, o_ahi, o_art, o_cnt, o_stats,
       o_params, o_craw, o_con, o_ckeys, o_rows, o_slots, o_warm, o_sched, o_tw, o_imp, o_aqd, o_tscr;
+  // Device-wide radix sort of a scene whose padded keys may exceed the block sort's shared array.
+  bool large_sort = false;
+  uint32_t sort_tiles = 0;
+  size_t o_rkeys1 = 0, o_rstat = 0, o_rhist = 0, o_rctr = 0;
   size_t art_floats = 0, sched_words = 0, warm_words = 0, tscr_floats = 0;
   std::vector<float> statF;
   std::vector<uint32_t> statU;
@@ -114,6 +118,7 @@ struct steel_batch {
   uint32_t narrow_blocks = 0;
   uint32_t debug_substep = 0;  // substep cursor of steel_debug_stage
   size_t sort_keys = 0;
+  std::vector<RadixDev> radix;  // large scenes' device-wide contact sorts
   bool use_graph = true;
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -247,7 +252,15 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, uint32_t th
   s.o_art = L.take(s.art_floats * 4);
   s.o_cnt = L.take(64); s.o_stats = L.take(64); s.o_params = L.take(sizeof(Params));
   s.o_craw = L.take((size_t)MAXC * 6 * 16); s.o_con = L.take((size_t)MAXC * 6 * 16);
-  s.o_ckeys = L.take(next_pow2(MAXC) * 16);
+  s.large_sort = next_pow2(MAXC) > SORT_SMEM_KEYS;
+  s.o_ckeys = L.take(s.large_sort ? (size_t)MAXC * 16 : 16);
+  if (s.large_sort) {
+    s.sort_tiles = (MAXC + RS_TILE - 1u) / RS_TILE;
+    s.o_rkeys1 = L.take((size_t)MAXC * 16);
+    s.o_rstat = L.take(4ull * RS_DIGITS * s.sort_tiles * 256u);
+    s.o_rhist = L.take(4ull * RS_DIGITS * 256u);
+    s.o_rctr = L.take(4ull * RS_DIGITS);
+  }
   s.o_rows = L.take((size_t)MAXC * d.ROWS * 16); s.o_slots = L.take((size_t)MAXC * 2 * 16);
   s.o_warm = L.take(s.warm_words * 4);
   s.o_sched = L.take(s.sched_words * 4);
@@ -287,7 +300,7 @@ void enqueue_substeps(steel_batch* b, cudaStream_t st) {
     launch_shapes(bd, st);
     launch_broad(bd, st);
     launch_narrow(bd, b->narrow_blocks, st);
-    launch_csort(bd, b->sort_keys, st);
+    launch_csort(bd, b->sort_keys, b->radix.data(), (uint32_t)b->radix.size(), st);
     launch_prepare(bd, st);
     launch_solve(bd, st);
   }
@@ -300,6 +313,8 @@ int check_device_error(steel_batch* b) {
   CU(cudaStreamSynchronize(b->ctx->stream));
   if (e == ERR_SORT_CAPACITY) return fail(STEEL_E_CAPACITY, "contact sort capacity exceeded");
   if (e == ERR_JOB_CAPACITY) return fail(STEEL_E_CAPACITY, "narrowphase job capacity exceeded");
+  if (e == ERR_SORT_TIMEOUT)
+    return fail(STEEL_E_TIMEOUT, "the contact radix sort's look-back gave up waiting for a preceding tile");
   if (e == ERR_STAGE_TIMEOUT)
     return fail(STEEL_E_TIMEOUT, "a shared-memory bulk copy did not complete within its wait limit; the scene's "
                                  "substep was skipped");
@@ -425,6 +440,17 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
     d.tw = at<float4>(A, s.o_tw); d.imp = at<float4>(A, s.o_imp); d.aqd = at<float>(A, s.o_aqd);
     d.tscr = at<float>(A, s.o_tscr);
     d.scene_index = i;
+    if (s.large_sort) {
+      RadixDev r{};
+      r.keys[0] = d.ckeys;
+      r.keys[1] = at<uint4>(A, s.o_rkeys1);
+      r.status = at<uint32_t>(A, s.o_rstat);
+      r.hist = at<uint32_t>(A, s.o_rhist);
+      r.ctr = at<uint32_t>(A, s.o_rctr);
+      r.tiles = s.sort_tiles;
+      r.scene = i;
+      b->radix.push_back(r);
+    }
     d.stage = 0u;
     if (d.NL > 0u && 4ull * d.NL * 268u <= STAGE_LINK_CAP) d.stage |= STAGE_LINKS;
     if (64ull * d.NB <= STAGE_BODY_CAP) d.stage |= STAGE_BODIES;
@@ -484,7 +510,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   CU(cudaMemcpyAsync(A + b->o_tgt_off, tgt_off.data(), 8ull * n, cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(A + b->o_pose_off, pose_off.data(), 8ull * n, cudaMemcpyHostToDevice, st));
   b->narrow_blocks = (uint32_t)ctx->sms * (uint32_t)narrow_blocks_per_sm();
-  b->sort_keys = std::min<size_t>(next_pow2(max_c), 8192);
+  b->sort_keys = std::min<size_t>(next_pow2(max_c), SORT_SMEM_KEYS);
   CU(configure_sort(b->sort_keys));
   CU(cudaEventCreate(&b->ev0));
   CU(cudaEventCreate(&b->ev1));
@@ -611,7 +637,7 @@ int steel_profile_kernels(steel_batch* b, uint32_t frames, float* ms_per_launch)
       CU(cudaEventRecord(e[2], st)); launch_shapes(b->bd, st); CU(cudaEventRecord(e[3], st));
       CU(cudaEventRecord(e[4], st)); launch_broad(b->bd, st); CU(cudaEventRecord(e[5], st));
       CU(cudaEventRecord(e[6], st)); launch_narrow(b->bd, b->narrow_blocks, st); CU(cudaEventRecord(e[7], st));
-      CU(cudaEventRecord(e[8], st)); launch_csort(b->bd, b->sort_keys, st); CU(cudaEventRecord(e[9], st));
+      CU(cudaEventRecord(e[8], st)); launch_csort(b->bd, b->sort_keys, b->radix.data(), (uint32_t)b->radix.size(), st); CU(cudaEventRecord(e[9], st));
       CU(cudaEventRecord(e[10], st)); launch_prepare(b->bd, st); CU(cudaEventRecord(e[11], st));
       CU(cudaEventRecord(e[12], st)); launch_solve(b->bd, st); CU(cudaEventRecord(e[13], st));
     }
@@ -746,7 +772,7 @@ int steel_collide(steel_batch* b) {
   launch_shapes(b->bd, st);
   launch_broad(b->bd, st);
   launch_narrow(b->bd, b->narrow_blocks, st);
-  launch_csort(b->bd, b->sort_keys, st);
+  launch_csort(b->bd, b->sort_keys, b->radix.data(), (uint32_t)b->radix.size(), st);
   CU(cudaGetLastError());
   int rc = steel_sync(b);
   if (rc) return rc;
@@ -770,7 +796,7 @@ int steel_debug_stage(steel_batch* b, int stage) {
     launch_shapes(b->bd, st);
     launch_broad(b->bd, st);
     launch_narrow(b->bd, b->narrow_blocks, st);
-    launch_csort(b->bd, b->sort_keys, st);
+    launch_csort(b->bd, b->sort_keys, b->radix.data(), (uint32_t)b->radix.size(), st);
   } else if (stage == 1) {
     launch_prepare(b->bd, st);
   } else if (stage == 2) {

@@ -44,7 +44,28 @@ constexpr int SOLVE_THREADS = 128;
 constexpr int BIG_THREADS = 512;
 
 // Device error codes written to BatchDev::error.
-enum : uint32_t { ERR_NONE = 0, ERR_SORT_CAPACITY = 1, ERR_JOB_CAPACITY = 2, ERR_STAGE_TIMEOUT = 3 };
+enum : uint32_t { ERR_NONE = 0, ERR_SORT_CAPACITY = 1, ERR_JOB_CAPACITY = 2, ERR_STAGE_TIMEOUT = 3, ERR_SORT_TIMEOUT = 4 };
+
+// Contact sort of scenes whose padded keys may exceed the block sort's shared array
+// (next_pow2(MAXC) > SORT_SMEM_KEYS): a device-wide LSD radix sort, onesweep style (one histogram
+// pass over all digits, then one launch per 8-bit digit that ranks a tile, looks back over the
+// preceding tiles' bucket counts and scatters). Keys are (pair, feature, point-bit hash) with the
+// raw index carried along; stable passes from the least significant digit give the lexicographic
+// order of (pair, feature, hash, raw index).
+constexpr uint32_t SORT_SMEM_KEYS = 8192;   // largest padded key count k_csort sorts in shared memory
+constexpr uint32_t RS_THREADS = 256;
+constexpr uint32_t RS_ITEMS = 16;           // keys per thread and tile
+constexpr uint32_t RS_TILE = RS_THREADS * RS_ITEMS;
+constexpr uint32_t RS_DIGITS = 12;          // 96 key bits, 8 per digit
+constexpr uint32_t RS_SPIN_LIMIT = 1u << 22;  // polls of a preceding tile's status before giving up
+struct RadixDev {
+  uint4* keys[2];     // ping-pong key buffers [MAXC] (x pair, y feature, z hash, w raw index)
+  uint32_t* status;   // [RS_DIGITS][tiles][256] look-back words: bits 30-31 flag (1 tile count, 2 prefix)
+  uint32_t* hist;     // [RS_DIGITS][256] bucket counts of all keys
+  uint32_t* ctr;      // [RS_DIGITS] tile tickets
+  uint32_t tiles;     // tiles of MAXC keys
+  uint32_t scene;
+};
 
 // Shared-memory staging of a scene inside k_prepare / k_solve. A scene is staged when its part
 // fits the cap; the launch's dynamic shared memory is the largest staged scene's need.
@@ -107,7 +128,7 @@ void launch_shapes(const BatchDev& b, cudaStream_t st);
 void launch_broad(const BatchDev& b, cudaStream_t st);
 void launch_narrow(const BatchDev& b, uint32_t narrow_blocks, cudaStream_t st);
 int narrow_blocks_per_sm();
-void launch_csort(const BatchDev& b, size_t smem_keys, cudaStream_t st);
+void launch_csort(const BatchDev& b, size_t smem_keys, const RadixDev* radix, uint32_t nradix, cudaStream_t st);
 cudaError_t configure_sort(size_t smem_keys);
 cudaError_t configure_prepare(size_t smem_bytes);
 cudaError_t configure_solve(size_t smem_bytes);

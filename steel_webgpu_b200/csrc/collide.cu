@@ -8,6 +8,8 @@
 // pairs of every scene of the batch go to one compacted list (warp-aggregated atomics); the
 // narrowphase runs one warp per pair with shuffle reductions over faces, edge pairs and
 // support points; each scene's contacts are sorted by one block.
+#include <algorithm>
+
 #include "batch.cuh"
 #include "contact_key.cuh"
 
@@ -1275,8 +1277,9 @@ __global__ void __launch_bounds__(NARROW_JOB_THREADS, 4) k_narrow_jobs(BatchDev 
 }
 
 // --------------------------------------------------------------------------------------------
-// Canonical contact sort (wgsl.js:3899-3982): key (pair, feature key, point-bit hash, raw index),
-// one block per scene, bitonic sort over a power-of-two key array in shared memory.
+// Canonical contact sort (wgsl.js:3899-3982): key (pair, feature key, point-bit hash, raw index).
+// Scenes whose padded keys fit the shared array sort there, one block per scene, with a bitonic
+// network; larger scenes are left to the device-wide radix sort below.
 __global__ void __launch_bounds__(SORT_THREADS) k_csort(BatchDev B, uint32_t smem_keys) {
   extern __shared__ uint4 sk[];
   if (B.active[blockIdx.x] == 0u) return;
@@ -1285,9 +1288,8 @@ __global__ void __launch_bounds__(SORT_THREADS) k_csort(BatchDev B, uint32_t sme
   if (nc == 0u) return;
   uint32_t n2 = 1u;
   while (n2 < nc) n2 <<= 1u;
-  // Scenes whose keys do not fit the shared array sort in their global scratch, which holds
-  // next_pow2(MAXC) >= n2 keys (nc <= MAXC).
-  uint4* keys = n2 <= smem_keys ? sk : S.ckeys;
+  if (n2 > smem_keys) return;  // the radix sort's scene
+  uint4* keys = sk;
   for (uint32_t q = threadIdx.x; q < n2; q += blockDim.x)
     keys[q] = q < nc ? contact_key(S.craw, q) : make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu);
   __syncthreads();
@@ -1303,6 +1305,183 @@ __global__ void __launch_bounds__(SORT_THREADS) k_csort(BatchDev B, uint32_t sme
   }
   for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) {
     uint32_t c = keys[i].w;
+#pragma unroll
+    for (uint32_t q = 0; q < 5u; q++) S.con[i * 5u + q] = S.craw[c * 5u + q];
+    S.con[S.MAXC * 5u + i] = S.craw[S.MAXC * 5u + c];
+  }
+}
+
+// --- device-wide radix sort of one large scene's contact keys ----------------------------------
+// Digit d (0 = least significant) of a key: byte d % 4 of word d / 4 counted from the hash.
+SD uint32_t rs_digit(const uint4& k, uint32_t d) {
+  const uint32_t w = d >> 2u;
+  const uint32_t word = w == 0u ? k.z : (w == 1u ? k.y : k.x);
+  return (word >> (8u * (d & 3u))) & 255u;
+}
+// The scene's contact count; `here` when this sort (not k_csort's shared array) handles it.
+SD uint32_t rs_count(const BatchDev& B, const RadixDev& R, uint32_t smem_keys, bool& here) {
+  const SceneDev& S = B.scenes[R.scene];
+  const uint32_t nc = min(S.counters[1], S.MAXC);
+  uint32_t n2 = 1u;
+  while (n2 < nc) n2 <<= 1u;
+  here = B.active[R.scene] != 0u && n2 > smem_keys;
+  return nc;
+}
+// Whether digit d leaves the order as it is (one bucket holds every key), decided by the whole
+// block from the key histogram (RS_THREADS == 256 buckets, one per thread).
+SD bool rs_trivial(const RadixDev& R, uint32_t d, uint32_t nc) {
+  return __syncthreads_or(R.hist[d * 256u + threadIdx.x] == nc) != 0;
+}
+// Index of the buffer that holds the keys before digit d: the non-trivial digits below d flip it.
+SD uint32_t rs_source(const RadixDev& R, uint32_t d, uint32_t nc) {
+  uint32_t cur = 0u;
+  for (uint32_t e = 0; e < d; e++) cur ^= rs_trivial(R, e, nc) ? 0u : 1u;
+  return cur;
+}
+
+__global__ void k_rsort_clear(RadixDev R) {
+  const uint32_t n = RS_DIGITS * R.tiles * 256u;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) R.status[i] = 0u;
+  if (blockIdx.x == 0u) {
+    for (uint32_t i = threadIdx.x; i < RS_DIGITS * 256u; i += blockDim.x) R.hist[i] = 0u;
+    if (threadIdx.x < RS_DIGITS) R.ctr[threadIdx.x] = 0u;
+  }
+}
+
+// Keys of one tile into keys[0], and their bucket counts for every digit into the histogram.
+__global__ void __launch_bounds__(RS_THREADS) k_rsort_init(BatchDev B, RadixDev R, uint32_t smem_keys) {
+  __shared__ uint32_t h[RS_DIGITS * 256u];
+  bool here;
+  const uint32_t nc = rs_count(B, R, smem_keys, here);
+  if (!here || blockIdx.x * RS_TILE >= nc) return;
+  const SceneDev& S = B.scenes[R.scene];
+  for (uint32_t i = threadIdx.x; i < RS_DIGITS * 256u; i += RS_THREADS) h[i] = 0u;
+  __syncthreads();
+  for (uint32_t r = 0; r < RS_ITEMS; r++) {
+    const uint32_t i = blockIdx.x * RS_TILE + r * RS_THREADS + threadIdx.x;
+    if (i >= nc) break;
+    const uint4 k = contact_key(S.craw, i);
+    R.keys[0][i] = k;
+#pragma unroll
+    for (uint32_t d = 0; d < RS_DIGITS; d++) atomicAdd(&h[d * 256u + rs_digit(k, d)], 1u);
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < RS_DIGITS * 256u; i += RS_THREADS)
+    if (h[i]) atomicAdd(&R.hist[i], h[i]);
+}
+
+// One stable pass over digit d. A block takes the next tile ticket, ranks its keys within the tile
+// (tile order = raw order within the tile: round, then warp, then lane), publishes its bucket
+// counts, sums the counts of the tiles before it (decoupled look-back, bounded polls) and
+// scatters every key to bucket start + preceding tiles' keys in that bucket + its rank.
+__global__ void __launch_bounds__(RS_THREADS) k_rsort_pass(BatchDev B, RadixDev R, uint32_t d, uint32_t smem_keys) {
+  __shared__ uint32_t warp_cnt[RS_THREADS / 32u][256];
+  __shared__ uint32_t warp_off[RS_THREADS / 32u][256];
+  __shared__ uint32_t tile_cnt[256];
+  __shared__ uint32_t dst_off[256];
+  __shared__ uint32_t wsum[RS_THREADS / 32u];
+  __shared__ uint32_t ticket;
+  bool here;
+  const uint32_t nc = rs_count(B, R, smem_keys, here);
+  const uint32_t ntiles = (nc + RS_TILE - 1u) / RS_TILE;
+  if (!here || blockIdx.x >= ntiles) return;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5u;
+  const uint32_t cur = rs_source(R, d, nc);
+  if (rs_trivial(R, d, nc)) return;
+  if (tid == 0u) ticket = atomicAdd(&R.ctr[d], 1u);
+  for (uint32_t w = 0; w < RS_THREADS / 32u; w++) warp_cnt[w][tid] = 0u;
+  tile_cnt[tid] = 0u;
+  __syncthreads();
+  const uint32_t t = ticket;
+  if (t >= ntiles) {  // more tickets than tiles: the counters were not cleared
+    if (tid == 0u) atomicCAS(B.error, 0u, (uint32_t)ERR_SORT_TIMEOUT);
+    return;
+  }
+  const uint4* src = cur ? R.keys[1] : R.keys[0];
+  uint4* dst = cur ? R.keys[0] : R.keys[1];
+  uint4 k[RS_ITEMS];
+  uint32_t rank[RS_ITEMS];
+  const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+  for (uint32_t r = 0; r < RS_ITEMS; r++) {
+    const uint32_t i = t * RS_TILE + r * RS_THREADS + tid;
+    const bool valid = i < nc;
+    k[r] = valid ? src[i] : make_uint4(0u, 0u, 0u, 0u);
+    const uint32_t dig = valid ? rs_digit(k[r], d) : 256u;
+    const uint32_t peers = __match_any_sync(0xffffffffu, dig);
+    const uint32_t below = __popc(peers & lt);
+    if (valid && below == 0u) warp_cnt[warp][dig] = __popc(peers);
+    __syncthreads();
+    // Bucket tid: offsets of each warp's keys after the earlier rounds and warps.
+    uint32_t run = tile_cnt[tid];
+#pragma unroll
+    for (uint32_t w = 0; w < RS_THREADS / 32u; w++) {
+      const uint32_t c = warp_cnt[w][tid];
+      warp_off[w][tid] = run;
+      run += c;
+      warp_cnt[w][tid] = 0u;
+    }
+    tile_cnt[tid] = run;
+    __syncthreads();
+    rank[r] = valid ? warp_off[warp][dig] + below : 0u;
+  }
+  // Publish this tile's counts (tile 0: already the inclusive prefix), then look back.
+  const uint32_t cnt = tile_cnt[tid];
+  volatile uint32_t* st = R.status + ((size_t)d * R.tiles) * 256u;
+  st[(size_t)t * 256u + tid] = (t == 0u ? 2u << 30 : 1u << 30) | cnt;
+  uint32_t excl = 0u;
+  if (t > 0u) {
+    uint32_t p = t - 1u;
+    for (;;) {
+      uint32_t w = 0u, polls = 0u;
+      do { w = st[(size_t)p * 256u + tid]; } while ((w >> 30) == 0u && ++polls < RS_SPIN_LIMIT);
+      if ((w >> 30) == 0u) {
+        atomicCAS(B.error, 0u, (uint32_t)ERR_SORT_TIMEOUT);
+        break;
+      }
+      excl += w & 0x3fffffffu;
+      if ((w >> 30) == 2u || p == 0u) break;
+      p--;
+    }
+    st[(size_t)t * 256u + tid] = (2u << 30) | (excl + cnt);
+  }
+  // Bucket starts over all keys (exclusive scan of the digit's histogram).
+  const uint32_t hv = R.hist[d * 256u + tid];
+  uint32_t incl = hv;
+#pragma unroll
+  for (uint32_t o = 1; o < 32u; o <<= 1u) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31u) wsum[warp] = incl;
+  __syncthreads();
+  uint32_t wbase = 0u;
+  for (uint32_t w = 0; w < warp; w++) wbase += wsum[w];
+  dst_off[tid] = wbase + incl - hv + excl;
+  __syncthreads();
+#pragma unroll
+  for (uint32_t r = 0; r < RS_ITEMS; r++) {
+    const uint32_t i = t * RS_TILE + r * RS_THREADS + tid;
+    if (i >= nc) continue;
+    const uint32_t j = dst_off[rs_digit(k[r], d)] + rank[r];
+    if (j < nc) dst[j] = k[r];
+    else atomicCAS(B.error, 0u, (uint32_t)ERR_SORT_TIMEOUT);  // inconsistent counts: never write past nc
+  }
+}
+
+// The records in sorted order: contact i of the output is raw contact keys[i].w.
+__global__ void __launch_bounds__(RS_THREADS) k_rsort_gather(BatchDev B, RadixDev R, uint32_t smem_keys) {
+  bool here;
+  const uint32_t nc = rs_count(B, R, smem_keys, here);
+  if (!here || blockIdx.x * RS_THREADS >= nc) return;
+  const SceneDev& S = B.scenes[R.scene];
+  const uint4* keys = rs_source(R, RS_DIGITS, nc) ? R.keys[1] : R.keys[0];
+  for (uint32_t i = blockIdx.x * RS_THREADS + threadIdx.x; i < nc; i += gridDim.x * RS_THREADS) {
+    const uint32_t c = keys[i].w;
+    if (c >= nc) {
+      atomicCAS(B.error, 0u, (uint32_t)ERR_SORT_TIMEOUT);
+      continue;
+    }
 #pragma unroll
     for (uint32_t q = 0; q < 5u; q++) S.con[i * 5u + q] = S.craw[c * 5u + q];
     S.con[S.MAXC * 5u + i] = S.craw[S.MAXC * 5u + c];
@@ -1355,8 +1534,16 @@ void launch_narrow(const BatchDev& b, uint32_t narrow_blocks, cudaStream_t st) {
 cudaError_t configure_sort(size_t smem_keys) {
   return cudaFuncSetAttribute(k_csort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smem_keys * sizeof(uint4)));
 }
-void launch_csort(const BatchDev& b, size_t smem_keys, cudaStream_t st) {
+void launch_csort(const BatchDev& b, size_t smem_keys, const RadixDev* radix, uint32_t nradix, cudaStream_t st) {
   k_csort<<<b.nscenes, SORT_THREADS, smem_keys * sizeof(uint4), st>>>(b, (uint32_t)smem_keys);
+  for (uint32_t k = 0; k < nradix; k++) {
+    const RadixDev& R = radix[k];
+    const uint32_t sk = (uint32_t)smem_keys;
+    k_rsort_clear<<<std::min<uint32_t>(R.tiles * 4u, 592u), 256, 0, st>>>(R);
+    k_rsort_init<<<R.tiles, RS_THREADS, 0, st>>>(b, R, sk);
+    for (uint32_t d = 0; d < RS_DIGITS; d++) k_rsort_pass<<<R.tiles, RS_THREADS, 0, st>>>(b, R, d, sk);
+    k_rsort_gather<<<std::min<uint32_t>(R.tiles * RS_ITEMS, 1184u), RS_THREADS, 0, st>>>(b, R, sk);
+  }
 }
 
 }  // namespace steel

@@ -339,3 +339,19 @@ def controlled(seed=61):
     body = b.add_body(xform=[-2.0, -1.0, 1.5, 0, 0, 0, 1])
     b.add_shape_box(body, hx=0.08, hy=0.12, hz=0.1, mu=0.6)
     return b.finalize()
+
+
+def box_carpet(n=2200, seed=67, spacing=0.35):
+    """n small boxes in a grid, each resting 1 mm into the plane and too far apart to touch: four
+    plane contacts per box, so the contact count passes the block sort's 8192 shared-memory keys
+    and the radix sort runs."""
+    rng = np.random.default_rng(seed)
+    b = SceneBuilder(fps=240, box_hulls="direct")
+    b.add_ground_plane(mu=0.6)
+    side = int(math.ceil(math.sqrt(n)))
+    for i in range(n):
+        x, y = (i % side - side / 2) * spacing, (i // side - side / 2) * spacing
+        h = float(rng.uniform(0.03, 0.05))
+        body = b.add_body(xform=[x, y, h - 0.001, 0, 0, 0, 1])
+        b.add_shape_box(body, hx=h, hy=h, hz=h, mu=0.6)
+    return b.finalize()
