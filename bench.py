@@ -336,6 +336,15 @@ def run_steel(args):
     nbodies = sum(pk.NB for pk in pks)
     iterations = pks[0].params["iterations"]
     substeps = pks[0].params["substeps"]
+    # Tile configuration: the autotuner's short timed search (it resets the batch afterwards), or
+    # the configuration given on the command line. Outside the timed region.
+    t_tune = time.perf_counter()
+    if args.tiles == "auto":
+        tiles, tune_ms = batch.autotune(args.tune_frames)
+    else:
+        batch.set_tiles(*[int(x) for x in args.tiles.split(",")])
+        tiles, tune_ms = batch.tiles(), None
+    tune_s = time.perf_counter() - t_tune
     batch.step(max(args.warmup, 3))
     batch.sync()
     barrier(world)
@@ -395,6 +404,8 @@ def run_steel(args):
                    "graph": True, "l2": "per-scene state is resident and re-read every substep; no L2 flush",
                    "contact_steps_per_s": world * counts["contacts"] * substeps * args.steps / (ms / 1000.0),
                    "build_s": round(build_s, 1), "overflow_scenes": overflow_scenes,
+                   "tiles": dict(tiles, source="autotuner" if args.tiles == "auto" else "command line",
+                                 tuning_ms_per_frame=tune_ms, tuning_s=round(tune_s, 2)),
                    "frame_latency_ms": {"p50": float(np.percentile(frame_ms, 50)),
                                         "p99": float(np.percentile(frame_ms, 99)),
                                         "what": "one frame of the whole batch through steel_step_io, host clock"},
@@ -476,6 +487,9 @@ def main():
     ap.add_argument("--ref-scenes", type=int, default=128)
     ap.add_argument("--plain-scenes", type=int, default=16)
     ap.add_argument("--mode", default="bench", choices=["bench", "serve"])
+    ap.add_argument("--tiles", default="auto",
+                    help='"auto" (autotuner) or block_threads,smem_budget,narrow_blocks_per_sm')
+    ap.add_argument("--tune-frames", type=int, default=3)
     ap.add_argument("--serve-instances", type=int, default=512)
     ap.add_argument("--serve-requests", type=int, default=3000)
     ap.add_argument("--serve-rate", type=float, default=2000.0)

@@ -76,6 +76,29 @@ int steel_sync(steel_batch* b);                                   /* queue.onSub
 /* Capture one frame's substeps into a CUDA graph and replay it (on by default). */
 int steel_set_graph(steel_batch* b, int enabled);
 
+/* Tile configuration of a batch's launches. No counterpart in the reference, whose workgroup sizes
+   are fixed in the WGSL (one 256-invocation workgroup per prepare/solve, wgsl.js:1222, :2501).
+   Prepare and solve run one block per scene; block_threads picks the kernel instance (32, 64, 128,
+   256 or 512 threads, all at 128 registers per thread, so 65536 / (128 * block_threads) blocks fit
+   an SM); smem_budget caps the dynamic shared memory a block uses to stage a scene's link blocks,
+   twists, qd and color masks (0: per-part caps only); narrow_blocks_per_sm sizes the persistent
+   narrowphase grid (0: as many as fit). A batch starts at 512 threads when it has no more scenes
+   than SMs (the per-thread scratch is sized for that), else at 128, which is also the largest
+   block it accepts. Results are the same bits under every configuration. */
+typedef struct {
+  uint32_t block_threads;
+  uint32_t smem_budget;
+  uint32_t narrow_blocks_per_sm;
+} steel_tiles;
+int steel_get_tiles(steel_batch* b, steel_tiles* out);
+int steel_set_tiles(steel_batch* b, const steel_tiles* tiles);
+/* Autotuner: steps the batch from its initial state under each candidate configuration (block
+   sizes with staging budgets that keep 1-16 blocks resident per SM, then one narrowphase grid
+   smaller than the default), times `frames` frames of each after two warm-up frames (CUDA events),
+   keeps the fastest and resets the batch (as steel_reset). Returns the chosen tiles and their device
+   time per frame in milliseconds. */
+int steel_autotune(steel_batch* b, uint32_t frames, steel_tiles* best, float* best_ms_per_frame);
+
 /* Readback (Sim.state, sim.js:732-763; Sim.poses, sim.js:804). Caller-owned buffers. */
 int steel_read_poses(steel_batch* b, uint32_t scene, float* poses /* NB*8 */);
 int steel_read_state(steel_batch* b, uint32_t scene, float* poses /* NB*8 */, float* vel /* NB*8 */,

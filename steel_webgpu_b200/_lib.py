@@ -32,6 +32,10 @@ class Stats(ctypes.Structure):
                                                "colors", "max_dense", "asleep", "overflow")]
 
 
+class Tiles(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("block_threads", "smem_budget", "narrow_blocks_per_sm")]
+
+
 class SceneInfo(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in ("NB", "NS", "NA", "NL", "ND", "NQ", "max_pairs", "max_contacts",
                                                "max_units", "max_dense")]
@@ -53,6 +57,9 @@ SIGNATURES = {
     "steel_step": [_VP, _U32],
     "steel_sync": [_VP],
     "steel_set_graph": [_VP, ctypes.c_int],
+    "steel_get_tiles": [_VP, ctypes.POINTER(Tiles)],
+    "steel_set_tiles": [_VP, ctypes.POINTER(Tiles)],
+    "steel_autotune": [_VP, _U32, ctypes.POINTER(Tiles), ctypes.POINTER(_F32)],
     "steel_read_poses": [_VP, _U32, _VP],
     "steel_read_state": [_VP, _U32, _VP, _VP, _VP, _VP, _VP],
     "steel_get_stats": [_VP, _U32, ctypes.POINTER(Stats)],

@@ -119,6 +119,9 @@ struct steel_batch {
   uint32_t debug_substep = 0;  // substep cursor of steel_debug_stage
   size_t sort_keys = 0;
   std::vector<RadixDev> radix;  // large scenes' device-wide contact sorts
+  uint32_t max_threads = DEFAULT_THREADS;  // largest prepare / solve block the per-thread scratch allows
+  steel_tiles tile_cfg{};                   // the launches' tile configuration (apply_tiles)
+  size_t o_stage = 0;                       // staging flags of every scene (apply_tiles upload)
   bool use_graph = true;
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -327,6 +330,68 @@ void drop_graph(steel_batch* b) {
   b->graph = nullptr;
 }
 
+// Shared-memory staging flags of a scene under a per-block budget of dynamic shared memory (0: the
+// per-part caps alone). Link blocks first, then twists and impulses, qd, and the color masks; a part
+// is staged when it is under its cap and both kernels' layouts stay within the budget.
+uint32_t stage_flags(const SceneDev& d, uint32_t budget) {
+  const uint64_t lim = budget ? budget : ~0ull;
+  auto fits = [&](uint32_t f) {
+    return prep_smem_layout(f, d.NL, d.NB, d.NCOLW, d.NCOL).total <= lim &&
+           solve_smem_layout(f, d.NB, d.ND, d.NCOL, d.NL).total <= lim;
+  };
+  uint32_t st = 0u;
+  if (d.NL > 0u && 4ull * d.NL * 268u <= STAGE_LINK_CAP && fits(st | STAGE_LINKS)) st |= STAGE_LINKS;
+  if (64ull * d.NB <= STAGE_BODY_CAP && fits(st | STAGE_BODIES)) st |= STAGE_BODIES;
+  if (4ull * d.ND <= STAGE_QD_CAP && fits(st | STAGE_QD)) st |= STAGE_QD;
+  if (4ull * d.NB * d.NCOLW <= STAGE_WMASK_CAP && fits(st | STAGE_WMASK)) st |= STAGE_WMASK;
+  return st;
+}
+
+bool valid_block(uint32_t t) {
+  for (uint32_t v : BLOCK_SIZES)
+    if (v == t) return true;
+  return false;
+}
+
+// Makes `t` the batch's tile configuration: block size of prepare and solve, each scene's
+// shared-memory staging under the budget, the launches' dynamic shared memory and the
+// narrowphase grid. The frame graph is captured again at the next step. Results do not depend on
+// the configuration.
+int apply_tiles(steel_batch* b, const steel_tiles& t) {
+  if (!valid_block(t.block_threads) || t.block_threads > b->max_threads)
+    return fail(STEEL_E_INVALID, "block_threads must be 32, 64, 128, 256 or 512 and at most " +
+                                     std::to_string(b->max_threads) + " for this batch");
+  const uint32_t narrow_max = (uint32_t)narrow_blocks_per_sm();
+  if (t.narrow_blocks_per_sm > narrow_max)
+    return fail(STEEL_E_INVALID, "narrow_blocks_per_sm above the " + std::to_string(narrow_max) + " that fit an SM");
+  const uint32_t n = (uint32_t)b->sc.size();
+  std::vector<uint32_t> stages(n);
+  size_t prep = 0, solve = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    SceneDev& d = b->sc[i].d;
+    d.stage = stage_flags(d, t.smem_budget);
+    stages[i] = d.stage;
+    prep = std::max<size_t>(prep, prep_smem_layout(d.stage, d.NL, d.NB, d.NCOLW, d.NCOL).total);
+    solve = std::max<size_t>(solve, solve_smem_layout(d.stage, d.NB, d.ND, d.NCOL, d.NL).total);
+  }
+  CU(cudaSetDevice(b->ctx->device));
+  cudaStream_t st = b->ctx->stream;
+  CU(cudaStreamSynchronize(st));
+  CU(configure_prepare(t.block_threads, prep));
+  CU(configure_solve(t.block_threads, solve));
+  CU(cudaMemcpyAsync(b->arena + b->o_stage, stages.data(), 4ull * n, cudaMemcpyHostToDevice, st));
+  launch_set_stage(b->bd, reinterpret_cast<const uint32_t*>(b->arena + b->o_stage), st);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(st));
+  b->bd.prep_smem = (uint32_t)prep;
+  b->bd.solve_smem = (uint32_t)solve;
+  b->bd.block_threads = t.block_threads;
+  b->narrow_blocks = (uint32_t)b->ctx->sms * (t.narrow_blocks_per_sm ? t.narrow_blocks_per_sm : narrow_max);
+  b->tile_cfg = t;
+  drop_graph(b);
+  return STEEL_OK;
+}
+
 SceneHost* scene_of(steel_batch* b, uint32_t s) { return (b && s < b->sc.size()) ? &b->sc[s] : nullptr; }
 
 }  // namespace
@@ -369,9 +434,10 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   b->sc.resize(n);
   Layout L;
   const bool big = n <= (uint32_t)ctx->sms;
+  b->max_threads = big ? BIG_THREADS : DEFAULT_THREADS;
   for (uint32_t i = 0; i < n; i++) {
     std::string why;
-    int rc = build_scene(b->sc[i], scenes[i], L, big ? BIG_THREADS : PREP_THREADS, why);
+    int rc = build_scene(b->sc[i], scenes[i], L, b->max_threads, why);
     if (rc) return fail(rc, "scene " + std::to_string(i) + ": " + why);
     if (i > 0 && b->sc[i].d.substeps != b->sc[0].d.substeps)
       return fail(STEEL_E_INVALID, "scenes of one batch must share the substep count");
@@ -401,6 +467,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   b->o_active = L.take(4ull * n);
   b->o_order = L.take(4ull * n);
   b->o_err = L.take(4);
+  b->o_stage = L.take(4ull * n);
   std::vector<uint64_t> tgt_off(n), pose_off(n);
   for (uint32_t i = 0; i < n; i++) {
     tgt_off[i] = b->n_targets;
@@ -419,7 +486,6 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   CU(cudaMemsetAsync(b->arena, 0, b->arena_bytes, st));
   uint8_t* A = b->arena;
   std::vector<SceneDev> dev(n);
-  size_t prep_smem = 0, solve_smem = 0;
   uint32_t art_f64 = 0, solve_ext = 0;
   for (uint32_t i = 0; i < n; i++) {
     SceneHost& s = b->sc[i];
@@ -451,13 +517,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
       r.scene = i;
       b->radix.push_back(r);
     }
-    d.stage = 0u;
-    if (d.NL > 0u && 4ull * d.NL * 268u <= STAGE_LINK_CAP) d.stage |= STAGE_LINKS;
-    if (64ull * d.NB <= STAGE_BODY_CAP) d.stage |= STAGE_BODIES;
-    if (4ull * d.ND <= STAGE_QD_CAP) d.stage |= STAGE_QD;
-    if (4ull * d.NB * d.NCOLW <= STAGE_WMASK_CAP) d.stage |= STAGE_WMASK;
-    prep_smem = std::max<size_t>(prep_smem, prep_smem_layout(d.stage, d.NL, d.NB, d.NCOLW, d.NCOL).total);
-    solve_smem = std::max<size_t>(solve_smem, solve_smem_layout(d.stage, d.NB, d.ND, d.NCOL, d.NL).total);
+    d.stage = 0u;  // set by apply_tiles below
     art_f64 |= d.ART_F64;
     solve_ext |= d.ANG_ART | d.CTI;
     dev[i] = d;
@@ -494,24 +554,27 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   }
   CU(cudaMemsetAsync(A + b->o_active, 1, 4ull * n, st));  // every scene steps (nonzero words)
   bd.error = at<uint32_t>(A, b->o_err);
-  bd.prep_smem = (uint32_t)prep_smem;
-  bd.solve_smem = (uint32_t)solve_smem;
   bd.art_f64 = art_f64 != 0u ? 1u : 0u;
   bd.solve_ext = solve_ext != 0u ? 1u : 0u;
-  bd.big = big ? 1u : 0u;
+  bd.block_threads = b->max_threads;
   bd.wait_limit = STEEL_WAIT_LIMIT_DEFAULT;
   static_assert(STEEL_WAIT_LIMIT_DEFAULT == BULK_WAIT_LIMIT, "one default wait limit");
-  CU(configure_prepare(prep_smem));
-  CU(configure_solve(solve_smem));
   CU(cudaMemcpyAsync(bd.scenes, dev.data(), sizeof(SceneDev) * n, cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync((void*)bd.shape_scene, b->shape_scene.data(), 4 * b->shape_scene.size(), cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync((void*)bd.shape_local, b->shape_local.data(), 4 * b->shape_local.size(), cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync((void*)bd.tiles, b->tiles.data(), 16 * b->tiles.size(), cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(A + b->o_tgt_off, tgt_off.data(), 8ull * n, cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(A + b->o_pose_off, pose_off.data(), 8ull * n, cudaMemcpyHostToDevice, st));
-  b->narrow_blocks = (uint32_t)ctx->sms * (uint32_t)narrow_blocks_per_sm();
   b->sort_keys = std::min<size_t>(next_pow2(max_c), SORT_SMEM_KEYS);
   CU(configure_sort(b->sort_keys));
+  {
+    steel_tiles t{};
+    t.block_threads = b->max_threads;  // one block per SM for few scenes, 4 per SM otherwise
+    t.smem_budget = 0;                 // the per-part staging caps alone
+    t.narrow_blocks_per_sm = 0;        // as many as fit
+    int rc = apply_tiles(b.get(), t);
+    if (rc) return rc;
+  }
   CU(cudaEventCreate(&b->ev0));
   CU(cudaEventCreate(&b->ev1));
   int rc = upload_state(b.get());
@@ -556,6 +619,64 @@ int steel_debug_set_wait_limit(steel_batch* b, uint32_t rounds) {
   CU(cudaStreamSynchronize(b->ctx->stream));
   b->bd.wait_limit = rounds;
   drop_graph(b);  // the limit is a launch argument: capture again
+  return STEEL_OK;
+}
+
+int steel_get_tiles(steel_batch* b, steel_tiles* out) {
+  if (!b || !out) return fail(STEEL_E_INVALID, "null argument");
+  *out = b->tile_cfg;
+  return STEEL_OK;
+}
+
+int steel_set_tiles(steel_batch* b, const steel_tiles* t) {
+  if (!b || !t) return fail(STEEL_E_INVALID, "null argument");
+  if (b->serve_on) return fail(STEEL_E_INVALID, "end the serving loop before changing tiles");
+  return apply_tiles(b, *t);
+}
+
+int steel_autotune(steel_batch* b, uint32_t frames, steel_tiles* best, float* best_ms_per_frame) {
+  if (!b || frames == 0) return fail(STEEL_E_INVALID, "null batch or zero frames");
+  if (b->serve_on) return fail(STEEL_E_INVALID, "end the serving loop before tuning");
+  // Candidates: block size with a staging budget that keeps that many blocks resident per SM
+  // (228 KiB of shared memory per SM, less 1 KiB reserved and about 2 KiB of static shared memory
+  // per block), and the default caps.
+  auto budget_for = [](uint32_t threads) { return 233472u / blocks_per_sm_of(threads) - 3328u; };
+  std::vector<steel_tiles> cands;
+  if (b->max_threads == BIG_THREADS) {
+    cands = {{512, 0, 0}, {256, 0, 0}, {256, budget_for(256), 0}, {128, budget_for(128), 0}};
+  } else {
+    cands = {{128, 0, 0}, {128, budget_for(128), 0}, {64, budget_for(64), 0}, {64, budget_for(64) / 2u, 0},
+             {32, budget_for(32), 0}, {32, budget_for(32) / 2u, 0}};
+  }
+  const uint32_t narrow_max = (uint32_t)narrow_blocks_per_sm();
+  if (narrow_max > 1u) cands.push_back({0u, 0u, narrow_max - 1u});  // block size filled in from the best so far
+  CU(cudaSetDevice(b->ctx->device));
+  cudaStream_t st = b->ctx->stream;
+  steel_tiles won = b->tile_cfg;
+  float won_ms = 1e30f;
+  for (steel_tiles c : cands) {
+    if (c.block_threads == 0u) {
+      c.block_threads = won.block_threads;
+      c.smem_budget = won.smem_budget;
+    }
+    if (int rc = apply_tiles(b, c)) return rc;
+    if (int rc = upload_state(b)) return rc;
+    if (int rc = steel_step(b, 2u)) return rc;  // warm-up, graph capture
+    CU(cudaEventRecord(b->ev0, st));
+    if (int rc = steel_step(b, frames)) return rc;
+    CU(cudaEventRecord(b->ev1, st));
+    CU(cudaEventSynchronize(b->ev1));
+    float ms = 0.0f;
+    CU(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    if (int rc = check_device_error(b)) return rc;
+    ms /= (float)frames;
+    if (ms < won_ms) { won_ms = ms; won = c; }
+  }
+  if (int rc = apply_tiles(b, won)) return rc;
+  if (int rc = upload_state(b)) return rc;
+  CU(cudaStreamSynchronize(st));
+  if (best) *best = won;
+  if (best_ms_per_frame) *best_ms_per_frame = won_ms;
   return STEEL_OK;
 }
 

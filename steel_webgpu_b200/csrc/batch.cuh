@@ -26,7 +26,7 @@ struct BatchDev {
   uint32_t solve_smem;
   uint32_t art_f64;           // some scene has ART_F64: launch the prepare instances that carry it
   uint32_t solve_ext;         // some scene has ANG_ART or CTI: launch the solve instances that carry them
-  uint32_t big;               // prepare and solve run BIG_THREADS blocks (few scenes)
+  uint32_t block_threads;     // threads per prepare / solve block (one of BLOCK_SIZES)
   uint32_t wait_limit;        // try_wait rounds of a shared-memory bulk copy (BULK_WAIT_LIMIT unless a test
                               // lowers it to make the bounded wait run out)
 };
@@ -36,12 +36,15 @@ constexpr int NARROW_WARPS = 8;          // warps per narrowphase block
 constexpr int NARROW_JOB_THREADS = 128;  // threads per block of the narrowphase job kernel
 constexpr uint32_t NJOB_WORDS = 44;     // words per narrowphase job record
 constexpr int SORT_THREADS = 512;
-constexpr int PREP_THREADS = 128;
-constexpr int SOLVE_THREADS = 128;
-// Batches of no more scenes than SMs run prepare and solve with one BIG_THREADS block per scene
-// (one per SM, the same 128 registers per thread): large scenes get four times the threads for
-// their parallel phases. Results do not depend on the block size.
-constexpr int BIG_THREADS = 512;
+// Prepare and solve run one block per scene. Every block size below has its own kernel instances
+// (prepare_<N>.o, solve_<N>.o), all at 128 registers per thread, so a size of N threads keeps
+// 65536 / (128 N) blocks per SM when shared memory allows: small blocks keep more scenes resident
+// and hide the latency of each scene's serial passes, large blocks give a few large scenes more
+// threads for their parallel phases. Results do not depend on the block size.
+constexpr uint32_t BLOCK_SIZES[] = {32u, 64u, 128u, 256u, 512u};
+constexpr uint32_t DEFAULT_THREADS = 128;  // batches with more scenes than SMs
+constexpr int BIG_THREADS = 512;           // batches of no more scenes than SMs: one block per SM
+constexpr uint32_t blocks_per_sm_of(uint32_t threads) { return 65536u / (threads * 128u); }
 
 // Device error codes written to BatchDev::error.
 enum : uint32_t { ERR_NONE = 0, ERR_SORT_CAPACITY = 1, ERR_JOB_CAPACITY = 2, ERR_STAGE_TIMEOUT = 3, ERR_SORT_TIMEOUT = 4 };
@@ -130,10 +133,27 @@ void launch_narrow(const BatchDev& b, uint32_t narrow_blocks, cudaStream_t st);
 int narrow_blocks_per_sm();
 void launch_csort(const BatchDev& b, size_t smem_keys, const RadixDev* radix, uint32_t nradix, cudaStream_t st);
 cudaError_t configure_sort(size_t smem_keys);
-cudaError_t configure_prepare(size_t smem_bytes);
-cudaError_t configure_solve(size_t smem_bytes);
+// One instance set per block size (template argument = threads per block).
+template <int T> cudaError_t configure_prepare_t(size_t smem_bytes);
+template <int T> cudaError_t configure_solve_t(size_t smem_bytes);
+template <int T> void launch_prepare_t(const BatchDev& b, cudaStream_t st);
+template <int T> void launch_solve_t(const BatchDev& b, cudaStream_t st);
+#define STEEL_DECLARE_BLOCK(N)                                                  \
+  template <> cudaError_t configure_prepare_t<N>(size_t smem_bytes);            \
+  template <> cudaError_t configure_solve_t<N>(size_t smem_bytes);              \
+  template <> void launch_prepare_t<N>(const BatchDev& b, cudaStream_t st);     \
+  template <> void launch_solve_t<N>(const BatchDev& b, cudaStream_t st);
+STEEL_DECLARE_BLOCK(32)
+STEEL_DECLARE_BLOCK(64)
+STEEL_DECLARE_BLOCK(128)
+STEEL_DECLARE_BLOCK(256)
+STEEL_DECLARE_BLOCK(512)
+#undef STEEL_DECLARE_BLOCK
+cudaError_t configure_prepare(uint32_t threads, size_t smem_bytes);
+cudaError_t configure_solve(uint32_t threads, size_t smem_bytes);
 void launch_prepare(const BatchDev& b, cudaStream_t st);
 void launch_solve(const BatchDev& b, cudaStream_t st);
+void launch_set_stage(const BatchDev& b, const uint32_t* stage, cudaStream_t st);
 void launch_frame_end(const BatchDev& b, cudaStream_t st);
 // Host-I/O staging: scatter packed joint targets into each scene, gather packed body poses.
 void launch_scatter_targets(const BatchDev& b, const float* packed, const uint64_t* offsets, cudaStream_t st);

@@ -1515,6 +1515,48 @@ void launch_scatter_targets(const BatchDev& b, const float* packed, const uint64
 void launch_gather_poses(const BatchDev& b, float* packed, const uint64_t* offsets, cudaStream_t st) {
   k_gather_poses<<<b.nscenes, 128, 0, st>>>(b, packed, offsets);
 }
+// Prepare / solve launches and their shared-memory configuration, by the batch's block size.
+#define STEEL_BY_BLOCK(threads, call)         \
+  switch (threads) {                          \
+    case 32: call(32); break;                 \
+    case 64: call(64); break;                 \
+    case 256: call(256); break;               \
+    case 512: call(512); break;               \
+    default: call(128); break;                \
+  }
+cudaError_t configure_prepare(uint32_t threads, size_t smem_bytes) {
+  cudaError_t e = cudaSuccess;
+#define STEEL_CALL(N) e = configure_prepare_t<N>(smem_bytes)
+  STEEL_BY_BLOCK(threads, STEEL_CALL)
+#undef STEEL_CALL
+  return e;
+}
+cudaError_t configure_solve(uint32_t threads, size_t smem_bytes) {
+  cudaError_t e = cudaSuccess;
+#define STEEL_CALL(N) e = configure_solve_t<N>(smem_bytes)
+  STEEL_BY_BLOCK(threads, STEEL_CALL)
+#undef STEEL_CALL
+  return e;
+}
+void launch_prepare(const BatchDev& b, cudaStream_t st) {
+#define STEEL_CALL(N) launch_prepare_t<N>(b, st)
+  STEEL_BY_BLOCK(b.block_threads, STEEL_CALL)
+#undef STEEL_CALL
+}
+void launch_solve(const BatchDev& b, cudaStream_t st) {
+#define STEEL_CALL(N) launch_solve_t<N>(b, st)
+  STEEL_BY_BLOCK(b.block_threads, STEEL_CALL)
+#undef STEEL_CALL
+}
+#undef STEEL_BY_BLOCK
+// Each scene's shared-memory staging flags (SceneDev::stage) from a packed array, one per scene.
+__global__ void k_set_stage(BatchDev B, const uint32_t* stage) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < B.nscenes) B.scenes[i].stage = stage[i];
+}
+void launch_set_stage(const BatchDev& b, const uint32_t* stage, cudaStream_t st) {
+  k_set_stage<<<(b.nscenes + 127) / 128, 128, 0, st>>>(b, stage);
+}
 void launch_shapes(const BatchDev& b, cudaStream_t st) {
   if (b.nshapes) k_shapes<<<(b.nshapes + 127) / 128, 128, 0, st>>>(b);
 }

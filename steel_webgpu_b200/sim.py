@@ -110,6 +110,23 @@ class Batch:
     def reset(self):
         _lib.check(_lib.load().steel_reset(self.h))
 
+    def tiles(self) -> dict:
+        t = _lib.Tiles()
+        _lib.check(_lib.load().steel_get_tiles(self.h, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in _lib.Tiles._fields_}
+
+    def set_tiles(self, block_threads: int, smem_budget: int = 0, narrow_blocks_per_sm: int = 0):
+        t = _lib.Tiles(block_threads, smem_budget, narrow_blocks_per_sm)
+        _lib.check(_lib.load().steel_set_tiles(self.h, ctypes.byref(t)))
+
+    def autotune(self, frames: int = 3) -> tuple[dict, float]:
+        """Times each candidate tile configuration over `frames` frames from the initial state, keeps
+        the fastest and resets the batch. Returns (tiles, ms per frame)."""
+        t = _lib.Tiles()
+        ms = ctypes.c_float()
+        _lib.check(_lib.load().steel_autotune(self.h, frames, ctypes.byref(t), ctypes.byref(ms)))
+        return {k: getattr(t, k) for k, _ in _lib.Tiles._fields_}, ms.value
+
     def info(self, scene: int = 0) -> _lib.SceneInfo:
         out = _lib.SceneInfo()
         _lib.check(_lib.load().steel_scene_info_get(self.h, scene, ctypes.byref(out)))

@@ -221,6 +221,66 @@ def test_block_size_does_not_change_results(steel):
         assert np.array_equal(_bits(small.raw_state()[2]), _bits(large.raw_state(i)[2]))
 
 
+@pytest.mark.parametrize("tiles", [(128, 0, 0), (128, 54000, 0), (64, 25000, 0), (64, 6000, 0), (32, 11000, 0),
+                                   (32, 2000, 1)])
+def test_tiles_do_not_change_results(tiles, steel):
+    """Every tile configuration (block size, shared-memory staging budget, narrowphase grid) gives
+    the same bits as the default, for a batch with more scenes than SMs (uneven scenes with chains,
+    quadrupeds and a plain box pile)."""
+    pks = [pack(s) for s in scenes.small_batch(n=6)] + [pack(scenes.chains_and_quads(n_quad=2)),
+                                                          pack(scenes.articulated()), pack(scenes.boxes(40))]
+    pks = pks * 17  # 153 scenes > 148 SMs
+    ref = Batch(pks)
+    g = Batch(pks)
+    assert ref.tiles()["block_threads"] == 128
+    g.set_tiles(*tiles)
+    assert g.tiles() == dict(block_threads=tiles[0], smem_budget=tiles[1], narrow_blocks_per_sm=tiles[2])
+    ref.step(20)
+    g.step(20)
+    for i in range(9):
+        assert np.array_equal(_bits(ref.poses(i)), _bits(g.poses(i))), f"scene {i} differs under {tiles}"
+        assert np.array_equal(_bits(ref.raw_state(i)[3]), _bits(g.raw_state(i)[3]))
+
+
+@pytest.mark.parametrize("threads", [512, 256, 64, 32])
+def test_tiles_of_a_single_large_scene(threads, steel):
+    """A batch of one scene starts at 512-thread blocks; every smaller block gives the same bits."""
+    pk = pack(scenes.chains_and_quads(n_quad=6))
+    ref = Batch([pk])
+    g = Batch([pk])
+    assert ref.tiles()["block_threads"] == 512
+    g.set_tiles(threads, 0 if threads >= 256 else 20000)
+    ref.step(20)
+    g.step(20)
+    assert np.array_equal(_bits(ref.poses()), _bits(g.poses()))
+    assert np.array_equal(_bits(ref.raw_state()[2]), _bits(g.raw_state()[2]))
+
+
+def test_autotune_picks_a_config_and_resets(steel, oracle_lib):
+    """The autotuner times its candidates, keeps one and resets the batch: stepping afterwards
+    matches the oracle from the initial state."""
+    pks = [pack(s) for s in scenes.small_batch(n=6)]
+    g = Batch(pks)
+    g.step(5)
+    tiles, ms = g.autotune(2)
+    assert tiles["block_threads"] in (32, 64, 128, 256, 512) and ms > 0
+    assert g.tiles() == tiles
+    g.step(20)
+    for i, pk in enumerate(pks):
+        o = oracle_lib.OracleSim(pk)
+        o.step(20)
+        assert np.array_equal(_bits(g.poses(i)), _bits(o.read("poses")[:pk.NB * 8])), f"scene {i} differs"
+
+
+def test_tiles_reject_bad_values(steel):
+    pks = [pack(scenes.boxes(8))] * 200
+    g = Batch(pks)
+    from steel_webgpu_b200 import _lib
+    for bad in ((512, 0, 0), (96, 0, 0), (128, 0, 99)):
+        with pytest.raises(_lib.SteelError):
+            g.set_tiles(*bad)
+
+
 def test_reset_replays_identically(steel):
     pk = pack(scenes.boxes(24))
     g = Batch([pk])
