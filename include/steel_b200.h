@@ -68,6 +68,27 @@ const char* steel_last_error(void);
 /* new Sim(device, scene) for n scenes at once (sim.js:63-75, 95-611). */
 int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t n, steel_batch** out);
 int steel_batch_destroy(steel_batch* b);                          /* Sim.destroy (sim.js:85-93) */
+
+/* new Sim(device, scene, opts) from the scene's own files: scene.json text and scene.bin bytes as
+   loadScene reads them (sim.js:40-61), packed by the library (the C++ restatement of Sim.build,
+   sim.js:95-521) and created as a batch of one. opts_json: the SimOptions object (sim.d.ts:3-28:
+   substeps, iterations, regularization, warmStart, colorWords, solver) or NULL, plus an optional
+   "capacities" object (MAXP, MAXC, MAXU, UH, WH, MAXDENSE, AH) replacing the reference's fixed
+   ones. Unsupported scenes and options fail with STEEL_E_INVALID and the reference's message
+   (sim.js:73, :128, :159, :166, :376-379, :412-420). */
+int steel_scene_create(steel_ctx* ctx, const char* json, uint64_t json_len, const void* bin, uint64_t bin_len,
+                       const char* opts_json, steel_batch** out);
+/* The same for n scenes stepped together (arrays of n; opts_json may be NULL, or hold NULLs). */
+int steel_batch_create_files(steel_ctx* ctx, uint32_t n, const char* const* json, const uint64_t* json_len,
+                             const void* const* bin, const uint64_t* bin_len, const char* const* opts_json,
+                             steel_batch** out);
+/* Packing alone, without a device (tools and tests): the steel_scene_desc a scene's files pack to.
+   The desc's pointers stay valid until steel_packed_free. */
+typedef struct steel_packed steel_packed;
+int steel_pack(const char* json, uint64_t json_len, const void* bin, uint64_t bin_len, const char* opts_json,
+               steel_packed** out);
+int steel_packed_desc(const steel_packed* p, steel_scene_desc* out);
+int steel_packed_free(steel_packed* p);
 int steel_scene_info_get(steel_batch* b, uint32_t scene, steel_scene_info* out);
 
 int steel_reset(steel_batch* b);                                  /* Sim.reset (sim.js:613-623) */
@@ -104,6 +125,25 @@ int steel_read_poses(steel_batch* b, uint32_t scene, float* poses /* NB*8 */);
 int steel_read_state(steel_batch* b, uint32_t scene, float* poses /* NB*8 */, float* vel /* NB*8 */,
                      float* q /* NQ */, float* qd /* ND */, float* link_v /* NL*6, (w, v) at the COM */);
 int steel_get_stats(steel_batch* b, uint32_t scene, steel_stats* out);  /* Sim.stats (sim.js:822-834) */
+/* Sim.state() (sim.js:732-763) in Newton's layout, for scenes created from their files:
+   bodyQ (body origin position, quaternion x y z w; 7 floats per body), bodyQd (COM linear and
+   angular velocity, world frame; 6 per body), jointQ and jointQd in Newton's joint layout (sizes from
+   steel_newton_info). Caller-owned buffers. */
+typedef struct {
+  uint32_t bodies, joint_coords, joint_dofs;
+} steel_newton_info_t;
+int steel_newton_info(steel_batch* b, uint32_t scene, steel_newton_info_t* out);
+int steel_state(steel_batch* b, uint32_t scene, float* bodyQ, float* bodyQd, float* jointQ, float* jointQd);
+/* The port dof of a Newton joint dof (Sim.dofMap, sim.js:716-719): the index the joint setters
+   below take. STEEL_E_INVALID with the reference's message for a dof outside the articulations. */
+int steel_newton_dof(steel_batch* b, uint32_t scene, uint32_t newton_dof, uint32_t* port_dof);
+/* Zero-copy pose export, the role of Sim.buffers.poses with PoseBridge.copy (sim.d.ts:75,
+   three/poseBridge.ts:12-45): copies scene s's body poses GPU to GPU into a caller-owned device
+   buffer of NB BodyPose records (COM position vec4, then quaternion x, y, z, w vec4; 32 bytes each,
+   16-byte aligned), e.g. a renderer's instance buffer mapped into CUDA. Enqueued on `stream` (a
+   cudaStream_t of the batch's device; NULL: the batch's own stream) after the frames already
+   queued; nothing passes through host memory and the call does not wait. */
+int steel_copy_poses_device(steel_batch* b, uint32_t scene, float* dst, void* stream);
 
 /* User control (sim.js:716-785), port dof/body indices; held until changed. */
 int steel_set_joint_target(steel_batch* b, uint32_t scene, uint32_t dof, float pos, float vel);

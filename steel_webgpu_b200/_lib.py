@@ -36,6 +36,10 @@ class Tiles(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in ("block_threads", "smem_budget", "narrow_blocks_per_sm")]
 
 
+class NewtonInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("bodies", "joint_coords", "joint_dofs")]
+
+
 class SceneInfo(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in ("NB", "NS", "NA", "NL", "ND", "NQ", "max_pairs", "max_contacts",
                                                "max_units", "max_dense")]
@@ -52,6 +56,15 @@ SIGNATURES = {
     "steel_last_error": [],
     "steel_batch_create": [_VP, ctypes.POINTER(SceneDesc), _U32, ctypes.POINTER(_VP)],
     "steel_batch_destroy": [_VP],
+    "steel_scene_create": [_VP, ctypes.c_char_p, ctypes.c_uint64, _VP, ctypes.c_uint64, ctypes.c_char_p,
+                           ctypes.POINTER(_VP)],
+    "steel_batch_create_files": [_VP, _U32, _VP, _VP, _VP, _VP, _VP, ctypes.POINTER(_VP)],
+    "steel_pack": [ctypes.c_char_p, ctypes.c_uint64, _VP, ctypes.c_uint64, ctypes.c_char_p, ctypes.POINTER(_VP)],
+    "steel_packed_desc": [_VP, ctypes.POINTER(SceneDesc)],
+    "steel_packed_free": [_VP],
+    "steel_newton_info": [_VP, _U32, ctypes.POINTER(NewtonInfo)],
+    "steel_state": [_VP, _U32, _VP, _VP, _VP, _VP],
+    "steel_newton_dof": [_VP, _U32, _U32, ctypes.POINTER(_U32)],
     "steel_scene_info_get": [_VP, _U32, ctypes.POINTER(SceneInfo)],
     "steel_reset": [_VP],
     "steel_step": [_VP, _U32],
@@ -62,6 +75,7 @@ SIGNATURES = {
     "steel_autotune": [_VP, _U32, ctypes.POINTER(Tiles), ctypes.POINTER(_F32)],
     "steel_read_poses": [_VP, _U32, _VP],
     "steel_read_state": [_VP, _U32, _VP, _VP, _VP, _VP, _VP],
+    "steel_copy_poses_device": [_VP, _U32, _VP, _VP],
     "steel_get_stats": [_VP, _U32, ctypes.POINTER(Stats)],
     "steel_set_joint_target": [_VP, _U32, _U32, _F32, _F32],
     "steel_set_joint_force": [_VP, _U32, _U32, _F32],

@@ -16,7 +16,8 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libsteel_b200.so")
 BLOCK_SIZES = [32, 64, 128, 256, 512]  # prepare / solve instance sets (csrc/batch.cuh BLOCK_SIZES)
 # (source, object, extra flags): prepare.cu and solve.cu are compiled once per block size.
-UNITS = [("collide.cu", "collide.o", []), ("api.cu", "api.o", []), ("sort_noalloc.cu", "sort_noalloc.o", [])]
+UNITS = [("collide.cu", "collide.o", []), ("api.cu", "api.o", []), ("sort_noalloc.cu", "sort_noalloc.o", []),
+         ("scene.cpp", "scene.o", [])]
 UNITS += [(f"{k}.cu", f"{k}_{n}.o", [f"-DSTEEL_BLOCK={n}"]) for k in ("prepare", "solve") for n in BLOCK_SIZES]
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "--fmad=false", "-prec-div=true",
@@ -32,7 +33,7 @@ def _stale(obj, deps):
 
 def build(verbose: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
-    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     headers.append(os.path.join(HERE, "..", "include", "steel_b200.h"))
 
     def compile_one(unit):

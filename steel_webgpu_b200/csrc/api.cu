@@ -16,6 +16,7 @@
 #include "../../include/steel_b200.h"
 #include "batch.cuh"
 #include "bulk.cuh"
+#include "scene.h"
 
 using namespace steel;
 
@@ -98,9 +99,16 @@ struct SceneHost {
   std::vector<float4> pos0, rot0, lv0, av0;
   std::vector<float> art0;
   uint32_t collide_pairs = 0, collide_contacts = 0;  // counts of the last steel_collide
+  // Newton index maps and scene data of a scene created from its files (steel_scene_create):
+  // what Sim.state() and the Newton-indexed setters need (sim.js:716-785).
+  std::shared_ptr<const scene::Packed> files;
 };
 
 }  // namespace
+
+struct steel_packed {
+  steel::scene::Packed p;
+};
 
 struct steel_ctx {
   int device = 0;
@@ -125,6 +133,7 @@ struct steel_batch {
   bool use_graph = true;
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev_pose = nullptr;  // orders a pose export on the caller's stream after the batch's frames
   size_t o_scenes, o_shape_scene, o_shape_local, o_tiles, o_pairs, o_pair_count, o_jobs, o_phase, o_ssc, o_active, o_order, o_err;
   std::vector<uint32_t> shape_scene, shape_local;
   std::vector<uint4> tiles;
@@ -214,6 +223,9 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, uint32_t th
     put(d.S_WMASK, (size_t)NB * d.NCOLW); put(d.S_WCOUNT, d.NCOL + 2); put(d.S_LINKHIT, NB); put(d.S_JSPLIT, NL);
     put(d.S_UF, NB + NA); put(d.S_UFF, NB + NA); put(d.S_UTP, MAXC);
     put(d.S_DSTART, NA + 1); put(d.S_DOFF, NA); put(d.S_DLIST, d.MAXDENSE);
+    // parallel coloring: per-body row lists and frontiers, row keys
+    put(d.S_BSTART, NB + 1); put(d.S_BPOS, NB); put(d.S_BREADY, NB); put(d.S_BLIST, 2 * (size_t)MAXC);
+    put(d.S_RKEY, MAXC);
     s.sched_words = so;
   }
   s.warm_words = 10ull * d.WH + 30ull * d.AH;
@@ -584,6 +596,132 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   return STEEL_OK;
 }
 
+int steel_pack(const char* json, uint64_t json_len, const void* bin, uint64_t bin_len, const char* opts_json,
+               steel_packed** out) {
+  if (!json || !out || (!bin && bin_len)) return fail(STEEL_E_INVALID, "null argument");
+  scene::JV js, opts;
+  std::string err;
+  if (!scene::parse_json(json, json_len, js, err)) return fail(STEEL_E_INVALID, "scene.json: " + err);
+  if (opts_json && *opts_json && !scene::parse_json(opts_json, std::strlen(opts_json), opts, err))
+    return fail(STEEL_E_INVALID, "options: " + err);
+  std::unique_ptr<steel_packed> p(new steel_packed());
+  if (!scene::pack(js, static_cast<const uint8_t*>(bin), bin_len, &opts, p->p, err)) return fail(STEEL_E_INVALID, err);
+  *out = p.release();
+  return STEEL_OK;
+}
+
+int steel_packed_desc(const steel_packed* p, steel_scene_desc* out) {
+  if (!p || !out) return fail(STEEL_E_INVALID, "null argument");
+  const scene::Packed& k = p->p;
+  out->constants = k.constants.c_str();
+  out->statF = k.statF.data();
+  out->statF_floats = k.statF.size();
+  out->statU = k.statU.data();
+  out->statU_words = k.statU.size();
+  out->body_pose = k.body_pose.data();
+  out->body_vel = k.body_vel.data();
+  out->art = k.art.data();
+  out->art_floats = k.art.size();
+  return STEEL_OK;
+}
+
+int steel_packed_free(steel_packed* p) {
+  delete p;
+  return STEEL_OK;
+}
+
+int steel_batch_create_files(steel_ctx* ctx, uint32_t n, const char* const* json, const uint64_t* json_len,
+                             const void* const* bin, const uint64_t* bin_len, const char* const* opts_json,
+                             steel_batch** out) {
+  if (!ctx || !json || !json_len || !bin || !bin_len || !out || n == 0) return fail(STEEL_E_INVALID, "null argument");
+  std::vector<std::shared_ptr<steel_packed>> packed(n);
+  std::vector<steel_scene_desc> descs(n);
+  for (uint32_t i = 0; i < n; i++) {
+    steel_packed* p = nullptr;
+    int rc = steel_pack(json[i], json_len[i], bin[i], bin_len[i], opts_json ? opts_json[i] : nullptr, &p);
+    if (rc) return fail(rc, "scene " + std::to_string(i) + ": " + g_err);
+    packed[i].reset(p);
+    steel_packed_desc(p, &descs[i]);
+  }
+  steel_batch* b = nullptr;
+  int rc = steel_batch_create(ctx, descs.data(), n, &b);
+  if (rc) return rc;
+  for (uint32_t i = 0; i < n; i++)
+    b->sc[i].files = std::shared_ptr<const scene::Packed>(packed[i], &packed[i]->p);
+  *out = b;
+  return STEEL_OK;
+}
+
+int steel_scene_create(steel_ctx* ctx, const char* json, uint64_t json_len, const void* bin, uint64_t bin_len,
+                       const char* opts_json, steel_batch** out) {
+  return steel_batch_create_files(ctx, 1, &json, &json_len, &bin, &bin_len, &opts_json, out);
+}
+
+int steel_newton_info(steel_batch* b, uint32_t scene, steel_newton_info_t* out) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || !out) return fail(STEEL_E_INVALID, "bad scene index or null output");
+  if (!s->files) return fail(STEEL_E_INVALID, "the scene was not created from its files (steel_scene_create)");
+  const scene::Packed& k = *s->files;
+  out->bodies = k.NB;
+  out->joint_coords = (uint32_t)k.joint_q.size();
+  out->joint_dofs = k.joint_qd_count;
+  return STEEL_OK;
+}
+
+int steel_newton_dof(steel_batch* b, uint32_t scene, uint32_t newton_dof, uint32_t* port_dof) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || !port_dof) return fail(STEEL_E_INVALID, "bad scene index or null output");
+  if (!s->files) return fail(STEEL_E_INVALID, "the scene was not created from its files (steel_scene_create)");
+  auto it = s->files->dof_map.find(newton_dof);
+  if (it == s->files->dof_map.end())
+    return fail(STEEL_E_INVALID, "dof " + std::to_string(newton_dof) + " is not simulated as an articulation dof");
+  *port_dof = it->second;
+  return STEEL_OK;
+}
+
+int steel_state(steel_batch* b, uint32_t scene, float* bodyQ, float* bodyQd, float* jointQ, float* jointQd) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || !bodyQ || !bodyQd || !jointQ || !jointQd) return fail(STEEL_E_INVALID, "bad scene index or null buffer");
+  if (!s->files) return fail(STEEL_E_INVALID, "the scene was not created from its files (steel_scene_create)");
+  const scene::Packed& k = *s->files;
+  const SceneDev& d = s->d;
+  const uint32_t NB = d.NB;
+  std::vector<float> poses(8ull * NB), vel(8ull * NB), q(std::max(d.NQ, 1u)), qd(std::max(d.ND, 1u)),
+      lv(6ull * std::max(d.NL, 1u));
+  int rc = steel_read_state(b, scene, poses.data(), vel.data(), q.data(), qd.data(), lv.data());
+  if (rc) return rc;
+  // Articulated links keep their COM twist in the link record (angular, then linear).
+  for (uint32_t l = 0; l < d.NL; l++) {
+    const uint32_t bd = k.link_body[l];
+    const float* t = &lv[6ull * l];
+    const float w[8] = {t[3], t[4], t[5], 0.0f, t[0], t[1], t[2], 0.0f};
+    std::memcpy(&vel[8ull * bd], w, sizeof w);
+  }
+  for (uint32_t i = 0; i < NB; i++) {
+    const double x = poses[8ull * i + 4], y = poses[8ull * i + 5], z = poses[8ull * i + 6], w = poses[8ull * i + 7];
+    const double* c = &k.body_com[3ull * i];
+    const double ux = 2 * (x * c[0] + y * c[1] + z * c[2]);
+    const double s2 = w * w - (x * x + y * y + z * z);
+    const double cx = y * c[2] - z * c[1], cy = z * c[0] - x * c[2], cz = x * c[1] - y * c[0];
+    const double r[3] = {ux * x + s2 * c[0] + 2 * w * cx, ux * y + s2 * c[1] + 2 * w * cy, ux * z + s2 * c[2] + 2 * w * cz};
+    float* bq = bodyQ + 7ull * i;
+    for (int a = 0; a < 3; a++) bq[a] = (float)((double)poses[8ull * i + a] - r[a]);
+    bq[3] = (float)x; bq[4] = (float)y; bq[5] = (float)z; bq[6] = (float)w;
+    float* bv = bodyQd + 6ull * i;
+    bv[0] = vel[8ull * i]; bv[1] = vel[8ull * i + 1]; bv[2] = vel[8ull * i + 2];
+    bv[3] = vel[8ull * i + 4]; bv[4] = vel[8ull * i + 5]; bv[5] = vel[8ull * i + 6];
+  }
+  std::memcpy(jointQ, k.joint_q.data(), 4 * k.joint_q.size());
+  std::memset(jointQd, 0, 4ull * k.joint_qd_count);
+  for (auto& kv : k.q_map) jointQ[kv.first] = q[kv.second];
+  for (auto& kv : k.dof_map) jointQd[kv.first] = qd[kv.second];
+  for (const auto& fj : k.free_joints) {
+    std::memcpy(jointQ + fj.q_start, bodyQ + 7ull * fj.body, 28);
+    std::memcpy(jointQd + fj.qd_start, bodyQd + 6ull * fj.body, 24);
+  }
+  return STEEL_OK;
+}
+
 int steel_batch_destroy(steel_batch* b) {
   if (!b) return STEEL_OK;
   cudaSetDevice(b->ctx->device);
@@ -591,6 +729,7 @@ int steel_batch_destroy(steel_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->ev_pose) cudaEventDestroy(b->ev_pose);
   if (b->arena) cudaFree(b->arena);
   delete b;
   return STEEL_OK;
@@ -797,6 +936,30 @@ int steel_read_poses(steel_batch* b, uint32_t scene, float* poses) {
     std::memcpy(poses + i * 8, &p[i], 16);
     std::memcpy(poses + i * 8 + 4, &q[i], 16);
   }
+  return STEEL_OK;
+}
+
+int steel_copy_poses_device(steel_batch* b, uint32_t scene, float* dst, void* stream) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || !dst) return fail(STEEL_E_INVALID, "bad scene index or null buffer");
+  if (reinterpret_cast<uintptr_t>(dst) & 15u) return fail(STEEL_E_INVALID, "pose buffer must be 16-byte aligned");
+  CU(cudaSetDevice(b->ctx->device));
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, dst) != cudaSuccess || !((a.type == cudaMemoryTypeDevice && a.device == b->ctx->device) ||
+                                                           a.type == cudaMemoryTypeManaged)) {
+    (void)cudaGetLastError();
+    return fail(STEEL_E_INVALID, "pose buffer must be device memory of the batch's device");
+  }
+  cudaStream_t st = b->ctx->stream;
+  cudaStream_t out = stream ? static_cast<cudaStream_t>(stream) : st;
+  if (out != st) {
+    if (!b->ev_pose) CU(cudaEventCreateWithFlags(&b->ev_pose, cudaEventDisableTiming));
+    CU(cudaEventRecord(b->ev_pose, st));
+    CU(cudaStreamWaitEvent(out, b->ev_pose, 0));
+  }
+  const SceneDev& d = s->d;
+  launch_copy_poses(d.pos, d.rot, d.NB, reinterpret_cast<float4*>(dst), out);
+  CU(cudaGetLastError());
   return STEEL_OK;
 }
 

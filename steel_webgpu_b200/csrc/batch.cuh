@@ -158,5 +158,6 @@ void launch_frame_end(const BatchDev& b, cudaStream_t st);
 // Host-I/O staging: scatter packed joint targets into each scene, gather packed body poses.
 void launch_scatter_targets(const BatchDev& b, const float* packed, const uint64_t* offsets, cudaStream_t st);
 void launch_gather_poses(const BatchDev& b, float* packed, const uint64_t* offsets, cudaStream_t st);
+void launch_copy_poses(const float4* pos, const float4* rot, uint32_t nb, float4* dst, cudaStream_t st);
 
 }  // namespace steel

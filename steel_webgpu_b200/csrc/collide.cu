@@ -1509,6 +1509,17 @@ __global__ void k_gather_poses(BatchDev B, float* packed, const uint64_t* offset
   float4* dst = reinterpret_cast<float4*>(packed + offsets[blockIdx.x]);
   for (uint32_t b = threadIdx.x; b < S.NB; b += blockDim.x) { dst[2 * b] = S.pos[b]; dst[2 * b + 1] = S.rot[b]; }
 }
+// One scene's body poses -> a caller's device buffer of BodyPose records (COM vec4, quaternion vec4).
+__global__ void k_copy_poses(const float4* __restrict__ pos, const float4* __restrict__ rot, uint32_t nb,
+                             float4* __restrict__ dst) {
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    dst[2 * b] = pos[b];
+    dst[2 * b + 1] = rot[b];
+  }
+}
+void launch_copy_poses(const float4* pos, const float4* rot, uint32_t nb, float4* dst, cudaStream_t st) {
+  k_copy_poses<<<std::max<uint32_t>(1u, std::min<uint32_t>((nb + 255u) / 256u, 592u)), 256, 0, st>>>(pos, rot, nb, dst);
+}
 void launch_scatter_targets(const BatchDev& b, const float* packed, const uint64_t* offsets, cudaStream_t st) {
   k_scatter_targets<<<b.nscenes, 128, 0, st>>>(b, packed, offsets);
 }

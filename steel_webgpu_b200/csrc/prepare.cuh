@@ -1067,31 +1067,93 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
     for (uint32_t i = tid; i < S.NCOL + 2u; i += nt) wcount[i] = 0u;
     if (S.stage & STAGE_WMASK)
       for (uint32_t i = tid; i < S.NB * NCOLW; i += nt) wmask[i] = 0u;
-    for (uint32_t r0 = 0; r0 < (S.LONGEST_FIRST == 0u ? total : 0u); r0 += COLOR_CHUNK) {
-      const uint32_t nrow = min(COLOR_CHUNK, total - r0);
+    (void)ckey;
+    if (S.LONGEST_FIRST == 0u) {
+      // First-fit in row order, in parallel rounds with the same colors (Jones-Plassmann with the
+      // row index as priority). Every body keeps its rows in row order and a frontier, the first
+      // of them not yet colored; rows on one body are colored in that order, so when a row is the
+      // frontier of both its bodies every earlier row touching them has its color, and the body
+      // masks hold exactly the colors the serial pass would see. Such rows share no body, so one
+      // round colors all of them without conflicts: phase A finds them (the row's lower body
+      // decides), phase B colors them and advances the frontiers. Each round colors at least the
+      // lowest uncolored row, so the rounds end.
+      uint32_t* bstart = sch + S.S_BSTART;  // [NB + 1] each body's first list entry
+      uint32_t* bpos = sch + S.S_BPOS;      // [NB] fill cursor, then frontier
+      uint32_t* bready = sch + S.S_BREADY;  // [NB] row this body's thread colors in the round
+      uint32_t* blist = sch + S.S_BLIST;    // [2 * MAXC] rows of each body
+      uint32_t* rkey = sch + S.S_RKEY;      // [MAXC] body-pair key of each row
+      const uint32_t NB = S.NB;
+      for (uint32_t b = tid; b <= NB; b += nt) bstart[b] = 0u;
       __syncthreads();
-      for (uint32_t i = tid; i < nrow; i += nt) ckey[i] = sch[S.S_UKEY + sch[S.S_RUNIT + r0 + i]];
+      for (uint32_t r = tid; r < total; r += nt) {
+        const uint32_t key = sch[S.S_UKEY + sch[S.S_RUNIT + r]];
+        rkey[r] = key;
+        const int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
+        if (a >= 0) atomicAdd(&bstart[a], 1u);
+        if (b >= 0 && b != a) atomicAdd(&bstart[b], 1u);
+      }
       __syncthreads();
-      if (tid == 0u) {
-        for (uint32_t i = 0; i < nrow; i++) {
-          uint32_t key = ckey[i];
-          int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
+      block_scan_array(bstart, NB + 1u, stmp);
+      for (uint32_t b = tid; b < NB; b += nt) bpos[b] = bstart[b];
+      __syncthreads();
+      for (uint32_t r = tid; r < total; r += nt) {
+        const uint32_t key = rkey[r];
+        const int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
+        if (a >= 0) blist[atomicAdd(&bpos[a], 1u)] = r;
+        if (b >= 0 && b != a) blist[atomicAdd(&bpos[b], 1u)] = r;
+      }
+      __syncthreads();
+      for (uint32_t b = tid; b < NB; b += nt) {  // each body's rows in row order
+        const uint32_t s0 = bstart[b], s1 = bstart[b + 1u];
+        for (uint32_t i = s0 + 1u; i < s1; i++) {
+          const uint32_t v = blist[i];
+          uint32_t j = i;
+          while (j > s0 && blist[j - 1u] > v) { blist[j] = blist[j - 1u]; j--; }
+          blist[j] = v;
+        }
+        bpos[b] = s0;
+      }
+      __syncthreads();
+      for (uint32_t round = 0; round <= total; round++) {
+        bool left = false;
+        for (uint32_t b = tid; b < NB; b += nt) {
+          uint32_t ready = 0xffffffffu;
+          const uint32_t p = bpos[b];
+          if (p < bstart[b + 1u]) {
+            left = true;
+            const uint32_t r = blist[p];
+            const uint32_t key = rkey[r];
+            const int x = (int)(key & 0xffffu) - 1, y = (int)(key >> 16u) - 1;
+            const int other = x == (int)b ? y : x;
+            if (other < 0 || other == (int)b || ((uint32_t)other > b && blist[bpos[other]] == r)) ready = r;
+          }
+          bready[b] = ready;
+        }
+        if (!__syncthreads_or(left)) break;
+        for (uint32_t b = tid; b < NB; b += nt) {
+          const uint32_t r = bready[b];
+          if (r == 0xffffffffu) continue;
+          const uint32_t key = rkey[r];
+          const int a = (int)(key & 0xffffu) - 1, c = (int)(key >> 16u) - 1;
           uint32_t col = S.NCOL;
           for (uint32_t w = 0; w < NCOLW; w++) {
             uint32_t used = 0u;
             if (a >= 0) used |= wmask[(uint32_t)a * NCOLW + w];
-            if (b >= 0) used |= wmask[(uint32_t)b * NCOLW + w];
+            if (c >= 0) used |= wmask[(uint32_t)c * NCOLW + w];
             if (used != 0xffffffffu) {
               uint32_t k = (uint32_t)__ffs(~used) - 1u;
               if (a >= 0) wmask[(uint32_t)a * NCOLW + w] |= 1u << k;
-              if (b >= 0) wmask[(uint32_t)b * NCOLW + w] |= 1u << k;
+              if (c >= 0) wmask[(uint32_t)c * NCOLW + w] |= 1u << k;
               col = w * 32u + k;
               break;
             }
           }
-          sch[S.S_PCOL + r0 + i] = col;
-          wcount[col]++;
+          sch[S.S_PCOL + r] = col;
+          atomicAdd(&wcount[col], 1u);
+          if (a >= 0) bpos[a]++;
+          if (c >= 0 && c != a) bpos[c]++;
         }
+        __syncthreads();
       }
     }
     __syncthreads();

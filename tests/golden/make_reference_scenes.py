@@ -4,7 +4,8 @@ skild-ai/steel-webgpu) into test fixtures for the CUDA-vs-oracle parity test
 
 The folders only exist where the reference is checked out, and the GPU box has no copy, so this
 script packs each scene with ``steel_webgpu_b200.pack`` (the restatement of sim.js:95-521) and
-writes the packed scene, a pickled ``Packed``, to ``tests/golden/_ref/<scene>.pkl.gz``. That
+writes the packed scene (a pickled ``Packed``) with the scene.json text and scene.bin bytes it came
+from to ``tests/golden/_ref/<scene>.pkl.gz``. That
 folder is kept out of version control and travels with the working tree.
 
 Usage: ``python tests/golden/make_reference_scenes.py <assets/scenes folder>`` (or set
@@ -34,10 +35,13 @@ def make(folder: str, out: str = OUT) -> list[str]:
     os.makedirs(out, exist_ok=True)
     names = scene_names(folder)
     for name in names:
-        pk = pack(load_scene(os.path.join(folder, name)))
+        sc = load_scene(os.path.join(folder, name))
+        pk = pack(sc)
+        with open(os.path.join(folder, name, "scene.json"), "rb") as f:
+            text = f.read()
         tmp = os.path.join(out, name + ".pkl.gz.tmp")
         with gzip.open(tmp, "wb") as f:
-            pickle.dump(pk, f, protocol=pickle.HIGHEST_PROTOCOL)
+            pickle.dump({"packed": pk, "json": text, "bin": sc.bin}, f, protocol=pickle.HIGHEST_PROTOCOL)
         os.replace(tmp, os.path.join(out, name + ".pkl.gz"))
     return names
 

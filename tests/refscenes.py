@@ -26,9 +26,20 @@ def names() -> list[str]:
     return sorted(f[:-len(".pkl.gz")] for f in os.listdir(DIR) if f.endswith(".pkl.gz"))
 
 
-def load(name: str):
+def _record(name: str) -> dict:
     with gzip.open(os.path.join(DIR, name + ".pkl.gz"), "rb") as f:
         return pickle.load(f)
+
+
+def load(name: str):
+    """The scene packed by steel_webgpu_b200.pack (the Python restatement of Sim.build)."""
+    return _record(name)["packed"]
+
+
+def files(name: str) -> tuple[bytes, bytes]:
+    """The scene's own files: scene.json text and scene.bin bytes."""
+    r = _record(name)
+    return r["json"], r["bin"]
 
 
 def frames_of(name: str) -> int:

@@ -200,3 +200,22 @@ def test_wait_timeout_is_reported_and_context_recovers(steel, oracle_lib):
     o.step(20)
     g.sync()
     _assert_same_state(g, o, pk, what="after the timeout and reset")
+
+
+def test_pose_export_device_to_device(steel):
+    """steel_copy_poses_device (the pose bridge's GPU-to-GPU copy) on a caller's stream gives the
+    same records as the host readback, for every scene of a batch."""
+    import torch
+    torch.cuda.init()
+    pks = [pack(s) for s in scenes.small_batch(n=4)]
+    g = Batch(pks)
+    g.step(12)
+    L = _lib.load()
+    side = torch.cuda.Stream()
+    for i, pk in enumerate(pks):
+        dst = torch.full((pk.NB * 8,), float("nan"), dtype=torch.float32, device="cuda:0")
+        _lib.check(L.steel_copy_poses_device(g.h, i, ctypes.c_void_p(dst.data_ptr()), ctypes.c_void_p(side.cuda_stream)))
+        side.synchronize()
+        assert np.array_equal(_bits(dst.cpu().numpy()), _bits(g.poses(i))), f"scene {i}"
+    host = np.zeros(8, dtype=np.float32)
+    assert L.steel_copy_poses_device(g.h, 0, ctypes.c_void_p(host.ctypes.data), None) == 1
