@@ -54,18 +54,22 @@ def _build_single(kind: str, seed: int):
 
 
 def _build_chunk(args):
-    seed, lo, hi, n_total, caps_mode = args
+    seed, lo, hi, n_total, caps_mode, fp64 = args
     from steel_webgpu_b200 import pack, synth
     from steel_webgpu_b200.sim import auto_caps
     # Every scene draws from its own generator seeded by (seed, index), so chunks are independent.
+    opts = {"solver": {"articulation_fp64": True}} if fp64 else None
     out = []
     for i in range(lo, hi):
         sc = synth.uneven_batch(n_scenes=1, seed=seed * 1000003 + i)[0]
-        out.append(pack(sc, caps=auto_caps(sc) if caps_mode == "auto" else None))
+        out.append(pack(sc, opts=opts, caps=auto_caps(sc) if caps_mode == "auto" else None))
     return out
 
 
-def build_workload(name: str, seed: int, caps_mode: str = "auto", nproc: int | None = None, limit: int | None = None):
+def build_workload(name: str, seed: int, caps_mode: str = "auto", nproc: int | None = None, limit: int | None = None,
+                   fp64: bool = False):
+    """The workload's packed scenes. fp64: the articulated-inertia pass's D factor/inverse and root
+    inertia accumulation in FP64 (the uneven batch's stated precision split)."""
     if "single" in WORKLOADS[name]:
         return _build_single(WORKLOADS[name]["single"], seed)
     n = WORKLOADS[name]["n_scenes"]
@@ -73,7 +77,7 @@ def build_workload(name: str, seed: int, caps_mode: str = "auto", nproc: int | N
         n = min(n, limit)
     nproc = nproc or min(os.cpu_count() or 1, 32)
     chunk = max(1, math.ceil(n / (nproc * 4)))
-    jobs = [(seed, lo, min(lo + chunk, n), n, caps_mode) for lo in range(0, n, chunk)]
+    jobs = [(seed, lo, min(lo + chunk, n), n, caps_mode, fp64) for lo in range(0, n, chunk)]
     if nproc <= 1 or len(jobs) == 1:
         parts = [_build_chunk(j) for j in jobs]
     else:
@@ -318,6 +322,7 @@ def run_reference(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": args.workload, "sample_scenes": len(sample), "sample_bodies": nb,
+                       "precision": "FP32 throughout, the reference's own arithmetic",
                        "fps": sample[0].params["fps"], "substeps": sample[0].params["substeps"], "iterations": sample[0].params["iterations"]},
             "cpu_baseline": {"value": value, "unit": "body-steps/s", "cores": nproc, "kind": "port",
                              "sample": f"{len(sample)} scenes ({nb} bodies) of {args.workload}, 1 frame per step"},
@@ -330,7 +335,8 @@ def run_steel(args):
     rank, world, local = dist_setup(args.gpus)
     from steel_webgpu_b200.sim import Batch
     t_build = time.perf_counter()
-    pks = build_workload(args.workload, args.seed + rank)
+    fp64 = args.fp64_dinv == "on"
+    pks = build_workload(args.workload, args.seed + rank, fp64=fp64)
     build_s = time.perf_counter() - t_build
     batch = Batch(pks, device=local)
     nbodies = sum(pk.NB for pk in pks)
@@ -404,6 +410,9 @@ def run_steel(args):
                    "graph": True, "l2": "per-scene state is resident and re-read every substep; no L2 flush",
                    "contact_steps_per_s": world * counts["contacts"] * substeps * args.steps / (ms / 1000.0),
                    "build_s": round(build_s, 1), "overflow_scenes": overflow_scenes,
+                   "fp64_dinv": fp64 and "single" not in WORKLOADS[args.workload],
+                   "placement": "each scene's boxes on a 0.4 m grid, dropped from 0.3-1.3 m onto its plane (a 2x2x2 m "
+                                "volume cannot hold 512 boxes of half-extents 0.05-0.15 m without overlaps)",
                    "tiles": dict(tiles, source="autotuner" if args.tiles == "auto" else "command line",
                                  tuning_ms_per_frame=tune_ms, tuning_s=round(tune_s, 2)),
                    "frame_latency_ms": {"p50": float(np.percentile(frame_ms, 50)),
@@ -490,6 +499,8 @@ def main():
     ap.add_argument("--tiles", default="auto",
                     help='"auto" (autotuner) or block_threads,smem_budget,narrow_blocks_per_sm')
     ap.add_argument("--tune-frames", type=int, default=3)
+    ap.add_argument("--fp64-dinv", default="on", choices=["on", "off"],
+                    help="FP64 in the articulated-inertia D factor/inverse and root inertia (uneven batch)")
     ap.add_argument("--serve-instances", type=int, default=512)
     ap.add_argument("--serve-requests", type=int, default=3000)
     ap.add_argument("--serve-rate", type=float, default=2000.0)
