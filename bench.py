@@ -37,6 +37,9 @@ WORKLOADS = {
     "convex_pour_8192": dict(n_scenes=1, single="convex_pour"),  # 8192 hulls, boxes, capsules in a bin
     "quadrupeds_1024": dict(n_scenes=1, single="quadrupeds"),  # 1024 quadrupeds + 64 x 40-link chains
     "boxes_64": dict(n_scenes=1, single="boxes"),  # 64 boxes on a plane
+    # Serving: resident instances of the articulation workload's sizes (1-4 quadrupeds, or one
+    # 40-link chain, on a plane; 500 fps), mixed so that instances differ in size.
+    "serve_quadrupeds_4096": dict(n_scenes=4096, serve=True),
 }
 
 
@@ -61,6 +64,12 @@ def _build_chunk(args):
     opts = {"solver": {"articulation_fp64": True}} if fp64 else None
     out = []
     for i in range(lo, hi):
+        if n_total < 0:  # serving instances
+            kind = i % 5
+            sc = synth.quadrupeds(n_quad=kind + 1 if kind < 4 else 0, n_chains=1 if kind == 4 else 0, chain_links=40,
+                                  seed=seed * 1000003 + i)
+            out.append(pack(sc, opts=opts, caps=auto_caps(sc)))
+            continue
         sc = synth.uneven_batch(n_scenes=1, seed=seed * 1000003 + i)[0]
         out.append(pack(sc, opts=opts, caps=auto_caps(sc) if caps_mode == "auto" else None))
     return out
@@ -77,7 +86,8 @@ def build_workload(name: str, seed: int, caps_mode: str = "auto", nproc: int | N
         n = min(n, limit)
     nproc = nproc or min(os.cpu_count() or 1, 32)
     chunk = max(1, math.ceil(n / (nproc * 4)))
-    jobs = [(seed, lo, min(lo + chunk, n), n, caps_mode, fp64) for lo in range(0, n, chunk)]
+    total = -1 if WORKLOADS[name].get("serve") else n
+    jobs = [(seed, lo, min(lo + chunk, n), total, caps_mode, fp64) for lo in range(0, n, chunk)]
     if nproc <= 1 or len(jobs) == 1:
         parts = [_build_chunk(j) for j in jobs]
     else:
@@ -441,23 +451,16 @@ def run_steel(args):
         dist.destroy_process_group()
 
 
-def run_serve(args):
-    """Serving: Poisson arrivals of 1-32-frame requests for random resident instances, continuous
-    batching (steel_serve_*); p50/p99 request latency and served body-steps/s (one JSON line)."""
-    from steel_webgpu_b200.sim import Batch, Server
-    pks = build_workload(args.workload, args.seed, limit=args.serve_instances)
-    batch = Batch(pks)
-    batch.step(3)
-    batch.sync()
-    srv = Server(batch, max_active=args.serve_max_active)
-    rng = np.random.default_rng(args.seed)
-    n = args.serve_requests
-    gaps = rng.exponential(1.0 / args.serve_rate, n)
-    arrive = np.cumsum(gaps)
+def _serve_at_rate(batch, pks, rate: float, n: int, seed: int, max_active: int, budget: int) -> dict:
+    """Poisson arrivals at `rate` requests/s of n requests (1-32 frames each, random instances),
+    continuous batching through steel_serve_*; latency from submit to completion."""
+    from steel_webgpu_b200.sim import Server
+    srv = Server(batch, max_active=max_active, budget_bytes=budget)
+    rng = np.random.default_rng(seed)
+    arrive = np.cumsum(rng.exponential(1.0 / rate, n))
     inst = rng.integers(0, len(pks), n)
     frames = rng.integers(1, 33, n)
-    done, k, lat = 0, 0, []
-    body_frames = 0
+    done, k, lat, body_frames, ticks, active = 0, 0, [], 0, 0, []
     t0 = time.perf_counter()
     while done < n:
         now = time.perf_counter() - t0
@@ -465,21 +468,51 @@ def run_serve(args):
             srv.submit(int(inst[k]), int(frames[k]))
             body_frames += pks[int(inst[k])].NB * int(frames[k])
             k += 1
-        if srv.tick() == 0 and k < n:
+        stepped = srv.tick()
+        if stepped == 0 and k < n:
             time.sleep(max(0.0, min(arrive[k] - (time.perf_counter() - t0), 0.001)))
+        else:
+            ticks += 1
+            active.append(stepped)
         for _, _, ms in srv.poll():
             lat.append(ms)
             done += 1
     wall = time.perf_counter() - t0
     srv.close()
+    return {"rate_per_s": rate, "requests": n, "completed_per_s": n / wall, "body_steps_per_s": body_frames / wall,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "ticks": ticks, "mean_admitted": float(np.mean(active)) if active else 0.0, "wall_s": round(wall, 2)}
+
+
+def run_serve(args):
+    """Serving: resident instances, Poisson arrivals of 1-32-frame requests for random instances at
+    each rate of a sweep, continuous batching (steel_serve_*) with admission by an HBM budget;
+    p50/p99 request latency and served body-steps/s per rate, beside the plain per-scene path."""
+    from steel_webgpu_b200.sim import Batch
+    pks = build_workload(args.workload, args.seed, limit=args.serve_instances)
+    batch = Batch(pks)
+    batch.step(2)
+    batch.sync()
+    inst_bytes = [batch.scene_bytes(i) for i in range(len(pks))]
+    budget = int(args.serve_budget_mb * 1e6)
+    rates = [float(r) for r in args.serve_rates.split(",")]
+    sweep = []
+    for r in rates:
+        n = int(min(max(r * args.serve_seconds, 300), args.serve_requests))
+        sweep.append(_serve_at_rate(batch, pks, r, n, args.seed, args.serve_max_active, budget))
+        print(json.dumps(sweep[-1]), file=sys.stderr, flush=True)
+    plain = plain_path_sample(pks[:16], 4, 0)
     print(json.dumps({
-        "metric": "served body-steps/s", "value": body_frames / wall, "unit": "body-steps/s", "n_gpus": 1,
-        "higher_is_better": True, "data": "synthetic (seeded scenes, no dataset)",
-        "config": {"workload": args.workload, "instances": len(pks), "requests": n, "rate_per_s": args.serve_rate,
-                   "frames_per_request": "uniform 1-32", "max_active": args.serve_max_active or len(pks)},
-        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                       "mean": float(np.mean(lat))},
-        "wall_s": wall}), flush=True)
+        "metric": "served body-steps/s", "value": max(x["body_steps_per_s"] for x in sweep), "unit": "body-steps/s",
+        "n_gpus": 1, "higher_is_better": True, "data": "synthetic (seeded scenes, no dataset)",
+        "config": {"workload": args.workload, "instances": len(pks), "bodies": sum(pk.NB for pk in pks),
+                   "instance_mb": {"min": min(inst_bytes) / 1e6, "max": max(inst_bytes) / 1e6,
+                                   "total": sum(inst_bytes) / 1e6},
+                   "hbm_budget_mb": args.serve_budget_mb, "max_active": args.serve_max_active or len(pks),
+                   "frames_per_request": "uniform 1-32", "arrivals": "Poisson"},
+        "sweep": sweep,
+        "plain_path": {"body_steps_per_s": plain, "sample": "16 instances, each alone (one scene per launch sequence)"},
+    }), flush=True)
     batch.close()
 
 
@@ -501,14 +534,18 @@ def main():
     ap.add_argument("--tune-frames", type=int, default=3)
     ap.add_argument("--fp64-dinv", default="on", choices=["on", "off"],
                     help="FP64 in the articulated-inertia D factor/inverse and root inertia (uneven batch)")
-    ap.add_argument("--serve-instances", type=int, default=512)
-    ap.add_argument("--serve-requests", type=int, default=3000)
-    ap.add_argument("--serve-rate", type=float, default=2000.0)
+    ap.add_argument("--serve-instances", type=int, default=4096)
+    ap.add_argument("--serve-requests", type=int, default=20000)
+    ap.add_argument("--serve-rates", default="1000,3000,10000,20000,50000")
+    ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--serve-budget-mb", type=float, default=0.0)
     ap.add_argument("--serve-max-active", type=int, default=0)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
     elif args.mode == "serve":
+        if args.workload == "uneven_batch_2048":
+            args.workload = "serve_quadrupeds_4096"
         run_serve(args)
     else:
         run_steel(args)

@@ -194,13 +194,25 @@ int steel_debug_set_wait_limit(steel_batch* b, uint32_t rounds);
    counterpart in the reference; the closest is Sim.run (sim.js:705-712), which keeps up to four
    frames of one scene in flight. Requests of `frames` frames queue per instance; up to max_active
    instances are admitted at a time, first come first served (0 or a value above the scene count:
-   all). Each tick steps every admitted instance by one frame and waits for it; an instance whose
-   request is done takes its next queued request or makes room for the next waiting instance.
+   all) and within the byte budget of steel_serve_budget. Each tick steps every admitted instance by
+   one frame and waits for it (the per-scene kernels launch one block per admitted instance; the
+   other instances' shape and pair work is skipped); an instance whose request is done takes its
+   next queued request or makes room for the next waiting instance.
    Latency is measured from submit to the end of the request's last tick. While the loop runs,
    steel_step and steel_collide step only the admitted instances; steel_serve_end makes every
    scene step again. Scenes are independent, so an instance's result is the same alone and in any
    mix. */
 int steel_serve_config(steel_batch* b, uint32_t max_active);
+/* Admission by memory: the admitted instances' state (their share of the batch's device arena:
+   static scene data, bodies, contacts, rows, articulation blocks, scratch) may total at most
+   `bytes` (0: no limit; the head of the queue is admitted whenever nothing is). This bounds the
+   working set each tick's kernels read and write, so instances of different sizes share the
+   device by size rather than by count. The per-scene kernels launch one block per admitted
+   instance (the others launch nothing), and ticks launch their kernels directly, without the
+   frame graph, since the launch sizes change from tick to tick. */
+int steel_serve_budget(steel_batch* b, uint64_t bytes);
+/* Bytes of one scene's state in the batch arena (the unit of steel_serve_budget). */
+int steel_scene_bytes(steel_batch* b, uint32_t scene, uint64_t* bytes);
 int steel_serve_submit(steel_batch* b, uint32_t instance, uint32_t frames, uint64_t* id);
 int steel_serve_tick(steel_batch* b, uint32_t* stepped /* instances stepped in this tick */);
 int steel_serve_poll(steel_batch* b, uint64_t* ids, uint32_t* instances, double* latency_ms, uint32_t cap,

@@ -94,6 +94,8 @@ SIGNATURES = {
     "steel_profile_kernels": [_VP, _U32, _VP],
     "steel_sort_contacts_noalloc": [_VP, _U32, _VP, _VP],
     "steel_serve_config": [_VP, _U32],
+    "steel_serve_budget": [_VP, ctypes.c_uint64],
+    "steel_scene_bytes": [_VP, _U32, ctypes.POINTER(ctypes.c_uint64)],
     "steel_serve_submit": [_VP, _U32, _U32, ctypes.POINTER(ctypes.c_uint64)],
     "steel_serve_tick": [_VP, ctypes.POINTER(_U32)],
     "steel_serve_poll": [_VP, _VP, _VP, _VP, _U32, ctypes.POINTER(_U32)],

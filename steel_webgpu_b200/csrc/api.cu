@@ -99,6 +99,7 @@ struct SceneHost {
   std::vector<float4> pos0, rot0, lv0, av0;
   std::vector<float> art0;
   uint32_t collide_pairs = 0, collide_contacts = 0;  // counts of the last steel_collide
+  size_t arena_bytes = 0;                             // this scene's share of the batch arena
   // Newton index maps and scene data of a scene created from its files (steel_scene_create):
   // what Sim.state() and the Newton-indexed setters need (sim.js:716-785).
   std::shared_ptr<const scene::Packed> files;
@@ -149,6 +150,8 @@ struct steel_batch {
   std::vector<uint32_t> serve_mask;            // host copy of the device activity mask
   std::vector<Done> serve_done;
   uint32_t serve_admitted = 0, serve_max_active = 0;
+  uint64_t serve_budget = 0, serve_bytes = 0;  // admission budget (bytes of admitted instances' state), in use
+  bool serve_dirty = false;                    // admitted set changed: upload the launch order
   std::vector<uint32_t> order_host;  // block order of the prepare and solve kernels
   uint64_t serve_next_id = 1;
   bool serve_on = false;
@@ -257,6 +260,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, uint32_t th
   copy_block(d.A_TGT, "A_TGT", ND);
   copy_block(d.A_TGTV, "A_TGTV", ND);
   // Arena pieces.
+  const size_t arena0 = L.bytes;
   s.o_sf = L.take(s.statF.size() * 4);
   s.o_su = L.take(s.statU.size() * 4);
   s.o_pos = L.take((size_t)NB * 16); s.o_rot = L.take((size_t)NB * 16);
@@ -282,6 +286,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, uint32_t th
   s.o_tw = L.take((size_t)NB * 32); s.o_imp = L.take((size_t)NB * 32);
   s.o_aqd = L.take((size_t)(ND > 0 ? ND : 1) * 4);
   s.o_tscr = L.take((size_t)threads * s.tscr_floats * 4);
+  s.arena_bytes = L.bytes - arena0;
   return STEEL_OK;
 }
 
@@ -552,6 +557,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   bd.substep_count = at<unsigned long long>(A, b->o_ssc);
   bd.active = at<uint32_t>(A, b->o_active);
   bd.order = at<uint32_t>(A, b->o_order);
+  bd.nlaunch = n;
   {
     // Prepare and solve blocks take the scenes longest first (chain length, then bodies), so
     // short scenes fill the end of the launch.
@@ -829,7 +835,8 @@ int steel_step(steel_batch* b, uint32_t frames) {
   if (!b) return fail(STEEL_E_INVALID, "null batch");
   CU(cudaSetDevice(b->ctx->device));
   cudaStream_t st = b->ctx->stream;
-  if (b->use_graph && !b->graph) {
+  const bool graph = b->use_graph && !b->serve_on;  // the serving loop's launch sizes change from tick to tick
+  if (graph && !b->graph) {
     cudaGraph_t g;
     CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     enqueue_substeps(b, st);
@@ -839,7 +846,7 @@ int steel_step(steel_batch* b, uint32_t frames) {
     if (e != cudaSuccess) return fail(STEEL_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   }
   for (uint32_t f = 0; f < frames; f++) {
-    if (b->use_graph) CU(cudaGraphLaunch(b->graph, st));
+    if (graph) CU(cudaGraphLaunch(b->graph, st));
     else enqueue_substeps(b, st);
   }
   CU(cudaGetLastError());
@@ -1165,16 +1172,48 @@ static int serve_begin(steel_batch* b) {
   b->serve_waiting.clear();
   b->serve_done.clear();
   b->serve_admitted = 0;
+  b->serve_bytes = 0;
   if (b->serve_max_active == 0 || b->serve_max_active > n) b->serve_max_active = n;
   CU(cudaSetDevice(b->ctx->device));
   CU(cudaMemcpyAsync(b->arena + b->o_active, b->serve_mask.data(), 4ull * n, cudaMemcpyHostToDevice, b->ctx->stream));
   b->serve_on = true;
+  b->serve_dirty = true;
+  return STEEL_OK;
+}
+
+// The per-scene kernels launch one block per admitted instance: the admitted instances, in the
+// batch's longest-first order, go to the front of the launch order.
+static int serve_upload_order(steel_batch* b) {
+  std::vector<uint32_t> order;
+  order.reserve(b->serve_admitted);
+  for (uint32_t i : b->order_host)
+    if (b->serve_state[i] == 2) order.push_back(i);
+  cudaStream_t st = b->ctx->stream;
+  CU(cudaMemcpyAsync(b->arena + b->o_active, b->serve_mask.data(), 4ull * b->sc.size(), cudaMemcpyHostToDevice, st));
+  if (!order.empty()) CU(cudaMemcpyAsync(b->arena + b->o_order, order.data(), 4ull * order.size(), cudaMemcpyHostToDevice, st));
+  // The host copy must outlive the copy: wait for it (the tick synchronizes anyway).
+  CU(cudaStreamSynchronize(st));
+  b->bd.nlaunch = (uint32_t)order.size();
+  b->serve_dirty = false;
   return STEEL_OK;
 }
 
 int steel_serve_config(steel_batch* b, uint32_t max_active) {
   if (!b) return fail(STEEL_E_INVALID, "null batch");
   b->serve_max_active = max_active;
+  return STEEL_OK;
+}
+
+int steel_serve_budget(steel_batch* b, uint64_t bytes) {
+  if (!b) return fail(STEEL_E_INVALID, "null batch");
+  b->serve_budget = bytes;
+  return STEEL_OK;
+}
+
+int steel_scene_bytes(steel_batch* b, uint32_t scene, uint64_t* bytes) {
+  SceneHost* s = scene_of(b, scene);
+  if (!s || !bytes) return fail(STEEL_E_INVALID, "bad scene index or null output");
+  *bytes = s->arena_bytes;
   return STEEL_OK;
 }
 
@@ -1197,23 +1236,26 @@ int steel_serve_tick(steel_batch* b, uint32_t* stepped) {
   if (int rc = serve_begin(b)) return rc;
   CU(cudaSetDevice(b->ctx->device));
   cudaStream_t st = b->ctx->stream;
-  bool changed = false;
+  // Admission, first come first served, within max_active instances and the byte budget of their
+  // state (the head of the queue is always admitted when nothing is).
   while (b->serve_admitted < b->serve_max_active && !b->serve_waiting.empty()) {
     uint32_t i = b->serve_waiting.front();
+    const uint64_t bytes = b->sc[i].arena_bytes;
+    if (b->serve_budget && b->serve_admitted > 0 && b->serve_bytes + bytes > b->serve_budget) break;
     b->serve_waiting.pop_front();
     b->serve_state[i] = 2;
     b->serve_mask[i] = 1u;
     b->serve_admitted++;
-    changed = true;
+    b->serve_bytes += bytes;
+    b->serve_dirty = true;
   }
   if (stepped) *stepped = b->serve_admitted;
   if (b->serve_admitted == 0) return STEEL_OK;
-  if (changed)
-    CU(cudaMemcpyAsync(b->arena + b->o_active, b->serve_mask.data(), 4ull * b->sc.size(), cudaMemcpyHostToDevice, st));
+  if (b->serve_dirty)
+    if (int rc = serve_upload_order(b)) return rc;
   if (int rc = steel_step(b, 1)) return rc;
   CU(cudaStreamSynchronize(st));
   const double t = now_ms();
-  changed = false;
   for (uint32_t i = 0; i < (uint32_t)b->sc.size(); i++) {
     if (b->serve_state[i] != 2) continue;
     auto& q = b->serve_queue[i];
@@ -1225,12 +1267,11 @@ int steel_serve_tick(steel_batch* b, uint32_t* stepped) {
       b->serve_state[i] = 0;
       b->serve_mask[i] = 0u;
       b->serve_admitted--;
-      changed = true;
+      b->serve_bytes -= b->sc[i].arena_bytes;
+      b->serve_dirty = true;
     }
   }
-  if (changed)
-    CU(cudaMemcpyAsync(b->arena + b->o_active, b->serve_mask.data(), 4ull * b->sc.size(), cudaMemcpyHostToDevice, st));
-  return STEEL_OK;
+  return check_device_error(b);
 }
 
 int steel_serve_poll(steel_batch* b, uint64_t* ids, uint32_t* instances, double* latency_ms, uint32_t cap,
@@ -1251,7 +1292,11 @@ int steel_serve_end(steel_batch* b) {
   if (!b) return fail(STEEL_E_INVALID, "null batch");
   if (!b->serve_on) return STEEL_OK;
   CU(cudaSetDevice(b->ctx->device));
-  CU(cudaMemsetAsync(b->arena + b->o_active, 1, 4ull * b->sc.size(), b->ctx->stream));
+  cudaStream_t st = b->ctx->stream;
+  CU(cudaMemsetAsync(b->arena + b->o_active, 1, 4ull * b->sc.size(), st));
+  CU(cudaMemcpyAsync(b->arena + b->o_order, b->order_host.data(), 4ull * b->order_host.size(), cudaMemcpyHostToDevice, st));
+  CU(cudaStreamSynchronize(st));
+  b->bd.nlaunch = (uint32_t)b->sc.size();
   b->serve_on = false;
   return STEEL_OK;
 }

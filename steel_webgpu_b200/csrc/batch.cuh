@@ -20,7 +20,9 @@ struct BatchDev {
   double* phase;              // per-scene clock (sim.js:674-678)
   unsigned long long* substep_count;  // [nscenes] substeps each scene has run (warm-table parity)
   const uint32_t* active;     // [nscenes] nonzero: the scene steps in this frame (serving loop mask)
-  const uint32_t* order;      // [nscenes] scenes in the prepare and solve kernels' block order (longest first)
+  const uint32_t* order;      // [nscenes] scenes in the per-scene kernels' block order (longest first)
+  uint32_t nlaunch;           // blocks of the per-scene kernels (csort, prepare, solve): order[0..nlaunch) step
+                              // (all scenes, or the serving loop's admitted instances)
   uint32_t* error;            // [1] first device-side error code (0 = none)
   uint32_t prep_smem;         // dynamic shared memory of k_prepare / k_solve launches (bytes)
   uint32_t solve_smem;

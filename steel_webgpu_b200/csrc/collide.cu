@@ -1282,8 +1282,9 @@ __global__ void __launch_bounds__(NARROW_JOB_THREADS, 4) k_narrow_jobs(BatchDev 
 // network; larger scenes are left to the device-wide radix sort below.
 __global__ void __launch_bounds__(SORT_THREADS) k_csort(BatchDev B, uint32_t smem_keys) {
   extern __shared__ uint4 sk[];
-  if (B.active[blockIdx.x] == 0u) return;
-  const SceneDev& S = B.scenes[blockIdx.x];
+  const uint32_t scene = B.order[blockIdx.x];
+  if (B.active[scene] == 0u) return;
+  const SceneDev& S = B.scenes[scene];
   uint32_t nc = min(S.counters[1], S.MAXC);
   if (nc == 0u) return;
   uint32_t n2 = 1u;
@@ -1588,7 +1589,7 @@ cudaError_t configure_sort(size_t smem_keys) {
   return cudaFuncSetAttribute(k_csort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smem_keys * sizeof(uint4)));
 }
 void launch_csort(const BatchDev& b, size_t smem_keys, const RadixDev* radix, uint32_t nradix, cudaStream_t st) {
-  k_csort<<<b.nscenes, SORT_THREADS, smem_keys * sizeof(uint4), st>>>(b, (uint32_t)smem_keys);
+  k_csort<<<b.nlaunch, SORT_THREADS, smem_keys * sizeof(uint4), st>>>(b, (uint32_t)smem_keys);
   for (uint32_t k = 0; k < nradix; k++) {
     const RadixDev& R = radix[k];
     const uint32_t sk = (uint32_t)smem_keys;

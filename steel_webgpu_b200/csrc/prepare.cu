@@ -31,8 +31,8 @@ cudaError_t configure_prepare_t<STEEL_BLOCK>(size_t smem_bytes) {
 }
 template <>
 void launch_prepare_t<STEEL_BLOCK>(const BatchDev& b, cudaStream_t st) {
-  if (b.art_f64) STEEL_NS::k_prepare<true><<<b.nscenes, STEEL_BLOCK, b.prep_smem, st>>>(b);
-  else STEEL_NS::k_prepare<false><<<b.nscenes, STEEL_BLOCK, b.prep_smem, st>>>(b);
+  if (b.art_f64) STEEL_NS::k_prepare<true><<<b.nlaunch, STEEL_BLOCK, b.prep_smem, st>>>(b);
+  else STEEL_NS::k_prepare<false><<<b.nlaunch, STEEL_BLOCK, b.prep_smem, st>>>(b);
 }
 
 }  // namespace steel

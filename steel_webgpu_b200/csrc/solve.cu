@@ -33,8 +33,8 @@ cudaError_t configure_solve_t<STEEL_BLOCK>(size_t smem_bytes) {
 }
 template <>
 void launch_solve_t<STEEL_BLOCK>(const BatchDev& b, cudaStream_t st) {
-  if (b.solve_ext) STEEL_NS::k_solve<true><<<b.nscenes, STEEL_BLOCK, b.solve_smem, st>>>(b);
-  else STEEL_NS::k_solve<false><<<b.nscenes, STEEL_BLOCK, b.solve_smem, st>>>(b);
+  if (b.solve_ext) STEEL_NS::k_solve<true><<<b.nlaunch, STEEL_BLOCK, b.solve_smem, st>>>(b);
+  else STEEL_NS::k_solve<false><<<b.nlaunch, STEEL_BLOCK, b.solve_smem, st>>>(b);
 }
 
 }  // namespace steel

@@ -127,6 +127,12 @@ class Batch:
         _lib.check(_lib.load().steel_autotune(self.h, frames, ctypes.byref(t), ctypes.byref(ms)))
         return {k: getattr(t, k) for k, _ in _lib.Tiles._fields_}, ms.value
 
+    def scene_bytes(self, scene: int = 0) -> int:
+        """Bytes of the scene's state in the batch arena (the serving budget's unit)."""
+        v = ctypes.c_uint64()
+        _lib.check(_lib.load().steel_scene_bytes(self.h, scene, ctypes.byref(v)))
+        return v.value
+
     def info(self, scene: int = 0) -> _lib.SceneInfo:
         out = _lib.SceneInfo()
         _lib.check(_lib.load().steel_scene_info_get(self.h, scene, ctypes.byref(out)))
@@ -199,9 +205,10 @@ class Server:
     frame; ``poll()`` returns finished requests with their latency (submit to completion, ms).
     """
 
-    def __init__(self, batch: Batch, max_active: int = 0):
+    def __init__(self, batch: Batch, max_active: int = 0, budget_bytes: int = 0):
         self.batch = batch
         _lib.check(_lib.load().steel_serve_config(batch.h, max_active))
+        _lib.check(_lib.load().steel_serve_budget(batch.h, budget_bytes))
 
     def submit(self, instance: int, frames: int) -> int:
         rid = ctypes.c_uint64()

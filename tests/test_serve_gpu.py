@@ -52,3 +52,32 @@ def test_served_instances_match_running_alone(steel):
         assert np.array_equal(got, ref)
     alone.close()
     b.close()
+
+
+def test_budget_admission_and_compacted_launches(steel):
+    """Admission by bytes: with a budget of the two largest instances' state, at most that much is
+    admitted per tick (the head of the queue always when nothing is); the per-scene kernels launch
+    only the admitted instances, and every instance still matches running alone."""
+    pks = [pack(s) for s in scenes.small_batch(seed=23, n=6)]
+    b = Batch(pks)
+    sizes = [b.scene_bytes(i) for i in range(len(pks))]
+    budget = sorted(sizes)[-1] + sorted(sizes)[-2]
+    srv = Server(b, budget_bytes=budget)
+    frames = {i: 3 + i for i in range(len(pks))}
+    for i, f in frames.items():
+        srv.submit(i, f)
+    done, ticks = [], 0
+    while len(done) < len(pks):
+        n = srv.tick()
+        assert n >= 1
+        done += srv.poll()
+        ticks += 1
+        assert ticks < 200
+    srv.close()
+    for i, pk in enumerate(pks):
+        alone = Batch([pk])
+        alone.step(frames[i])
+        for got, ref in zip(_state(b, i), _state(alone, 0)):
+            assert np.array_equal(got, ref), f"instance {i} differs from running alone"
+        alone.close()
+    b.close()
