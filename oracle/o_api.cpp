@@ -5,6 +5,7 @@
 #include <cstring>
 #include <sstream>
 
+#include "o_cone5.h"
 #include "oracle.h"
 #include "smath_o.h"
 
@@ -131,6 +132,15 @@ void Oracle::step(uint32_t frames) {
 using orc::Oracle;
 
 extern "C" {
+
+// One visit of the articulated angular friction block (o_cone5.h ell_block5), for the cone tests:
+// H 25 floats (row-major 5x5 response), g, mu, lam 5 floats each, the normal load, pyramidal or
+// elliptic, creep speed and relaxation; out gets the block's new impulses.
+void oracle_cone5(const float* H, const float* g, const float* mu, const float* lam, float load, int pyr, float creep,
+                  float omega, float* out) {
+  orc::ell_block5(H, g, mu, lam, load, pyr != 0, creep, omega, out);
+}
+
 
 // The oracle's float sin / cos / atan2 (smath_o.h), for accuracy tests.
 void oracle_trig(const float* x, float* s, float* c, size_t n) {

@@ -44,6 +44,8 @@ def lib():
         L.oracle_write.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t]
         L.oracle_trig.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]
         L.oracle_atan2.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]
+        L.oracle_cone5.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_float, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                                           ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -115,4 +117,13 @@ def atan2(y, x):
     x = np.ascontiguousarray(x, dtype=np.float32)
     out = np.zeros_like(y)
     lib().oracle_atan2(y.ctypes.data, x.ctypes.data, out.ctypes.data, y.size)
+    return out
+
+
+def cone5(H, g, mu, lam, load, pyramidal=False, creep=0.0, omega=1.0):
+    """The oracle's articulated angular friction block (t1, t2, spin, roll1, roll2): new impulses."""
+    a = [np.ascontiguousarray(np.asarray(x, dtype=np.float32).reshape(-1)) for x in (H, g, mu, lam)]
+    out = np.zeros(5, dtype=np.float32)
+    lib().oracle_cone5(a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, a[3].ctypes.data, load, int(pyramidal),
+                       creep, omega, out.ctypes.data)
     return out
