@@ -9,6 +9,8 @@
 // narrowphase runs one warp per pair with shuffle reductions over faces, edge pairs and
 // support points; each scene's contacts are sorted by one block.
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 #include "batch.cuh"
 #include "contact_key.cuh"
@@ -1536,16 +1538,30 @@ void launch_gather_poses(const BatchDev& b, float* packed, const uint64_t* offse
     case 512: call(512); break;               \
     default: call(128); break;                \
   }
+// A kernel's largest dynamic shared memory is an attribute of the function for the whole process,
+// not of a batch: every batch needs it at least as large as its own launches, so it only grows.
+namespace {
+std::mutex g_smem_mu;
+std::map<std::pair<int, int>, size_t> g_smem_max;  // (kernel set, block size) -> bytes set so far
+size_t grow_smem(int set, uint32_t threads, size_t bytes) {
+  std::lock_guard<std::mutex> lock(g_smem_mu);
+  size_t& m = g_smem_max[{set, (int)threads}];
+  m = std::max(m, bytes);
+  return m;
+}
+}  // namespace
 cudaError_t configure_prepare(uint32_t threads, size_t smem_bytes) {
   cudaError_t e = cudaSuccess;
-#define STEEL_CALL(N) e = configure_prepare_t<N>(smem_bytes)
+  const size_t bytes = grow_smem(0, threads, smem_bytes);
+#define STEEL_CALL(N) e = configure_prepare_t<N>(bytes)
   STEEL_BY_BLOCK(threads, STEEL_CALL)
 #undef STEEL_CALL
   return e;
 }
 cudaError_t configure_solve(uint32_t threads, size_t smem_bytes) {
   cudaError_t e = cudaSuccess;
-#define STEEL_CALL(N) e = configure_solve_t<N>(smem_bytes)
+  const size_t bytes = grow_smem(1, threads, smem_bytes);
+#define STEEL_CALL(N) e = configure_solve_t<N>(bytes)
   STEEL_BY_BLOCK(threads, STEEL_CALL)
 #undef STEEL_CALL
   return e;
@@ -1586,7 +1602,8 @@ void launch_narrow(const BatchDev& b, uint32_t narrow_blocks, cudaStream_t st) {
   k_narrow_jobs<<<narrow_blocks * 2u, NARROW_JOB_THREADS, 0, st>>>(b);
 }
 cudaError_t configure_sort(size_t smem_keys) {
-  return cudaFuncSetAttribute(k_csort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smem_keys * sizeof(uint4)));
+  const size_t bytes = grow_smem(2, SORT_THREADS, smem_keys * sizeof(uint4));
+  return cudaFuncSetAttribute(k_csort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 void launch_csort(const BatchDev& b, size_t smem_keys, const RadixDev* radix, uint32_t nradix, cudaStream_t st) {
   k_csort<<<b.nlaunch, SORT_THREADS, smem_keys * sizeof(uint4), st>>>(b, (uint32_t)smem_keys);

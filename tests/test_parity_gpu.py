@@ -298,3 +298,17 @@ def test_graph_and_eager_launches_agree(steel):
     g1.step(20)
     g2.step(20)
     assert np.array_equal(_bits(g1.poses()), _bits(g2.poses()))
+
+
+def test_batches_with_different_shared_memory_coexist(steel):
+    """A kernel's largest dynamic shared memory is set for the whole process: a batch created
+    after another, with smaller staging needs, must not break the first one's launches (graph
+    capture included)."""
+    big = Batch([pack(scenes.chains_and_quads(n_quad=2))] * 3)
+    small = Batch([pack(scenes.boxes(8))] * 3)
+    small.step(2)
+    big.step(2)
+    big.sync()
+    ref = Batch([pack(scenes.chains_and_quads(n_quad=2))])
+    ref.step(2)
+    assert np.array_equal(_bits(big.poses(1)), _bits(ref.poses()))
