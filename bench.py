@@ -173,10 +173,10 @@ def scene_counts(batch, pks):
 
 
 # DRAM bytes (read + write) per body and launch, from one ncu capture of the 512-scene uneven batch
-# (80,090 bodies, the 128-thread kernel instances at the bench batch's blocks per SM; cold cache).
-# Scaled by a batch's body count for the bench line's roofline traffic; the narrow stage is
-# k_narrow + k_narrow_jobs.
-NCU_TRAFFIC_PER_BODY = {"narrow": 2013.0, "prepare": 2180.0, "solve": 1646.0}
+# (80,090 bodies, FP64 D-inverse, the 64-thread kernel instances and 12.9 KB staging budget the
+# autotuner picks for the bench batch; cold cache). Scaled by a batch's body count for the bench
+# line's roofline traffic; the narrow stage is k_narrow + k_narrow_jobs.
+NCU_TRAFFIC_PER_BODY = {"narrow": 2031.0, "prepare": 1902.0, "solve": 1575.0}
 
 
 def kernel_bytes(k: str, c: dict, rows_vec4: int, iterations: int) -> float:
@@ -436,8 +436,8 @@ def run_steel(args):
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": NCU_TRAFFIC_PER_BODY[dom] * nbodies if dom in NCU_TRAFFIC_PER_BODY else None,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of uneven_batch_512, "
-                                       "per body, scaled to this batch",
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of uneven_batch_512 "
+                                       "(64-thread tiles, FP64 D-inverse), per body, scaled to this batch",
                      "algorithmic_bytes_per_launch": bytes_dom, "ms_per_launch": prof[dom],
                      "kernel_share": {k: round(v / total_ms, 4) for k, v in prof.items()}},
         "cpu_baseline": {"value": cpu_val, "unit": "body-steps/s", "cores": 1, "kind": "port",
