@@ -80,18 +80,15 @@ constexpr uint32_t STAGE_LINK_CAP = 44u * 1024u;   // link blocks (NL * 1072 B)
 constexpr uint32_t STAGE_BODY_CAP = 8u * 1024u;    // twists + impulses (NB * 64 B)
 constexpr uint32_t STAGE_QD_CAP = 8u * 1024u;      // generalized velocities of the solve (ND * 4 B)
 constexpr uint32_t STAGE_WMASK_CAP = 16u * 1024u;  // per-body color masks (NB * NCOLW words)
-constexpr uint32_t COLOR_CHUNK = 512u;             // row keys staged per round of the serial coloring
 // Byte offsets of a scene's parts in k_prepare's dynamic shared memory: link blocks (if staged),
-// coloring key chunk, color counts, color masks (if staged).
-struct PrepSmem { uint32_t links, ckey, wcount, wmask, total; };
+// color counts, color masks (if staged).
+struct PrepSmem { uint32_t links, wcount, wmask, total; };
 __host__ __device__ inline PrepSmem prep_smem_layout(uint32_t stage, uint32_t NL, uint32_t NB, uint32_t NCOLW,
                                                      uint32_t NCOL) {
   PrepSmem m{};
   uint32_t o = 0;
   m.links = o;
   if (stage & STAGE_LINKS) o += 4u * NL * 268u;
-  m.ckey = o;
-  o += 4u * COLOR_CHUNK;
   m.wcount = o;
   o += 4u * (NCOL + 2u);
   m.wmask = o;

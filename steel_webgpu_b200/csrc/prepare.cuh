@@ -1055,19 +1055,17 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
   if (S.PATCH == 1u)
     for (uint32_t u = tid; u < nu; u += nt) pr.build_patch(u);
   __syncthreads();
-  // Phase 6c: greedy first-fit coloring of the rows in contact order (serial on one thread, as
-  // the reference), with the per-body color masks and the color counts in shared memory and the
-  // rows' body-pair keys staged COLOR_CHUNK at a time; then the rows bucketed by color in row
-  // order (warp 0, match/ballot ranks).
+  // Phase 6c: greedy first-fit coloring of the rows in contact order (the reference's serial pass,
+  // W:1254-1267, reproduced in parallel rounds below; the longest-first order keeps a serial pass),
+  // with the per-body color masks (in shared memory when staged) and the color counts in shared
+  // memory; then the rows bucketed by color in row order (warp 0, match/ballot ranks).
   {
-    uint32_t* ckey = reinterpret_cast<uint32_t*>(pb + lay.ckey);
     uint32_t* wcount = reinterpret_cast<uint32_t*>(pb + lay.wcount);
     uint32_t* wmask = (S.stage & STAGE_WMASK) ? reinterpret_cast<uint32_t*>(pb + lay.wmask) : sch + S.S_WMASK;
     const uint32_t NCOLW = S.NCOLW;
     for (uint32_t i = tid; i < S.NCOL + 2u; i += nt) wcount[i] = 0u;
     if (S.stage & STAGE_WMASK)
       for (uint32_t i = tid; i < S.NB * NCOLW; i += nt) wmask[i] = 0u;
-    (void)ckey;
     if (S.LONGEST_FIRST == 0u) {
       // First-fit in row order, in parallel rounds with the same colors (Jones-Plassmann with the
       // row index as priority). Every body keeps its rows in row order and a frontier, the first
