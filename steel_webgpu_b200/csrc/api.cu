@@ -228,7 +228,7 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, uint32_t th
     put(d.S_DSTART, NA + 1); put(d.S_DOFF, NA); put(d.S_DLIST, d.MAXDENSE);
     // parallel coloring: per-body row lists and frontiers, row keys
     put(d.S_BSTART, NB + 1); put(d.S_BPOS, NB); put(d.S_BREADY, NB); put(d.S_BLIST, 2 * (size_t)MAXC);
-    put(d.S_RKEY, MAXC);
+    put(d.S_RKEY, MAXC); put(d.S_RFLAG, MAXC); put(d.S_WL, 2 * (size_t)NB);
     s.sched_words = so;
   }
   s.warm_words = 10ull * d.WH + 30ull * d.AH;

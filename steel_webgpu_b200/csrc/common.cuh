@@ -226,7 +226,7 @@ struct SceneDev {
   uint32_t S_UNITOF, S_DSLOT, S_CORDER, S_UKEY, S_USTART0, S_USIZE, S_USTART, S_RK0, S_RK1, S_RK2, S_BPC, S_LEAD,
       S_KEEP, S_SLOT, S_KEPT, S_ROWOF, S_RUNIT, S_RCON, S_PCOL, S_PORD, S_CSTART, S_META, S_WWIN, S_WSLOT, S_WMASK,
       S_WCOUNT, S_LINKHIT, S_JSPLIT, S_UF, S_UFF, S_UTP, S_DSTART, S_DOFF, S_DLIST, S_BSTART, S_BPOS, S_BREADY,
-      S_BLIST, S_RKEY;
+      S_BLIST, S_RKEY, S_RFLAG, S_WL;
   float* tscr;                       // per-thread scratch slices (path temporaries), TSCR floats each
   uint32_t TSCR;
   float4 *tw, *imp;                  // solve: body twists and link impulses [NB * 2]

@@ -1072,20 +1072,28 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
       // of them not yet colored; rows on one body are colored in that order, so when a row is the
       // frontier of both its bodies every earlier row touching them has its color, and the body
       // masks hold exactly the colors the serial pass would see. Such rows share no body, so one
-      // round colors all of them without conflicts: phase A finds them (the row's lower body
-      // decides), phase B colors them and advances the frontiers. Each round colors at least the
-      // lowest uncolored row, so the rounds end.
+      // round colors all of them without conflicts. A round only looks at the bodies whose
+      // frontier moved in the previous one (all bodies in the first): phase A finds the ready rows
+      // among their frontier rows (a row whose two bodies both look at it is listed once), phase B
+      // colors them, advances the frontiers and lists the moved bodies for the next round. A row
+      // is found in the round its last frontier reaches it, since that body is on the list. Each
+      // round colors at least the lowest uncolored row, so the rounds end.
       uint32_t* bstart = sch + S.S_BSTART;  // [NB + 1] each body's first list entry
       uint32_t* bpos = sch + S.S_BPOS;      // [NB] fill cursor, then frontier
-      uint32_t* bready = sch + S.S_BREADY;  // [NB] row this body's thread colors in the round
+      uint32_t* rdy = sch + S.S_BREADY;     // [NB] rows found ready in a round
       uint32_t* blist = sch + S.S_BLIST;    // [2 * MAXC] rows of each body
       uint32_t* rkey = sch + S.S_RKEY;      // [MAXC] body-pair key of each row
+      uint32_t* rflag = sch + S.S_RFLAG;    // [MAXC] the row is on the ready list
+      uint32_t* wl[2] = {sch + S.S_WL, sch + S.S_WL + S.NB};  // [2][NB] bodies to look at
+      __shared__ uint32_t wl_n[2], rdy_n;
       const uint32_t NB = S.NB;
       for (uint32_t b = tid; b <= NB; b += nt) bstart[b] = 0u;
+      if (tid == 0u) { wl_n[0] = 0u; wl_n[1] = 0u; rdy_n = 0u; }
       __syncthreads();
       for (uint32_t r = tid; r < total; r += nt) {
         const uint32_t key = sch[S.S_UKEY + sch[S.S_RUNIT + r]];
         rkey[r] = key;
+        rflag[r] = 0u;
         const int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
         if (a >= 0) atomicAdd(&bstart[a], 1u);
         if (b >= 0 && b != a) atomicAdd(&bstart[b], 1u);
@@ -1110,27 +1118,30 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
           blist[j] = v;
         }
         bpos[b] = s0;
+        if (s1 > s0) wl[0][atomicAdd(&wl_n[0], 1u)] = b;
       }
       __syncthreads();
+      uint32_t cur = 0u;
       for (uint32_t round = 0; round <= total; round++) {
-        bool left = false;
-        for (uint32_t b = tid; b < NB; b += nt) {
-          uint32_t ready = 0xffffffffu;
+        const uint32_t n = wl_n[cur];
+        if (n == 0u) break;  // the same value in every thread (read after the last barrier)
+        for (uint32_t i = tid; i < n; i += nt) {
+          const uint32_t b = wl[cur][i];
           const uint32_t p = bpos[b];
-          if (p < bstart[b + 1u]) {
-            left = true;
-            const uint32_t r = blist[p];
-            const uint32_t key = rkey[r];
-            const int x = (int)(key & 0xffffu) - 1, y = (int)(key >> 16u) - 1;
-            const int other = x == (int)b ? y : x;
-            if (other < 0 || other == (int)b || ((uint32_t)other > b && blist[bpos[other]] == r)) ready = r;
-          }
-          bready[b] = ready;
+          if (p >= bstart[b + 1u]) continue;
+          const uint32_t r = blist[p];
+          const uint32_t key = rkey[r];
+          const int x = (int)(key & 0xffffu) - 1, y = (int)(key >> 16u) - 1;
+          const int other = x == (int)b ? y : x;
+          if (other >= 0 && other != (int)b && blist[bpos[other]] != r) continue;
+          if (atomicExch(&rflag[r], 1u) == 0u) rdy[atomicAdd(&rdy_n, 1u)] = r;
         }
-        if (!__syncthreads_or(left)) break;
-        for (uint32_t b = tid; b < NB; b += nt) {
-          const uint32_t r = bready[b];
-          if (r == 0xffffffffu) continue;
+        __syncthreads();
+        const uint32_t nr = rdy_n;
+        if (tid == 0u) wl_n[cur ^ 1u] = 0u;
+        __syncthreads();
+        for (uint32_t k = tid; k < nr; k += nt) {
+          const uint32_t r = rdy[k];
           const uint32_t key = rkey[r];
           const int a = (int)(key & 0xffffu) - 1, c = (int)(key >> 16u) - 1;
           uint32_t col = S.NCOL;
@@ -1139,18 +1150,22 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
             if (a >= 0) used |= wmask[(uint32_t)a * NCOLW + w];
             if (c >= 0) used |= wmask[(uint32_t)c * NCOLW + w];
             if (used != 0xffffffffu) {
-              uint32_t k = (uint32_t)__ffs(~used) - 1u;
-              if (a >= 0) wmask[(uint32_t)a * NCOLW + w] |= 1u << k;
-              if (c >= 0) wmask[(uint32_t)c * NCOLW + w] |= 1u << k;
-              col = w * 32u + k;
+              uint32_t kk = (uint32_t)__ffs(~used) - 1u;
+              if (a >= 0) wmask[(uint32_t)a * NCOLW + w] |= 1u << kk;
+              if (c >= 0) wmask[(uint32_t)c * NCOLW + w] |= 1u << kk;
+              col = w * 32u + kk;
               break;
             }
           }
           sch[S.S_PCOL + r] = col;
           atomicAdd(&wcount[col], 1u);
-          if (a >= 0) bpos[a]++;
-          if (c >= 0 && c != a) bpos[c]++;
+          // Advance the frontiers; a body with rows left is looked at in the next round.
+          if (a >= 0 && ++bpos[a] < bstart[a + 1u]) wl[cur ^ 1u][atomicAdd(&wl_n[cur ^ 1u], 1u)] = (uint32_t)a;
+          if (c >= 0 && c != a && ++bpos[c] < bstart[c + 1u]) wl[cur ^ 1u][atomicAdd(&wl_n[cur ^ 1u], 1u)] = (uint32_t)c;
         }
+        __syncthreads();
+        if (tid == 0u) rdy_n = 0u;
+        cur ^= 1u;
         __syncthreads();
       }
     }
@@ -1217,7 +1232,40 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
       }
     }
     __syncthreads();
-    if (tid < 32u) {
+    // Rows bucketed by color, row order kept within a color (a stable counting sort): the block
+    // takes nt rows at a time; a row's place is its color's next free slot plus the rows of its
+    // color in earlier warps of the chunk plus those before it in its warp (match ranks).
+#ifdef STEEL_BLOCK
+    constexpr uint32_t BK_COLORS = 65u, BK_WARPS = STEEL_BLOCK / 32u;
+#else
+    constexpr uint32_t BK_COLORS = 65u, BK_WARPS = BIG_THREADS / 32u;
+#endif
+    __shared__ uint32_t bk_cnt[BK_WARPS][BK_COLORS], bk_off[BK_WARPS][BK_COLORS];
+    const uint32_t nw = nt >> 5u, lane = tid & 31u, warp = tid >> 5u;
+    if (S.NCOL + 1u <= BK_COLORS) {
+      for (uint32_t i = tid; i < BK_WARPS * BK_COLORS; i += nt) (&bk_cnt[0][0])[i] = 0u;
+      __syncthreads();
+      for (uint32_t r0 = 0; r0 < total; r0 += nt) {
+        const uint32_t row = r0 + tid;
+        const bool in = row < total;
+        const uint32_t col = in ? sch[S.S_PCOL + row] : 0xffffffffu;
+        const uint32_t same = __match_any_sync(0xffffffffu, col);
+        const uint32_t below = (uint32_t)__popc(same & ((1u << lane) - 1u));
+        if (in && below == 0u) bk_cnt[warp][col] = (uint32_t)__popc(same);
+        __syncthreads();
+        for (uint32_t c = tid; c <= S.NCOL; c += nt) {
+          uint32_t run = wcount[c];
+          for (uint32_t w = 0; w < nw; w++) {
+            bk_off[w][c] = run;
+            run += bk_cnt[w][c];
+            bk_cnt[w][c] = 0u;
+          }
+          wcount[c] = run;
+        }
+        __syncthreads();
+        if (in) sch[S.S_PORD + bk_off[warp][col] + below] = row;
+      }
+    } else if (tid < 32u) {
       for (uint32_t r0 = 0; r0 < total; r0 += 32u) {
         const uint32_t row = r0 + tid;
         const bool in = row < total;
