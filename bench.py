@@ -524,8 +524,8 @@ def main():
     ap.add_argument("--impl", default="steel", choices=["steel", "reference"])
     ap.add_argument("--workload", default="uneven_batch_2048", choices=list(WORKLOADS))
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--cpu-scenes", type=int, default=16)
-    ap.add_argument("--cpu-frames", type=int, default=4)
+    ap.add_argument("--cpu-scenes", type=int, default=128)
+    ap.add_argument("--cpu-frames", type=int, default=8)
     ap.add_argument("--ref-scenes", type=int, default=128)
     ap.add_argument("--plain-scenes", type=int, default=16)
     ap.add_argument("--mode", default="bench", choices=["bench", "serve"])

@@ -1123,6 +1123,24 @@ struct Narrow {
   }
 
   // narrow_pair (wgsl.js:1072-1195): all lanes enter; the serial paths become jobs of lane 0.
+  // Plane pairs and primitive-primitive pairs need no lane cooperation: the calling lane alone
+  // records the pair's job (the same record pair() would have lane 0 write) and returns true.
+  __device__ bool solo_pair(uint32_t p0, uint32_t p1) const {
+    bool swp = geo_type(p0) > geo_type(p1);
+    uint32_t sa = swp ? p1 : p0, sb = swp ? p0 : p1;
+    float4 ka = shp(sa, 3), kb = shp(sb, 3);
+    const bool plane = ka.x == 4.0f || kb.x == 4.0f;
+    if (!plane && !(ka.x != 0.0f && kb.x != 0.0f)) return false;
+    f3 pa = v3(S.spos[sa]);
+    float4 qa = S.srot[sa];
+    f3 pb = v3(S.spos[sb]);
+    float4 qb = S.srot[sb];
+    float thresh = fmn(shp(sa, 0).w + shp(sb, 0).w, S.F_GAP_GATE);
+    JobW j;
+    j.u(sa); j.u(sb); j.v(pa); j.q(qa); j.v(pb); j.q(qb); j.f(thresh);
+    defer(plane ? (geo_type(sb) == GT_CONVEX ? J_PLANE_CONVEX : J_PLANE) : J_PRIM, j);
+    return true;
+  }
   __device__ void pair(uint32_t p0, uint32_t p1) const {
     bool swp = geo_type(p0) > geo_type(p1);
     uint32_t sa = swp ? p1 : p0, sb = swp ? p0 : p1;
@@ -1229,15 +1247,33 @@ struct Narrow {
   }
 };
 
+// Each warp takes 32 pairs at a time: every lane loads one pair and, if it is a plane or a
+// primitive-primitive pair, records its job alone; the remaining pairs are then run one after
+// another by the whole warp. Only the order in which jobs and contacts are appended changes, and
+// the canonical sort removes it.
 __global__ void __launch_bounds__(NARROW_WARPS * 32, 3) k_narrow(BatchDev B) {
-  uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5u;
-  uint32_t nwarps = (gridDim.x * blockDim.x) >> 5u;
-  uint32_t total = *B.pair_count;
-  for (uint32_t g = warp; g < total; g += nwarps) {
-    uint4 pr = B.pairs[g];
-    Narrow N(B.scenes[pr.x], &B, pr.x);
-    N.pair(pr.y, pr.z);
-    __syncwarp();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5u, lane = threadIdx.x & 31u;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5u;
+  const uint32_t total = *B.pair_count;
+  for (uint32_t g0 = warp * 32u; g0 < total; g0 += nwarps * 32u) {
+    const uint32_t g = g0 + lane;
+    const bool valid = g < total;
+    const uint4 mine = valid ? B.pairs[g] : make_uint4(0u, 0u, 0u, 0u);
+    bool solo = false;
+    if (valid) {
+      Narrow N(B.scenes[mine.x], &B, mine.x);
+      solo = N.solo_pair(mine.y, mine.z);
+    }
+    uint32_t work = __ballot_sync(0xffffffffu, valid && !solo);
+    while (work != 0u) {
+      const uint32_t k = (uint32_t)__ffs(work) - 1u;
+      work &= work - 1u;
+      const uint4 pr = make_uint4(__shfl_sync(0xffffffffu, mine.x, k), __shfl_sync(0xffffffffu, mine.y, k),
+                                  __shfl_sync(0xffffffffu, mine.z, k), 0u);
+      Narrow N(B.scenes[pr.x], &B, pr.x);
+      N.pair(pr.y, pr.z);
+      __syncwarp();
+    }
   }
 }
 

@@ -938,12 +938,27 @@ struct Solver {
     if (ph != 1u)
       for (uint32_t a = tid; a < S.NA; a += nt) joint_rows(a);
     if (S.PATCH == 1u && mode == 1u) {
-      for (uint32_t us = tid; us < nu; us += nt) {
-        uint32_t s0 = S.sched[S.S_USTART + us];
-        float load = 0.0f;
-        for (uint32_t m = s0; m < s0 + S.sched[S.S_USIZE + us]; m++)
-          if (S.rows[m * S.ROWS + S.PO].w != 1.0f) load += S.rows[m * S.ROWS + 6u].x;
-        S.art[S.A_ULOAD + us] = load;
+      // Four units per thread at a time, their loads issued together (each unit's sum keeps its
+      // row order).
+      constexpr uint32_t UL = 4u;
+      for (uint32_t us0 = tid; us0 < nu; us0 += UL * nt) {
+        uint32_t s0[UL], n[UL];
+#pragma unroll
+        for (uint32_t k = 0; k < UL; k++) {
+          const uint32_t us = us0 + k * nt;
+          s0[k] = us < nu ? S.sched[S.S_USTART + us] : 0u;
+          n[k] = us < nu ? S.sched[S.S_USIZE + us] : 0u;
+        }
+        float load[UL];
+#pragma unroll
+        for (uint32_t k = 0; k < UL; k++) {
+          load[k] = 0.0f;
+          for (uint32_t m = s0[k]; m < s0[k] + n[k]; m++)
+            if (S.rows[m * S.ROWS + S.PO].w != 1.0f) load[k] += S.rows[m * S.ROWS + 6u].x;
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < UL; k++)
+          if (us0 + k * nt < nu) S.art[S.A_ULOAD + us0 + k * nt] = load[k];
       }
     }
     __syncthreads();
