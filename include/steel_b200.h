@@ -103,19 +103,23 @@ int steel_set_graph(steel_batch* b, int enabled);
    256 or 512 threads, all at 128 registers per thread, so 65536 / (128 * block_threads) blocks fit
    an SM); smem_budget caps the dynamic shared memory a block uses to stage a scene's link blocks,
    twists, qd and color masks (0: per-part caps only); narrow_blocks_per_sm sizes the persistent
-   narrowphase grid (0: as many as fit). A batch starts at 512 threads when it has no more scenes
-   than SMs (the per-thread scratch is sized for that), else at 128, which is also the largest
-   block it accepts. Results are the same bits under every configuration. */
+   narrowphase grid (0: as many as fit); stream_groups splits the scenes into that many contiguous
+   groups of about equal size whose launch sequences run on parallel streams (branches of the frame
+   graph), so one group's kernels use the SMs another group's kernel tails leave idle (0 or 1: one
+   sequence; the serving loop always uses one). A batch starts at 512 threads when it has no more
+   scenes than SMs (the per-thread scratch is sized for that), else at 128, which is also the
+   largest block it accepts. Results are the same bits under every configuration. */
 typedef struct {
   uint32_t block_threads;
   uint32_t smem_budget;
   uint32_t narrow_blocks_per_sm;
+  uint32_t stream_groups;
 } steel_tiles;
 int steel_get_tiles(steel_batch* b, steel_tiles* out);
 int steel_set_tiles(steel_batch* b, const steel_tiles* tiles);
 /* Autotuner: steps the batch from its initial state under each candidate configuration (block
    sizes with staging budgets that keep 1-16 blocks resident per SM, then one narrowphase grid
-   smaller than the default), times `frames` frames of each after two warm-up frames (CUDA events),
+   smaller than the default, then two stream groups for batches of more than twice the SM count), times `frames` frames of each after two warm-up frames (CUDA events),
    keeps the fastest and resets the batch (as steel_reset). Returns the chosen tiles and their device
    time per frame in milliseconds. */
 int steel_autotune(steel_batch* b, uint32_t frames, steel_tiles* best, float* best_ms_per_frame);

@@ -33,7 +33,7 @@ class Stats(ctypes.Structure):
 
 
 class Tiles(ctypes.Structure):
-    _fields_ = [(n, ctypes.c_uint32) for n in ("block_threads", "smem_budget", "narrow_blocks_per_sm")]
+    _fields_ = [(n, ctypes.c_uint32) for n in ("block_threads", "smem_budget", "narrow_blocks_per_sm", "stream_groups")]
 
 
 class NewtonInfo(ctypes.Structure):

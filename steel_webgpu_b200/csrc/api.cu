@@ -135,6 +135,20 @@ struct steel_batch {
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t ev_pose = nullptr;  // orders a pose export on the caller's stream after the batch's frames
+  // Scene groups: contiguous ranges of scenes whose launch sequences run on parallel streams (graph
+  // branches), so one group's kernels fill the SMs the other group's kernel tails leave idle.
+  struct Group {
+    uint32_t lo = 0, hi = 0;                  // scene range
+    size_t shape_lo = 0, tile_lo = 0, pair_lo = 0;
+    BatchDev bd{};                            // the batch's view restricted to the range
+    std::vector<RadixDev> radix;
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    uint8_t* mem = nullptr;                   // group-local tables (shape scenes, tiles, order, pair counters)
+  };
+  std::vector<Group> groups;                  // empty: one launch sequence for the whole batch
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<uint32_t> pair_cap_of;          // MAXP of each scene (pair and job list partitions)
   size_t o_scenes, o_shape_scene, o_shape_local, o_tiles, o_pairs, o_pair_count, o_jobs, o_phase, o_ssc, o_active, o_order, o_err;
   std::vector<uint32_t> shape_scene, shape_local;
   std::vector<uint4> tiles;
@@ -313,18 +327,34 @@ int upload_state(steel_batch* b) {
   return STEEL_OK;
 }
 
-void enqueue_substeps(steel_batch* b, cudaStream_t st) {
-  const BatchDev& bd = b->bd;
+void enqueue_sequence(const steel_batch* b, const BatchDev& bd, const std::vector<RadixDev>& radix, cudaStream_t st) {
   for (uint32_t s = 0; s < b->substeps; s++) {
     launch_params(bd, s, st);
     launch_shapes(bd, st);
     launch_broad(bd, st);
     launch_narrow(bd, b->narrow_blocks, st);
-    launch_csort(bd, b->sort_keys, b->radix.data(), (uint32_t)b->radix.size(), st);
+    launch_csort(bd, b->sort_keys, radix.data(), (uint32_t)radix.size(), st);
     launch_prepare(bd, st);
     launch_solve(bd, st);
   }
   launch_frame_end(bd, st);
+}
+
+// One frame's launches. With scene groups (not while serving, whose launch sizes change per tick),
+// each group's sequence goes to its own stream, forked from and joined back into `st` by events;
+// captured, they become parallel branches of the frame graph.
+void enqueue_substeps(steel_batch* b, cudaStream_t st) {
+  if (b->groups.empty() || b->serve_on) {
+    enqueue_sequence(b, b->bd, b->radix, st);
+    return;
+  }
+  cudaEventRecord(b->ev_fork, st);
+  for (auto& g : b->groups) {
+    cudaStreamWaitEvent(g.st, b->ev_fork, 0);
+    enqueue_sequence(b, g.bd, g.radix, g.st);
+    cudaEventRecord(g.done, g.st);
+    cudaStreamWaitEvent(st, g.done, 0);
+  }
 }
 
 int check_device_error(steel_batch* b) {
@@ -370,6 +400,121 @@ bool valid_block(uint32_t t) {
   return false;
 }
 
+void free_groups(steel_batch* b) {
+  for (auto& g : b->groups) {
+    if (g.st) cudaStreamDestroy(g.st);
+    if (g.done) cudaEventDestroy(g.done);
+    if (g.mem) cudaFree(g.mem);
+  }
+  b->groups.clear();
+}
+
+// The group views of the batch: the batch's launch parameters (tiles, wait limit) with scene,
+// shape, tile, pair and job tables restricted to each group's scene range.
+void refresh_groups(steel_batch* b) {
+  for (auto& g : b->groups) {
+    BatchDev v = b->bd;  // pointers, tables and counters below are the group's
+    const uint32_t n = g.hi - g.lo;
+    v.scenes = b->bd.scenes + g.lo;
+    v.nscenes = n;
+    v.nlaunch = n;
+    v.nshapes = g.bd.nshapes;
+    v.shape_scene = g.bd.shape_scene;
+    v.shape_local = b->bd.shape_local + g.shape_lo;
+    v.tiles = g.bd.tiles;
+    v.ntiles = g.bd.ntiles;
+    v.pairs = b->bd.pairs + g.pair_lo;
+    v.pair_cap = g.bd.pair_cap;
+    v.pair_count = g.bd.pair_count;
+    v.jobs = b->bd.jobs + g.pair_lo * (NJOB_WORDS / 4u);
+    v.phase = b->bd.phase + g.lo;
+    v.substep_count = b->bd.substep_count + g.lo;
+    v.active = b->bd.active + g.lo;
+    v.order = g.bd.order;
+    g.bd = v;
+  }
+}
+
+// Splits the batch into `count` groups of contiguous scenes with about equal body counts (1: one
+// launch sequence for the whole batch).
+int make_groups(steel_batch* b, uint32_t count) {
+  CU(cudaSetDevice(b->ctx->device));
+  CU(cudaStreamSynchronize(b->ctx->stream));
+  free_groups(b);
+  const uint32_t n = (uint32_t)b->sc.size();
+  if (count <= 1u || n < 2u * count) return STEEL_OK;
+  if (!b->ev_fork) CU(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+  uint64_t total = 0;
+  for (auto& s : b->sc) total += s.d.NB + 8ull * s.d.NL;
+  std::vector<uint32_t> cut{0u};
+  uint64_t acc = 0;
+  for (uint32_t i = 0; i < n && cut.size() < count; i++) {
+    acc += b->sc[i].d.NB + 8ull * b->sc[i].d.NL;
+    if (acc * count >= total * cut.size() && i + 1u < n) cut.push_back(i + 1u);
+  }
+  cut.push_back(n);
+  size_t shape_lo = 0, tile_lo = 0, pair_lo = 0;
+  uint32_t tile_i = 0;
+  for (size_t k = 0; k + 1 < cut.size(); k++) {
+    steel_batch::Group g;
+    g.lo = cut[k];
+    g.hi = cut[k + 1];
+    if (g.hi <= g.lo) continue;
+    std::vector<uint32_t> shape_scene, order;
+    std::vector<uint4> tiles;
+    uint32_t cap = 0;
+    for (uint32_t s = g.lo; s < g.hi; s++) {
+      for (uint32_t q = 0; q < b->sc[s].d.NS; q++) shape_scene.push_back(s - g.lo);
+      cap += b->pair_cap_of[s];
+    }
+    while (tile_i < b->tiles.size() && b->tiles[tile_i].x < g.hi) {
+      uint4 t = b->tiles[tile_i++];
+      t.x -= g.lo;
+      tiles.push_back(t);
+    }
+    for (uint32_t s : b->order_host)
+      if (s >= g.lo && s < g.hi) order.push_back(s - g.lo);
+    for (const RadixDev& r : b->radix)
+      if (r.scene >= g.lo && r.scene < g.hi) {
+        RadixDev rr = r;
+        rr.scene -= g.lo;
+        g.radix.push_back(rr);
+      }
+    g.shape_lo = shape_lo;
+    g.tile_lo = tile_lo;
+    g.pair_lo = pair_lo;
+    shape_lo += shape_scene.size();
+    tile_lo += tiles.size();
+    pair_lo += cap;
+    // Tables: shape scenes, tiles, order, pair counters (each 256-byte aligned).
+    Layout L;
+    const size_t o_ss = L.take(4 * shape_scene.size() + 4), o_t = L.take(16 * tiles.size() + 16),
+                 o_o = L.take(4 * order.size() + 4), o_pc = L.take(8);
+    if (cudaMalloc(&g.mem, L.bytes) != cudaSuccess) {
+      free_groups(b);
+      return fail(STEEL_E_NOMEM, "scene group tables");
+    }
+    cudaStream_t st = b->ctx->stream;
+    CU(cudaMemcpyAsync(g.mem + o_ss, shape_scene.data(), 4 * shape_scene.size(), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(g.mem + o_t, tiles.data(), 16 * tiles.size(), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(g.mem + o_o, order.data(), 4 * order.size(), cudaMemcpyHostToDevice, st));
+    CU(cudaMemsetAsync(g.mem + o_pc, 0, 8, st));
+    CU(cudaStreamSynchronize(st));
+    g.bd.nshapes = (uint32_t)shape_scene.size();
+    g.bd.shape_scene = at<uint32_t>(g.mem, o_ss);
+    g.bd.tiles = at<uint4>(g.mem, o_t);
+    g.bd.ntiles = (uint32_t)tiles.size();
+    g.bd.order = at<uint32_t>(g.mem, o_o);
+    g.bd.pair_count = at<uint32_t>(g.mem, o_pc);
+    g.bd.pair_cap = cap;
+    CU(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
+    CU(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+    b->groups.push_back(std::move(g));
+  }
+  refresh_groups(b);
+  return STEEL_OK;
+}
+
 // Makes `t` the batch's tile configuration: block size of prepare and solve, each scene's
 // shared-memory staging under the budget, the launches' dynamic shared memory and the
 // narrowphase grid. The frame graph is captured again at the next step. Results do not depend on
@@ -381,6 +526,7 @@ int apply_tiles(steel_batch* b, const steel_tiles& t) {
   const uint32_t narrow_max = (uint32_t)narrow_blocks_per_sm();
   if (t.narrow_blocks_per_sm > narrow_max)
     return fail(STEEL_E_INVALID, "narrow_blocks_per_sm above the " + std::to_string(narrow_max) + " that fit an SM");
+  if (t.stream_groups > 8u) return fail(STEEL_E_INVALID, "at most 8 stream groups");
   const uint32_t n = (uint32_t)b->sc.size();
   std::vector<uint32_t> stages(n);
   size_t prep = 0, solve = 0;
@@ -404,7 +550,14 @@ int apply_tiles(steel_batch* b, const steel_tiles& t) {
   b->bd.solve_smem = (uint32_t)solve;
   b->bd.block_threads = t.block_threads;
   b->narrow_blocks = (uint32_t)b->ctx->sms * (t.narrow_blocks_per_sm ? t.narrow_blocks_per_sm : narrow_max);
+  const uint32_t want_groups = t.stream_groups > 1u ? t.stream_groups : 1u;
+  const uint32_t have_groups = b->groups.empty() ? 1u : (uint32_t)b->groups.size();
+  if (want_groups != have_groups || t.stream_groups != b->tile_cfg.stream_groups) {
+    if (int rc = make_groups(b, want_groups)) return rc;
+  }
+  refresh_groups(b);
   b->tile_cfg = t;
+  b->tile_cfg.stream_groups = b->groups.empty() ? 1u : (uint32_t)b->groups.size();
   drop_graph(b);
   return STEEL_OK;
 }
@@ -470,6 +623,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
     for (uint32_t ti = 0; ti < nt; ti++)
       for (uint32_t tj = ti; tj < nt; tj++) b->tiles.push_back(make_uint4(i, ti, tj, 0u));
     pair_cap += d.MAXP;
+    b->pair_cap_of.push_back(d.MAXP);
     max_c = std::max<size_t>(max_c, d.MAXC);
   }
   b->o_scenes = L.take(sizeof(SceneDev) * n);
@@ -590,6 +744,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
     t.block_threads = b->max_threads;  // one block per SM for few scenes, 4 per SM otherwise
     t.smem_budget = 0;                 // the per-part staging caps alone
     t.narrow_blocks_per_sm = 0;        // as many as fit
+    t.stream_groups = 1;               // one launch sequence
     int rc = apply_tiles(b.get(), t);
     if (rc) return rc;
   }
@@ -736,6 +891,8 @@ int steel_batch_destroy(steel_batch* b) {
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->ev_pose) cudaEventDestroy(b->ev_pose);
+  free_groups(b);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   if (b->arena) cudaFree(b->arena);
   delete b;
   return STEEL_OK;
@@ -763,6 +920,7 @@ int steel_debug_set_wait_limit(steel_batch* b, uint32_t rounds) {
   CU(cudaSetDevice(b->ctx->device));
   CU(cudaStreamSynchronize(b->ctx->stream));
   b->bd.wait_limit = rounds;
+  refresh_groups(b);
   drop_graph(b);  // the limit is a launch argument: capture again
   return STEEL_OK;
 }
@@ -788,13 +946,14 @@ int steel_autotune(steel_batch* b, uint32_t frames, steel_tiles* best, float* be
   auto budget_for = [](uint32_t threads) { return 233472u / blocks_per_sm_of(threads) - 3328u; };
   std::vector<steel_tiles> cands;
   if (b->max_threads == BIG_THREADS) {
-    cands = {{512, 0, 0}, {256, 0, 0}, {256, budget_for(256), 0}, {128, budget_for(128), 0}};
+    cands = {{512, 0, 0, 1}, {256, 0, 0, 1}, {256, budget_for(256), 0, 1}, {128, budget_for(128), 0, 1}};
   } else {
-    cands = {{128, 0, 0}, {128, budget_for(128), 0}, {64, budget_for(64), 0}, {64, budget_for(64) / 2u, 0},
-             {32, budget_for(32), 0}, {32, budget_for(32) / 2u, 0}};
+    cands = {{128, 0, 0, 1}, {128, budget_for(128), 0, 1}, {64, budget_for(64), 0, 1}, {64, budget_for(64) / 2u, 0, 1},
+             {32, budget_for(32), 0, 1}, {32, budget_for(32) / 2u, 0, 1}};
   }
   const uint32_t narrow_max = (uint32_t)narrow_blocks_per_sm();
-  if (narrow_max > 1u) cands.push_back({0u, 0u, narrow_max - 1u});  // block size filled in from the best so far
+  if (narrow_max > 1u) cands.push_back({0u, 0u, narrow_max - 1u, 1u});  // block size filled in from the best so far
+  if (b->sc.size() > 2u * (size_t)b->ctx->sms) cands.push_back({0u, 0u, 0u, 2u});  // the best so far, two groups
   CU(cudaSetDevice(b->ctx->device));
   cudaStream_t st = b->ctx->stream;
   steel_tiles won = b->tile_cfg;
@@ -803,6 +962,7 @@ int steel_autotune(steel_batch* b, uint32_t frames, steel_tiles* best, float* be
     if (c.block_threads == 0u) {
       c.block_threads = won.block_threads;
       c.smem_budget = won.smem_budget;
+      if (c.stream_groups == 2u) c.narrow_blocks_per_sm = won.narrow_blocks_per_sm;
     }
     if (int rc = apply_tiles(b, c)) return rc;
     if (int rc = upload_state(b)) return rc;

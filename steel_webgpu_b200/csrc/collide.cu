@@ -8,6 +8,8 @@
 // pairs of every scene of the batch go to one compacted list (warp-aggregated atomics); the
 // narrowphase runs one warp per pair with shuffle reductions over faces, edge pairs and
 // support points; each scene's contacts are sorted by one block.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -232,6 +234,18 @@ struct JobR {
   }
 };
 
+// Warp-aggregated counter increment: the lanes that reach it together and share `label` (the
+// counter's scene) take consecutive slots with one atomic by their first lane. Works in divergent
+// code (the coalesced group of the calling lanes).
+SD uint32_t warp_agg_inc(uint32_t* ctr, uint32_t label) {
+  namespace cg = cooperative_groups;
+  cg::coalesced_group g = cg::coalesced_threads();
+  cg::coalesced_group same = cg::labeled_partition(g, label);
+  uint32_t base = 0u;
+  if (same.thread_rank() == 0u) base = atomicAdd(ctr, same.size());
+  return same.shfl(base, 0u) + same.thread_rank();
+}
+
 struct Narrow {
   const SceneDev& S;
   uint32_t lane;
@@ -241,7 +255,7 @@ struct Narrow {
 
   // Appends a job (lane 0 of k_narrow). Each pair adds at most one, so the list holds pair_cap.
   __device__ void defer(uint32_t kind, JobW& j) const {
-    uint32_t slot = atomicAdd(B->pair_count + 1, 1u);
+    uint32_t slot = warp_agg_inc(B->pair_count + 1, 0u);
     if (slot >= B->pair_cap) { atomicCAS(B->error, 0u, (uint32_t)ERR_JOB_CAPACITY); return; }
     j.w[0] = kind;
     j.w[1] = scene;
@@ -547,7 +561,7 @@ struct Narrow {
     f3 nn = n;
     float smx = A0.z, smy = B0.z;
     if (a > b) { a = bb; b = ba; nn = -n; float tt = smx; smx = smy; smy = tt; }
-    uint32_t k = atomicAdd(&S.counters[1], 1u);
+    uint32_t k = warp_agg_inc(&S.counters[1], S.scene_index);
     if (k >= S.MAXC) return;
     float4* rec = S.craw + k * 5u;
     S.craw[S.MAXC * 5u + k] = make_float4(smx, smy, 0.0f, 0.0f);
@@ -1123,24 +1137,6 @@ struct Narrow {
   }
 
   // narrow_pair (wgsl.js:1072-1195): all lanes enter; the serial paths become jobs of lane 0.
-  // Plane pairs and primitive-primitive pairs need no lane cooperation: the calling lane alone
-  // records the pair's job (the same record pair() would have lane 0 write) and returns true.
-  __device__ bool solo_pair(uint32_t p0, uint32_t p1) const {
-    bool swp = geo_type(p0) > geo_type(p1);
-    uint32_t sa = swp ? p1 : p0, sb = swp ? p0 : p1;
-    float4 ka = shp(sa, 3), kb = shp(sb, 3);
-    const bool plane = ka.x == 4.0f || kb.x == 4.0f;
-    if (!plane && !(ka.x != 0.0f && kb.x != 0.0f)) return false;
-    f3 pa = v3(S.spos[sa]);
-    float4 qa = S.srot[sa];
-    f3 pb = v3(S.spos[sb]);
-    float4 qb = S.srot[sb];
-    float thresh = fmn(shp(sa, 0).w + shp(sb, 0).w, S.F_GAP_GATE);
-    JobW j;
-    j.u(sa); j.u(sb); j.v(pa); j.q(qa); j.v(pb); j.q(qb); j.f(thresh);
-    defer(plane ? (geo_type(sb) == GT_CONVEX ? J_PLANE_CONVEX : J_PLANE) : J_PRIM, j);
-    return true;
-  }
   __device__ void pair(uint32_t p0, uint32_t p1) const {
     bool swp = geo_type(p0) > geo_type(p1);
     uint32_t sa = swp ? p1 : p0, sb = swp ? p0 : p1;
@@ -1247,33 +1243,15 @@ struct Narrow {
   }
 };
 
-// Each warp takes 32 pairs at a time: every lane loads one pair and, if it is a plane or a
-// primitive-primitive pair, records its job alone; the remaining pairs are then run one after
-// another by the whole warp. Only the order in which jobs and contacts are appended changes, and
-// the canonical sort removes it.
 __global__ void __launch_bounds__(NARROW_WARPS * 32, 3) k_narrow(BatchDev B) {
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5u, lane = threadIdx.x & 31u;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5u;
-  const uint32_t total = *B.pair_count;
-  for (uint32_t g0 = warp * 32u; g0 < total; g0 += nwarps * 32u) {
-    const uint32_t g = g0 + lane;
-    const bool valid = g < total;
-    const uint4 mine = valid ? B.pairs[g] : make_uint4(0u, 0u, 0u, 0u);
-    bool solo = false;
-    if (valid) {
-      Narrow N(B.scenes[mine.x], &B, mine.x);
-      solo = N.solo_pair(mine.y, mine.z);
-    }
-    uint32_t work = __ballot_sync(0xffffffffu, valid && !solo);
-    while (work != 0u) {
-      const uint32_t k = (uint32_t)__ffs(work) - 1u;
-      work &= work - 1u;
-      const uint4 pr = make_uint4(__shfl_sync(0xffffffffu, mine.x, k), __shfl_sync(0xffffffffu, mine.y, k),
-                                  __shfl_sync(0xffffffffu, mine.z, k), 0u);
-      Narrow N(B.scenes[pr.x], &B, pr.x);
-      N.pair(pr.y, pr.z);
-      __syncwarp();
-    }
+  uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5u;
+  uint32_t nwarps = (gridDim.x * blockDim.x) >> 5u;
+  uint32_t total = *B.pair_count;
+  for (uint32_t g = warp; g < total; g += nwarps) {
+    uint4 pr = B.pairs[g];
+    Narrow N(B.scenes[pr.x], &B, pr.x);
+    N.pair(pr.y, pr.z);
+    __syncwarp();
   }
 }
 

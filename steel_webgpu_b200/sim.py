@@ -115,8 +115,8 @@ class Batch:
         _lib.check(_lib.load().steel_get_tiles(self.h, ctypes.byref(t)))
         return {k: getattr(t, k) for k, _ in _lib.Tiles._fields_}
 
-    def set_tiles(self, block_threads: int, smem_budget: int = 0, narrow_blocks_per_sm: int = 0):
-        t = _lib.Tiles(block_threads, smem_budget, narrow_blocks_per_sm)
+    def set_tiles(self, block_threads: int, smem_budget: int = 0, narrow_blocks_per_sm: int = 0, stream_groups: int = 1):
+        t = _lib.Tiles(block_threads, smem_budget, narrow_blocks_per_sm, stream_groups)
         _lib.check(_lib.load().steel_set_tiles(self.h, ctypes.byref(t)))
 
     def autotune(self, frames: int = 3) -> tuple[dict, float]:

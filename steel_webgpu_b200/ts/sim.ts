@@ -238,13 +238,19 @@ export class Sim {
   }
 
   /** Picks the tile configuration for this scene (steel_autotune); resets the Sim. */
-  autotune(frames = 3): { blockThreads: number; smemBudget: number; narrowBlocksPerSm: number; msPerFrame: number } {
-    const t = new Uint32Array(3);
+  autotune(frames = 3): {
+    blockThreads: number;
+    smemBudget: number;
+    narrowBlocksPerSm: number;
+    streamGroups: number;
+    msPerFrame: number;
+  } {
+    const t = new Uint32Array(4);
     const ms = new Float32Array(1);
     check(lib.steel_autotune(this.handle, frames, ptr(t), ptr(ms)));
     this.time = 0;
     this.frame = 0;
-    return { blockThreads: t[0], smemBudget: t[1], narrowBlocksPerSm: t[2], msPerFrame: ms[0] };
+    return { blockThreads: t[0], smemBudget: t[1], narrowBlocksPerSm: t[2], streamGroups: t[3], msPerFrame: ms[0] };
   }
 
   private portDof(newtonDof: number): number {

@@ -221,12 +221,12 @@ def test_block_size_does_not_change_results(steel):
         assert np.array_equal(_bits(small.raw_state()[2]), _bits(large.raw_state(i)[2]))
 
 
-@pytest.mark.parametrize("tiles", [(128, 0, 0), (128, 54000, 0), (64, 25000, 0), (64, 6000, 0), (32, 11000, 0),
-                                   (32, 2000, 1)])
+@pytest.mark.parametrize("tiles", [(128, 0, 0, 1), (128, 54000, 0, 1), (64, 25000, 0, 1), (64, 6000, 0, 1),
+                                   (32, 11000, 0, 1), (32, 2000, 1, 1), (64, 12928, 0, 2), (128, 0, 0, 3)])
 def test_tiles_do_not_change_results(tiles, steel):
-    """Every tile configuration (block size, shared-memory staging budget, narrowphase grid) gives
-    the same bits as the default, for a batch with more scenes than SMs (uneven scenes with chains,
-    quadrupeds and a plain box pile)."""
+    """Every tile configuration (block size, shared-memory staging budget, narrowphase grid, scene
+    groups on parallel streams) gives the same bits as the default, for a batch with more scenes
+    than SMs (uneven scenes with chains, quadrupeds and a plain box pile)."""
     pks = [pack(s) for s in scenes.small_batch(n=6)] + [pack(scenes.chains_and_quads(n_quad=2)),
                                                           pack(scenes.articulated()), pack(scenes.boxes(40))]
     pks = pks * 17  # 153 scenes > 148 SMs
@@ -234,10 +234,11 @@ def test_tiles_do_not_change_results(tiles, steel):
     g = Batch(pks)
     assert ref.tiles()["block_threads"] == 128
     g.set_tiles(*tiles)
-    assert g.tiles() == dict(block_threads=tiles[0], smem_budget=tiles[1], narrow_blocks_per_sm=tiles[2])
+    assert g.tiles() == dict(block_threads=tiles[0], smem_budget=tiles[1], narrow_blocks_per_sm=tiles[2],
+                             stream_groups=tiles[3])
     ref.step(20)
     g.step(20)
-    for i in range(9):
+    for i in (0, 1, 5, 6, 7, 8, 76, 77, 150, 152):
         assert np.array_equal(_bits(ref.poses(i)), _bits(g.poses(i))), f"scene {i} differs under {tiles}"
         assert np.array_equal(_bits(ref.raw_state(i)[3]), _bits(g.raw_state(i)[3]))
 
@@ -276,7 +277,7 @@ def test_tiles_reject_bad_values(steel):
     pks = [pack(scenes.boxes(8))] * 200
     g = Batch(pks)
     from steel_webgpu_b200 import _lib
-    for bad in ((512, 0, 0), (96, 0, 0), (128, 0, 99)):
+    for bad in ((512, 0, 0), (96, 0, 0), (128, 0, 99), (128, 0, 0, 9)):
         with pytest.raises(_lib.SteelError):
             g.set_tiles(*bad)
 
