@@ -312,6 +312,35 @@ def plain_path_sample(pks, frames: int, device: int):
     return bodies / (ms / 1000.0)
 
 
+def single_scenes(device: int, frames: int = 3, warmup: int = 3) -> dict:
+    """The plain method at scale on one scene each: the 8192-body convex pour (240 fps) and 1024
+    quadrupeds with 64 40-link chains (500 fps), created from their scene files through the C ABI
+    (packed in C++), tiles from the autotuner; device-timed body-steps/s."""
+    import json as _json
+    from steel_webgpu_b200 import synth
+    from steel_webgpu_b200.sim import Batch, auto_caps
+    out = {}
+    for name, make, extra_caps in (
+            ("convex_pour_8192", lambda: synth.convex_pour(n=8192, seed=0),
+             dict(MAXP=1 << 18, MAXC=1 << 18, MAXU=1 << 18, UH=1 << 18, WH=1 << 19, AH=1 << 18)),
+            ("quadrupeds_1024", lambda: synth.quadrupeds(n_quad=1024, n_chains=64, chain_links=40, seed=0), {})):
+        t0 = time.perf_counter()
+        sc = make()
+        caps = auto_caps(sc)
+        caps.update(extra_caps)
+        b = Batch.from_files([(_json.dumps(sc.json).encode(), sc.bin, {"capacities": caps})], device=device)
+        build_s = time.perf_counter() - t0
+        tiles, _ = b.autotune(2)
+        b.step(warmup)
+        ms = b.step_timed(frames) / frames
+        nb = sc.json["bodies"]["count"]
+        out[name] = {"body_steps_per_s": nb / (ms / 1000.0), "ms_per_frame": ms, "bodies": nb,
+                     "fps": sc.json["fps"], "tiles": tiles, "build_s": round(build_s, 1),
+                     "timed": f"{frames} frames after {warmup} warm-up frames, CUDA events"}
+        b.close()
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
@@ -408,6 +437,7 @@ def run_steel(args):
     if rank != 0:
         return
     plain = plain_path_sample(pks[:args.plain_scenes], 2, local) if args.plain_scenes > 0 else None
+    singles = single_scenes(local) if (args.single_scenes == "on" and world == 1) else None
     cpu_sample = pks[:args.cpu_scenes]
     cpu_val, cpu_dt = cpu_baseline_sample(cpu_sample, args.cpu_frames)
     clocks = clk.summary()
@@ -440,6 +470,7 @@ def run_steel(args):
                                        "(64-thread tiles, FP64 D-inverse), per body, scaled to this batch",
                      "algorithmic_bytes_per_launch": bytes_dom, "ms_per_launch": prof[dom],
                      "kernel_share": {k: round(v / total_ms, 4) for k, v in prof.items()}},
+        "single_scenes": singles,
         "cpu_baseline": {"value": cpu_val, "unit": "body-steps/s", "cores": 1, "kind": "port",
                          "sample": f"{len(cpu_sample)} scenes x {args.cpu_frames} frames on the CPU oracle "
                                    f"({cpu_dt:.1f} s)"},
@@ -532,6 +563,8 @@ def main():
     ap.add_argument("--tiles", default="auto",
                     help='"auto" (autotuner) or block_threads,smem_budget,narrow_blocks_per_sm')
     ap.add_argument("--tune-frames", type=int, default=3)
+    ap.add_argument("--single-scenes", default="on", choices=["on", "off"],
+                    help="also time the 8192-body pour and the 1024-quadruped scene (one scene each)")
     ap.add_argument("--fp64-dinv", default="on", choices=["on", "off"],
                     help="FP64 in the articulated-inertia D factor/inverse and root inertia (uneven batch)")
     ap.add_argument("--serve-instances", type=int, default=4096)

@@ -72,6 +72,32 @@ class Batch:
         if not graph:
             _lib.check(L.steel_set_graph(self.h, 0))
 
+    @classmethod
+    def from_files(cls, scenes: list, device: int = 0, graph: bool = True) -> "Batch":
+        """A batch created from the scenes' own files through the C ABI (steel_batch_create_files: the
+        library reads scene.json and packs in C++). scenes: (json text bytes, bin bytes, options dict or
+        None) per scene."""
+        import json as _json
+        L = _lib.load()
+        n = len(scenes)
+        texts = [t if isinstance(t, bytes) else t.encode() for t, _, _ in scenes]
+        bins = [ctypes.create_string_buffer(bytes(b), len(b)) for _, b, _ in scenes]
+        opts = [(_json.dumps(o).encode() if o else None) for _, _, o in scenes]
+        jp = (ctypes.c_char_p * n)(*texts)
+        jl = (ctypes.c_uint64 * n)(*[len(t) for t in texts])
+        bp = (ctypes.c_void_p * n)(*[ctypes.cast(b, ctypes.c_void_p) for b in bins])
+        bl = (ctypes.c_uint64 * n)(*[len(sc[1]) for sc in scenes])
+        op = (ctypes.c_char_p * n)(*opts)
+        h = ctypes.c_void_p()
+        _lib.check(L.steel_batch_create_files(_Context.get(device), n, jp, jl, bp, bl, op, ctypes.byref(h)))
+        self = cls.__new__(cls)
+        self.packed = []
+        self._keep = []
+        self.h = h.value
+        if not graph:
+            _lib.check(L.steel_set_graph(self.h, 0))
+        return self
+
     def close(self):
         if getattr(self, "h", None):
             _lib.load().steel_batch_destroy(self.h)

@@ -81,3 +81,25 @@ def test_steel_state_matches_the_python_state(steel):
     assert b"is not simulated as an articulation dof" in L.steel_last_error()
     L.steel_batch_destroy(h)
     sim.destroy()
+
+
+def test_batch_from_files_matches_packed_batch(steel):
+    """Several scenes created from their files in one batch (steel_batch_create_files) step like the
+    same scenes packed in Python, options included."""
+    scs = [scenes.boxes(20), scenes.articulated()]
+    opts = [None, {"solver": {"drive_mode": "rows"}}]
+    fb = Batch.from_files([(json.dumps(sc.json).encode(), sc.bin, o) for sc, o in zip(scs, opts)])
+    pb = Batch([pack(sc, opts=o) for sc, o in zip(scs, opts)])
+    L = _lib.load()
+    _lib.check(L.steel_step(fb.h, 15))
+    pb.step(15)
+    for i, sc in enumerate(scs):
+        nb = sc.json["bodies"]["count"]
+        assert np.array_equal(_bits(_poses_of(fb.h, i, nb)), _bits(pb.poses(i))), f"scene {i}"
+    fb.close()
+
+
+def _poses_of(h, scene, nb):
+    out = np.zeros(nb * 8, dtype=np.float32)
+    _lib.check(_lib.load().steel_read_poses(h, scene, out.ctypes.data))
+    return out
