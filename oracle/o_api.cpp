@@ -23,8 +23,25 @@ static bool parse_consts(const char* text, std::map<std::string, double>& kv) {
   return true;
 }
 
-bool Oracle::init(const char* constants, const float* statF_, size_t nF, const uint32_t* statU_, size_t nU,
-                  const float* body_pose, const float* body_vel, const float* art_init, size_t nArt) {
+// The buffer boundary: binary32 words in and out. The float instance copies them; the all-FP64
+// instance (o_f64.h) converts each word to and from double.
+static void f32_in(float* dst, const f32_t* src, size_t n) {
+#ifndef ORC_F64
+  std::memcpy(dst, src, n * 4);
+#else
+  for (size_t i = 0; i < n; i++) dst[i] = (double)src[i];
+#endif
+}
+static void f32_out(f32_t* dst, const float* src, size_t n) {
+#ifndef ORC_F64
+  std::memcpy(dst, src, n * 4);
+#else
+  for (size_t i = 0; i < n; i++) dst[i] = (f32_t)src[i];
+#endif
+}
+
+bool Oracle::init(const char* constants, const f32_t* statF_, size_t nF, const uint32_t* statU_, size_t nU,
+                  const f32_t* body_pose, const f32_t* body_vel, const f32_t* art_init, size_t nArt) {
   std::map<std::string, double> kv;
   if (!parse_consts(constants, kv)) { error = "bad constants text"; return false; }
   auto get = [&](const char* k, double def) { auto it = kv.find(k); return it == kv.end() ? def : it->second; };
@@ -47,13 +64,14 @@ bool Oracle::init(const char* constants, const float* statF_, size_t nF, const u
   // The oracle restates every solver option of the path.
   if (nF != (size_t)C.LEN_STATF4 * 4u || nU != C.LEN_STATU || nArt != C.LEN_ART) { error = "buffer size mismatch"; return false; }
   statF.resize(C.LEN_STATF4);
-  std::memcpy(statF.data(), statF_, nF * 4);
+  f32_in(&statF.data()->x, statF_, nF);
   statU.assign(statU_, statU_ + nU);
   init_poses.assign(C.NB * 4u + C.NS * 4u, mk4(0, 0, 0, 0));
-  std::memcpy(init_poses.data(), body_pose, C.NB * 8u * 4u);
+  f32_in(&init_poses.data()->x, body_pose, C.NB * 8u);
   init_vel.assign(C.NB * 2u, mk4(0, 0, 0, 0));
-  std::memcpy(init_vel.data(), body_vel, C.NB * 8u * 4u);
-  init_art.assign(art_init, art_init + nArt);
+  f32_in(&init_vel.data()->x, body_vel, C.NB * 8u);
+  init_art.assign(nArt, 0.0f);
+  f32_in(init_art.data(), art_init, nArt);
   pairs.assign(C.MAXP * 2u, 0u);
   contacts.assign(C.MAXC * 6u, mk4(0, 0, 0, 0));
   craw.assign(C.MAXC * 6u, mk4(0, 0, 0, 0));
@@ -150,8 +168,8 @@ void oracle_atan2(const float* y, const float* x, float* out, size_t n) {
   for (size_t i = 0; i < n; i++) out[i] = orc::atan2_o(y[i], x[i]);
 }
 
-void* oracle_create(const char* constants, const float* statF, size_t nF, const uint32_t* statU, size_t nU,
-                    const float* poses, const float* vel, const float* art, size_t nArt, char* err, size_t errlen) {
+void* oracle_create(const char* constants, const f32_t* statF, size_t nF, const uint32_t* statU, size_t nU,
+                    const f32_t* poses, const f32_t* vel, const f32_t* art, size_t nArt, char* err, size_t errlen) {
   Oracle* o = new Oracle();
   if (!o->init(constants, statF, nF, statU, nU, poses, vel, art, nArt)) {
     if (err && errlen) { std::strncpy(err, o->error.c_str(), errlen - 1); err[errlen - 1] = 0; }
@@ -199,41 +217,43 @@ void oracle_stage(void* h, int stage) {
   }
 }
 
-// Buffer access by name: float buffers copy 4-byte words; returns the element count copied.
+// Buffer access by name, in 4-byte words (binary32 for the float buffers); returns the words copied.
 size_t oracle_read(void* h, const char* name, void* out, size_t max_words) {
   Oracle* o = (Oracle*)h;
-  const void* src = nullptr;
+  const float* fsrc = nullptr;
+  const uint32_t* usrc = nullptr;
   size_t n = 0;
   std::string s(name);
-  if (s == "poses") { src = o->poses.data(); n = o->poses.size() * 4; }
-  else if (s == "vel") { src = o->vel.data(); n = o->vel.size() * 4; }
-  else if (s == "art") { src = o->art.data(); n = o->art.size(); }
-  else if (s == "contacts") { src = o->contacts.data(); n = o->contacts.size() * 4; }
-  else if (s == "craw") { src = o->craw.data(); n = o->craw.size() * 4; }
-  else if (s == "pairs") { src = o->pairs.data(); n = o->pairs.size(); }
-  else if (s == "sched") { src = o->sched.data(); n = o->sched.size(); }
-  else if (s == "rows") { src = o->rows.data(); n = o->rows.size() * 4; }
-  else if (s == "warm") { src = o->warm.data(); n = o->warm.size(); }
-  else if (s == "counters") { src = o->counters; n = 16; }
-  else if (s == "collide_counts") { src = o->collide_counts; n = 2; }
-  else if (s == "stats") { src = o->stats; n = 16; }
+  if (s == "poses") { fsrc = &o->poses.data()->x; n = o->poses.size() * 4; }
+  else if (s == "vel") { fsrc = &o->vel.data()->x; n = o->vel.size() * 4; }
+  else if (s == "art") { fsrc = o->art.data(); n = o->art.size(); }
+  else if (s == "contacts") { fsrc = &o->contacts.data()->x; n = o->contacts.size() * 4; }
+  else if (s == "craw") { fsrc = &o->craw.data()->x; n = o->craw.size() * 4; }
+  else if (s == "pairs") { usrc = o->pairs.data(); n = o->pairs.size(); }
+  else if (s == "sched") { usrc = o->sched.data(); n = o->sched.size(); }
+  else if (s == "rows") { fsrc = &o->rows.data()->x; n = o->rows.size() * 4; }
+  else if (s == "warm") { usrc = o->warm.data(); n = o->warm.size(); }
+  else if (s == "counters") { usrc = o->counters; n = 16; }
+  else if (s == "collide_counts") { usrc = o->collide_counts; n = 2; }
+  else if (s == "stats") { usrc = o->stats; n = 16; }
   else return 0;
   if (n > max_words) n = max_words;
-  std::memcpy(out, src, n * 4);
+  if (fsrc) orc::f32_out((f32_t*)out, fsrc, n);
+  else std::memcpy(out, usrc, n * 4);
   return n;
 }
 // Write words into a named state buffer at a word offset (the Sim setters, sim.js:716-785).
 int oracle_write(void* h, const char* name, size_t offset, const void* data, size_t words) {
   Oracle* o = (Oracle*)h;
   std::string s(name);
-  uint32_t* dst = nullptr;
+  float* dst = nullptr;
   size_t n = 0;
-  if (s == "poses") { dst = (uint32_t*)o->poses.data(); n = o->poses.size() * 4; }
-  else if (s == "vel") { dst = (uint32_t*)o->vel.data(); n = o->vel.size() * 4; }
-  else if (s == "art") { dst = (uint32_t*)o->art.data(); n = o->art.size(); }
+  if (s == "poses") { dst = &o->poses.data()->x; n = o->poses.size() * 4; }
+  else if (s == "vel") { dst = &o->vel.data()->x; n = o->vel.size() * 4; }
+  else if (s == "art") { dst = o->art.data(); n = o->art.size(); }
   else return -1;
   if (offset + words > n) return -1;
-  std::memcpy(dst + offset, data, words * 4);
+  orc::f32_in(dst + offset, (const f32_t*)data, words);
   return 0;
 }
 }

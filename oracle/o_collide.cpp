@@ -22,7 +22,7 @@ static const v2 PENT[5] = {{1.0f, 0.0f},
                            {-0.8090169943749476f, -0.587785252292473f},
                            {0.30901699437494723f, -0.9510565162951536f}};
 
-template <class T> static inline T sel(T f, T t, bool c) { return c ? t : f; }
+static inline float sel(float f, float t, bool c) { return c ? t : f; }
 
 // --- shapes (wgsl.js:117-150) ---
 void Oracle::k_shapes() {

@@ -18,6 +18,10 @@
 #include <cstdint>
 #include <cstring>
 
+#ifndef ORC_F64
+typedef float f32_t;  // IEEE binary32 at the buffer boundary (o_f64.h keeps it when float is widened)
+#endif
+
 namespace orc {
 
 struct v2 { float x, y; };
@@ -90,8 +94,14 @@ static inline int32_t f2i(float f) {
   if (f <= -2147483648.0f) return (int32_t)0x80000000u;
   return (int32_t)f;
 }
+#ifndef ORC_F64
 static inline uint32_t fbits(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
 static inline float bitsf(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
+#else
+// All-FP64 instance: a word carrying u32 bits holds the binary32 value of those bits.
+static inline uint32_t fbits(double d) { f32_t f = (f32_t)d; uint32_t u; std::memcpy(&u, &f, 4); return u; }
+static inline double bitsf(uint32_t u) { f32_t f; std::memcpy(&f, &u, 4); return (double)f; }
+#endif
 
 // Matrices (column-major).
 static inline m3 mcols(v3 a, v3 b, v3 c) { return {{a, b, c}}; }

@@ -107,8 +107,8 @@ struct Oracle {
   std::string error;
 
   // --- setup / driver ---
-  bool init(const char* constants, const float* statF_, size_t nF, const uint32_t* statU_, size_t nU,
-            const float* body_pose, const float* body_vel, const float* art_init, size_t nArt);
+  bool init(const char* constants, const f32_t* statF_, size_t nF, const uint32_t* statU_, size_t nU,
+            const f32_t* body_pose, const f32_t* body_vel, const f32_t* art_init, size_t nArt);
   void reset();
   void write_params(uint32_t substep);
   void step(uint32_t frames);

@@ -15,7 +15,8 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "_build", "liboracle.so")
-_lib = None
+_LIB64 = os.path.join(_HERE, "_build", "liboracle64.so")  # all-FP64 instance (o_f64.h), the precision reference
+_libs = {}
 
 
 def build(quiet: bool = True) -> str:
@@ -23,12 +24,14 @@ def build(quiet: bool = True) -> str:
     return _LIB
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(_LIB):
+def lib(f64: bool = False):
+    """The float oracle, or with f64 its all-FP64 instance (same entry points; buffers in and out
+    stay binary32 words)."""
+    if f64 not in _libs:
+        path = _LIB64 if f64 else _LIB
+        if not os.path.exists(path):
             build()
-        L = ctypes.CDLL(_LIB)
+        L = ctypes.CDLL(path)
         L.oracle_create.restype = ctypes.c_void_p
         L.oracle_create.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
@@ -46,15 +49,16 @@ def lib():
         L.oracle_atan2.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]
         L.oracle_cone5.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_float, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                                            ctypes.c_void_p]
-        _lib = L
-    return _lib
+        _libs[f64] = L
+    return _libs[f64]
 
 
 class OracleSim:
-    """One packed scene stepped by the CPU oracle, with the reference's buffer layout."""
+    """One packed scene stepped by the CPU oracle, with the reference's buffer layout. With f64 the
+    all-FP64 instance steps it (every float operation in double; reads round to binary32)."""
 
-    def __init__(self, pk):
-        L = lib()
+    def __init__(self, pk, f64: bool = False):
+        self.L = L = lib(f64)
         self.pk = pk
         C = pk.C
         self._keep = [np.ascontiguousarray(a) for a in (pk.statF, pk.statU, pk.body_pose, pk.body_vel, pk.art)]
@@ -71,30 +75,34 @@ class OracleSim:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().oracle_destroy(self.h)
+            self.L.oracle_destroy(self.h)
             self.h = None
 
     def step(self, frames=1):
-        lib().oracle_step(self.h, frames)
+        self.L.oracle_step(self.h, frames)
+
+    def set_user_targets(self, on: bool = True):
+        """Joint targets written into art[A_TGT] replace the scene's drive paths (sim.js:716-731)."""
+        self.L.oracle_set_user_targets(self.h, int(on))
 
     def reset(self):
-        lib().oracle_reset(self.h)
+        self.L.oracle_reset(self.h)
 
     def collide(self):
-        lib().oracle_collide(self.h)
+        self.L.oracle_collide(self.h)
 
     def stage(self, k: int):
-        lib().oracle_stage(self.h, k)
+        self.L.oracle_stage(self.h, k)
 
     def read(self, name, dtype=np.float32):
         n = self.sizes[name]
         out = np.zeros(n, dtype=np.uint32)
-        got = lib().oracle_read(self.h, name.encode(), out.ctypes.data, n)
+        got = self.L.oracle_read(self.h, name.encode(), out.ctypes.data, n)
         return out[:got].view(dtype)
 
     def write(self, name, offset, values, dtype=np.float32):
         a = np.ascontiguousarray(np.asarray(values, dtype=dtype))
-        if lib().oracle_write(self.h, name.encode(), offset, a.ctypes.data, a.size) != 0:
+        if self.L.oracle_write(self.h, name.encode(), offset, a.ctypes.data, a.size) != 0:
             raise IndexError(name)
 
     def body_poses(self):
