@@ -355,7 +355,7 @@ struct Narrow {
     for (uint32_t v = 0; v < hnv(h); v++) m = fmx(m, dot(n, hv(h, v)));
     return m;
   }
-  __device__ __noinline__ EdgeQ edge_query(uint32_t ha, uint32_t hb, float4 rq, f3 t) const {
+  __device__ __noinline__ EdgeQ edge_query_strided(uint32_t ha, uint32_t hb, float4 rq, f3 t) const {
     EdgeQ best{-1e30f, sp3(0), sp3(0), sp3(0), sp3(0), sp3(0), 0u};
     uint32_t foa = hfo(ha), fob = hfo(hb);
     f3 cena = v3(S.sf[S.SF_HAABB + ha * 2u]);
@@ -385,6 +385,89 @@ struct Narrow {
       if (s > best.sep) best = EdgeQ{s, ax, a0, a1, b0, b1, (ea_.x << 24u) ^ (ea_.y << 16u) ^ (eb_.x << 8u) ^ eb_.y};
     }
     uint32_t w = best_lane(best.sep, true);
+    EdgeQ r;
+    r.sep = __shfl_sync(0xffffffffu, best.sep, w);
+    r.axis = shfl3(best.axis, w); r.a0 = shfl3(best.a0, w); r.a1 = shfl3(best.a1, w);
+    r.b0 = shfl3(best.b0, w); r.b1 = shfl3(best.b1, w);
+    r.id = __shfl_sync(0xffffffffu, best.id, w);
+    return r;
+  }
+  // Gauss-map test of edge pair k (A's edge k / neb, B's edge k % neb): their arcs intersect.
+  __device__ bool edge_arcs_meet(uint32_t ha, uint32_t hb, float4 rq, uint32_t k, uint32_t neb) const {
+    const uint32_t foa = hfo(ha), fob = hfo(hb);
+    uint4 ea_ = hedge(ha, k / neb), eb_ = hedge(hb, k % neb);
+    f3 a = v3(fplane(foa + ea_.z)), b = v3(fplane(foa + ea_.w));
+    f3 c = -qrot(rq, v3(fplane(fob + eb_.z))), d = -qrot(rq, v3(fplane(fob + eb_.w)));
+    f3 bxa = cross(b, a), dxc = cross(d, c);
+    float cba = dot(c, bxa), dba = dot(d, bxa), adc = dot(a, dxc), bdc = dot(b, dxc);
+    return !(cba * dba > 1e-3f || adc * bdc > 1e-3f || cba * bdc < -1e-3f);
+  }
+  // Edge-pair axes (wgsl.js edge query). The lane-strided scan (pair k on lane k mod 32, pairs in
+  // increasing k, the first maximum per lane, then the lowest lane among equal maxima) spends most
+  // of its time in the support scans of the few pairs that pass the Gauss-map test, one lane at a
+  // time. Here pass 1 runs the test over all pairs, 32 per round, keeping each round's ballot in
+  // a register; pass 2 hands the surviving pairs to the lanes in order, so the support scans run
+  // side by side. The winner is the same pair: the largest separation, ties broken by the strided
+  // scan's order (the lowest k mod 32, then the lowest k). Hulls with more than 256 edge pairs use
+  // the strided scan.
+  static constexpr uint32_t EDGE_ROUNDS = 8u;
+  __device__ __noinline__ EdgeQ edge_query(uint32_t ha, uint32_t hb, float4 rq, f3 t) const {
+    const uint32_t nea = hne(ha), neb = hne(hb), n = nea * neb;
+    if (n > 32u * EDGE_ROUNDS) return edge_query_strided(ha, hb, rq, t);
+    uint32_t pass[EDGE_ROUNDS];
+    uint32_t total = 0u;
+#pragma unroll
+    for (uint32_t r = 0; r < EDGE_ROUNDS; r++) {
+      const uint32_t k = r * 32u + lane;
+      pass[r] = r * 32u < n ? __ballot_sync(0xffffffffu, k < n && edge_arcs_meet(ha, hb, rq, k, neb)) : 0u;
+      total += __popc(pass[r]);
+    }
+    EdgeQ best{-1e30f, sp3(0), sp3(0), sp3(0), sp3(0), sp3(0), 0u};
+    uint32_t bkey = 0xffffffffu;
+    const f3 cena = v3(S.sf[S.SF_HAABB + ha * 2u]);
+    const f3 cenb = qrot(rq, v3(S.sf[S.SF_HAABB + hb * 2u])) + t;
+    for (uint32_t j = lane; j < total; j += 32u) {
+      uint32_t rem = j, k = 0u;
+#pragma unroll
+      for (uint32_t r = 0; r < EDGE_ROUNDS; r++) {
+        const uint32_t c = __popc(pass[r]);
+        if (rem < c) {  // the rem-th set bit of this round's ballot
+          uint32_t m = pass[r];
+          for (uint32_t i = 0; i < rem; i++) m &= m - 1u;
+          k = r * 32u + (uint32_t)(__ffs(m) - 1);
+          break;
+        }
+        rem -= c;
+      }
+      uint4 ea_ = hedge(ha, k / neb), eb_ = hedge(hb, k % neb);
+      f3 a0 = hv(ha, ea_.x), a1 = hv(ha, ea_.y);
+      f3 ea = a1 - a0;
+      f3 b0 = qrot(rq, hv(hb, eb_.x)) + t, b1 = qrot(rq, hv(hb, eb_.y)) + t;
+      f3 ax = cross(ea, b1 - b0);
+      float l = len(ax);
+      if (l < (1e-6f * len(ea)) * len(b1 - b0)) continue;
+      ax = ax / l;
+      if (dot(ax, cenb - cena) < 0.0f) ax = -ax;
+      float amax = support_max(ha, ax);
+      float bmin = dot(ax, t) + support_min(hb, qinv(rq, ax));
+      float s = bmin - amax;
+      float tol = 1e-4f + 1e-3f * (len(ea) + len(b1 - b0));
+      if (dot(ax, a0) < amax - tol || dot(ax, a1) < amax - tol || dot(ax, b0) > bmin + tol || dot(ax, b1) > bmin + tol)
+        continue;
+      const uint32_t key = ((k & 31u) << 8u) | (k >> 5u);
+      if (s > -1e30f && (s > best.sep || (s == best.sep && key < bkey))) {
+        best = EdgeQ{s, ax, a0, a1, b0, b1, (ea_.x << 24u) ^ (ea_.y << 16u) ^ (eb_.x << 8u) ^ eb_.y};
+        bkey = key;
+      }
+    }
+    float bv = best.sep;
+    uint32_t bk = bkey, w = lane;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const uint32_t ok = __shfl_xor_sync(0xffffffffu, bk, o), ow = __shfl_xor_sync(0xffffffffu, w, o);
+      if (ov > bv || (ov == bv && (ok < bk || (ok == bk && ow < w)))) { bv = ov; bk = ok; w = ow; }
+    }
     EdgeQ r;
     r.sep = __shfl_sync(0xffffffffu, best.sep, w);
     r.axis = shfl3(best.axis, w); r.a0 = shfl3(best.a0, w); r.a1 = shfl3(best.a1, w);

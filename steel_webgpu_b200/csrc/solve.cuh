@@ -418,11 +418,14 @@ struct Solver {
         add_imp(b, fn2 + ft, cross(rb, fn2) + cross(frb, ft));
         lam = mf4(nlam, lam.w);
       } else if (role != 0.0f && it >= S.FSTART) {
-        f3 vr2 = (tb[0] + cross(tb[1], frb)) - (ta[0] + cross(ta[1], fra));
-        float4 ki = rows[o + 5u];
-        float v1 = dot(t1, vr2) + bias.x, v2_ = dot(t2, vr2) + bias.y;
-        float kd = ki.x * ki.z - ki.y * ki.y;
-        f2 lt = friction_pair(ki.z / kd, -ki.y / kd, ki.x / kd, v1, v2_, lam.y, lam.z, lim, S.F_OMEGA);
+        f2 lt = mf2(0.0f, 0.0f);  // friction_pair's zero-radius exit: no tangential velocities needed
+        if (!(lim <= 0.0f)) {
+          f3 vr2 = (tb[0] + cross(tb[1], frb)) - (ta[0] + cross(ta[1], fra));
+          float4 ki = rows[o + 5u];
+          float v1 = dot(t1, vr2) + bias.x, v2_ = dot(t2, vr2) + bias.y;
+          float kd = ki.x * ki.z - ki.y * ki.y;
+          lt = friction_pair(ki.z / kd, -ki.y / kd, ki.x / kd, v1, v2_, lam.y, lam.z, lim, S.F_OMEGA);
+        }
         float dt1 = lt.x - lam.y, dt2 = lt.y - lam.z;
         lam.y = lt.x;
         lam.z = lt.y;
@@ -637,6 +640,7 @@ struct Solver {
     const float w = vpass ? 1.0f : d.m24;
     float nl = fmx(lam.x + S.F_OMEGA * ((((-(jv + d.m4)) * d.m5) * w) - (1.0f - w) * lam.x), 0.0f);
     float dn = nl - lam.x;
+    float lim = it < S.FSTART ? 0.0f : d.m3_ * nl;
     float p1 = 0.0f, p2 = 0.0f;
 #pragma unroll
     for (uint32_t j = 0; j < DENSE_REG; j++) {
@@ -647,10 +651,14 @@ struct Solver {
         p2 += d.J[2][j] * q[j];
       }
     }
-    float s1 = lane_sum(p1), s2 = lane_sum(p2);
-    float lim = it < S.FSTART ? 0.0f : d.m3_ * nl;
-    float kd = d.m6 * d.m8 - d.m7 * d.m7;
-    f2 lt = friction_pair(d.m8 / kd, -d.m7 / kd, d.m6 / kd, s1, s2, lam.y, lam.z, lim, S.F_OMEGA);
+    // friction_pair's zero-radius exit returns (0, 0) without the tangential sums (a separated or
+    // unloaded contact, or before the friction iterations): skip their lane reductions.
+    f2 lt = mf2(0.0f, 0.0f);
+    if (!(lim <= 0.0f)) {
+      float s1 = lane_sum(p1), s2 = lane_sum(p2);
+      float kd = d.m6 * d.m8 - d.m7 * d.m7;
+      lt = friction_pair(d.m8 / kd, -d.m7 / kd, d.m6 / kd, s1, s2, lam.y, lam.z, lim, S.F_OMEGA);
+    }
     float d1 = lt.x - lam.y, d2 = lt.y - lam.z;
 #pragma unroll
     for (uint32_t j = 0; j < DENSE_REG; j++) {
@@ -698,16 +706,19 @@ struct Solver {
       float w = vpass ? 1.0f : A[o + 24u];
       float nl = fmx(lam.x + S.F_OMEGA * ((((-(jv + A[o + 4u])) * A[o + 5u]) * w) - (1.0f - w) * lam.x), 0.0f);
       float dn = nl - lam.x;
+      float lim = it < S.FSTART ? 0.0f : A[o + 3u] * nl;
       float p1 = 0.0f, p2 = 0.0f;
       for (uint32_t k = lane; k < ai.w; k += 32u) {
         aqd[ai.z + k] += A[yo + k] * dn;
         p1 += A[jo + NDA + k] * aqd[ai.z + k];
         p2 += A[jo + 2u * NDA + k] * aqd[ai.z + k];
       }
-      float s1 = lane_sum(p1), s2 = lane_sum(p2);
-      float lim = it < S.FSTART ? 0.0f : A[o + 3u] * nl;
-      float kd = A[o + 6u] * A[o + 8u] - A[o + 7u] * A[o + 7u];
-      f2 lt = friction_pair(A[o + 8u] / kd, -A[o + 7u] / kd, A[o + 6u] / kd, s1, s2, lam.y, lam.z, lim, S.F_OMEGA);
+      f2 lt = mf2(0.0f, 0.0f);
+      if (!(lim <= 0.0f)) {  // friction_pair's zero-radius exit, as in dense_row
+        float s1 = lane_sum(p1), s2 = lane_sum(p2);
+        float kd = A[o + 6u] * A[o + 8u] - A[o + 7u] * A[o + 7u];
+        lt = friction_pair(A[o + 8u] / kd, -A[o + 7u] / kd, A[o + 6u] / kd, s1, s2, lam.y, lam.z, lim, S.F_OMEGA);
+      }
       float d1 = lt.x - lam.y, d2 = lt.y - lam.z;
       for (uint32_t k = lane; k < ai.w; k += 32u) aqd[ai.z + k] += A[yo + NDA + k] * d1 + A[yo + 2u * NDA + k] * d2;
       if (lane == 0u) { A[o + 9u] = nl; A[o + 10u] = lt.x; A[o + 11u] = lt.y; }
