@@ -246,12 +246,18 @@ SD uint32_t warp_agg_inc(uint32_t* ctr, uint32_t label) {
   return same.shfl(base, 0u) + same.thread_rank();
 }
 
+// Per-warp shared scratch of the edge query: the Gauss-map arcs of up to EDGE_MAX edges of each hull.
+constexpr uint32_t EDGE_MAX = 32u;
+constexpr uint32_t EDGE_SCRATCH = 2u * 9u * EDGE_MAX;  // floats per warp
+
 struct Narrow {
   const SceneDev& S;
   uint32_t lane;
   const BatchDev* B;  // job list of the batch
   uint32_t scene;
-  __device__ Narrow(const SceneDev& s, const BatchDev* b, uint32_t sc) : S(s), lane(threadIdx.x & 31u), B(b), scene(sc) {}
+  float* ew;          // this warp's edge scratch in shared memory (k_narrow), or null
+  __device__ Narrow(const SceneDev& s, const BatchDev* b, uint32_t sc, float* edge_scratch = nullptr)
+      : S(s), lane(threadIdx.x & 31u), B(b), scene(sc), ew(edge_scratch) {}
 
   // Appends a job (lane 0 of k_narrow). Each pair adds at most one, so the list holds pair_cap.
   __device__ void defer(uint32_t kind, JobW& j) const {
@@ -392,36 +398,72 @@ struct Narrow {
     r.id = __shfl_sync(0xffffffffu, best.id, w);
     return r;
   }
-  // Gauss-map test of edge pair k (A's edge k / neb, B's edge k % neb): their arcs intersect.
-  __device__ bool edge_arcs_meet(uint32_t ha, uint32_t hb, float4 rq, uint32_t k, uint32_t neb) const {
-    const uint32_t foa = hfo(ha), fob = hfo(hb);
-    uint4 ea_ = hedge(ha, k / neb), eb_ = hedge(hb, k % neb);
-    f3 a = v3(fplane(foa + ea_.z)), b = v3(fplane(foa + ea_.w));
-    f3 c = -qrot(rq, v3(fplane(fob + eb_.z))), d = -qrot(rq, v3(fplane(fob + eb_.w)));
-    f3 bxa = cross(b, a), dxc = cross(d, c);
-    float cba = dot(c, bxa), dba = dot(d, bxa), adc = dot(a, dxc), bdc = dot(b, dxc);
-    return !(cba * dba > 1e-3f || adc * bdc > 1e-3f || cba * bdc < -1e-3f);
-  }
   // Edge-pair axes (wgsl.js edge query). The lane-strided scan (pair k on lane k mod 32, pairs in
-  // increasing k, the first maximum per lane, then the lowest lane among equal maxima) spends most
-  // of its time in the support scans of the few pairs that pass the Gauss-map test, one lane at a
-  // time. Here pass 1 runs the test over all pairs, 32 per round, keeping each round's ballot in
-  // a register; pass 2 hands the surviving pairs to the lanes in order, so the support scans run
-  // side by side. The winner is the same pair: the largest separation, ties broken by the strided
-  // scan's order (the lowest k mod 32, then the lowest k). Hulls with more than 256 edge pairs use
-  // the strided scan.
+  // increasing k, the first maximum per lane, then the lowest lane among equal maxima) recomputes
+  // both edges' Gauss-map arcs for every pair and runs the support scans of the few pairs that
+  // pass the Gauss-map test one lane at a time. Here each edge's arcs (its two face normals and
+  // their cross product; B's negated and rotated into A's frame) are computed once, into the
+  // warp's shared scratch; pass 1 runs the test over all pairs, 32 per round, from the scratch,
+  // keeping each round's ballot in a register; pass 2 hands the surviving pairs to the lanes in
+  // order, so the support scans run side by side. Every value is computed by the same operations,
+  // and the winner is the same pair: the largest separation, ties broken by the strided scan's
+  // order (the lowest k mod 32, then the lowest k). Hulls with more than EDGE_MAX edges or 256
+  // edge pairs use the strided scan.
   static constexpr uint32_t EDGE_ROUNDS = 8u;
   __device__ __noinline__ EdgeQ edge_query(uint32_t ha, uint32_t hb, float4 rq, f3 t) const {
     const uint32_t nea = hne(ha), neb = hne(hb), n = nea * neb;
-    if (n > 32u * EDGE_ROUNDS) return edge_query_strided(ha, hb, rq, t);
+    if (ew == nullptr || n > 32u * EDGE_ROUNDS || nea > EDGE_MAX || neb > EDGE_MAX) return edge_query_strided(ha, hb, rq, t);
+    if (n == 0u) return EdgeQ{-1e30f, sp3(0), sp3(0), sp3(0), sp3(0), sp3(0), 0u};
+    float* EA = ew;                    // [component][edge]: a, b, b x a
+    float* EB = ew + 9u * EDGE_MAX;    // c, d, d x c
+    if (lane < nea) {
+      const uint32_t foa = hfo(ha);
+      const uint4 e = hedge(ha, lane);
+      const f3 a = v3(fplane(foa + e.z)), b = v3(fplane(foa + e.w));
+      const f3 bxa = cross(b, a);
+      const float w[9] = {a.x, a.y, a.z, b.x, b.y, b.z, bxa.x, bxa.y, bxa.z};
+#pragma unroll
+      for (uint32_t c = 0; c < 9u; c++) EA[c * EDGE_MAX + lane] = w[c];
+    }
+    if (lane < neb) {
+      const uint32_t fob = hfo(hb);
+      const uint4 e = hedge(hb, lane);
+      const f3 c = -qrot(rq, v3(fplane(fob + e.z))), d = -qrot(rq, v3(fplane(fob + e.w)));
+      const f3 dxc = cross(d, c);
+      const float w[9] = {c.x, c.y, c.z, d.x, d.y, d.z, dxc.x, dxc.y, dxc.z};
+#pragma unroll
+      for (uint32_t k = 0; k < 9u; k++) EB[k * EDGE_MAX + lane] = w[k];
+    }
+    __syncwarp();
     uint32_t pass[EDGE_ROUNDS];
     uint32_t total = 0u;
+    uint32_t ia = lane / neb, ib = lane % neb;  // pair k = 32 r + lane: A's edge k / neb, B's edge k % neb
+    const uint32_t step_a = 32u / neb, step_b = 32u % neb;
 #pragma unroll
     for (uint32_t r = 0; r < EDGE_ROUNDS; r++) {
       const uint32_t k = r * 32u + lane;
-      pass[r] = r * 32u < n ? __ballot_sync(0xffffffffu, k < n && edge_arcs_meet(ha, hb, rq, k, neb)) : 0u;
+      if (r * 32u < n) {
+        bool meet = false;
+        if (k < n) {
+          const f3 a = mf3(EA[ia], EA[EDGE_MAX + ia], EA[2u * EDGE_MAX + ia]);
+          const f3 b = mf3(EA[3u * EDGE_MAX + ia], EA[4u * EDGE_MAX + ia], EA[5u * EDGE_MAX + ia]);
+          const f3 bxa = mf3(EA[6u * EDGE_MAX + ia], EA[7u * EDGE_MAX + ia], EA[8u * EDGE_MAX + ia]);
+          const f3 c = mf3(EB[ib], EB[EDGE_MAX + ib], EB[2u * EDGE_MAX + ib]);
+          const f3 d = mf3(EB[3u * EDGE_MAX + ib], EB[4u * EDGE_MAX + ib], EB[5u * EDGE_MAX + ib]);
+          const f3 dxc = mf3(EB[6u * EDGE_MAX + ib], EB[7u * EDGE_MAX + ib], EB[8u * EDGE_MAX + ib]);
+          const float cba = dot(c, bxa), dba = dot(d, bxa), adc = dot(a, dxc), bdc = dot(b, dxc);
+          meet = !(cba * dba > 1e-3f || adc * bdc > 1e-3f || cba * bdc < -1e-3f);
+        }
+        pass[r] = __ballot_sync(0xffffffffu, meet);
+      } else {
+        pass[r] = 0u;
+      }
       total += __popc(pass[r]);
+      ia += step_a;
+      ib += step_b;
+      if (ib >= neb) { ib -= neb; ia++; }
     }
+    __syncwarp();  // the scratch is free for the next pair once every lane has read it
     EdgeQ best{-1e30f, sp3(0), sp3(0), sp3(0), sp3(0), sp3(0), 0u};
     uint32_t bkey = 0xffffffffu;
     const f3 cena = v3(S.sf[S.SF_HAABB + ha * 2u]);
@@ -1327,12 +1369,14 @@ struct Narrow {
 };
 
 __global__ void __launch_bounds__(NARROW_WARPS * 32, 3) k_narrow(BatchDev B) {
+  __shared__ float edge_scratch[NARROW_WARPS * EDGE_SCRATCH];
   uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5u;
   uint32_t nwarps = (gridDim.x * blockDim.x) >> 5u;
   uint32_t total = *B.pair_count;
+  float* ew = edge_scratch + (threadIdx.x >> 5u) * EDGE_SCRATCH;
   for (uint32_t g = warp; g < total; g += nwarps) {
     uint4 pr = B.pairs[g];
-    Narrow N(B.scenes[pr.x], &B, pr.x);
+    Narrow N(B.scenes[pr.x], &B, pr.x, ew);
     N.pair(pr.y, pr.z);
     __syncwarp();
   }
