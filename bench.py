@@ -156,6 +156,36 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def trace_summary(batch, pks) -> dict:
+    """One traced frame (steel_trace): for the last prepare and solve launches, the launch span, the
+    longest block and its scene, the mean block time and the most blocks resident at once; the span
+    over the work per slot says how far the launch is from a balanced one."""
+    batch.trace(True)
+    batch.step(1)
+    rec = batch.trace_read()
+    batch.trace(False)
+    out = {}
+    for k in ("prepare", "solve"):
+        r = rec[k]
+        ran = r[:, 0] > 0
+        st, en = r[ran, 0], r[ran, 1]
+        dur = (en - st) / 1e3
+        ev = sorted([(t, 1) for t in st] + [(t, -1) for t in en], key=lambda x: (x[0], x[1]))
+        cur = peak = 0
+        for _, d in ev:
+            cur += d
+            peak = max(peak, cur)
+        i = int(np.argmax(dur))
+        scene = int(np.nonzero(ran)[0][i])
+        out[k] = {"span_us": round(float((en.max() - st.min()) / 1e3), 1), "longest_block_us": round(float(dur[i]), 1),
+                  "longest_scene": {"links": pks[scene].NL, "bodies": pks[scene].NB},
+                  "mean_block_us": round(float(dur.mean()), 1), "max_resident_blocks": peak,
+                  "balanced_span_us": round(float(dur.sum() / max(peak, 1)), 1)}
+    out["what"] = ("steel_trace of one frame after the timed regions: block start/end from the global timer, "
+                   "last launch of the frame; balanced_span_us = summed block time / max resident blocks")
+    return out
+
+
 def scene_counts(batch, pks):
     """Run-measured per-scene counts for the algorithmic byte model (last substep)."""
     tot = dict(NB=0, NS=0, NL=0, pairs=0, contacts=0, rows=0, hull_bytes=0)
@@ -428,6 +458,7 @@ def run_steel(args):
     counts = scene_counts(batch, pks)
     # Capacities change results only when a buffer overflows; count the scenes where one did.
     overflow_scenes = sum(1 for i in range(len(pks)) if batch.stats(i)["overflow"])
+    block_trace = trace_summary(batch, pks) if pks and pks[0].NB else None
     rows_vec4 = pks[0].C["ROWS"]
     total_ms = sum(prof.values())
     dom = max(prof, key=prof.get)
@@ -471,6 +502,7 @@ def run_steel(args):
                      "algorithmic_bytes_per_launch": bytes_dom, "ms_per_launch": prof[dom],
                      "kernel_share": {k: round(v / total_ms, 4) for k, v in prof.items()}},
         "single_scenes": singles,
+        "block_trace": block_trace,
         "cpu_baseline": {"value": cpu_val, "unit": "body-steps/s", "cores": 1, "kind": "port",
                          "sample": f"{len(cpu_sample)} scenes x {args.cpu_frames} frames on the CPU oracle "
                                    f"({cpu_dt:.1f} s)"},

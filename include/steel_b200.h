@@ -185,6 +185,16 @@ int steel_step_io(steel_batch* b, uint32_t frames, const float* targets, uint64_
 int steel_profile_kernels(steel_batch* b, uint32_t frames, float* ms_per_launch);
 /* Device time of the last steel_step_timed call's frames, in milliseconds (CUDA events). */
 int steel_step_timed(steel_batch* b, uint32_t frames, float* ms);
+/* Block trace of the per-scene kernels, the batched counterpart of Sim.step(frames, timestamps)'s
+   pass timestamps (sim.js:606-610, 681-698): with tracing on, every prepare and solve block
+   records its start and end (the GPU's global timer, ns) and its SM. Off by default; turning it
+   on or off allocates or frees the record buffer and recaptures the frame graph, so call it
+   outside stream capture. Results do not change. */
+int steel_trace(steel_batch* b, int on);
+/* The records of the last prepare and solve launches: 6 words per scene, out[3 s + k] for the
+   prepare block of scene s and out[3 (n_scenes + s) + k] for its solve block, k = 0 start,
+   1 end, 2 SM index; zeros for scenes that have not run since tracing was turned on. */
+int steel_trace_read(steel_batch* b, uint64_t* out, uint64_t words);
 /* Failure-path testing: the number of try_wait rounds the prepare and solve kernels give a
    shared-memory bulk copy before they record STEEL_E_TIMEOUT. steel_batch_create sets
    STEEL_WAIT_LIMIT_DEFAULT; 0 makes every staged scene's wait run out at once. After a timeout the

@@ -92,6 +92,8 @@ SIGNATURES = {
     "steel_debug_set_wait_limit": [_VP, _U32],
     "steel_step_io": [_VP, _U32, _VP, ctypes.c_uint64, _VP, ctypes.c_uint64],
     "steel_profile_kernels": [_VP, _U32, _VP],
+    "steel_trace": [_VP, ctypes.c_int],
+    "steel_trace_read": [_VP, _VP, ctypes.c_uint64],
     "steel_sort_contacts_noalloc": [_VP, _U32, _VP, _VP],
     "steel_serve_config": [_VP, _U32],
     "steel_serve_budget": [_VP, ctypes.c_uint64],

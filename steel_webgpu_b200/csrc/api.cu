@@ -133,6 +133,7 @@ struct steel_batch {
   size_t o_stage = 0;                       // staging flags of every scene (apply_tiles upload)
   bool use_graph = true;
   cudaGraphExec_t graph = nullptr;
+  unsigned long long* trace = nullptr;  // steel_trace records (6 words per scene), or null
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t ev_pose = nullptr;  // orders a pose export on the caller's stream after the batch's frames
   // Scene groups: contiguous ranges of scenes whose launch sequences run on parallel streams (graph
@@ -431,6 +432,8 @@ void refresh_groups(steel_batch* b) {
     v.substep_count = b->bd.substep_count + g.lo;
     v.active = b->bd.active + g.lo;
     v.order = g.bd.order;
+    v.trace_prep = b->bd.trace_prep ? b->bd.trace_prep + 3ull * g.lo : nullptr;
+    v.trace_solve = b->bd.trace_solve ? b->bd.trace_solve + 3ull * g.lo : nullptr;
     g.bd = v;
   }
 }
@@ -714,7 +717,8 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   bd.nlaunch = n;
   {
     // Prepare and solve blocks take the scenes longest first (chain length, then bodies), so
-    // short scenes fill the end of the launch.
+    // short scenes fill the end of the launch. (An order by estimated block time, 16 bodies per
+    // chain link plus bodies, measured the same frame time on the uneven batch.)
     std::vector<uint32_t> order(n);
     for (uint32_t i = 0; i < n; i++) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
@@ -730,6 +734,8 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   bd.solve_ext = solve_ext != 0u ? 1u : 0u;
   bd.block_threads = b->max_threads;
   bd.wait_limit = STEEL_WAIT_LIMIT_DEFAULT;
+  bd.trace_prep = nullptr;
+  bd.trace_solve = nullptr;
   static_assert(STEEL_WAIT_LIMIT_DEFAULT == BULK_WAIT_LIMIT, "one default wait limit");
   CU(cudaMemcpyAsync(bd.scenes, dev.data(), sizeof(SceneDev) * n, cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync((void*)bd.shape_scene, b->shape_scene.data(), 4 * b->shape_scene.size(), cudaMemcpyHostToDevice, st));
@@ -894,6 +900,7 @@ int steel_batch_destroy(steel_batch* b) {
   free_groups(b);
   if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   if (b->arena) cudaFree(b->arena);
+  if (b->trace) cudaFree(b->trace);
   delete b;
   return STEEL_OK;
 }
@@ -922,6 +929,36 @@ int steel_debug_set_wait_limit(steel_batch* b, uint32_t rounds) {
   b->bd.wait_limit = rounds;
   refresh_groups(b);
   drop_graph(b);  // the limit is a launch argument: capture again
+  return STEEL_OK;
+}
+
+int steel_trace(steel_batch* b, int on) {
+  if (!b) return fail(STEEL_E_INVALID, "null batch");
+  CU(cudaSetDevice(b->ctx->device));
+  CU(cudaStreamSynchronize(b->ctx->stream));
+  const size_t n = b->sc.size();
+  if (on && !b->trace) {
+    CU(cudaMalloc(&b->trace, 6 * n * sizeof(unsigned long long)));
+    CU(cudaMemset(b->trace, 0, 6 * n * sizeof(unsigned long long)));
+  } else if (!on && b->trace) {
+    CU(cudaFree(b->trace));
+    b->trace = nullptr;
+  }
+  b->bd.trace_prep = b->trace;
+  b->bd.trace_solve = b->trace ? b->trace + 3 * n : nullptr;
+  refresh_groups(b);
+  drop_graph(b);  // the record pointers are launch arguments: capture again
+  return STEEL_OK;
+}
+
+int steel_trace_read(steel_batch* b, uint64_t* out, uint64_t words) {
+  if (!b || !out) return fail(STEEL_E_INVALID, "null argument");
+  if (!b->trace) return fail(STEEL_E_INVALID, "tracing is off (steel_trace)");
+  const size_t n = b->sc.size();
+  if (words < 6 * n) return fail(STEEL_E_INVALID, "trace buffer needs 6 words per scene");
+  CU(cudaSetDevice(b->ctx->device));
+  CU(cudaStreamSynchronize(b->ctx->stream));
+  CU(cudaMemcpy(out, b->trace, 6 * n * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   return STEEL_OK;
 }
 

@@ -31,7 +31,27 @@ struct BatchDev {
   uint32_t block_threads;     // threads per prepare / solve block (one of BLOCK_SIZES)
   uint32_t wait_limit;        // try_wait rounds of a shared-memory bulk copy (BULK_WAIT_LIMIT unless a test
                               // lowers it to make the bounded wait run out)
+  unsigned long long* trace_prep;   // null, or [nscenes][3]: each scene's last k_prepare block, its start and
+  unsigned long long* trace_solve;  // end (%globaltimer, ns) and SM; the same for k_solve (steel_trace)
 };
+
+// Block trace: the global timer (ns) and the block's record after the scene's body, written by
+// thread 0 once every thread is done. Called by all threads, only when tracing is on.
+__device__ __forceinline__ unsigned long long trace_clock() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void trace_block(unsigned long long* rec, unsigned long long t0) {
+  __syncthreads();
+  if (threadIdx.x == 0u) {
+    uint32_t sm;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+    rec[0] = t0;
+    rec[1] = trace_clock();
+    rec[2] = sm;
+  }
+}
 
 constexpr uint32_t BROAD_TILE = 32;
 constexpr int NARROW_WARPS = 8;          // warps per narrowphase block

@@ -16,7 +16,10 @@ namespace STEEL_NS {
 // has ART_F64 (scenes without it still run the FP32 branch in that instance).
 template <bool F64>
 __global__ void __launch_bounds__(STEEL_BLOCK, blocks_per_sm_of(STEEL_BLOCK)) k_prepare(BatchDev B) {
-  prepare_scene<F64>(B, B.order[blockIdx.x]);
+  const uint32_t sc = B.order[blockIdx.x];
+  const unsigned long long t0 = B.trace_prep ? trace_clock() : 0ull;
+  prepare_scene<F64>(B, sc);
+  if (B.trace_prep) trace_block(B.trace_prep + 3ull * sc, t0);
 }
 }  // namespace STEEL_NS
 

@@ -18,7 +18,10 @@ namespace STEEL_NS {
 // contact loop and the two-phase iteration.
 template <bool EXT>
 __global__ void __launch_bounds__(STEEL_BLOCK, blocks_per_sm_of(STEEL_BLOCK)) k_solve(BatchDev B) {
-  solve_scene<EXT>(B, B.order[blockIdx.x]);
+  const uint32_t sc = B.order[blockIdx.x];
+  const unsigned long long t0 = B.trace_solve ? trace_clock() : 0ull;
+  solve_scene<EXT>(B, sc);
+  if (B.trace_solve) trace_block(B.trace_solve + 3ull * sc, t0);
 }
 }  // namespace STEEL_NS
 

@@ -68,6 +68,7 @@ class Batch:
         h = ctypes.c_void_p()
         _lib.check(L.steel_batch_create(ctx, descs, len(self.packed), ctypes.byref(h)))
         self.h = h.value
+        self.n_scenes = len(self.packed)
         self._keep.clear()
         if not graph:
             _lib.check(L.steel_set_graph(self.h, 0))
@@ -94,6 +95,7 @@ class Batch:
         self.packed = []
         self._keep = []
         self.h = h.value
+        self.n_scenes = n
         if not graph:
             _lib.check(L.steel_set_graph(self.h, 0))
         return self
@@ -135,6 +137,19 @@ class Batch:
 
     def reset(self):
         _lib.check(_lib.load().steel_reset(self.h))
+
+    def trace(self, on: bool = True):
+        """Turns the per-scene block trace of the prepare and solve kernels on or off."""
+        _lib.check(_lib.load().steel_trace(self.h, 1 if on else 0))
+
+    def trace_read(self) -> dict:
+        """The last prepare and solve launches' block records, per scene: start and end (global
+        timer, ns) and SM, as int64 arrays of shape (n_scenes, 3)."""
+        n = self.n_scenes
+        out = np.zeros(6 * n, dtype=np.uint64)
+        _lib.check(_lib.load().steel_trace_read(self.h, out.ctypes.data, out.size))
+        rec = out.astype(np.int64).reshape(2, n, 3)
+        return {"prepare": rec[0], "solve": rec[1]}
 
     def tiles(self) -> dict:
         t = _lib.Tiles()
