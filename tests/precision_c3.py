@@ -82,6 +82,8 @@ def run_leg(args):
     A_TGT = pk.C["A_TGT"]
     port = [pk.dof_map[d] for d in pd]
     out = {}
+    blowup = None  # first frame after which a body pose is not finite
+    nb = pk.NB
     t0 = time.time()
     for f in range(frames):
         if f % 50 == 0:
@@ -90,8 +92,11 @@ def run_leg(args):
                 o.write("art", A_TGT + d, [v])
             o.set_user_targets(True)
         o.step(1)
+        if blowup is None and not np.isfinite(o.read("poses")[:nb * 8]).all():
+            blowup = f + 1
         if f + 1 in checkpoints:
             out[f + 1] = snapshot(o, pk)
+    out["blowup"] = blowup
     return leg, out, time.time() - t0
 
 
@@ -149,10 +154,12 @@ def main(argv=None):
     ref = res["fp64"][0]
     report = {"scene": dict(quads=a.quads, chains=a.chains, links=a.links, bodies=pk32.NB, dofs=pk32.ND, fps=500,
                             frames=a.frames, seed=a.seed, swing=a.swing),
-              "seconds": {leg: round(res[leg][1], 1) for leg in LEGS}, "errors": {}}
+              "seconds": {leg: round(res[leg][1], 1) for leg in LEGS},
+              "first_nonfinite_frame": {leg: res[leg][0].pop("blowup") for leg in LEGS}, "errors": {}}
     grp = groups(pk32, a.quads)
     for leg in LEGS[:2]:
         report["errors"][leg] = {f: errors(res[leg][0][f], ref[f], grp) for f in checkpoints}
+    print("first frame with a non-finite body pose (None: finite throughout):", report["first_nonfinite_frame"])
     print("relative L2 error against the all-FP64 run")
     print(f"{'frame':>6} {'run':<16} {'group':<11} " + " ".join(f"{q:>16}" for q in QUANTITIES))
     for f in checkpoints:
