@@ -365,7 +365,7 @@ def single_scenes(device: int, frames: int = 3, warmup: int = 3) -> dict:
         ms = b.step_timed(frames) / frames
         nb = sc.json["bodies"]["count"]
         out[name] = {"body_steps_per_s": nb / (ms / 1000.0), "ms_per_frame": ms, "bodies": nb,
-                     "fps": sc.json["fps"], "tiles": tiles, "build_s": round(build_s, 1),
+                     "fps": sc.json["fps"], "tiles": tiles, "team_blocks": b.team(), "build_s": round(build_s, 1),
                      "timed": f"{frames} frames after {warmup} warm-up frames, CUDA events"}
         b.close()
     return out

@@ -119,10 +119,25 @@ int steel_get_tiles(steel_batch* b, steel_tiles* out);
 int steel_set_tiles(steel_batch* b, const steel_tiles* tiles);
 /* Autotuner: steps the batch from its initial state under each candidate configuration (block
    sizes with staging budgets that keep 1-16 blocks resident per SM, then one narrowphase grid
-   smaller than the default, then two stream groups for batches of more than twice the SM count), times `frames` frames of each after two warm-up frames (CUDA events),
-   keeps the fastest and resets the batch (as steel_reset). Returns the chosen tiles and their device
-   time per frame in milliseconds. */
+   smaller than the default, then two stream groups for batches of more than twice the SM count;
+   for a batch of one scene, then team sizes of the solve, see steel_set_team), times `frames`
+   frames of each after two warm-up frames (CUDA events), keeps the fastest and resets the batch
+   (as steel_reset). Returns the chosen tiles and their device time per frame in milliseconds
+   (steel_get_team gives the chosen team). */
 int steel_autotune(steel_batch* b, uint32_t frames, steel_tiles* best, float* best_ms_per_frame);
+
+/* Team solve of a batch of one large scene. No counterpart in the reference, which solves a scene
+   on one 256-invocation workgroup (wgsl.js:2501-2504, sim.js:663). The solve kernel is launched
+   cooperatively with `blocks` blocks of the batch's block size that share the scene's bodies, rows
+   and articulations and meet at grid barriers (bounded waits: STEEL_E_TIMEOUT, never a hang).
+   0: one block (the batched path). STEEL_TEAM_AUTO, the default: a scene of at least 2048 bodies or
+   64 articulations gets one thread per body or a warp per articulation, capped by the blocks that
+   fit the GPU. Other values: that many blocks (STEEL_E_INVALID if more than fit). Batches of
+   several scenes and scenes with Nesterov momentum always solve on one block per scene. Results
+   are the same bits either way. steel_get_team returns the blocks in use (0: one block). */
+#define STEEL_TEAM_AUTO 0xffffffffu
+int steel_set_team(steel_batch* b, uint32_t blocks);
+int steel_get_team(steel_batch* b, uint32_t* blocks);
 
 /* Readback (Sim.state, sim.js:732-763; Sim.poses, sim.js:804). Caller-owned buffers. */
 int steel_read_poses(steel_batch* b, uint32_t scene, float* poses /* NB*8 */);

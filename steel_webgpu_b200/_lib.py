@@ -73,6 +73,8 @@ SIGNATURES = {
     "steel_get_tiles": [_VP, ctypes.POINTER(Tiles)],
     "steel_set_tiles": [_VP, ctypes.POINTER(Tiles)],
     "steel_autotune": [_VP, _U32, ctypes.POINTER(Tiles), ctypes.POINTER(_F32)],
+    "steel_set_team": [_VP, _U32],
+    "steel_get_team": [_VP, ctypes.POINTER(_U32)],
     "steel_read_poses": [_VP, _U32, _VP],
     "steel_read_state": [_VP, _U32, _VP, _VP, _VP, _VP, _VP],
     "steel_copy_poses_device": [_VP, _U32, _VP, _VP],

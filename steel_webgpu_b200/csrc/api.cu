@@ -168,6 +168,8 @@ struct steel_batch {
   uint64_t serve_budget = 0, serve_bytes = 0;  // admission budget (bytes of admitted instances' state), in use
   bool serve_dirty = false;                    // admitted set changed: upload the launch order
   std::vector<uint32_t> order_host;  // block order of the prepare and solve kernels
+  uint32_t team_req = STEEL_TEAM_AUTO;  // steel_set_team request (0 off, STEEL_TEAM_AUTO, or blocks)
+  size_t o_team = 0;                    // the team solve's grid-barrier counter
   uint64_t serve_next_id = 1;
   bool serve_on = false;
 };
@@ -369,6 +371,8 @@ int check_device_error(steel_batch* b) {
   if (e == ERR_STAGE_TIMEOUT)
     return fail(STEEL_E_TIMEOUT, "a shared-memory bulk copy did not complete within its wait limit; the scene's "
                                  "substep was skipped");
+  if (e == ERR_TEAM_TIMEOUT)
+    return fail(STEEL_E_TIMEOUT, "a block of the team solve gave up waiting at a grid barrier");
   if (e != 0) return fail(STEEL_E_CUDA, "device error " + std::to_string(e));
   return STEEL_OK;
 }
@@ -393,6 +397,41 @@ uint32_t stage_flags(const SceneDev& d, uint32_t budget) {
   if (4ull * d.ND <= STAGE_QD_CAP && fits(st | STAGE_QD)) st |= STAGE_QD;
   if (4ull * d.NB * d.NCOLW <= STAGE_WMASK_CAP && fits(st | STAGE_WMASK)) st |= STAGE_WMASK;
   return st;
+}
+
+// Blocks of the team solve (team.cuh) for the batch's block size and shared memory: a batch of one
+// scene without Nesterov momentum; STEEL_TEAM_AUTO takes scenes of at least TEAM_MIN_BODIES bodies
+// or TEAM_MIN_ARTS articulations, with one thread per body or a warp per articulation, capped by the
+// blocks that fit the GPU. Fewer than two blocks: the one-block path. `strict`: a request for more
+// blocks than fit is an error (steel_set_team) rather than capped (a later change of tiles).
+constexpr uint32_t TEAM_MIN_BODIES = 2048u, TEAM_MIN_ARTS = 64u;
+int team_blocks_for(const steel_batch* b, uint32_t req, bool strict, uint32_t* out) {
+  *out = 0u;
+  if (req == 0u || b->sc.size() != 1u || b->sc[0].d.NEST != 0u) return STEEL_OK;
+  const SceneDev& d = b->sc[0].d;
+  const uint32_t T = b->bd.block_threads;
+  const int per_sm = solve_team_blocks_per_sm(T, b->bd.solve_smem);
+  const uint32_t cap = per_sm > 0 ? (uint32_t)per_sm * (uint32_t)b->ctx->sms : 0u;
+  uint32_t n = 0u;
+  if (req == STEEL_TEAM_AUTO) {
+    if (d.NB >= TEAM_MIN_BODIES || d.NA >= TEAM_MIN_ARTS) n = std::min((std::max(d.NB, 32u * d.NA) + T - 1u) / T, cap);
+  } else {
+    if (req > cap && strict)
+      return fail(STEEL_E_INVALID, "at most " + std::to_string(cap) + " team blocks of " + std::to_string(T) +
+                                       " threads fit this GPU");
+    n = std::min(req, cap);
+  }
+  *out = n >= 2u ? n : 0u;
+  return STEEL_OK;
+}
+int update_team(steel_batch* b) {
+  uint32_t n = 0u;
+  if (int rc = team_blocks_for(b, b->team_req, false, &n)) return rc;
+  if (n != b->bd.team_blocks) {
+    b->bd.team_blocks = n;
+    drop_graph(b);
+  }
+  return STEEL_OK;
 }
 
 bool valid_block(uint32_t t) {
@@ -562,7 +601,7 @@ int apply_tiles(steel_batch* b, const steel_tiles& t) {
   b->tile_cfg = t;
   b->tile_cfg.stream_groups = b->groups.empty() ? 1u : (uint32_t)b->groups.size();
   drop_graph(b);
-  return STEEL_OK;
+  return update_team(b);
 }
 
 SceneHost* scene_of(steel_batch* b, uint32_t s) { return (b && s < b->sc.size()) ? &b->sc[s] : nullptr; }
@@ -641,6 +680,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   b->o_active = L.take(4ull * n);
   b->o_order = L.take(4ull * n);
   b->o_err = L.take(4);
+  b->o_team = L.take(16);
   b->o_stage = L.take(4ull * n);
   std::vector<uint64_t> tgt_off(n), pose_off(n);
   for (uint32_t i = 0; i < n; i++) {
@@ -730,6 +770,8 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   }
   CU(cudaMemsetAsync(A + b->o_active, 1, 4ull * n, st));  // every scene steps (nonzero words)
   bd.error = at<uint32_t>(A, b->o_err);
+  bd.team_bar = at<uint32_t>(A, b->o_team);
+  bd.team_blocks = 0;
   bd.art_f64 = art_f64 != 0u ? 1u : 0u;
   bd.solve_ext = solve_ext != 0u ? 1u : 0u;
   bd.block_threads = b->max_threads;
@@ -974,6 +1016,23 @@ int steel_set_tiles(steel_batch* b, const steel_tiles* t) {
   return apply_tiles(b, *t);
 }
 
+int steel_set_team(steel_batch* b, uint32_t blocks) {
+  if (!b) return fail(STEEL_E_INVALID, "null batch");
+  if (b->serve_on) return fail(STEEL_E_INVALID, "end the serving loop before changing the team");
+  uint32_t n = 0u;
+  if (int rc = team_blocks_for(b, blocks, true, &n)) return rc;
+  CU(cudaSetDevice(b->ctx->device));
+  CU(cudaStreamSynchronize(b->ctx->stream));
+  b->team_req = blocks;
+  return update_team(b);
+}
+
+int steel_get_team(steel_batch* b, uint32_t* blocks) {
+  if (!b || !blocks) return fail(STEEL_E_INVALID, "null argument");
+  *blocks = b->bd.team_blocks;
+  return STEEL_OK;
+}
+
 int steel_autotune(steel_batch* b, uint32_t frames, steel_tiles* best, float* best_ms_per_frame) {
   if (!b || frames == 0) return fail(STEEL_E_INVALID, "null batch or zero frames");
   if (b->serve_on) return fail(STEEL_E_INVALID, "end the serving loop before tuning");
@@ -1015,6 +1074,36 @@ int steel_autotune(steel_batch* b, uint32_t frames, steel_tiles* best, float* be
     if (ms < won_ms) { won_ms = ms; won = c; }
   }
   if (int rc = apply_tiles(b, won)) return rc;
+  // A batch of one scene: team sizes of the solve with the fastest tiles (one block, the default
+  // rule's count, half and twice that, all that fit), kept as an explicit request when one wins.
+  if (b->sc.size() == 1u && b->sc[0].d.NEST == 0u) {
+    const uint32_t req0 = b->team_req;
+    uint32_t n_auto = 0u, n_cap = 0u;
+    if (int rc = team_blocks_for(b, STEEL_TEAM_AUTO, false, &n_auto)) return rc;
+    if (int rc = team_blocks_for(b, 0x7fffffffu, false, &n_cap)) return rc;
+    std::vector<uint32_t> teams{b->bd.team_blocks};  // the configuration timed last (current request)
+    for (uint32_t t : {0u, n_auto, n_auto / 2u, 2u * n_auto, n_cap, 4u, 16u})
+      if ((t == 0u || (t >= 2u && t <= n_cap)) && std::find(teams.begin(), teams.end(), t) == teams.end())
+        teams.push_back(t);
+    uint32_t won_team = b->bd.team_blocks;
+    for (size_t k = 1; k < teams.size(); k++) {
+      b->team_req = teams[k];
+      if (int rc = update_team(b)) return rc;
+      if (int rc = upload_state(b)) return rc;
+      if (int rc = steel_step(b, 2u)) return rc;
+      CU(cudaEventRecord(b->ev0, st));
+      if (int rc = steel_step(b, frames)) return rc;
+      CU(cudaEventRecord(b->ev1, st));
+      CU(cudaEventSynchronize(b->ev1));
+      float ms = 0.0f;
+      CU(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+      if (int rc = check_device_error(b)) return rc;
+      ms /= (float)frames;
+      if (ms < won_ms) { won_ms = ms; won_team = teams[k]; }
+    }
+    b->team_req = won_team == teams[0] ? req0 : won_team;
+    if (int rc = update_team(b)) return rc;
+  }
   if (int rc = upload_state(b)) return rc;
   CU(cudaStreamSynchronize(st));
   if (best) *best = won;

@@ -33,6 +33,8 @@ struct BatchDev {
                               // lowers it to make the bounded wait run out)
   unsigned long long* trace_prep;   // null, or [nscenes][3]: each scene's last k_prepare block, its start and
   unsigned long long* trace_solve;  // end (%globaltimer, ns) and SM; the same for k_solve (steel_trace)
+  uint32_t team_blocks;       // nonzero: the batch's one scene is solved by this many cooperating blocks
+  uint32_t* team_bar;         // [1] grid-barrier arrival counter of that solve (zeroed before each launch)
 };
 
 // Block trace: the global timer (ns) and the block's record after the scene's body, written by
@@ -69,7 +71,8 @@ constexpr int BIG_THREADS = 512;           // batches of no more scenes than SMs
 constexpr uint32_t blocks_per_sm_of(uint32_t threads) { return 65536u / (threads * 128u); }
 
 // Device error codes written to BatchDev::error.
-enum : uint32_t { ERR_NONE = 0, ERR_SORT_CAPACITY = 1, ERR_JOB_CAPACITY = 2, ERR_STAGE_TIMEOUT = 3, ERR_SORT_TIMEOUT = 4 };
+enum : uint32_t { ERR_NONE = 0, ERR_SORT_CAPACITY = 1, ERR_JOB_CAPACITY = 2, ERR_STAGE_TIMEOUT = 3, ERR_SORT_TIMEOUT = 4,
+                  ERR_TEAM_TIMEOUT = 5 };
 
 // Contact sort of scenes whose padded keys may exceed the block sort's shared array
 // (next_pow2(MAXC) > SORT_SMEM_KEYS): a device-wide LSD radix sort, onesweep style (one histogram
@@ -83,6 +86,7 @@ constexpr uint32_t RS_ITEMS = 16;           // keys per thread and tile
 constexpr uint32_t RS_TILE = RS_THREADS * RS_ITEMS;
 constexpr uint32_t RS_DIGITS = 12;          // 96 key bits, 8 per digit
 constexpr uint32_t RS_SPIN_LIMIT = 1u << 22;  // polls of a preceding tile's status before giving up
+constexpr uint32_t TEAM_WAIT_LIMIT = 1u << 22;  // polls of a team solve's grid barrier before giving up
 struct RadixDev {
   uint4* keys[2];     // ping-pong key buffers [MAXC] (x pair, y feature, z hash, w raw index)
   uint32_t* status;   // [RS_DIGITS][tiles][256] look-back words: bits 30-31 flag (1 tile count, 2 prefix)
@@ -157,11 +161,13 @@ template <int T> cudaError_t configure_prepare_t(size_t smem_bytes);
 template <int T> cudaError_t configure_solve_t(size_t smem_bytes);
 template <int T> void launch_prepare_t(const BatchDev& b, cudaStream_t st);
 template <int T> void launch_solve_t(const BatchDev& b, cudaStream_t st);
+template <int T> int solve_team_blocks_per_sm_t(size_t smem_bytes);
 #define STEEL_DECLARE_BLOCK(N)                                                  \
   template <> cudaError_t configure_prepare_t<N>(size_t smem_bytes);            \
   template <> cudaError_t configure_solve_t<N>(size_t smem_bytes);              \
   template <> void launch_prepare_t<N>(const BatchDev& b, cudaStream_t st);     \
-  template <> void launch_solve_t<N>(const BatchDev& b, cudaStream_t st);
+  template <> void launch_solve_t<N>(const BatchDev& b, cudaStream_t st);       \
+  template <> int solve_team_blocks_per_sm_t<N>(size_t smem_bytes);
 STEEL_DECLARE_BLOCK(32)
 STEEL_DECLARE_BLOCK(64)
 STEEL_DECLARE_BLOCK(128)
@@ -172,6 +178,8 @@ cudaError_t configure_prepare(uint32_t threads, size_t smem_bytes);
 cudaError_t configure_solve(uint32_t threads, size_t smem_bytes);
 void launch_prepare(const BatchDev& b, cudaStream_t st);
 void launch_solve(const BatchDev& b, cudaStream_t st);
+// Resident blocks per SM of the team solve kernel at this block size and dynamic shared memory.
+int solve_team_blocks_per_sm(uint32_t threads, size_t smem_bytes);
 void launch_set_stage(const BatchDev& b, const uint32_t* stage, cudaStream_t st);
 void launch_frame_end(const BatchDev& b, cudaStream_t st);
 // Host-I/O staging: scatter packed joint targets into each scene, gather packed body poses.

@@ -16,12 +16,14 @@
 #include "block.cuh"
 #include "bulk.cuh"
 #include "cone5.cuh"
+#include "team.cuh"
 
 namespace steel {
 
 static constexpr uint32_t AVN_S = 14u;
 
-struct Solver {
+template <bool TEAM>
+struct SolverT {
   const SceneDev& S;
   const Params& P;
   Art ar;
@@ -29,8 +31,10 @@ struct Solver {
   float4* imp;
   float* aqd;
   bool vpass = false;  // velocity pass (wgsl.js:2928): rows without position bias or regularization
-  __device__ Solver(const SceneDev& s, const Params& p, float* lb, float4* tw_, float4* imp_, float* aqd_)
-      : S(s), P(p), ar(s, lb), tw(tw_), imp(imp_), aqd(aqd_) {}
+  Team<TEAM> tm;       // the threads that solve the scene: the block, or every block of a team launch
+  __device__ SolverT(Team<TEAM> tm_, const SceneDev& s, const Params& p, float* lb, float4* tw_, float4* imp_,
+                     float* aqd_)
+      : S(s), P(p), ar(s, lb), tw(tw_), imp(imp_), aqd(aqd_), tm(tm_) {}
 
   __device__ uint32_t bkind(int b) const { return f2u(S.sf[S.SF_BODY + (uint32_t)b * 8u].y); }
   __device__ uint32_t bflags(int b) const { return b < 0 ? 0u : f2u(S.sf[S.SF_BODY + (uint32_t)b * 8u + 7u].w); }
@@ -498,8 +502,8 @@ struct Solver {
   }
   // Each articulation's dense rows in slot order (S_DSTART / S_DLIST), by a stable counting sort
   // once per solve, so the dense passes walk their own rows instead of filtering all of them (the
-  // order within an articulation, the one the Gauss-Seidel pass needs, is kept). All threads call
-  // it.
+  // order within an articulation, the one the Gauss-Seidel pass needs, is kept). All threads of
+  // one block call it (in a team launch, block 0's).
   __device__ void dense_lists(uint32_t* tmp) const {
     const uint32_t tid = threadIdx.x, nt = blockDim.x, lane = tid & 31u, warp = tid >> 5u, nw = nt >> 5u;
     const uint32_t nd = min(S.sched[S.S_META + 3u], S.MAXDENSE);
@@ -837,14 +841,14 @@ struct Solver {
   // moved (wgsl.js:3366-3377). Articulations share no qd, rows or links, so each warp goes on to
   // its next articulation without a block barrier.
   __device__ void dense_phase(uint32_t mode, uint32_t it, uint32_t ph) const {
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5u, nw = blockDim.x >> 5u;
+    const uint32_t lane = threadIdx.x & 31u, warp = tm.rank() >> 5u, nw = tm.size() >> 5u;
     for (uint32_t a = warp; a < S.NA; a += nw) {
       bool touched = dense(a, mode, it, ph, lane);
       __syncwarp();
       if (touched) ar.twists_warp(a, aqd, tw, lane);
       __syncwarp();
     }
-    __syncthreads();
+    tm.sync();
   }
   // nesterov_momentum (wgsl.js:3491-3557): MuJoCo's PGS acceleration on the contact rows. Each
   // row's impulse is extrapolated by beta along its change since the last extrapolation, and the
@@ -944,7 +948,7 @@ struct Solver {
   // dense rows); 2 joint-internal rows only (no contact slots, no contact dense rows). The two
   // partial sweeps serve row_schedule "contact_then_internal" (wgsl.js:3559-3590).
   __device__ void sweep(uint32_t mode, uint32_t ncol0, uint32_t it, const uint32_t* wcs, uint32_t nu, uint32_t ph) const {
-    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t tid = tm.rank(), nt = tm.size();
     const uint32_t ncol = ph == 2u ? 0u : ncol0;
     if (ph != 1u)
       for (uint32_t a = tid; a < S.NA; a += nt) joint_rows(a);
@@ -972,20 +976,20 @@ struct Solver {
           if (us0 + k * nt < nu) S.art[S.A_ULOAD + us0 + k * nt] = load[k];
       }
     }
-    __syncthreads();
+    tm.sync();
     dense_phase(1u, it, ph);
     for (uint32_t c = 0; c < ncol; c++) {
       for (uint32_t u = wcs[c] + tid; u < wcs[c + 1u]; u += nt) solve_slot<EXT>(u, mode, it);
-      __syncthreads();
+      tm.sync();
     }
     if (tid == 0u && ph != 2u)
       for (uint32_t u = wcs[S.NCOL]; u < wcs[S.NCOL + 1u]; u++) solve_slot<EXT>(u, mode, it);
-    __syncthreads();
+    tm.sync();
     for (uint32_t a = tid; a < S.NA; a += nt) {
       contact_impulses(a);
       if (S.VLIM_ON == 1u && ph != 1u) vlim_rows(a);
     }
-    __syncthreads();
+    tm.sync();
     if (S.VLIM_FREE == 1u) {
       for (uint32_t b = tid; b < S.NB; b += nt) {
         if (bkind((int)b) != 1u || (bflags((int)b) & 1u) != 0u) continue;
@@ -1011,7 +1015,7 @@ struct Solver {
           tw[b * 2u + 1u] = mf4(w, 0.0f);
         }
       }
-      __syncthreads();
+      tm.sync();
     }
   }
   __device__ float4 warm_value(uint32_t i, uint32_t nc) const {
@@ -1034,36 +1038,41 @@ struct Solver {
   }
 };
 
-// Solve of scene sc by the calling block (all its threads).
-template <bool EXT>
-__device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
+// Solve of scene sc by a team (all its threads): the calling block (TEAM false, the batched path),
+// or every block of a cooperative launch on a batch of one large scene (TEAM true). A team launch
+// stages nothing in shared memory: twists, impulses, qd and link blocks stay in global memory,
+// where every block sees them after a grid barrier. Each block keeps its own copy of the scene
+// descriptor, the parameters and the color starts.
+template <bool EXT, bool TEAM>
+__device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc, Team<TEAM> tm) {
   extern __shared__ float4 ssm4[];  // solve_smem_layout: [tw | imp], qd, color starts, link blocks
   __shared__ Params Ps;
   __shared__ SceneDev Ss;  // the scene's offsets and sizes, read everywhere in the serial passes
-  const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  const uint32_t tid = tm.rank(), nt = tm.size();
   if (B.active[sc] == 0u) return;  // not stepping in this frame (serving loop)
   copy_scene(Ss, B.scenes[sc]);
   const SceneDev& S = Ss;
-  if (tid == 0u) Ps = *S.params;
+  if (threadIdx.x == 0u) Ps = *S.params;
   uint8_t* sb = reinterpret_cast<uint8_t*>(ssm4);
-  const SolveSmem lay = solve_smem_layout(S.stage, S.NB, S.ND, S.NCOL, S.NL);
-  const bool staged_links = (S.stage & STAGE_LINKS) != 0u, staged_bodies = (S.stage & STAGE_BODIES) != 0u;
+  const uint32_t stage = TEAM ? 0u : S.stage;
+  const SolveSmem lay = solve_smem_layout(stage, S.NB, S.ND, S.NCOL, S.NL);
+  const bool staged_links = (stage & STAGE_LINKS) != 0u, staged_bodies = (stage & STAGE_BODIES) != 0u;
   uint32_t* wcs = reinterpret_cast<uint32_t*>(sb + lay.wcs);
   float* lb = staged_links ? reinterpret_cast<float*>(sb + lay.links) : S.art + S.A_LINK;
   const uint32_t nu = S.sched[S.S_META];
   const uint32_t ncol = min(S.sched[S.S_META + 1u], S.NCOL);
-  for (uint32_t i = tid; i < S.NCOL + 2u; i += nt) wcs[i] = S.sched[S.S_CSTART + i];
+  for (uint32_t i = threadIdx.x; i < S.NCOL + 2u; i += blockDim.x) wcs[i] = S.sched[S.S_CSTART + i];
   // Link blocks into shared memory with one bulk copy (A_LINK is 16-byte aligned).
   __shared__ __align__(8) uint64_t stage_bar;
   if (staged_links && !stage_to_shared(lb, S.art + S.A_LINK, 4u * S.NL * LBLK, &stage_bar, B.wait_limit)) {
-    if (tid == 0u) atomicCAS(B.error, 0u, (uint32_t)ERR_STAGE_TIMEOUT);
+    if (threadIdx.x == 0u) atomicCAS(B.error, 0u, (uint32_t)ERR_STAGE_TIMEOUT);
     return;  // the whole block: the result above is the same in every thread
   }
   __syncthreads();
   const Params& P = Ps;
-  Solver sv(S, P, lb, staged_bodies ? reinterpret_cast<float4*>(sb + lay.tw) : S.tw,
-            staged_bodies ? reinterpret_cast<float4*>(sb + lay.imp) : S.imp,
-            (S.stage & STAGE_QD) ? reinterpret_cast<float*>(sb + lay.aqd) : S.aqd);
+  SolverT<TEAM> sv(tm, S, P, lb, staged_bodies ? reinterpret_cast<float4*>(sb + lay.tw) : S.tw,
+                   staged_bodies ? reinterpret_cast<float4*>(sb + lay.imp) : S.imp,
+                   (stage & STAGE_QD) ? reinterpret_cast<float*>(sb + lay.aqd) : S.aqd);
   float* A = S.art;
   // Prologue (wgsl.js:3635-3691).
   for (uint32_t i = tid; i < S.ND; i += nt) sv.aqd[i] = A[S.A_QDH + i];
@@ -1071,7 +1080,7 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
   if (S.SLEEP == 1u) {
     // Sleeping articulations start the solve at rest (wgsl.js:3640-3646). The reference zeroes
     // them with no barrier after the copy above; the zeros are its intent and are what runs here.
-    __syncthreads();
+    tm.sync();
     for (uint32_t a = tid; a < S.NA; a += nt) {
       if (!asleep(S.NB + a)) continue;
       uint4 ai = sv.ar.info(a);
@@ -1101,7 +1110,7 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     bool iso = I.c[0].x == I.c[1].y && I.c[1].y == I.c[2].z && I.c[0].y == 0.0f && I.c[0].z == 0.0f && I.c[1].z == 0.0f;
     if ((fl & 1u) == 0u && !iso && nonzero(w)) {
       m3 R = qmat(S.rot[b]);
-      w = mul(R, Solver::gyro(I, mul(tr(R), w), P.dt));
+      w = mul(R, SolverT<TEAM>::gyro(I, mul(tr(R), w), P.dt));
     }
     sv.tw[b * 2u] = mf4(v, 0.0f);
     sv.tw[b * 2u + 1u] = mf4(w, 0.0f);
@@ -1113,17 +1122,19 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     uint32_t row = S.sched[S.S_PORD + u], us = S.sched[S.S_RUNIT + row], key = S.sched[S.S_UKEY + us];
     S.slots[2u * u] = make_float4((float)row, (float)us, (float)((int)(key & 0xffffu) - 1), (float)((int)(key >> 16u) - 1));
   }
-  __syncthreads();
+  tm.sync();
   // Few articulations: a warp each (the chain recursion shortened); many: a thread each.
   if (S.NA <= (nt >> 5u)) {
     for (uint32_t a = tid >> 5u; a < S.NA; a += nt >> 5u) sv.ar.twists_warp(a, sv.aqd, sv.tw, tid & 31u);
   } else {
     for (uint32_t a = tid; a < S.NA; a += nt) sv.ar.twists(a, sv.aqd, sv.tw);
   }
-  __syncthreads();
+  tm.sync();
   {
+    // The dense lists are built by one block (the whole team's block 0), then published.
     __shared__ uint32_t dtmp[33];
-    sv.dense_lists(dtmp);
+    if (!TEAM || blockIdx.x == 0u) sv.dense_lists(dtmp);
+    if (TEAM) tm.sync();
   }
   sv.dense_phase(0u, 0u, 0u);
   sv.sweep<EXT>(0u, ncol, 0u, wcs, nu, 0u);
@@ -1134,7 +1145,8 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
   const uint32_t npass = cti ? 2u : 1u;
   for (uint32_t pass = 0; pass < npass; pass++)
     for (uint32_t it = 0; it < P.iterations; it++) {
-      if (S.NEST == 1u && pass == 0u) sv.momentum_step(ncol, it, wcs);
+      // Nesterov momentum keeps block-wide sums: a team launch is never made for a scene with it.
+      if (!TEAM && S.NEST == 1u && pass == 0u) sv.momentum_step(ncol, it, wcs);
       sv.sweep<EXT>(1u, ncol, it, wcs, nu, cti ? pass + 1u : 0u);
     }
   // Velocity pass (velocity_iterations, wgsl.js:3700-3736): positions integrate with the velocities
@@ -1172,7 +1184,7 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
       const float phi = A[o + 22u];
       A[o + 4u] = (phi > 0.0f && phi + P.dt * jv > 1e-6f) ? phi / P.dt : 0.0f;
     }
-    __syncthreads();
+    tm.sync();
     sv.vpass = true;
     for (uint32_t it = 0; it < S.VELITERS; it++) sv.sweep<EXT>(1u, ncol, P.iterations + it, wcs, nu, 0u);
     sv.vpass = false;
@@ -1194,7 +1206,7 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
       h = (h + 1u) % WH;
     }
   }
-  __syncthreads();
+  tm.sync();
   for (uint32_t i = tid; i < nc + ndense; i += nt) {
     uint32_t key = sv.warm_key(i, nc);
     if (key == 0xffffffffu) continue;
@@ -1208,7 +1220,7 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
   // unsynchronised loops; here the copy completes before the damping.
   if (S.PATCH == 1u) {
     for (uint32_t b = tid; b < S.NB; b += nt) { S.ppos[b] = S.pos[b]; S.prot[b] = S.rot[b]; }
-    __syncthreads();
+    tm.sync();
   }
   for (uint32_t b = tid; b < S.NB; b += nt) {
     if (sv.bkind((int)b) != 1u) continue;
@@ -1237,14 +1249,14 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     A[S.A_QD + i] = sv.aqd[i];
     if (S.VELITERS > 0u) sv.aqd[i] = A[S.A_SNAP + S.NB * 8u + i];
   }
-  __syncthreads();
+  tm.sync();
   for (uint32_t l = tid; l < S.NL; l += nt) {
     if (sv.ar.ltype(l) != 4u || sv.ar.lparent(l) >= 0) continue;
     float k = 1.0f - S.sf[S.SF_BODY + (uint32_t)sv.ar.lbody(l) * 8u + 3u].w * P.dt;
     uint32_t d = sv.ar.ldof(l);
     A[S.A_QD + d + 3u] *= k; A[S.A_QD + d + 4u] *= k; A[S.A_QD + d + 5u] *= k;
   }
-  __syncthreads();
+  tm.sync();
   // Joint integration of link l (wgsl.js:3797-3826).
   auto integrate_link = [&](uint32_t l) {
     float* Q = A + S.A_Q;
@@ -1293,7 +1305,7 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
   }
   // Friction anchors: advance and store for the next substep (wgsl.js:3832-3878).
   if (S.PATCH == 1u) {
-    __syncthreads();
+    tm.sync();
     const uint32_t AH = S.AH, ab = 10u * WH + (1u - P.parity) * AH, AVb = 10u * WH + 2u * AH;
     const float keep_frac = (float)(1.0 - 1e-5);
     for (uint32_t i = tid; i < nc; i += nt) {
@@ -1358,7 +1370,7 @@ __device__ __forceinline__ void solve_scene(const BatchDev& B, uint32_t sc) {
     S.counters[1] = 0u;
   }
   if (staged_links) {
-    __syncthreads();
+    tm.sync();
     for (uint32_t i = tid; i < S.NL * LBLK; i += nt) S.art[S.A_LINK + i] = lb[i];
   }
 }

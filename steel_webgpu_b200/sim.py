@@ -160,6 +160,19 @@ class Batch:
         t = _lib.Tiles(block_threads, smem_budget, narrow_blocks_per_sm, stream_groups)
         _lib.check(_lib.load().steel_set_tiles(self.h, ctypes.byref(t)))
 
+    TEAM_AUTO = 0xFFFFFFFF
+
+    def set_team(self, blocks: int = TEAM_AUTO):
+        """Blocks that solve the batch's one scene together (steel_set_team): 0 one block,
+        TEAM_AUTO the default rule for large scenes, else that many."""
+        _lib.check(_lib.load().steel_set_team(self.h, blocks))
+
+    def team(self) -> int:
+        """Blocks of the team solve in use (0: one block per scene)."""
+        v = ctypes.c_uint32()
+        _lib.check(_lib.load().steel_get_team(self.h, ctypes.byref(v)))
+        return v.value
+
     def autotune(self, frames: int = 3) -> tuple[dict, float]:
         """Times each candidate tile configuration over `frames` frames from the initial state, keeps
         the fastest and resets the batch. Returns (tiles, ms per frame)."""
