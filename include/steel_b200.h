@@ -126,10 +126,12 @@ int steel_set_tiles(steel_batch* b, const steel_tiles* tiles);
    (steel_get_team gives the chosen team). */
 int steel_autotune(steel_batch* b, uint32_t frames, steel_tiles* best, float* best_ms_per_frame);
 
-/* Team solve of a batch of one large scene. No counterpart in the reference, which solves a scene
-   on one 256-invocation workgroup (wgsl.js:2501-2504, sim.js:663). The solve kernel is launched
-   cooperatively with `blocks` blocks of the batch's block size that share the scene's bodies, rows
-   and articulations and meet at grid barriers (bounded waits: STEEL_E_TIMEOUT, never a hang).
+/* Team launches for a batch of one large scene. No counterpart in the reference, which prepares and
+   solves a scene on one 256-invocation workgroup (wgsl.js:1222, :2501-2504, sim.js:663). The prepare
+   and solve kernels are launched cooperatively with `blocks` blocks of the batch's block size that
+   share the scene's bodies, contacts, rows and articulations and meet at grid barriers (bounded
+   waits: STEEL_E_TIMEOUT, never a hang); the prepare's scan-based passes (contact classification,
+   unit scan, sleep islands, coloring) stay on the team's first block.
    0: one block (the batched path). STEEL_TEAM_AUTO, the default: a scene of at least 2048 bodies or
    64 articulations gets one thread per body or a warp per articulation, capped by the blocks that
    fit the GPU. Other values: that many blocks (STEEL_E_INVALID if more than fit). Batches of

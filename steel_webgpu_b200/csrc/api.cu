@@ -169,14 +169,17 @@ struct steel_batch {
   bool serve_dirty = false;                    // admitted set changed: upload the launch order
   std::vector<uint32_t> order_host;  // block order of the prepare and solve kernels
   uint32_t team_req = STEEL_TEAM_AUTO;  // steel_set_team request (0 off, STEEL_TEAM_AUTO, or blocks)
-  size_t o_team = 0;                    // the team solve's grid-barrier counter
+  size_t o_team = 0;                    // the team launches' words (BatchDev::team_bar)
   uint64_t serve_next_id = 1;
   bool serve_on = false;
 };
 
 namespace {
 
-int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, uint32_t threads, std::string& why) {
+// threads: the largest prepare / solve block; one_scene: the batch has this scene alone (a team
+// launch may run it, whose scratch passes use TEAM_SCRATCH_BLOCKS blocks' threads).
+int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, uint32_t threads, bool one_scene,
+                std::string& why) {
   Consts& C = s.C;
   if (!C.parse(in.constants)) { why = "malformed constants text"; return STEEL_E_INVALID; }
   if (in.statF_floats != (uint64_t)C.u("LEN_STATF4") * 4u || in.statU_words != C.u("LEN_STATU") ||
@@ -302,7 +305,9 @@ int build_scene(SceneHost& s, const steel_scene_desc& in, Layout& L, uint32_t th
   s.o_sched = L.take(s.sched_words * 4);
   s.o_tw = L.take((size_t)NB * 32); s.o_imp = L.take((size_t)NB * 32);
   s.o_aqd = L.take((size_t)(ND > 0 ? ND : 1) * 4);
-  s.o_tscr = L.take((size_t)threads * s.tscr_floats * 4);
+  const bool team_sized = one_scene && (NB >= TEAM_MIN_BODIES || d.NA >= TEAM_MIN_ARTS);
+  d.TSCR_T = team_sized ? threads * TEAM_SCRATCH_BLOCKS : threads;
+  s.o_tscr = L.take((size_t)d.TSCR_T * s.tscr_floats * 4);
   s.arena_bytes = L.bytes - arena0;
   return STEEL_OK;
 }
@@ -372,7 +377,7 @@ int check_device_error(steel_batch* b) {
     return fail(STEEL_E_TIMEOUT, "a shared-memory bulk copy did not complete within its wait limit; the scene's "
                                  "substep was skipped");
   if (e == ERR_TEAM_TIMEOUT)
-    return fail(STEEL_E_TIMEOUT, "a block of the team solve gave up waiting at a grid barrier");
+    return fail(STEEL_E_TIMEOUT, "a block of a team launch gave up waiting at a grid barrier");
   if (e != 0) return fail(STEEL_E_CUDA, "device error " + std::to_string(e));
   return STEEL_OK;
 }
@@ -399,18 +404,18 @@ uint32_t stage_flags(const SceneDev& d, uint32_t budget) {
   return st;
 }
 
-// Blocks of the team solve (team.cuh) for the batch's block size and shared memory: a batch of one
-// scene without Nesterov momentum; STEEL_TEAM_AUTO takes scenes of at least TEAM_MIN_BODIES bodies
-// or TEAM_MIN_ARTS articulations, with one thread per body or a warp per articulation, capped by the
-// blocks that fit the GPU. Fewer than two blocks: the one-block path. `strict`: a request for more
+// Blocks of the team launches of prepare and solve (team.cuh) for the batch's block size and shared
+// memory: a batch of one scene without Nesterov momentum; STEEL_TEAM_AUTO takes scenes of at least
+// TEAM_MIN_BODIES bodies or TEAM_MIN_ARTS articulations, with one thread per body or a warp per
+// articulation, capped by the blocks that fit the GPU. Fewer than two blocks: the one-block path. `strict`: a request for more
 // blocks than fit is an error (steel_set_team) rather than capped (a later change of tiles).
-constexpr uint32_t TEAM_MIN_BODIES = 2048u, TEAM_MIN_ARTS = 64u;
 int team_blocks_for(const steel_batch* b, uint32_t req, bool strict, uint32_t* out) {
   *out = 0u;
   if (req == 0u || b->sc.size() != 1u || b->sc[0].d.NEST != 0u) return STEEL_OK;
   const SceneDev& d = b->sc[0].d;
   const uint32_t T = b->bd.block_threads;
-  const int per_sm = solve_team_blocks_per_sm(T, b->bd.solve_smem);
+  const int per_sm = std::min(solve_team_blocks_per_sm(T, b->bd.solve_smem),
+                              prepare_team_blocks_per_sm(T, b->bd.prep_smem));
   const uint32_t cap = per_sm > 0 ? (uint32_t)per_sm * (uint32_t)b->ctx->sms : 0u;
   uint32_t n = 0u;
   if (req == STEEL_TEAM_AUTO) {
@@ -649,7 +654,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   b->max_threads = big ? BIG_THREADS : DEFAULT_THREADS;
   for (uint32_t i = 0; i < n; i++) {
     std::string why;
-    int rc = build_scene(b->sc[i], scenes[i], L, b->max_threads, why);
+    int rc = build_scene(b->sc[i], scenes[i], L, b->max_threads, n == 1u, why);
     if (rc) return fail(rc, "scene " + std::to_string(i) + ": " + why);
     if (i > 0 && b->sc[i].d.substeps != b->sc[0].d.substeps)
       return fail(STEEL_E_INVALID, "scenes of one batch must share the substep count");
@@ -680,7 +685,7 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   b->o_active = L.take(4ull * n);
   b->o_order = L.take(4ull * n);
   b->o_err = L.take(4);
-  b->o_team = L.take(16);
+  b->o_team = L.take(32);
   b->o_stage = L.take(4ull * n);
   std::vector<uint64_t> tgt_off(n), pose_off(n);
   for (uint32_t i = 0; i < n; i++) {

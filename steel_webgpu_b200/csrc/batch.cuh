@@ -33,8 +33,10 @@ struct BatchDev {
                               // lowers it to make the bounded wait run out)
   unsigned long long* trace_prep;   // null, or [nscenes][3]: each scene's last k_prepare block, its start and
   unsigned long long* trace_solve;  // end (%globaltimer, ns) and SM; the same for k_solve (steel_trace)
-  uint32_t team_blocks;       // nonzero: the batch's one scene is solved by this many cooperating blocks
-  uint32_t* team_bar;         // [1] grid-barrier arrival counter of that solve (zeroed before each launch)
+  uint32_t team_blocks;       // nonzero: the batch's one scene is prepared and solved by this many
+                              // cooperating blocks (team.cuh)
+  uint32_t* team_bar;         // [8]: [0] grid-barrier arrival counter of a team launch (zeroed before each
+                              // launch), [4..7] counts the prepare's block 0 hands to the other blocks
 };
 
 // Block trace: the global timer (ns) and the block's record after the scene's body, written by
@@ -86,7 +88,11 @@ constexpr uint32_t RS_ITEMS = 16;           // keys per thread and tile
 constexpr uint32_t RS_TILE = RS_THREADS * RS_ITEMS;
 constexpr uint32_t RS_DIGITS = 12;          // 96 key bits, 8 per digit
 constexpr uint32_t RS_SPIN_LIMIT = 1u << 22;  // polls of a preceding tile's status before giving up
-constexpr uint32_t TEAM_WAIT_LIMIT = 1u << 22;  // polls of a team solve's grid barrier before giving up
+constexpr uint32_t TEAM_WAIT_LIMIT = 1u << 22;  // polls of a team launch's grid barrier before giving up
+// Team launches (team.cuh) on a batch of one scene: the default takes scenes of at least
+// TEAM_MIN_BODIES bodies or TEAM_MIN_ARTS articulations; such a scene's per-thread scratch has
+// slices for TEAM_SCRATCH_BLOCKS blocks, so the prepare's scratch passes spread over that many.
+constexpr uint32_t TEAM_MIN_BODIES = 2048u, TEAM_MIN_ARTS = 64u, TEAM_SCRATCH_BLOCKS = 32u;
 struct RadixDev {
   uint4* keys[2];     // ping-pong key buffers [MAXC] (x pair, y feature, z hash, w raw index)
   uint32_t* status;   // [RS_DIGITS][tiles][256] look-back words: bits 30-31 flag (1 tile count, 2 prefix)
@@ -162,12 +168,14 @@ template <int T> cudaError_t configure_solve_t(size_t smem_bytes);
 template <int T> void launch_prepare_t(const BatchDev& b, cudaStream_t st);
 template <int T> void launch_solve_t(const BatchDev& b, cudaStream_t st);
 template <int T> int solve_team_blocks_per_sm_t(size_t smem_bytes);
+template <int T> int prepare_team_blocks_per_sm_t(size_t smem_bytes);
 #define STEEL_DECLARE_BLOCK(N)                                                  \
   template <> cudaError_t configure_prepare_t<N>(size_t smem_bytes);            \
   template <> cudaError_t configure_solve_t<N>(size_t smem_bytes);              \
   template <> void launch_prepare_t<N>(const BatchDev& b, cudaStream_t st);     \
   template <> void launch_solve_t<N>(const BatchDev& b, cudaStream_t st);       \
-  template <> int solve_team_blocks_per_sm_t<N>(size_t smem_bytes);
+  template <> int solve_team_blocks_per_sm_t<N>(size_t smem_bytes);      \
+  template <> int prepare_team_blocks_per_sm_t<N>(size_t smem_bytes);
 STEEL_DECLARE_BLOCK(32)
 STEEL_DECLARE_BLOCK(64)
 STEEL_DECLARE_BLOCK(128)
@@ -180,6 +188,7 @@ void launch_prepare(const BatchDev& b, cudaStream_t st);
 void launch_solve(const BatchDev& b, cudaStream_t st);
 // Resident blocks per SM of the team solve kernel at this block size and dynamic shared memory.
 int solve_team_blocks_per_sm(uint32_t threads, size_t smem_bytes);
+int prepare_team_blocks_per_sm(uint32_t threads, size_t smem_bytes);
 void launch_set_stage(const BatchDev& b, const uint32_t* stage, cudaStream_t st);
 void launch_frame_end(const BatchDev& b, cudaStream_t st);
 // Host-I/O staging: scatter packed joint targets into each scene, gather packed body poses.

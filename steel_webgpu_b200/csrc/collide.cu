@@ -1724,6 +1724,13 @@ int solve_team_blocks_per_sm(uint32_t threads, size_t smem_bytes) {
 #undef STEEL_CALL
   return n;
 }
+int prepare_team_blocks_per_sm(uint32_t threads, size_t smem_bytes) {
+  int n = 0;
+#define STEEL_CALL(N) n = prepare_team_blocks_per_sm_t<N>(smem_bytes)
+  STEEL_BY_BLOCK(threads, STEEL_CALL)
+#undef STEEL_CALL
+  return n;
+}
 #undef STEEL_BY_BLOCK
 // Each scene's shared-memory staging flags (SceneDev::stage) from a packed array, one per scene.
 __global__ void k_set_stage(BatchDev B, const uint32_t* stage) {

@@ -229,6 +229,7 @@ struct SceneDev {
       S_BLIST, S_RKEY, S_RFLAG, S_WL;
   float* tscr;                       // per-thread scratch slices (path temporaries), TSCR floats each
   uint32_t TSCR;
+  uint32_t TSCR_T;                   // threads the scratch has slices for
   float4 *tw, *imp;                  // solve: body twists and link impulses [NB * 2]
   uint32_t stage;                    // shared-memory staging: bit 0 link blocks (prepare, solve),
                                      // bit 1 twists, impulses and qd (solve)

@@ -18,14 +18,26 @@ template <bool F64>
 __global__ void __launch_bounds__(STEEL_BLOCK, blocks_per_sm_of(STEEL_BLOCK)) k_prepare(BatchDev B) {
   const uint32_t sc = B.order[blockIdx.x];
   const unsigned long long t0 = B.trace_prep ? trace_clock() : 0ull;
-  prepare_scene<F64>(B, sc);
+  prepare_scene<F64, false>(B, sc, Team<false>{});
   if (B.trace_prep) trace_block(B.trace_prep + 3ull * sc, t0);
+}
+// A batch of one large scene: every block of this cooperative launch prepares it together
+// (team.cuh).
+template <bool F64>
+__global__ void __launch_bounds__(STEEL_BLOCK, blocks_per_sm_of(STEEL_BLOCK)) k_prepare_team(BatchDev B) {
+  __shared__ uint32_t team_state[2];
+  if (threadIdx.x == 0u) { team_state[0] = 0u; team_state[1] = 0u; }  // published by copy_scene's barrier
+  const uint32_t sc = B.order[0];
+  const unsigned long long t0 = B.trace_prep ? trace_clock() : 0ull;
+  prepare_scene<F64, true>(B, sc, Team<true>{B.team_bar, B.error, TEAM_WAIT_LIMIT, team_state});
+  if (B.trace_prep && blockIdx.x == 0u) trace_block(B.trace_prep + 3ull * sc, t0);
 }
 }  // namespace STEEL_NS
 
 template <>
 cudaError_t configure_prepare_t<STEEL_BLOCK>(size_t smem_bytes) {
-  const void* fns[] = {(const void*)STEEL_NS::k_prepare<false>, (const void*)STEEL_NS::k_prepare<true>};
+  const void* fns[] = {(const void*)STEEL_NS::k_prepare<false>, (const void*)STEEL_NS::k_prepare<true>,
+                       (const void*)STEEL_NS::k_prepare_team<false>, (const void*)STEEL_NS::k_prepare_team<true>};
   for (const void* f : fns) {
     cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
     if (e != cudaSuccess) return e;
@@ -34,8 +46,32 @@ cudaError_t configure_prepare_t<STEEL_BLOCK>(size_t smem_bytes) {
 }
 template <>
 void launch_prepare_t<STEEL_BLOCK>(const BatchDev& b, cudaStream_t st) {
+  if (b.team_blocks) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(b.team_blocks);
+    cfg.blockDim = dim3(STEEL_BLOCK);
+    cfg.dynamicSmemBytes = b.prep_smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;  // every block resident: the grid barrier's guarantee
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaMemsetAsync(b.team_bar, 0, sizeof(uint32_t), st);
+    if (b.art_f64) cudaLaunchKernelEx(&cfg, STEEL_NS::k_prepare_team<true>, b);
+    else cudaLaunchKernelEx(&cfg, STEEL_NS::k_prepare_team<false>, b);
+    return;
+  }
   if (b.art_f64) STEEL_NS::k_prepare<true><<<b.nlaunch, STEEL_BLOCK, b.prep_smem, st>>>(b);
   else STEEL_NS::k_prepare<false><<<b.nlaunch, STEEL_BLOCK, b.prep_smem, st>>>(b);
+}
+template <>
+int prepare_team_blocks_per_sm_t<STEEL_BLOCK>(size_t smem_bytes) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, STEEL_NS::k_prepare_team<true>, STEEL_BLOCK, smem_bytes) !=
+      cudaSuccess)
+    return 0;
+  return n;
 }
 
 }  // namespace steel

@@ -13,6 +13,7 @@
 // runs through a unit hash and a walk list, here they come straight from one block scan. Rows
 // are numbered unit by unit in contact order, so rows are also in contact order, which makes
 // the serial overflow color's contact-order sort the identity.
+#include "team.cuh"
 #include "art.cuh"
 #include "batch.cuh"
 #include "bulk.cuh"
@@ -748,26 +749,35 @@ __device__ __forceinline__ void sleep_islands(const Prep& pr, uint32_t tid, uint
   }
 }
 
-// Prepare of scene sc by the calling block (all its threads).
-template <bool F64>
-__device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
+// Prepare of scene sc by a team (all its threads): the calling block (TEAM false, the batched
+// path), or every block of a cooperative launch on a batch of one large scene (TEAM true). In a
+// team launch the passes over articulations, contacts, units and rows are spread over all blocks
+// and meet at grid barriers; the passes built on block-wide scans and shared counters (contact
+// classification, the unit scan, sleep islands, coloring and the color buckets) run on block 0
+// exactly as in the one-block kernel, and their counts reach the other blocks through the team's
+// words (B.team_bar[4..7]). Nothing is staged in shared memory; the per-thread scratch serves the
+// first TSCR_T threads of the team (all threads of a block).
+template <bool F64, bool TEAM>
+__device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc, Team<TEAM> tm) {
   extern __shared__ float4 psm4[];  // prep_smem_layout: link blocks, coloring
   __shared__ uint32_t stmp[40];
   __shared__ Params Ps;
   __shared__ SceneDev Ss;  // the scene's offsets and sizes, read everywhere in the serial passes
-  const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  const uint32_t tid = tm.rank(), nt = tm.size();
+  const bool b0 = !TEAM || blockIdx.x == 0u;  // this block runs the block-wide passes
   if (B.active[sc] == 0u) return;  // not stepping in this frame (serving loop)
   copy_scene(Ss, B.scenes[sc]);
   const SceneDev& S = Ss;
-  if (tid == 0u) Ps = *B.scenes[sc].params;
+  if (threadIdx.x == 0u) Ps = *B.scenes[sc].params;
   uint8_t* pb = reinterpret_cast<uint8_t*>(psm4);
-  const PrepSmem lay = prep_smem_layout(S.stage, S.NL, S.NB, S.NCOLW, S.NCOL);
-  const bool staged = (S.stage & STAGE_LINKS) != 0u;
+  const uint32_t stage = TEAM ? 0u : S.stage;
+  const PrepSmem lay = prep_smem_layout(stage, S.NL, S.NB, S.NCOLW, S.NCOL);
+  const bool staged = (stage & STAGE_LINKS) != 0u;
   float* lb = staged ? reinterpret_cast<float*>(pb + lay.links) : S.art + S.A_LINK;
   // Link blocks into shared memory with one bulk copy (A_LINK is 16-byte aligned).
   __shared__ __align__(8) uint64_t stage_bar;
   if (staged && !stage_to_shared(lb, S.art + S.A_LINK, 4u * S.NL * LBLK, &stage_bar, B.wait_limit)) {
-    if (tid == 0u) atomicCAS(B.error, 0u, (uint32_t)ERR_STAGE_TIMEOUT);
+    if (threadIdx.x == 0u) atomicCAS(B.error, 0u, (uint32_t)ERR_STAGE_TIMEOUT);
     return;  // the whole block: the result above is the same in every thread
   }
   __syncthreads();
@@ -776,7 +786,9 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
   const Art& ar = pr.ar;
   float* A = S.art;
   uint32_t* sch = S.sched;
-  float* tscr = S.tscr + (size_t)tid * S.TSCR;
+  // Threads that own a scratch slice: every thread of a block, the first TSCR_T of a team.
+  const uint32_t sn = TEAM ? min(nt, S.TSCR_T) : nt;
+  float* tscr = S.tscr + (size_t)tid * S.TSCR;  // dereferenced only by threads below sn
 
   // Phase 0: clear this substep's warm table halves and scratch; drive targets.
   const uint32_t wbase = (1u - P.parity) * S.WH;
@@ -809,8 +821,11 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
     float4 c = S.sf[S.SF_CTRL];
     A[S.A_TGTV + S.CTRL_B] = c.y * clmp(A[S.A_Q + S.CTRL_A] / c.x, 0.0f, 1.0f);
   }
-  if (S.SLEEP == 1u) sleep_islands(pr, tid, nt);
-  __syncthreads();
+  if (S.SLEEP == 1u) {
+    if (TEAM) tm.sync();  // the clears and targets above, from every block
+    if (b0) sleep_islands(pr, threadIdx.x, blockDim.x);
+  }
+  tm.sync();
   // Joint-limit gating, listed joint rows, FK and factorisation per articulation.
   auto gate = [&](uint32_t a) {
     uint4 ai = ar.info(a);
@@ -882,68 +897,74 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
       factor(a);
     }
   }
-  // Phase 1: classify the sorted contacts; units are runs of one body pair.
+  // Phase 1: classify the sorted contacts; units are runs of one body pair (block-wide scans: one
+  // block).
   const uint32_t nc = min(S.counters[1], S.MAXC);
-  const uint32_t ch = (nc + nt - 1u) / nt;
-  const uint32_t c_lo = min(tid * ch, nc), c_hi = min(c_lo + ch, nc);
-  uint32_t heads = 0u, listed = 0u, dn = 0u;
-  auto pair_of = [&](uint32_t c) {
-    float4 m = S.con[c * 5u + 2u];
-    return (uint32_t)(f2i(m.x) + 1) | ((uint32_t)(f2i(m.y) + 1) << 16u);
-  };
-  auto is_dense = [&](uint32_t c) {
-    float4 m = S.con[c * 5u + 2u];
-    int a = f2i(m.x), b = f2i(m.y);
-    return a >= 0 && b >= 0 && pr.bkind(a) == 2u && pr.bkind(b) == 2u && pr.bart(a) == pr.bart(b);
-  };
-  // Contacts between sleeping (or static) sides make no rows (wgsl.js:1905). A same-articulation
-  // contact is asleep exactly when its articulation is, so every dense contact left has rows.
-  auto asleep = [&](uint32_t c) {
-    if (S.SLEEP == 0u) return false;
-    float4 m = S.con[c * 5u + 2u];
-    return pr.pair_asleep(f2i(m.x), f2i(m.y));
-  };
-  for (uint32_t c = c_lo; c < c_hi; c++) {
-    if (asleep(c)) continue;
-    if (is_dense(c)) { dn++; continue; }
-    listed++;
-    if (c == 0u || pair_of(c - 1u) != pair_of(c)) heads++;
-  }
-  uint32_t nu, nl, ndc;
-  uint32_t ubase = block_excl_scan(heads, stmp, &nu);
-  uint32_t lbase = block_excl_scan(listed, stmp, &nl);
-  uint32_t dbase = block_excl_scan(dn, stmp, &ndc);
-  {
-    uint32_t unit = ubase, pos = lbase, ds = dbase;
-    for (uint32_t c = c_lo; c < c_hi; c++) {
-      if (asleep(c)) {
-        sch[S.S_UNITOF + c] = 0xffffffffu;
-        sch[S.S_DSLOT + c] = 0xffffffffu;
-        continue;
-      }
-      if (is_dense(c)) {
-        sch[S.S_UNITOF + c] = 0xffffffffu;
-        sch[S.S_DSLOT + c] = ds++;
-        continue;
-      }
-      sch[S.S_DSLOT + c] = 0xffffffffu;
-      uint32_t pk = pair_of(c);
-      if (c == 0u || pair_of(c - 1u) != pk) {
-        sch[S.S_UKEY + unit] = pk;
-        sch[S.S_USTART0 + unit] = pos;
-        unit++;
-      }
-      sch[S.S_UNITOF + c] = unit - 1u;
-      sch[S.S_CORDER + pos] = c;
-      pos++;
+  uint32_t nu = 0u, nl = 0u, ndc = 0u;
+  if (b0) {
+    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t ch = (nc + nt - 1u) / nt;
+    const uint32_t c_lo = min(tid * ch, nc), c_hi = min(c_lo + ch, nc);
+    uint32_t heads = 0u, listed = 0u, dn = 0u;
+    auto pair_of = [&](uint32_t c) {
+      float4 m = S.con[c * 5u + 2u];
+      return (uint32_t)(f2i(m.x) + 1) | ((uint32_t)(f2i(m.y) + 1) << 16u);
+    };
+    auto is_dense = [&](uint32_t c) {
       float4 m = S.con[c * 5u + 2u];
       int a = f2i(m.x), b = f2i(m.y);
-      if (a >= 0 && pr.bkind(a) == 2u) sch[S.S_LINKHIT + a] = 1u;
-      if (b >= 0 && pr.bkind(b) == 2u) sch[S.S_LINKHIT + b] = 1u;
+      return a >= 0 && b >= 0 && pr.bkind(a) == 2u && pr.bkind(b) == 2u && pr.bart(a) == pr.bart(b);
+    };
+    // Contacts between sleeping (or static) sides make no rows (wgsl.js:1905). A same-articulation
+    // contact is asleep exactly when its articulation is, so every dense contact left has rows.
+    auto asleep = [&](uint32_t c) {
+      if (S.SLEEP == 0u) return false;
+      float4 m = S.con[c * 5u + 2u];
+      return pr.pair_asleep(f2i(m.x), f2i(m.y));
+    };
+    for (uint32_t c = c_lo; c < c_hi; c++) {
+      if (asleep(c)) continue;
+      if (is_dense(c)) { dn++; continue; }
+      listed++;
+      if (c == 0u || pair_of(c - 1u) != pair_of(c)) heads++;
     }
+    uint32_t ubase = block_excl_scan(heads, stmp, &nu);
+    uint32_t lbase = block_excl_scan(listed, stmp, &nl);
+    uint32_t dbase = block_excl_scan(dn, stmp, &ndc);
+    {
+      uint32_t unit = ubase, pos = lbase, ds = dbase;
+      for (uint32_t c = c_lo; c < c_hi; c++) {
+        if (asleep(c)) {
+          sch[S.S_UNITOF + c] = 0xffffffffu;
+          sch[S.S_DSLOT + c] = 0xffffffffu;
+          continue;
+        }
+        if (is_dense(c)) {
+          sch[S.S_UNITOF + c] = 0xffffffffu;
+          sch[S.S_DSLOT + c] = ds++;
+          continue;
+        }
+        sch[S.S_DSLOT + c] = 0xffffffffu;
+        uint32_t pk = pair_of(c);
+        if (c == 0u || pair_of(c - 1u) != pk) {
+          sch[S.S_UKEY + unit] = pk;
+          sch[S.S_USTART0 + unit] = pos;
+          unit++;
+        }
+        sch[S.S_UNITOF + c] = unit - 1u;
+        sch[S.S_CORDER + pos] = c;
+        pos++;
+        float4 m = S.con[c * 5u + 2u];
+        int a = f2i(m.x), b = f2i(m.y);
+        if (a >= 0 && pr.bkind(a) == 2u) sch[S.S_LINKHIT + a] = 1u;
+        if (b >= 0 && pr.bkind(b) == 2u) sch[S.S_LINKHIT + b] = 1u;
+      }
+    }
+    if (tid == 0u) sch[S.S_USTART0 + nu] = nl;
+    if (TEAM && tid == 0u) { B.team_bar[4] = nu; B.team_bar[5] = nl; B.team_bar[6] = ndc; }
   }
-  if (tid == 0u) sch[S.S_USTART0 + nu] = nl;
-  __syncthreads();
+  tm.sync();
+  if (TEAM) { nu = B.team_bar[4]; nl = B.team_bar[5]; ndc = B.team_bar[6]; }
   for (uint32_t u = tid; u < nu; u += nt) sch[S.S_USIZE + u] = sch[S.S_USTART0 + u + 1u] - sch[S.S_USTART0 + u];
   // Phase 2: joint split, link responses of contact-bearing links, H^-1 diagonals.
   for (uint32_t l = tid; l < S.NL; l += nt) {
@@ -951,18 +972,18 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
     int j = (int)l;
     while (j >= 0) { atomicAdd(&sch[S.S_JSPLIT + j], 1u); j = ar.lparent((uint32_t)j); }
   }
-  __syncthreads();
+  tm.sync();
   {
     uint32_t* pth = (uint32_t*)tscr;
     uint32_t* cnt = pth + S.MAXPATH;
     float* ub = (float*)(cnt + S.MAXPATH);
-    for (uint32_t l = tid; l < S.NL; l += nt) {
+    for (uint32_t l = tid; tid < sn && l < S.NL; l += sn) {
       if (sch[S.S_LINKHIT + ar.lbody(l)] == 0u) continue;
       uint32_t np = ar.path(l, pth);
       for (uint32_t i = 0; i < np; i++) cnt[i] = sch[S.S_JSPLIT + pth[i]];
       ar.response(l, cnt, pth, ub);
     }
-    for (uint32_t d = tid; d < S.ND; d += nt) {
+    for (uint32_t d = tid; tid < sn && d < S.ND; d += sn) {
       float4 lim = ar.dof_limit(d);
       const float4 drv = ar.dof_drive(d);
       if (lim.z > 0.5f || ar.dof_passive(d).y > 0.0f || ar.dof_passive(d).z >= 0.0f ||
@@ -981,7 +1002,7 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
     uint32_t* bpc = sch + S.S_BPC + p * 4u;
     bpc[0] = __float_as_uint(px); bpc[1] = __float_as_uint(py); bpc[2] = __float_as_uint(gap); bpc[3] = pk;
   }
-  __syncthreads();
+  tm.sync();
   for (uint32_t p = tid; p < nl; p += nt) {
     uint32_t st = sch[S.S_USTART0 + sch[S.S_UNITOF + sch[S.S_CORDER + p]]];
     uint32_t k0 = sch[S.S_RK0 + p], k1 = sch[S.S_RK1 + p], k2 = sch[S.S_RK2 + p];
@@ -991,7 +1012,7 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
     sch[S.S_LEAD + p] = lead;
     for (uint32_t q = 0; q < 26u; q++) sch[S.S_SLOT + p * 26u + q] = 0u;
   }
-  __syncthreads();
+  tm.sync();
   for (uint32_t p = tid; p < nl; p += nt) {
     const uint32_t* bpc = sch + S.S_BPC + p * 4u;
     uint32_t* sl = sch + S.S_SLOT + sch[S.S_LEAD + p] * 26u;
@@ -1001,7 +1022,7 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
       if (id != 0u) atomicMax(&sl[q * 2u], s_);
     }
   }
-  __syncthreads();
+  tm.sync();
   for (uint32_t p = tid; p < nl; p += nt) {
     const uint32_t* bpc = sch + S.S_BPC + p * 4u;
     uint32_t* sl = sch + S.S_SLOT + sch[S.S_LEAD + p] * 26u;
@@ -1011,7 +1032,7 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
       if (id != 0u && s_ == sl[q * 2u]) atomicMax(&sl[q * 2u + 1u], id);
     }
   }
-  __syncthreads();
+  tm.sync();
   for (uint32_t p = tid; p < nl; p += nt) {
     const uint32_t* bpc = sch + S.S_BPC + p * 4u;
     const uint32_t* sl = sch + S.S_SLOT + sch[S.S_LEAD + p] * 26u;
@@ -1023,7 +1044,7 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
     }
     sch[S.S_KEEP + p] = (win || S.COMPL == 1u) ? 1u : 0u;  // compliant contacts stay whole
   }
-  __syncthreads();
+  tm.sync();
   for (uint32_t u = tid; u < nu; u += nt) {
     uint32_t n = sch[S.S_USIZE + u], st = sch[S.S_USTART0 + u], kept = 0u;
     for (uint32_t j = 0; j < n; j++)
@@ -1032,9 +1053,19 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
     sch[S.S_USTART + u] = kept;
   }
   for (uint32_t c = tid; c < nc; c += nt) sch[S.S_ROWOF + c] = 0xffffffffu;
-  __syncthreads();
-  const uint32_t total = block_scan_array(sch + S.S_USTART, nu, stmp);
-  if (tid == 0u) sch[S.S_USTART + nu] = total;
+  tm.sync();
+  uint32_t total = 0u;
+  if (b0) {
+    total = block_scan_array(sch + S.S_USTART, nu, stmp);
+    if (threadIdx.x == 0u) {
+      sch[S.S_USTART + nu] = total;
+      if (TEAM) B.team_bar[7] = total;
+    }
+  }
+  if (TEAM) {
+    tm.sync();
+    total = B.team_bar[7];
+  }
   for (uint32_t u = tid; u < nu; u += nt) {
     uint32_t st = sch[S.S_USTART + u], st0 = sch[S.S_USTART0 + u];
     for (uint32_t j = 0; j < sch[S.S_USIZE + u]; j++) {
@@ -1044,240 +1075,245 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
       sch[S.S_ROWOF + c] = st + j;
     }
   }
-  __syncthreads();
+  tm.sync();
   // Phase 6: rows, then friction patches.
   for (uint32_t idx = tid; idx < total; idx += nt) pr.build_row(idx, sch[S.S_RCON + idx]);
-  __syncthreads();
+  tm.sync();
   if (S.TORS == 1u) {
     for (uint32_t u = tid; u < nu; u += nt) pr.build_torsion(u);
-    __syncthreads();
+    tm.sync();
   }
   if (S.PATCH == 1u)
     for (uint32_t u = tid; u < nu; u += nt) pr.build_patch(u);
-  __syncthreads();
-  // Phase 6c: greedy first-fit coloring of the rows in contact order (the reference's serial pass,
-  // W:1254-1267, reproduced in parallel rounds below; the longest-first order keeps a serial pass),
-  // with the per-body color masks (in shared memory when staged) and the color counts in shared
-  // memory; then the rows bucketed by color in row order (warp 0, match/ballot ranks).
-  {
-    uint32_t* wcount = reinterpret_cast<uint32_t*>(pb + lay.wcount);
-    uint32_t* wmask = (S.stage & STAGE_WMASK) ? reinterpret_cast<uint32_t*>(pb + lay.wmask) : sch + S.S_WMASK;
-    const uint32_t NCOLW = S.NCOLW;
-    for (uint32_t i = tid; i < S.NCOL + 2u; i += nt) wcount[i] = 0u;
-    if (S.stage & STAGE_WMASK)
-      for (uint32_t i = tid; i < S.NB * NCOLW; i += nt) wmask[i] = 0u;
-    if (S.LONGEST_FIRST == 0u) {
-      // First-fit in row order, in parallel rounds with the same colors (Jones-Plassmann with the
-      // row index as priority). Every body keeps its rows in row order and a frontier, the first
-      // of them not yet colored; rows on one body are colored in that order, so when a row is the
-      // frontier of both its bodies every earlier row touching them has its color, and the body
-      // masks hold exactly the colors the serial pass would see. Such rows share no body, so one
-      // round colors all of them without conflicts. A round only looks at the bodies whose
-      // frontier moved in the previous one (all bodies in the first): phase A finds the ready rows
-      // among their frontier rows (a row whose two bodies both look at it is listed once), phase B
-      // colors them, advances the frontiers and lists the moved bodies for the next round. A row
-      // is found in the round its last frontier reaches it, since that body is on the list. Each
-      // round colors at least the lowest uncolored row, so the rounds end.
-      uint32_t* bstart = sch + S.S_BSTART;  // [NB + 1] each body's first list entry
-      uint32_t* bpos = sch + S.S_BPOS;      // [NB] fill cursor, then frontier
-      uint32_t* rdy = sch + S.S_BREADY;     // [NB] rows found ready in a round
-      uint32_t* blist = sch + S.S_BLIST;    // [2 * MAXC] rows of each body
-      uint32_t* rkey = sch + S.S_RKEY;      // [MAXC] body-pair key of each row
-      uint32_t* rflag = sch + S.S_RFLAG;    // [MAXC] the row is on the ready list
-      uint32_t* wl[2] = {sch + S.S_WL, sch + S.S_WL + S.NB};  // [2][NB] bodies to look at
-      __shared__ uint32_t wl_n[2], rdy_n;
-      const uint32_t NB = S.NB;
-      for (uint32_t b = tid; b <= NB; b += nt) bstart[b] = 0u;
-      if (tid == 0u) { wl_n[0] = 0u; wl_n[1] = 0u; rdy_n = 0u; }
-      __syncthreads();
-      for (uint32_t r = tid; r < total; r += nt) {
-        const uint32_t key = sch[S.S_UKEY + sch[S.S_RUNIT + r]];
-        rkey[r] = key;
-        rflag[r] = 0u;
-        const int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
-        if (a >= 0) atomicAdd(&bstart[a], 1u);
-        if (b >= 0 && b != a) atomicAdd(&bstart[b], 1u);
-      }
-      __syncthreads();
-      block_scan_array(bstart, NB + 1u, stmp);
-      for (uint32_t b = tid; b < NB; b += nt) bpos[b] = bstart[b];
-      __syncthreads();
-      for (uint32_t r = tid; r < total; r += nt) {
-        const uint32_t key = rkey[r];
-        const int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
-        if (a >= 0) blist[atomicAdd(&bpos[a], 1u)] = r;
-        if (b >= 0 && b != a) blist[atomicAdd(&bpos[b], 1u)] = r;
-      }
-      __syncthreads();
-      for (uint32_t b = tid; b < NB; b += nt) {  // each body's rows in row order
-        const uint32_t s0 = bstart[b], s1 = bstart[b + 1u];
-        for (uint32_t i = s0 + 1u; i < s1; i++) {
-          const uint32_t v = blist[i];
-          uint32_t j = i;
-          while (j > s0 && blist[j - 1u] > v) { blist[j] = blist[j - 1u]; j--; }
-          blist[j] = v;
-        }
-        bpos[b] = s0;
-        if (s1 > s0) wl[0][atomicAdd(&wl_n[0], 1u)] = b;
-      }
-      __syncthreads();
-      uint32_t cur = 0u;
-      for (uint32_t round = 0; round <= total; round++) {
-        const uint32_t n = wl_n[cur];
-        if (n == 0u) break;  // the same value in every thread (read after the last barrier)
-        for (uint32_t i = tid; i < n; i += nt) {
-          const uint32_t b = wl[cur][i];
-          const uint32_t p = bpos[b];
-          if (p >= bstart[b + 1u]) continue;
-          const uint32_t r = blist[p];
-          const uint32_t key = rkey[r];
-          const int x = (int)(key & 0xffffu) - 1, y = (int)(key >> 16u) - 1;
-          const int other = x == (int)b ? y : x;
-          if (other >= 0 && other != (int)b && blist[bpos[other]] != r) continue;
-          if (atomicExch(&rflag[r], 1u) == 0u) rdy[atomicAdd(&rdy_n, 1u)] = r;
-        }
+  tm.sync();
+  // Phase 6c on one block (shared counters and block-wide scans); in a team launch the other
+  // blocks go on to the dense rows, which do not read the colors.
+  if (b0) {
+    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    // Phase 6c: greedy first-fit coloring of the rows in contact order (the reference's serial pass,
+    // W:1254-1267, reproduced in parallel rounds below; the longest-first order keeps a serial pass),
+    // with the per-body color masks (in shared memory when staged) and the color counts in shared
+    // memory; then the rows bucketed by color in row order (warp 0, match/ballot ranks).
+    {
+      uint32_t* wcount = reinterpret_cast<uint32_t*>(pb + lay.wcount);
+      uint32_t* wmask = (stage & STAGE_WMASK) ? reinterpret_cast<uint32_t*>(pb + lay.wmask) : sch + S.S_WMASK;
+      const uint32_t NCOLW = S.NCOLW;
+      for (uint32_t i = tid; i < S.NCOL + 2u; i += nt) wcount[i] = 0u;
+      if (stage & STAGE_WMASK)
+        for (uint32_t i = tid; i < S.NB * NCOLW; i += nt) wmask[i] = 0u;
+      if (S.LONGEST_FIRST == 0u) {
+        // First-fit in row order, in parallel rounds with the same colors (Jones-Plassmann with the
+        // row index as priority). Every body keeps its rows in row order and a frontier, the first
+        // of them not yet colored; rows on one body are colored in that order, so when a row is the
+        // frontier of both its bodies every earlier row touching them has its color, and the body
+        // masks hold exactly the colors the serial pass would see. Such rows share no body, so one
+        // round colors all of them without conflicts. A round only looks at the bodies whose
+        // frontier moved in the previous one (all bodies in the first): phase A finds the ready rows
+        // among their frontier rows (a row whose two bodies both look at it is listed once), phase B
+        // colors them, advances the frontiers and lists the moved bodies for the next round. A row
+        // is found in the round its last frontier reaches it, since that body is on the list. Each
+        // round colors at least the lowest uncolored row, so the rounds end.
+        uint32_t* bstart = sch + S.S_BSTART;  // [NB + 1] each body's first list entry
+        uint32_t* bpos = sch + S.S_BPOS;      // [NB] fill cursor, then frontier
+        uint32_t* rdy = sch + S.S_BREADY;     // [NB] rows found ready in a round
+        uint32_t* blist = sch + S.S_BLIST;    // [2 * MAXC] rows of each body
+        uint32_t* rkey = sch + S.S_RKEY;      // [MAXC] body-pair key of each row
+        uint32_t* rflag = sch + S.S_RFLAG;    // [MAXC] the row is on the ready list
+        uint32_t* wl[2] = {sch + S.S_WL, sch + S.S_WL + S.NB};  // [2][NB] bodies to look at
+        __shared__ uint32_t wl_n[2], rdy_n;
+        const uint32_t NB = S.NB;
+        for (uint32_t b = tid; b <= NB; b += nt) bstart[b] = 0u;
+        if (tid == 0u) { wl_n[0] = 0u; wl_n[1] = 0u; rdy_n = 0u; }
         __syncthreads();
-        const uint32_t nr = rdy_n;
-        if (tid == 0u) wl_n[cur ^ 1u] = 0u;
-        __syncthreads();
-        for (uint32_t k = tid; k < nr; k += nt) {
-          const uint32_t r = rdy[k];
-          const uint32_t key = rkey[r];
-          const int a = (int)(key & 0xffffu) - 1, c = (int)(key >> 16u) - 1;
-          uint32_t col = S.NCOL;
-          for (uint32_t w = 0; w < NCOLW; w++) {
-            uint32_t used = 0u;
-            if (a >= 0) used |= wmask[(uint32_t)a * NCOLW + w];
-            if (c >= 0) used |= wmask[(uint32_t)c * NCOLW + w];
-            if (used != 0xffffffffu) {
-              uint32_t kk = (uint32_t)__ffs(~used) - 1u;
-              if (a >= 0) wmask[(uint32_t)a * NCOLW + w] |= 1u << kk;
-              if (c >= 0) wmask[(uint32_t)c * NCOLW + w] |= 1u << kk;
-              col = w * 32u + kk;
-              break;
-            }
-          }
-          sch[S.S_PCOL + r] = col;
-          atomicAdd(&wcount[col], 1u);
-          // Advance the frontiers; a body with rows left is looked at in the next round.
-          if (a >= 0 && ++bpos[a] < bstart[a + 1u]) wl[cur ^ 1u][atomicAdd(&wl_n[cur ^ 1u], 1u)] = (uint32_t)a;
-          if (c >= 0 && c != a && ++bpos[c] < bstart[c + 1u]) wl[cur ^ 1u][atomicAdd(&wl_n[cur ^ 1u], 1u)] = (uint32_t)c;
-        }
-        __syncthreads();
-        if (tid == 0u) rdy_n = 0u;
-        cur ^= 1u;
-        __syncthreads();
-      }
-    }
-    __syncthreads();
-    if (S.LONGEST_FIRST == 1u && tid == 0u) {
-      // propagation_color_order "longest_first" (wgsl.js:2331-2346): first-fit by row count first
-      // (7 rows down to 1), then contact index. A unit's torsion row is its last row of its highest
-      // color; that color + 1 is kept as PCOL of the unit's current pick, so it needs no array.
-      for (uint32_t u = 0; u < nu; u++) sch[S.S_UTP + u] = 0xffffffffu;
-      for (uint32_t lp = 0; lp < 8u; lp++)
-        for (uint32_t c = 0; c < nc; c++) {
-          const uint32_t row = sch[S.S_ROWOF + c];
-          if (row >= total || pr.row_count(row) != 7u - lp) continue;
-          const uint32_t u = sch[S.S_RUNIT + row];
-          const uint32_t key = sch[S.S_UKEY + u];
+        for (uint32_t r = tid; r < total; r += nt) {
+          const uint32_t key = sch[S.S_UKEY + sch[S.S_RUNIT + r]];
+          rkey[r] = key;
+          rflag[r] = 0u;
           const int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
-          uint32_t col = S.NCOL;
-          for (uint32_t w = 0; w < NCOLW; w++) {
-            uint32_t used = 0u;
-            if (a >= 0) used |= wmask[(uint32_t)a * NCOLW + w];
-            if (b >= 0) used |= wmask[(uint32_t)b * NCOLW + w];
-            if (used != 0xffffffffu) {
-              uint32_t k = (uint32_t)__ffs(~used) - 1u;
-              if (a >= 0) wmask[(uint32_t)a * NCOLW + w] |= 1u << k;
-              if (b >= 0) wmask[(uint32_t)b * NCOLW + w] |= 1u << k;
-              col = w * 32u + k;
-              break;
+          if (a >= 0) atomicAdd(&bstart[a], 1u);
+          if (b >= 0 && b != a) atomicAdd(&bstart[b], 1u);
+        }
+        __syncthreads();
+        block_scan_array(bstart, NB + 1u, stmp);
+        for (uint32_t b = tid; b < NB; b += nt) bpos[b] = bstart[b];
+        __syncthreads();
+        for (uint32_t r = tid; r < total; r += nt) {
+          const uint32_t key = rkey[r];
+          const int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
+          if (a >= 0) blist[atomicAdd(&bpos[a], 1u)] = r;
+          if (b >= 0 && b != a) blist[atomicAdd(&bpos[b], 1u)] = r;
+        }
+        __syncthreads();
+        for (uint32_t b = tid; b < NB; b += nt) {  // each body's rows in row order
+          const uint32_t s0 = bstart[b], s1 = bstart[b + 1u];
+          for (uint32_t i = s0 + 1u; i < s1; i++) {
+            const uint32_t v = blist[i];
+            uint32_t j = i;
+            while (j > s0 && blist[j - 1u] > v) { blist[j] = blist[j - 1u]; j--; }
+            blist[j] = v;
+          }
+          bpos[b] = s0;
+          if (s1 > s0) wl[0][atomicAdd(&wl_n[0], 1u)] = b;
+        }
+        __syncthreads();
+        uint32_t cur = 0u;
+        for (uint32_t round = 0; round <= total; round++) {
+          const uint32_t n = wl_n[cur];
+          if (n == 0u) break;  // the same value in every thread (read after the last barrier)
+          for (uint32_t i = tid; i < n; i += nt) {
+            const uint32_t b = wl[cur][i];
+            const uint32_t p = bpos[b];
+            if (p >= bstart[b + 1u]) continue;
+            const uint32_t r = blist[p];
+            const uint32_t key = rkey[r];
+            const int x = (int)(key & 0xffffu) - 1, y = (int)(key >> 16u) - 1;
+            const int other = x == (int)b ? y : x;
+            if (other >= 0 && other != (int)b && blist[bpos[other]] != r) continue;
+            if (atomicExch(&rflag[r], 1u) == 0u) rdy[atomicAdd(&rdy_n, 1u)] = r;
+          }
+          __syncthreads();
+          const uint32_t nr = rdy_n;
+          if (tid == 0u) wl_n[cur ^ 1u] = 0u;
+          __syncthreads();
+          for (uint32_t k = tid; k < nr; k += nt) {
+            const uint32_t r = rdy[k];
+            const uint32_t key = rkey[r];
+            const int a = (int)(key & 0xffffu) - 1, c = (int)(key >> 16u) - 1;
+            uint32_t col = S.NCOL;
+            for (uint32_t w = 0; w < NCOLW; w++) {
+              uint32_t used = 0u;
+              if (a >= 0) used |= wmask[(uint32_t)a * NCOLW + w];
+              if (c >= 0) used |= wmask[(uint32_t)c * NCOLW + w];
+              if (used != 0xffffffffu) {
+                uint32_t kk = (uint32_t)__ffs(~used) - 1u;
+                if (a >= 0) wmask[(uint32_t)a * NCOLW + w] |= 1u << kk;
+                if (c >= 0) wmask[(uint32_t)c * NCOLW + w] |= 1u << kk;
+                col = w * 32u + kk;
+                break;
+              }
             }
+            sch[S.S_PCOL + r] = col;
+            atomicAdd(&wcount[col], 1u);
+            // Advance the frontiers; a body with rows left is looked at in the next round.
+            if (a >= 0 && ++bpos[a] < bstart[a + 1u]) wl[cur ^ 1u][atomicAdd(&wl_n[cur ^ 1u], 1u)] = (uint32_t)a;
+            if (c >= 0 && c != a && ++bpos[c] < bstart[c + 1u]) wl[cur ^ 1u][atomicAdd(&wl_n[cur ^ 1u], 1u)] = (uint32_t)c;
           }
-          sch[S.S_PCOL + row] = col;
-          wcount[col]++;
-          const uint32_t utp = sch[S.S_UTP + u];
-          const uint32_t utc = utp == 0xffffffffu ? 0u : sch[S.S_PCOL + utp] + 1u;
-          if (col + 1u >= utc) sch[S.S_UTP + u] = row;
+          __syncthreads();
+          if (tid == 0u) rdy_n = 0u;
+          cur ^= 1u;
+          __syncthreads();
         }
-    }
-    __syncthreads();
-    if (tid == 0u) {
-      uint32_t acc = 0u, ncol = 0u;
-      for (uint32_t c = 0; c <= S.NCOL; c++) {
-        uint32_t n = wcount[c];
-        sch[S.S_CSTART + c] = acc;
-        wcount[c] = acc;
-        acc += n;
-        if (n > 0u) ncol = c + 1u;
       }
-      sch[S.S_CSTART + S.NCOL + 1u] = acc;
-      sch[S.S_META + 0u] = nu;
-      sch[S.S_META + 1u] = ncol;
-      sch[S.S_META + 2u] = nc;
-    }
-    if (S.TORS == 1u && S.LONGEST_FIRST == 0u) {
-      // Each unit's torsion row is its row of the highest color, the latest contact among equals:
-      // (color + 1, contact) packed as the reference packs it, 16 bits of contact index
-      // (wgsl.js:2288-2325).
-      for (uint32_t u = tid; u < nu; u += nt) sch[S.S_UTP + u] = 0u;
       __syncthreads();
-      for (uint32_t row = tid; row < total; row += nt)
-        atomicMax(&sch[S.S_UTP + sch[S.S_RUNIT + row]], ((sch[S.S_PCOL + row] + 1u) << 16u) | sch[S.S_RCON + row]);
-      __syncthreads();
-      for (uint32_t u = tid; u < nu; u += nt) {
-        uint32_t packed = sch[S.S_UTP + u];
-        sch[S.S_UTP + u] = packed != 0u ? sch[S.S_ROWOF + (packed & 0xffffu)] : 0xffffffffu;
-      }
-    }
-    __syncthreads();
-    // Rows bucketed by color, row order kept within a color (a stable counting sort): the block
-    // takes nt rows at a time; a row's place is its color's next free slot plus the rows of its
-    // color in earlier warps of the chunk plus those before it in its warp (match ranks).
-#ifdef STEEL_BLOCK
-    constexpr uint32_t BK_COLORS = 65u, BK_WARPS = STEEL_BLOCK / 32u;
-#else
-    constexpr uint32_t BK_COLORS = 65u, BK_WARPS = BIG_THREADS / 32u;
-#endif
-    __shared__ uint32_t bk_cnt[BK_WARPS][BK_COLORS], bk_off[BK_WARPS][BK_COLORS];
-    const uint32_t nw = nt >> 5u, lane = tid & 31u, warp = tid >> 5u;
-    if (S.NCOL + 1u <= BK_COLORS) {
-      for (uint32_t i = tid; i < BK_WARPS * BK_COLORS; i += nt) (&bk_cnt[0][0])[i] = 0u;
-      __syncthreads();
-      for (uint32_t r0 = 0; r0 < total; r0 += nt) {
-        const uint32_t row = r0 + tid;
-        const bool in = row < total;
-        const uint32_t col = in ? sch[S.S_PCOL + row] : 0xffffffffu;
-        const uint32_t same = __match_any_sync(0xffffffffu, col);
-        const uint32_t below = (uint32_t)__popc(same & ((1u << lane) - 1u));
-        if (in && below == 0u) bk_cnt[warp][col] = (uint32_t)__popc(same);
-        __syncthreads();
-        for (uint32_t c = tid; c <= S.NCOL; c += nt) {
-          uint32_t run = wcount[c];
-          for (uint32_t w = 0; w < nw; w++) {
-            bk_off[w][c] = run;
-            run += bk_cnt[w][c];
-            bk_cnt[w][c] = 0u;
+      if (S.LONGEST_FIRST == 1u && tid == 0u) {
+        // propagation_color_order "longest_first" (wgsl.js:2331-2346): first-fit by row count first
+        // (7 rows down to 1), then contact index. A unit's torsion row is its last row of its highest
+        // color; that color + 1 is kept as PCOL of the unit's current pick, so it needs no array.
+        for (uint32_t u = 0; u < nu; u++) sch[S.S_UTP + u] = 0xffffffffu;
+        for (uint32_t lp = 0; lp < 8u; lp++)
+          for (uint32_t c = 0; c < nc; c++) {
+            const uint32_t row = sch[S.S_ROWOF + c];
+            if (row >= total || pr.row_count(row) != 7u - lp) continue;
+            const uint32_t u = sch[S.S_RUNIT + row];
+            const uint32_t key = sch[S.S_UKEY + u];
+            const int a = (int)(key & 0xffffu) - 1, b = (int)(key >> 16u) - 1;
+            uint32_t col = S.NCOL;
+            for (uint32_t w = 0; w < NCOLW; w++) {
+              uint32_t used = 0u;
+              if (a >= 0) used |= wmask[(uint32_t)a * NCOLW + w];
+              if (b >= 0) used |= wmask[(uint32_t)b * NCOLW + w];
+              if (used != 0xffffffffu) {
+                uint32_t k = (uint32_t)__ffs(~used) - 1u;
+                if (a >= 0) wmask[(uint32_t)a * NCOLW + w] |= 1u << k;
+                if (b >= 0) wmask[(uint32_t)b * NCOLW + w] |= 1u << k;
+                col = w * 32u + k;
+                break;
+              }
+            }
+            sch[S.S_PCOL + row] = col;
+            wcount[col]++;
+            const uint32_t utp = sch[S.S_UTP + u];
+            const uint32_t utc = utp == 0xffffffffu ? 0u : sch[S.S_PCOL + utp] + 1u;
+            if (col + 1u >= utc) sch[S.S_UTP + u] = row;
           }
-          wcount[c] = run;
-        }
-        __syncthreads();
-        if (in) sch[S.S_PORD + bk_off[warp][col] + below] = row;
       }
-    } else if (tid < 32u) {
-      for (uint32_t r0 = 0; r0 < total; r0 += 32u) {
-        const uint32_t row = r0 + tid;
-        const bool in = row < total;
-        const uint32_t col = in ? sch[S.S_PCOL + row] : 0xffffffffu;
-        const uint32_t same = __match_any_sync(0xffffffffu, col);
-        const uint32_t base = in ? wcount[col] : 0u;
-        __syncwarp();
-        if (in) {
-          sch[S.S_PORD + base + (uint32_t)__popc(same & ((1u << tid) - 1u))] = row;
-          if (tid == 31u - (uint32_t)__clz(same)) wcount[col] = base + (uint32_t)__popc(same);
+      __syncthreads();
+      if (tid == 0u) {
+        uint32_t acc = 0u, ncol = 0u;
+        for (uint32_t c = 0; c <= S.NCOL; c++) {
+          uint32_t n = wcount[c];
+          sch[S.S_CSTART + c] = acc;
+          wcount[c] = acc;
+          acc += n;
+          if (n > 0u) ncol = c + 1u;
         }
-        __syncwarp();
+        sch[S.S_CSTART + S.NCOL + 1u] = acc;
+        sch[S.S_META + 0u] = nu;
+        sch[S.S_META + 1u] = ncol;
+        sch[S.S_META + 2u] = nc;
+      }
+      if (S.TORS == 1u && S.LONGEST_FIRST == 0u) {
+        // Each unit's torsion row is its row of the highest color, the latest contact among equals:
+        // (color + 1, contact) packed as the reference packs it, 16 bits of contact index
+        // (wgsl.js:2288-2325).
+        for (uint32_t u = tid; u < nu; u += nt) sch[S.S_UTP + u] = 0u;
+        __syncthreads();
+        for (uint32_t row = tid; row < total; row += nt)
+          atomicMax(&sch[S.S_UTP + sch[S.S_RUNIT + row]], ((sch[S.S_PCOL + row] + 1u) << 16u) | sch[S.S_RCON + row]);
+        __syncthreads();
+        for (uint32_t u = tid; u < nu; u += nt) {
+          uint32_t packed = sch[S.S_UTP + u];
+          sch[S.S_UTP + u] = packed != 0u ? sch[S.S_ROWOF + (packed & 0xffffu)] : 0xffffffffu;
+        }
+      }
+      __syncthreads();
+      // Rows bucketed by color, row order kept within a color (a stable counting sort): the block
+      // takes nt rows at a time; a row's place is its color's next free slot plus the rows of its
+      // color in earlier warps of the chunk plus those before it in its warp (match ranks).
+  #ifdef STEEL_BLOCK
+      constexpr uint32_t BK_COLORS = 65u, BK_WARPS = STEEL_BLOCK / 32u;
+  #else
+      constexpr uint32_t BK_COLORS = 65u, BK_WARPS = BIG_THREADS / 32u;
+  #endif
+      __shared__ uint32_t bk_cnt[BK_WARPS][BK_COLORS], bk_off[BK_WARPS][BK_COLORS];
+      const uint32_t nw = nt >> 5u, lane = tid & 31u, warp = tid >> 5u;
+      if (S.NCOL + 1u <= BK_COLORS) {
+        for (uint32_t i = tid; i < BK_WARPS * BK_COLORS; i += nt) (&bk_cnt[0][0])[i] = 0u;
+        __syncthreads();
+        for (uint32_t r0 = 0; r0 < total; r0 += nt) {
+          const uint32_t row = r0 + tid;
+          const bool in = row < total;
+          const uint32_t col = in ? sch[S.S_PCOL + row] : 0xffffffffu;
+          const uint32_t same = __match_any_sync(0xffffffffu, col);
+          const uint32_t below = (uint32_t)__popc(same & ((1u << lane) - 1u));
+          if (in && below == 0u) bk_cnt[warp][col] = (uint32_t)__popc(same);
+          __syncthreads();
+          for (uint32_t c = tid; c <= S.NCOL; c += nt) {
+            uint32_t run = wcount[c];
+            for (uint32_t w = 0; w < nw; w++) {
+              bk_off[w][c] = run;
+              run += bk_cnt[w][c];
+              bk_cnt[w][c] = 0u;
+            }
+            wcount[c] = run;
+          }
+          __syncthreads();
+          if (in) sch[S.S_PORD + bk_off[warp][col] + below] = row;
+        }
+      } else if (tid < 32u) {
+        for (uint32_t r0 = 0; r0 < total; r0 += 32u) {
+          const uint32_t row = r0 + tid;
+          const bool in = row < total;
+          const uint32_t col = in ? sch[S.S_PCOL + row] : 0xffffffffu;
+          const uint32_t same = __match_any_sync(0xffffffffu, col);
+          const uint32_t base = in ? wcount[col] : 0u;
+          __syncwarp();
+          if (in) {
+            sch[S.S_PORD + base + (uint32_t)__popc(same & ((1u << tid) - 1u))] = row;
+            if (tid == 31u - (uint32_t)__clz(same)) wcount[col] = base + (uint32_t)__popc(same);
+          }
+          __syncwarp();
+        }
       }
     }
   }
@@ -1285,14 +1321,14 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
   uint32_t nloop_rows = 0u;
   for (uint32_t k = 0; k < S.NLOOP; k++) nloop_rows += S.sf[S.SF_LOOP + k * 5u].w > 0.5f ? 2u : 1u;
   if (tid == 0u) sch[S.S_META + 3u] = ndc + nloop_rows + S.NMIMIC;
-  for (uint32_t c = tid; c < nc; c += nt) {
+  for (uint32_t c = tid; tid < sn && c < nc; c += sn) {
     uint32_t slot = sch[S.S_DSLOT + c];
     if (slot == 0xffffffffu || slot >= S.MAXDENSE) continue;
-    pr.dense_row(slot, c, Lane{S.tscr + tid, nt});
+    pr.dense_row(slot, c, Lane{S.tscr + tid, sn});
   }
-  __syncthreads();  // the loop and mimic rows below use per-thread contiguous scratch slices
+  tm.sync();  // the loop and mimic rows below use per-thread contiguous scratch slices
   const uint32_t JDIM = 3u * S.NDA;
-  for (uint32_t i = tid; i < S.NLOOP; i += nt) {
+  for (uint32_t i = tid; tid < sn && i < S.NLOOP; i += sn) {
     float4 L0 = S.sf[S.SF_LOOP + i * 5u];
     int pl = f2i(L0.x);
     uint32_t cl = f2u(L0.y), art_id = f2u(L0.z);
@@ -1329,7 +1365,7 @@ __device__ __forceinline__ void prepare_scene(const BatchDev& B, uint32_t sc) {
                        (P.beta * mf3(dot(e1, err), dot(e2, err), 0.0f)) / P.dt, rest);
     }
   }
-  for (uint32_t i = tid; i < S.NMIMIC; i += nt) {
+  for (uint32_t i = tid; tid < sn && i < S.NMIMIC; i += sn) {
     float4 M0 = S.sf[S.SF_MIMIC + i * 2u], M1 = S.sf[S.SF_MIMIC + i * 2u + 1u];
     uint32_t slot = ndc + nloop_rows + i;
     if (slot >= S.MAXDENSE) continue;
