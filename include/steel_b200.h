@@ -82,6 +82,17 @@ int steel_scene_create(steel_ctx* ctx, const char* json, uint64_t json_len, cons
 int steel_batch_create_files(steel_ctx* ctx, uint32_t n, const char* const* json, const uint64_t* json_len,
                              const void* const* bin, const uint64_t* bin_len, const char* const* opts_json,
                              steel_batch** out);
+/* Convex hull of a point cloud, the hull SceneBuilder.addConvexHull stores for a hull shape
+   (builder.js:61-173), in C++ (host only, no device needed): quickhull in double with the
+   reference's steps and order, coplanar triangles merged into polygons. pts: n points (x, y, z).
+   Caller buffers sized for n points: verts [3n] the hull's vertices in increasing order of their
+   index among the distinct input points; planes [8n] per face the outward unit normal and d
+   (n . x = d); face_start [2n + 1] offsets into face_verts; face_verts [6n] each face's vertices
+   counter-clockwise about its normal. *nv, *nf: vertex and face counts. STEEL_E_INVALID for fewer
+   than 4 distinct points, or collinear or coplanar points. */
+int steel_convex_hull(const double* pts, uint32_t n, double* verts, double* planes, uint32_t* face_start,
+                      uint32_t* face_verts, uint32_t* nv, uint32_t* nf);
+
 /* Packing alone, without a device (tools and tests): the steel_scene_desc a scene's files pack to.
    The desc's pointers stay valid until steel_packed_free. */
 typedef struct steel_packed steel_packed;

@@ -59,6 +59,7 @@ SIGNATURES = {
     "steel_scene_create": [_VP, ctypes.c_char_p, ctypes.c_uint64, _VP, ctypes.c_uint64, ctypes.c_char_p,
                            ctypes.POINTER(_VP)],
     "steel_batch_create_files": [_VP, _U32, _VP, _VP, _VP, _VP, _VP, ctypes.POINTER(_VP)],
+    "steel_convex_hull": [_VP, _U32, _VP, _VP, _VP, _VP, ctypes.POINTER(_U32), ctypes.POINTER(_U32)],
     "steel_pack": [ctypes.c_char_p, ctypes.c_uint64, _VP, ctypes.c_uint64, ctypes.c_char_p, ctypes.POINTER(_VP)],
     "steel_packed_desc": [_VP, ctypes.POINTER(SceneDesc)],
     "steel_packed_free": [_VP],

@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "libsteel_b200.so")
 BLOCK_SIZES = [32, 64, 128, 256, 512]  # prepare / solve instance sets (csrc/batch.cuh BLOCK_SIZES)
 # (source, object, extra flags): prepare.cu and solve.cu are compiled once per block size.
 UNITS = [("collide.cu", "collide.o", []), ("api.cu", "api.o", []), ("sort_noalloc.cu", "sort_noalloc.o", []),
-         ("scene.cpp", "scene.o", [])]
+         ("scene.cpp", "scene.o", []), ("hull.cpp", "hull.o", [])]
 UNITS += [(f"{k}.cu", f"{k}_{n}.o", [f"-DSTEEL_BLOCK={n}"]) for k in ("prepare", "solve") for n in BLOCK_SIZES]
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "--fmad=false", "-prec-div=true",

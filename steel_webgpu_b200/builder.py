@@ -285,6 +285,31 @@ def convex_hull(points):
     return {"verts": verts, "faces": out}
 
 
+def convex_hull_native(points):
+    """``convex_hull`` computed by the library's C++ quickhull (``steel_convex_hull``; host only, no
+    device needed): the same steps in the same order, so the same vertices, faces and planes, at a
+    fraction of the cost. Raises ``SteelError`` where ``convex_hull`` raises ``ValueError``."""
+    import ctypes
+
+    from . import _lib
+    pts = np.ascontiguousarray(np.asarray(points, dtype=np.float64).reshape(-1, 3))
+    n = int(pts.shape[0])
+    m = max(n, 1)
+    verts = np.zeros(3 * m, np.float64)
+    planes = np.zeros(8 * m, np.float64)
+    start = np.zeros(2 * m + 1, np.uint32)
+    fv = np.zeros(6 * m, np.uint32)
+    nv, nf = ctypes.c_uint32(), ctypes.c_uint32()
+    _lib.check(_lib.load().steel_convex_hull(pts.ctypes.data, n, verts.ctypes.data, planes.ctypes.data,
+                                             start.ctypes.data, fv.ctypes.data, ctypes.byref(nv), ctypes.byref(nf)))
+    V = verts[:3 * nv.value].reshape(-1, 3).tolist()
+    faces = []
+    for k in range(nf.value):
+        pl = planes[4 * k:4 * k + 4].tolist()
+        faces.append({"n": pl[:3], "d": pl[3], "v": fv[start[k]:start[k + 1]].astype(int).tolist()})
+    return {"verts": V, "faces": faces}
+
+
 def box_hull(h):
     """Hull of a box with half extents h, built directly: the 8 corners in shape_points order and
     6 quads counter-clockwise about their outward normals (planes n . x = d). Same solid as
@@ -408,23 +433,26 @@ def load_scene(base: str) -> LoadedScene:
 _HULL_CACHE: dict = {}
 
 
-def _hull_cached(gtype, size, pts):
+def _hull_cached(gtype, size, pts, native=False):
+    hull = convex_hull_native if native else convex_hull
     if pts is None:
-        key = (gtype, tuple(size))
+        key = (gtype, tuple(size), native)
         h = _HULL_CACHE.get(key)
         if h is None:
-            h = convex_hull(shape_points(gtype, size))
+            h = hull(shape_points(gtype, size))
             _HULL_CACHE[key] = h
         return h
-    return convex_hull(pts)
+    return hull(pts)
 
 
 class SceneBuilder:
     """Newton-style ModelBuilder (builder.js:241-491). ``finalize()`` returns a ``LoadedScene``."""
 
-    def __init__(self, gravity=(0.0, 0.0, -9.81), fps=60, box_hulls="quickhull"):
-        """box_hulls: "quickhull" (builder.js:264) or "direct" (box_hull, same solid, fixed order)."""
+    def __init__(self, gravity=(0.0, 0.0, -9.81), fps=60, box_hulls="quickhull", native_hulls=False):
+        """box_hulls: "quickhull" (builder.js:264) or "direct" (box_hull, same solid, fixed order).
+        native_hulls: compute hulls with the library's C++ quickhull (convex_hull_native)."""
         self.box_hulls = box_hulls
+        self.native_hulls = native_hulls
         self.gravity = list(gravity)
         self.fps = fps
         self.bodies = []
@@ -448,7 +476,7 @@ class SceneBuilder:
         elif gtype == GT["BOX"] and hull_points is None and self.box_hulls == "direct":
             hull = box_hull([float(x) for x in size])
         else:
-            hull = _hull_cached(gtype, size, hull_points)
+            hull = _hull_cached(gtype, size, hull_points, self.native_hulls)
         self.shapes.append(dict(body=body, type=gtype, size=list(size), xform=list(o.get("xform", IDENTITY)),
                                 hull=hull, o=o))
         return len(self.shapes) - 1

@@ -17,6 +17,7 @@
 #include "batch.cuh"
 #include "bulk.cuh"
 #include "scene.h"
+#include "hull.h"
 
 using namespace steel;
 
@@ -807,6 +808,25 @@ int steel_batch_create(steel_ctx* ctx, const steel_scene_desc* scenes, uint32_t 
   if (rc) return rc;
   CU(cudaStreamSynchronize(st));
   *out = b.release();
+  return STEEL_OK;
+}
+
+int steel_convex_hull(const double* pts, uint32_t n, double* verts, double* planes, uint32_t* face_start,
+                      uint32_t* face_verts, uint32_t* nv, uint32_t* nf) {
+  if (!pts || !verts || !planes || !face_start || !face_verts || !nv || !nf) return fail(STEEL_E_INVALID, "null argument");
+  hull::Hull h;
+  std::string err;
+  if (!hull::convex_hull(pts, n, h, err)) return fail(STEEL_E_INVALID, err);
+  const size_t faces = h.face_start.size() - 1u;
+  // Euler's formula bounds a hull of v <= n vertices by 2v - 4 faces and 6v - 12 face corners.
+  if (h.verts.size() > 3ull * n || faces > 2ull * n || h.face_verts.size() > 6ull * n)
+    return fail(STEEL_E_INVALID, "hull larger than its bounds");
+  std::memcpy(verts, h.verts.data(), h.verts.size() * sizeof(double));
+  std::memcpy(planes, h.planes.data(), h.planes.size() * sizeof(double));
+  std::memcpy(face_start, h.face_start.data(), h.face_start.size() * sizeof(uint32_t));
+  std::memcpy(face_verts, h.face_verts.data(), h.face_verts.size() * sizeof(uint32_t));
+  *nv = (uint32_t)(h.verts.size() / 3u);
+  *nf = (uint32_t)faces;
   return STEEL_OK;
 }
 
