@@ -145,9 +145,10 @@ int steel_autotune(steel_batch* b, uint32_t frames, steel_tiles* best, float* be
    unit scan, sleep islands, coloring) stay on the team's first block.
    0: one block (the batched path). STEEL_TEAM_AUTO, the default: a scene of at least 2048 bodies or
    64 articulations gets one thread per body or a warp per articulation, capped by the blocks that
-   fit the GPU. Other values: that many blocks (STEEL_E_INVALID if more than fit). Batches of
-   several scenes and scenes with Nesterov momentum always solve on one block per scene. Results
-   are the same bits either way. steel_get_team returns the blocks in use (0: one block). */
+   fit the GPU. Other values: that many blocks (STEEL_E_INVALID if more than fit). Team launches
+   run the 512-thread kernel instances (one block per SM): under tiles of another block size, and
+   for batches of several scenes or scenes with Nesterov momentum, the batch runs one block per
+   scene. Results are the same bits either way. steel_get_team returns the blocks in use (0: one block). */
 #define STEEL_TEAM_AUTO 0xffffffffu
 int steel_set_team(steel_batch* b, uint32_t blocks);
 int steel_get_team(steel_batch* b, uint32_t* blocks);

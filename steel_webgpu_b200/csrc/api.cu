@@ -415,6 +415,11 @@ int team_blocks_for(const steel_batch* b, uint32_t req, bool strict, uint32_t* o
   if (req == 0u || b->sc.size() != 1u || b->sc[0].d.NEST != 0u) return STEEL_OK;
   const SceneDev& d = b->sc[0].d;
   const uint32_t T = b->bd.block_threads;
+  if (T != (uint32_t)BIG_THREADS) {  // team launches run the 512-thread instances, one block per SM
+    if (strict && req != STEEL_TEAM_AUTO)
+      return fail(STEEL_E_INVALID, "team launches use 512-thread blocks; the batch's tiles have " + std::to_string(T));
+    return STEEL_OK;
+  }
   const int per_sm = std::min(solve_team_blocks_per_sm(T, b->bd.solve_smem),
                               prepare_team_blocks_per_sm(T, b->bd.prep_smem));
   const uint32_t cap = per_sm > 0 ? (uint32_t)per_sm * (uint32_t)b->ctx->sms : 0u;

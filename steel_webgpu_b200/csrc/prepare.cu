@@ -21,6 +21,7 @@ __global__ void __launch_bounds__(STEEL_BLOCK, blocks_per_sm_of(STEEL_BLOCK)) k_
   prepare_scene<F64, false>(B, sc, Team<false>{});
   if (B.trace_prep) trace_block(B.trace_prep + 3ull * sc, t0);
 }
+#if STEEL_BLOCK == 512  // team launches run the 512-thread instances (one block per SM)
 // A batch of one large scene: every block of this cooperative launch prepares it together
 // (team.cuh).
 template <bool F64>
@@ -32,12 +33,16 @@ __global__ void __launch_bounds__(STEEL_BLOCK, blocks_per_sm_of(STEEL_BLOCK)) k_
   prepare_scene<F64, true>(B, sc, Team<true>{B.team_bar, B.error, TEAM_WAIT_LIMIT, team_state});
   if (B.trace_prep && blockIdx.x == 0u) trace_block(B.trace_prep + 3ull * sc, t0);
 }
+#endif
 }  // namespace STEEL_NS
 
 template <>
 cudaError_t configure_prepare_t<STEEL_BLOCK>(size_t smem_bytes) {
   const void* fns[] = {(const void*)STEEL_NS::k_prepare<false>, (const void*)STEEL_NS::k_prepare<true>,
-                       (const void*)STEEL_NS::k_prepare_team<false>, (const void*)STEEL_NS::k_prepare_team<true>};
+#if STEEL_BLOCK == 512
+                       (const void*)STEEL_NS::k_prepare_team<false>, (const void*)STEEL_NS::k_prepare_team<true>
+#endif
+  };
   for (const void* f : fns) {
     cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
     if (e != cudaSuccess) return e;
@@ -46,6 +51,7 @@ cudaError_t configure_prepare_t<STEEL_BLOCK>(size_t smem_bytes) {
 }
 template <>
 void launch_prepare_t<STEEL_BLOCK>(const BatchDev& b, cudaStream_t st) {
+#if STEEL_BLOCK == 512
   if (b.team_blocks) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(b.team_blocks);
@@ -62,16 +68,22 @@ void launch_prepare_t<STEEL_BLOCK>(const BatchDev& b, cudaStream_t st) {
     else cudaLaunchKernelEx(&cfg, STEEL_NS::k_prepare_team<false>, b);
     return;
   }
+#endif
   if (b.art_f64) STEEL_NS::k_prepare<true><<<b.nlaunch, STEEL_BLOCK, b.prep_smem, st>>>(b);
   else STEEL_NS::k_prepare<false><<<b.nlaunch, STEEL_BLOCK, b.prep_smem, st>>>(b);
 }
 template <>
 int prepare_team_blocks_per_sm_t<STEEL_BLOCK>(size_t smem_bytes) {
+#if STEEL_BLOCK == 512
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, STEEL_NS::k_prepare_team<true>, STEEL_BLOCK, smem_bytes) !=
       cudaSuccess)
     return 0;
   return n;
+#else
+  (void)smem_bytes;
+  return 0;
+#endif
 }
 
 }  // namespace steel

@@ -23,6 +23,7 @@ __global__ void __launch_bounds__(STEEL_BLOCK, blocks_per_sm_of(STEEL_BLOCK)) k_
   solve_scene<EXT, false>(B, sc, Team<false>{});
   if (B.trace_solve) trace_block(B.trace_solve + 3ull * sc, t0);
 }
+#if STEEL_BLOCK == 512  // team launches run the 512-thread instances (one block per SM)
 // A batch of one large scene: every block of this cooperative launch solves it together (team.cuh).
 template <bool EXT>
 __global__ void __launch_bounds__(STEEL_BLOCK, blocks_per_sm_of(STEEL_BLOCK)) k_solve_team(BatchDev B) {
@@ -33,12 +34,16 @@ __global__ void __launch_bounds__(STEEL_BLOCK, blocks_per_sm_of(STEEL_BLOCK)) k_
   solve_scene<EXT, true>(B, sc, Team<true>{B.team_bar, B.error, TEAM_WAIT_LIMIT, team_state});
   if (B.trace_solve && blockIdx.x == 0u) trace_block(B.trace_solve + 3ull * sc, t0);
 }
+#endif
 }  // namespace STEEL_NS
 
 template <>
 cudaError_t configure_solve_t<STEEL_BLOCK>(size_t smem_bytes) {
   const void* fns[] = {(const void*)STEEL_NS::k_solve<false>, (const void*)STEEL_NS::k_solve<true>,
-                       (const void*)STEEL_NS::k_solve_team<false>, (const void*)STEEL_NS::k_solve_team<true>};
+#if STEEL_BLOCK == 512
+                       (const void*)STEEL_NS::k_solve_team<false>, (const void*)STEEL_NS::k_solve_team<true>
+#endif
+  };
   for (const void* f : fns) {
     cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
     if (e != cudaSuccess) return e;
@@ -47,6 +52,7 @@ cudaError_t configure_solve_t<STEEL_BLOCK>(size_t smem_bytes) {
 }
 template <>
 void launch_solve_t<STEEL_BLOCK>(const BatchDev& b, cudaStream_t st) {
+#if STEEL_BLOCK == 512
   if (b.team_blocks) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(b.team_blocks);
@@ -63,16 +69,22 @@ void launch_solve_t<STEEL_BLOCK>(const BatchDev& b, cudaStream_t st) {
     else cudaLaunchKernelEx(&cfg, STEEL_NS::k_solve_team<false>, b);
     return;
   }
+#endif
   if (b.solve_ext) STEEL_NS::k_solve<true><<<b.nlaunch, STEEL_BLOCK, b.solve_smem, st>>>(b);
   else STEEL_NS::k_solve<false><<<b.nlaunch, STEEL_BLOCK, b.solve_smem, st>>>(b);
 }
 template <>
 int solve_team_blocks_per_sm_t<STEEL_BLOCK>(size_t smem_bytes) {
+#if STEEL_BLOCK == 512
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, STEEL_NS::k_solve_team<true>, STEEL_BLOCK, smem_bytes) !=
       cudaSuccess)
     return 0;
   return n;
+#else
+  (void)smem_bytes;
+  return 0;
+#endif
 }
 
 }  // namespace steel
