@@ -1,0 +1,133 @@
+"""Known physical answers for the oracle (CPU): the laws the reference's contact solve is built to
+satisfy, checked on small scenes where the answer is analytic.
+
+- Coulomb friction (the fixed-normal rows with friction anchors, wgsl.js:2952-3011, 3033-3231): a
+  box on a tilted-gravity plane sticks below the friction angle and slides above it with
+  acceleration g (sin t - mu cos t), along the tangential part of gravity whatever its direction.
+- Restitution (wgsl.js:1333-1337 and 2166-2173, a firing row targets e times the closing speed):
+  the rebound speed of a sphere dropped on the plane is e times the impact speed.
+- Momentum (equal and opposite row impulses): a perfectly inelastic head-on collision in zero
+  gravity keeps the total momentum and ends at the common velocity p / (m1 + m2).
+- Free rotation (the Cayley gyroscopic microsteps, wgsl.js:2543-2562): an asymmetric box spinning
+  in zero gravity without damping keeps its angular momentum and kinetic energy, also about the
+  unstable middle axis.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from steel_webgpu_b200 import SceneBuilder, pack
+
+G = 9.81
+
+
+def _box_on_tilted_plane(oracle_lib, gx, gy, mu, frames):
+    gz = -math.sqrt(G * G - gx * gx - gy * gy)
+    b = SceneBuilder(fps=240, box_hulls="direct", gravity=(gx, gy, gz))
+    b.add_ground_plane(mu=mu)
+    body = b.add_body(xform=[0.0, 0.0, 0.1, 0, 0, 0, 1])
+    b.add_shape_box(body, hx=0.2, hy=0.15, hz=0.1, mu=mu)
+    o = oracle_lib.OracleSim(pack(b.finalize()))
+    pos, vel = [], []
+    for _ in range(frames):
+        o.step(1)
+        pos.append(o.body_poses()[0, :3].astype(np.float64))
+        vel.append(o.read("vel")[:3].astype(np.float64))
+    return np.array(pos), np.array(vel)
+
+
+@pytest.mark.parametrize("tan_t,mu", [(0.3, 0.6), (0.55, 0.6)])
+def test_incline_sticks_below_the_friction_angle(oracle_lib, tan_t, mu):
+    t = math.atan(tan_t)
+    pos, vel = _box_on_tilted_plane(oracle_lib, G * math.sin(t), 0.0, mu, 240)
+    assert np.abs(pos[-1, :2]).max() < 1e-4
+    assert np.abs(vel[-1]).max() < 1e-3
+
+
+@pytest.mark.parametrize("tan_t,mu", [(1.0, 0.3), (0.8, 0.5), (0.7, 0.2)])
+def test_incline_slides_with_coulomb_acceleration(oracle_lib, tan_t, mu):
+    t = math.atan(tan_t)
+    _, vel = _box_on_tilted_plane(oracle_lib, G * math.sin(t), 0.0, mu, 240)
+    a = (vel[200, 0] - vel[100, 0]) / (100.0 / 240.0)
+    expected = G * (math.sin(t) - mu * math.cos(t))
+    assert abs(a - expected) / expected < 5e-3
+    assert np.abs(vel[200, 1:]).max() < 1e-4
+
+
+def test_sliding_follows_the_tangential_gravity(oracle_lib):
+    """Gravity tilted along the diagonal of the plane: the box slides along that diagonal at the
+    Coulomb rate (the friction cone is round, not a pyramid along the box's axes)."""
+    t, mu = math.atan(0.9), 0.4
+    s = G * math.sin(t) / math.sqrt(2.0)
+    _, vel = _box_on_tilted_plane(oracle_lib, s, s, mu, 240)
+    v = vel[200, :2]
+    assert abs(v[0] - v[1]) / abs(v[0]) < 1e-3
+    a = (np.linalg.norm(vel[200, :2]) - np.linalg.norm(vel[100, :2])) / (100.0 / 240.0)
+    expected = G * (math.sin(t) - mu * math.cos(t))
+    assert abs(a - expected) / expected < 5e-3
+
+
+@pytest.mark.parametrize("e,tol", [(0.5, 1e-3), (0.8, 5e-3)])
+def test_restitution_rebound_speed(oracle_lib, e, tol):
+    b = SceneBuilder(fps=240, gravity=(0.0, 0.0, -G))
+    b.add_ground_plane(restitution=e)
+    ball = b.add_body(xform=[0.0, 0.0, 1.0, 0, 0, 0, 1])
+    b.add_shape_sphere(ball, radius=0.1, restitution=e)
+    o = oracle_lib.OracleSim(pack(b.finalize()))
+    vz = []
+    for _ in range(300):
+        o.step(1)
+        vz.append(float(o.read("vel")[2]))
+    vz = np.array(vz)
+    k = int(np.argmax(vz > 0.0))  # first frame moving up
+    assert k > 0
+    assert abs(-vz[k] / vz[k - 1] - e) < tol * e
+
+
+def test_inelastic_collision_keeps_momentum(oracle_lib):
+    b = SceneBuilder(fps=240, box_hulls="direct", gravity=(0.0, 0.0, 0.0))
+    a = b.add_body(xform=[-0.5, 0.0, 1.0, 0, 0, 0, 1], twist=(1.0, 0.0, 0.0, 0, 0, 0))
+    b.add_shape_box(a, hx=0.1, hy=0.1, hz=0.1, restitution=0.0)
+    c = b.add_body(xform=[0.5, 0.0, 1.0, 0, 0, 0, 1], twist=(-0.5, 0.0, 0.0, 0, 0, 0))
+    b.add_shape_box(c, hx=0.15, hy=0.1, hz=0.1, restitution=0.0)
+    o = oracle_lib.OracleSim(pack(b.finalize()))
+    ma, mc = 1000.0 * 0.2 * 0.2 * 0.2, 1000.0 * 0.3 * 0.2 * 0.2
+    p0 = ma * 1.0 - mc * 0.5
+    o.step(240)
+    v = o.read("vel")[:16].reshape(2, 8).astype(np.float64)
+    p = ma * v[0, :3] + mc * v[1, :3]
+    assert abs(p[0] - p0) / p0 < 1e-6 and np.abs(p[1:]).max() < 1e-6
+    np.testing.assert_allclose(v[:, 0], p0 / (ma + mc), rtol=1e-3)  # they move together
+
+
+def _qmat(q):
+    x, y, z, w = q
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                     [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                     [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+
+
+@pytest.mark.parametrize("w0", [(0.3, 4.0, 0.2), (5.0, 0.1, 0.1), (0.05, 0.2, 6.0)])
+def test_free_spin_keeps_angular_momentum_and_energy(oracle_lib, w0):
+    b = SceneBuilder(fps=240, box_hulls="direct", gravity=(0.0, 0.0, 0.0))
+    body = b.add_body(xform=[0.0, 0.0, 1.0, 0, 0, 0, 1], twist=(0.0, 0.0, 0.0) + tuple(w0))
+    b.add_shape_box(body, hx=0.3, hy=0.2, hz=0.1)
+    sc = b.finalize()
+    sc.json["bodies"]["angular_damping"] = [0.0]
+    o = oracle_lib.OracleSim(pack(sc))
+    m = 1000.0 * 0.6 * 0.4 * 0.2
+    inertia = np.diag([m / 3 * (0.2 ** 2 + 0.1 ** 2), m / 3 * (0.3 ** 2 + 0.1 ** 2), m / 3 * (0.3 ** 2 + 0.2 ** 2)])
+    L, E = [], []
+    for _ in range(480):
+        pose, vel = o.body_poses()[0], o.read("vel")[:8]
+        R = _qmat(pose[4:8].astype(np.float64))
+        w = vel[4:7].astype(np.float64)
+        Iw = R @ inertia @ R.T
+        L.append(Iw @ w)
+        E.append(0.5 * w @ Iw @ w)
+        o.step(1)
+    L, E = np.array(L), np.array(E)
+    assert np.abs(L - L[0]).max() / np.linalg.norm(L[0]) < 2e-3
+    assert np.abs(E - E[0]).max() / E[0] < 2e-3
+    assert np.array_equal(o.body_poses()[0, :3], np.float32([0.0, 0.0, 1.0]))  # no drift of the centre
