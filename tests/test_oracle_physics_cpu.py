@@ -11,6 +11,10 @@ satisfy, checked on small scenes where the answer is analytic.
 - Free rotation (the Cayley gyroscopic microsteps, wgsl.js:2543-2562): an asymmetric box spinning
   in zero gravity without damping keeps its angular momentum and kinetic energy, also about the
   unstable middle axis.
+- Articulated dynamics (the articulated-body factorisation and propagation, artwgsl.js, whose link
+  motion is (w, v_com) at each link's COM, artwgsl.js:1-6): a floating base with a three-link
+  revolute chain in zero gravity, set moving through its joint speeds, keeps its linear and
+  angular momentum up to the first-order error of the time step: the drift halves with the step.
 """
 import math
 
@@ -18,6 +22,7 @@ import numpy as np
 import pytest
 
 from steel_webgpu_b200 import SceneBuilder, pack
+from steel_webgpu_b200.packer import LB, L_V
 
 G = 9.81
 
@@ -131,3 +136,59 @@ def test_free_spin_keeps_angular_momentum_and_energy(oracle_lib, w0):
     assert np.abs(L - L[0]).max() / np.linalg.norm(L[0]) < 2e-3
     assert np.abs(E - E[0]).max() / E[0] < 2e-3
     assert np.array_equal(o.body_poses()[0, :3], np.float32([0.0, 0.0, 1.0]))  # no drift of the centre
+
+
+def _floating_chain_drift(oracle_lib, fps, seconds=0.5):
+    """Largest relative change of the total linear and angular momentum over `seconds`."""
+    b = SceneBuilder(fps=fps, box_hulls="direct", gravity=(0.0, 0.0, 0.0))
+    base = b.add_body(xform=[0.0, 0.0, 1.0, 0, 0, 0, 1])
+    b.add_shape_box(base, hx=0.2, hy=0.1, hz=0.05, mass=2.0)
+    b.add_joint_free(base)
+    parent, L = base, 0.3
+    for k, axis in enumerate(([0, 1, 0], [1, 0, 0], [0, 0, 1])):
+        link = b.add_body(xform=[0.2 + L * (k + 0.5), 0.0, 1.0, 0, 0, 0, 1])
+        b.add_shape_capsule(link, radius=0.03, half_height=0.1, mass=0.5 + 0.5 * k)
+        b.add_joint_revolute(parent, link, axis=axis,
+                             parent_xform=[0.2 if k == 0 else L / 2, 0.0, 0.0, 0, 0, 0, 1],
+                             child_xform=[-L / 2, 0.0, 0.0, 0, 0, 0, 1])
+        parent = link
+    sc = b.finalize()
+    sc.json["bodies"]["angular_damping"] = [0.0] * 4
+    pk = pack(sc)
+    C = pk.C
+    o = oracle_lib.OracleSim(pk)
+    o.write("art", C["A_QD"], [0.1, 0.0, 0.0, 0.0, 0.0, 0.5, 2.0, -1.5, 3.0])  # free joint, then revolutes
+    rec = pk.statF.reshape(-1, 4)[C["SF_BODY"]:C["SF_BODY"] + pk.NB * 8].astype(np.float64).reshape(pk.NB, 8, 4)
+    mass = 1.0 / rec[:, 0, 0]
+    inertia = rec[:, 2:5, :3]
+
+    def momentum():
+        poses, art = o.body_poses(), o.read("art")
+        lin, ang = np.zeros(3), np.zeros(3)
+        for l, link in enumerate(pk.links):
+            bb = link["body"]
+            o6 = C["A_LINK"] + l * LB + L_V
+            w, v = art[o6:o6 + 3].astype(np.float64), art[o6 + 3:o6 + 6].astype(np.float64)
+            c = poses[bb, :3].astype(np.float64)
+            R = _qmat(poses[bb, 4:8].astype(np.float64))
+            lin += mass[bb] * v
+            ang += R @ inertia[bb] @ R.T @ w + mass[bb] * np.cross(c, v)
+        return lin, ang
+
+    o.step(1)  # the link motion follows the written joint speeds from the first step on
+    l0, a0 = momentum()
+    dl = da = 0.0
+    for _ in range(int(seconds * fps)):
+        o.step(1)
+        lin, ang = momentum()
+        dl = max(dl, np.linalg.norm(lin - l0) / np.linalg.norm(l0))
+        da = max(da, np.linalg.norm(ang - a0) / np.linalg.norm(a0))
+    return dl, da
+
+
+def test_floating_chain_keeps_momentum_to_first_order(oracle_lib):
+    d240 = _floating_chain_drift(oracle_lib, 240)
+    d480 = _floating_chain_drift(oracle_lib, 480)
+    assert max(d240) < 3e-3
+    for coarse, fine in zip(d240, d480):
+        assert 0.4 < fine / coarse < 0.6  # first order in the time step
