@@ -485,7 +485,8 @@ def run_steel(args):
                    "placement": "each scene's boxes on a 0.4 m grid, dropped from 0.3-1.3 m onto its plane (a 2x2x2 m "
                                 "volume cannot hold 512 boxes of half-extents 0.05-0.15 m without overlaps)",
                    "tiles": dict(tiles, source="autotuner" if args.tiles == "auto" else "command line",
-                                 tuning_ms_per_frame=tune_ms, tuning_s=round(tune_s, 2)),
+                                 tuning_ms_per_frame=tune_ms, tuning_s=round(tune_s, 2),
+                                 team_blocks=batch.team()),
                    "frame_latency_ms": {"p50": float(np.percentile(frame_ms, 50)),
                                         "p99": float(np.percentile(frame_ms, 99)),
                                         "what": "one frame of the whole batch through steel_step_io, host clock"},

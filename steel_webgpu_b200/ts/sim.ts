@@ -37,9 +37,33 @@ export const symbols = {
   steel_set_body_twist: { args: [P, u32, u32, P], returns: i32 },
   steel_copy_poses_device: { args: [P, u32, P, P], returns: i32 },
   steel_autotune: { args: [P, u32, P, P], returns: i32 },
+  steel_set_team: { args: [P, u32], returns: i32 },
+  steel_get_team: { args: [P, P], returns: i32 },
+  steel_convex_hull: { args: [P, u32, P, P, P, P, P, P], returns: i32 },
 } as const;
 
 const lib = dlopen(LIB, symbols).symbols;
+
+/** steel_set_team's default: a team launch for scenes of at least 2048 bodies or 64 articulations. */
+export const TEAM_AUTO = 0xffffffff;
+
+/** Convex hull of a point cloud as SceneBuilder.addConvexHull computes it (builder.js:61-173), in
+ *  the library's C++ (steel_convex_hull): vertices, outward planes n . x = d and each face's
+ *  vertices counter-clockwise about n. */
+export function convexHull(points: Float64Array): { verts: Float64Array; planes: Float64Array; faces: number[][] } {
+  const n = points.length / 3;
+  const m = Math.max(n, 1);
+  const verts = new Float64Array(3 * m);
+  const planes = new Float64Array(8 * m);
+  const start = new Uint32Array(2 * m + 1);
+  const fv = new Uint32Array(6 * m);
+  const counts = new Uint32Array(2);
+  check(lib.steel_convex_hull(ptr(points), n, ptr(verts), ptr(planes), ptr(start), ptr(fv), ptr(counts),
+                              ptr(counts.subarray(1))));
+  const faces: number[][] = [];
+  for (let k = 0; k < counts[1]; k++) faces.push(Array.from(fv.subarray(start[k], start[k + 1])));
+  return { verts: verts.slice(0, 3 * counts[0]), planes: planes.slice(0, 4 * counts[1]), faces };
+}
 
 function check(rc: number): void {
   if (rc !== 0) throw new Error(`steel: ${String(lib.steel_last_error())}`);
@@ -251,6 +275,15 @@ export class Sim {
     this.time = 0;
     this.frame = 0;
     return { blockThreads: t[0], smemBudget: t[1], narrowBlocksPerSm: t[2], streamGroups: t[3], msPerFrame: ms[0] };
+  }
+
+  /** Blocks that prepare and solve this scene together (steel_set_team): 0 one block,
+   *  TEAM_AUTO the default rule for large scenes, else that many. Returns the blocks in use. */
+  setTeam(blocks: number = TEAM_AUTO): number {
+    check(lib.steel_set_team(this.handle, blocks));
+    const out = new Uint32Array(1);
+    check(lib.steel_get_team(this.handle, ptr(out)));
+    return out[0];
   }
 
   private portDof(newtonDof: number): number {
