@@ -15,6 +15,12 @@ satisfy, checked on small scenes where the answer is analytic.
   motion is (w, v_com) at each link's COM, artwgsl.js:1-6): a floating base with a three-link
   revolute chain in zero gravity, set moving through its joint speeds, keeps its linear and
   angular momentum up to the first-order error of the time step: the drift halves with the step.
+- Joints (articulated-body dynamics with implicit PD drives in D, artwgsl.js:4-6; limit rows,
+  wgsl.js:3404-3468; joint integration, wgsl.js:3797-3826): a PD-driven pendulum settles where the
+  drive torque balances gravity, ke (q* - q) = m g d sin q; a revolute limit holds against a swing
+  that would pass it; a prismatic slide along a tilted axis follows the semi-implicit Euler
+  recurrence of g . axis exactly; a ball-joint conical pendulum started at the steady rate
+  sqrt(g / (L cos t)) keeps its cone angle and that rate.
 """
 import math
 
@@ -192,3 +198,86 @@ def test_floating_chain_keeps_momentum_to_first_order(oracle_lib):
     assert max(d240) < 3e-3
     for coarse, fine in zip(d240, d480):
         assert 0.4 < fine / coarse < 0.6  # first order in the time step
+
+
+def _pendulum(ke=0.0, kd=0.0, target=0.0, limits=None, m=None, d=0.5, r=0.05):
+    b = SceneBuilder(fps=240)
+    bob = b.add_body(xform=[0.0, 0.0, 2.0 - d, 0, 0, 0, 1])
+    b.add_shape_sphere(bob, radius=r, **({} if m is None else {"mass": m}))
+    lim = {} if limits is None else {"limitLower": limits[0], "limitUpper": limits[1]}
+    b.add_joint_revolute(-1, bob, axis=[0, 1, 0], parent_xform=[0.0, 0.0, 2.0, 0, 0, 0, 1],
+                         child_xform=[0.0, 0.0, d, 0, 0, 0, 1], targetKe=ke, targetKd=kd, targetPos=target, **lim)
+    return pack(b.finalize())
+
+
+@pytest.mark.parametrize("ke", [50.0, 200.0])
+def test_pd_drive_settles_at_the_torque_balance(oracle_lib, ke):
+    m, d, target = 2.0, 0.5, 0.5
+    pk = _pendulum(ke=ke, kd=5.0, target=target, m=m, d=d)
+    o = oracle_lib.OracleSim(pk)
+    o.step(1200)
+    art = o.read("art")
+    f = lambda t: ke * (target - t) - m * G * d * math.sin(t)  # noqa: E731
+    lo, hi = 0.0, target
+    for _ in range(100):  # bisection on the balance
+        mid = 0.5 * (lo + hi)
+        lo, hi = (mid, hi) if f(mid) > 0.0 else (lo, mid)
+    assert abs(art[pk.C["A_Q"]] - 0.5 * (lo + hi)) < 1e-5
+    assert abs(art[pk.C["A_QD"]]) < 1e-4
+
+
+def test_revolute_limit_holds(oracle_lib):
+    pk = _pendulum(limits=(-0.3, 0.3))
+    o = oracle_lib.OracleSim(pk)
+    o.write("art", pk.C["A_QD"], [4.0])  # enough to swing past 1 rad without the limit
+    q = []
+    for _ in range(480):
+        o.step(1)
+        q.append(o.read("art")[pk.C["A_Q"]])
+    q = np.array(q)
+    assert q.max() <= 0.3 + 1e-4 and q.min() >= -0.3 - 1e-4
+    assert q.max() > 0.29  # it did reach the limit
+
+
+def test_prismatic_slide_follows_the_euler_recurrence(oracle_lib):
+    axis = np.array([1.0, 0.0, -1.0]) / math.sqrt(2.0)
+    b = SceneBuilder(fps=240)
+    body = b.add_body(xform=[0.0, 0.0, 2.0, 0, 0, 0, 1])
+    b.add_shape_sphere(body, radius=0.05)
+    b.add_joint_prismatic(-1, body, axis=list(axis), parent_xform=[0.0, 0.0, 2.0, 0, 0, 0, 1])
+    pk = pack(b.finalize())
+    o = oracle_lib.OracleSim(pk)
+    o.step(120)
+    dt = np.float32(1.0 / (240 * pk.params["substeps"]))
+    a = np.float32(G * -axis[2])
+    v = x = np.float32(0.0)
+    for _ in range(120 * pk.params["substeps"]):
+        v = np.float32(v + a * dt)
+        x = np.float32(x + v * dt)
+    art = o.read("art")
+    assert art[pk.C["A_Q"]] == x and art[pk.C["A_QD"]] == v
+
+
+def test_conical_pendulum_on_a_ball_joint(oracle_lib):
+    L, th = 0.6, 0.5
+    omega = math.sqrt(G / (L * math.cos(th)))
+    b = SceneBuilder(fps=240)
+    bob = b.add_body(xform=[0.0, 0.0, 2.0 - L, 0, 0, 0, 1])
+    b.add_shape_sphere(bob, radius=0.02)
+    b.add_joint_ball(-1, bob, parent_xform=[0.0, 0.0, 2.0, 0, 0, 0, 1], child_xform=[0.0, 0.0, L, 0, 0, 0, 1],
+                     q=[0.0, math.sin(th / 2), 0.0, math.cos(th / 2)])
+    pk = pack(b.finalize())
+    o = oracle_lib.OracleSim(pk)
+    o.write("art", pk.C["A_QD"], [0.0, 0.0, omega])  # a ball joint's speed is its angular velocity (world)
+    period = 2.0 * math.pi / omega
+    frames = int(2.0 * period * 240)
+    cone, azimuth = [], []
+    for _ in range(frames):
+        o.step(1)
+        p = o.body_poses()[0, :3].astype(np.float64) - np.array([0.0, 0.0, 2.0])
+        cone.append(math.acos(-p[2] / np.linalg.norm(p)))
+        azimuth.append(math.atan2(p[1], p[0]))
+    cone = np.array(cone)
+    assert np.abs(cone - th).max() < 1e-4
+    rate = (np.unwrap(azimuth)[-1] - np.unwrap(azimuth)[0]) / ((frames - 1) / 240.0)
+    assert abs(rate - omega) / omega < 1e-3
