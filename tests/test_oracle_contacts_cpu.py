@@ -4,10 +4,10 @@ distances of shape pairs whose contact is analytic.
 A contact record holds the point halfway between the two surfaces, the signed distance phi
 (negative in penetration) and the unit normal from the lower-indexed body to the higher (the
 ground, body -1, first), as the reference's emit writes them (wgsl.js:269-307). Sphere pairs
-(the primitive routines of narrow_pair), faces resting on the plane (plane contacts), a face-to-face
-box pair (the SAT manifold clipped to the overlap rectangle), crossed box edges (the SAT edge
-query) and a capsule on the plane (segment against plane) are checked against their closed forms; boxes apart by more than the speculative
-margin make no contact.
+(the primitive routines of narrow_pair), faces resting on the plane (plane contacts), a
+face-to-face box pair (the SAT manifold clipped to the overlap rectangle), crossed box edges (the
+SAT edge query) and a capsule on the plane (segment against plane) are checked against their
+closed forms; boxes apart by more than the speculative margin make no contact.
 """
 import math
 
