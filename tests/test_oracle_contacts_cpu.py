@@ -107,3 +107,24 @@ def test_separated_boxes_make_no_contact(oracle_lib):
         s = b.add_body(xform=[x, 0.0, 1.0, 0, 0, 0, 1])
         b.add_shape_box(s, hx=0.1, hy=0.1, hz=0.1)
     assert _contacts(oracle_lib, b.finalize()) == []
+
+
+def test_sorted_contacts_are_a_permutation_in_key_order(oracle_lib):
+    """The canonical sort (wgsl.js:3899-3982) on a pile of hulls, boxes and capsules: the sorted
+    records are the raw records permuted, in nondecreasing (body pair, feature) order."""
+    from tests import scenes
+    pk = pack(scenes.hull_bin())
+    o = oracle_lib.OracleSim(pk)
+    o.step(40)
+    o.collide()
+    n = int(o.read("collide_counts", np.uint32)[1])
+    assert n > 100
+    raw = o.read("craw")[:n * 20].reshape(n, 20)
+    srt = o.read("contacts")[:n * 20].reshape(n, 20)
+    as_rows = lambda a: sorted(map(bytes, a.view(np.uint32)))  # noqa: E731
+    assert as_rows(raw) == as_rows(srt)
+    m = srt.reshape(n, 5, 4)[:, 2, :].astype(np.int64)
+    pair = (m[:, 0] + 1) | ((m[:, 1] + 1) << 16)
+    feat = m[:, 2] | (m[:, 3] << 16)
+    key = pair * (1 << 32) + feat
+    assert np.all(np.diff(key) >= 0)
