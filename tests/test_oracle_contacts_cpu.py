@@ -128,3 +128,32 @@ def test_sorted_contacts_are_a_permutation_in_key_order(oracle_lib):
     feat = m[:, 2] | (m[:, 3] << 16)
     key = pair * (1 << 32) + feat
     assert np.all(np.diff(key) >= 0)
+
+
+def test_colors_are_first_fit_in_row_order(oracle_lib):
+    """The row coloring (first_free_color and its serial pass, wgsl.js:1233-1267) restated over the
+    oracle's rows of a pile: every row takes the lowest color that no earlier row on either of its
+    bodies holds (the overflow color when all are taken), so no color holds two rows of a body."""
+    from tests import scenes
+    pk = pack(scenes.hull_bin())
+    C = pk.C
+    o = oracle_lib.OracleSim(pk)
+    o.step(40)
+    sch = o.read("sched", np.uint32).astype(np.int64)
+    nu = int(sch[C["S_META"]])
+    total = int(sch[C["S_USTART"] + nu])
+    ncol = C["NCOL"]
+    assert total > 100
+    used: dict = {}
+    colors = set()
+    for r in range(total):
+        key = int(sch[C["S_UKEY"] + sch[C["S_RUNIT"] + r]])
+        bodies = [x for x in ((key & 0xFFFF) - 1, (key >> 16) - 1) if x >= 0]
+        taken = set().union(*(used.get(x, set()) for x in bodies))
+        expected = next((k for k in range(ncol) if k not in taken), ncol)
+        assert int(sch[C["S_PCOL"] + r]) == expected, f"row {r}"
+        if expected < ncol:
+            for x in bodies:
+                used.setdefault(x, set()).add(expected)
+        colors.add(expected)
+    assert len(colors) > 3
