@@ -20,7 +20,9 @@ satisfy, checked on small scenes where the answer is analytic.
   drive torque balances gravity, ke (q* - q) = m g d sin q; a revolute limit holds against a swing
   that would pass it; a prismatic slide along a tilted axis follows the semi-implicit Euler
   recurrence of g . axis exactly; a ball-joint conical pendulum started at the steady rate
-  sqrt(g / (L cos t)) keeps its cone angle and that rate.
+  sqrt(g / (L cos t)) keeps its cone angle and that rate; a three-link arm held by PD drives
+  comes to rest where each joint's drive and damping balance the gravity torque of the links below
+  it, ke (q* - q) - kd qd + sum_j m_j g (x_j - x_joint) = 0.
 """
 import math
 
@@ -281,3 +283,32 @@ def test_conical_pendulum_on_a_ball_joint(oracle_lib):
     assert np.abs(cone - th).max() < 1e-4
     rate = (np.unwrap(azimuth)[-1] - np.unwrap(azimuth)[0]) / ((frames - 1) / 240.0)
     assert abs(rate - omega) / omega < 1e-3
+
+
+def test_pd_arm_static_equilibrium(oracle_lib):
+    ell, ke, kd = 0.3, 300.0, 20.0
+    targets, masses = [0.6, -0.4, 0.8], [1.0, 0.7, 0.4]
+    b = SceneBuilder(fps=240)
+    parent = -1
+    for k in range(3):
+        body = b.add_body(xform=[0.0, 0.0, 2.0 - ell * (k + 0.5), 0, 0, 0, 1])
+        b.add_shape_capsule(body, radius=0.02, half_height=0.1, mass=masses[k])
+        b.add_joint_revolute(parent, body, axis=[0, 1, 0],
+                             parent_xform=[0.0, 0.0, -ell / 2 if parent >= 0 else 2.0, 0, 0, 0, 1],
+                             child_xform=[0.0, 0.0, ell / 2, 0, 0, 0, 1], targetKe=ke, targetKd=kd,
+                             targetPos=targets[k])
+        parent = body
+    pk = pack(b.finalize())
+    C = pk.C
+    o = oracle_lib.OracleSim(pk)
+    o.step(2400)
+    art = o.read("art").astype(np.float64)
+    q, qd = art[C["A_Q"]:C["A_Q"] + 3], art[C["A_QD"]:C["A_QD"] + 3]
+    poses = o.body_poses().astype(np.float64)
+    rec = pk.statF.reshape(-1, 4)[C["SF_BODY"]:C["SF_BODY"] + pk.NB * 8].astype(np.float64).reshape(pk.NB, 8, 4)
+    mass = 1.0 / rec[:, 0, 0]
+    joint_x = [poses[k, 0] + (_qmat(poses[k, 4:8]) @ np.array([0.0, 0.0, ell / 2]))[0] for k in range(3)]
+    for i in range(3):
+        gravity = sum(mass[j] * G * (poses[j, 0] - joint_x[i]) for j in range(i, 3))  # torque about +y
+        assert abs(gravity) > 0.3
+        assert abs(ke * (targets[i] - q[i]) - kd * qd[i] + gravity) < 1e-5
