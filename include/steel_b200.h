@@ -26,8 +26,9 @@ extern "C" {
 #define STEEL_E_CUDA 4        /* CUDA runtime error */
 #define STEEL_E_NOMEM 5       /* device allocation failed */
 #define STEEL_E_NODEVICE 6    /* no CUDA device; the reference's UnsupportedError (device.js:2-9) */
-#define STEEL_E_TIMEOUT 7     /* a bounded device-side wait ran out (a shared-memory bulk copy); the scene's
-                                 work of that substep was skipped, so reset before trusting its state */
+#define STEEL_E_TIMEOUT 7     /* a bounded device-side wait ran out (a shared-memory bulk copy, the radix
+                                 sort's look-back, a team launch's grid barrier); the work that waited was
+                                 skipped or is void, so reset before trusting the state */
 
 typedef struct steel_ctx steel_ctx;
 typedef struct steel_batch steel_batch;
