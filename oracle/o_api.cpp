@@ -198,6 +198,14 @@ void oracle_collide(void* h) {
   o->collide_counts[1] = o->counters[1];
   o->counters[0] = o->counters[1] = 0u;
 }
+// The canonical contact sort alone over the raw records craw[0, n) as they stand (a test hook: a
+// permuted raw buffer must sort to the same records, W:3895-3898).
+void oracle_sort_raw(void* h, uint32_t n) {
+  Oracle* o = (Oracle*)h;
+  o->counters[1] = n;
+  o->k_csort();
+  o->counters[1] = 0u;
+}
 // One substep in stages, as step() runs it: stage 0 writes the substep's parameters and runs the
 // collision kernels, 1 prepare, 2 solve (ending the frame after the last substep).
 void oracle_stage(void* h, int stage) {
@@ -251,6 +259,7 @@ int oracle_write(void* h, const char* name, size_t offset, const void* data, siz
   if (s == "poses") { dst = &o->poses.data()->x; n = o->poses.size() * 4; }
   else if (s == "vel") { dst = &o->vel.data()->x; n = o->vel.size() * 4; }
   else if (s == "art") { dst = o->art.data(); n = o->art.size(); }
+  else if (s == "craw") { dst = &o->craw.data()->x; n = o->craw.size() * 4; }
   else return -1;
   if (offset + words > n) return -1;
   orc::f32_in(dst + offset, (const f32_t*)data, words);

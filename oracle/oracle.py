@@ -39,6 +39,7 @@ def lib(f64: bool = False):
         for f in ("oracle_destroy", "oracle_reset", "oracle_collide"):
             getattr(L, f).argtypes = [ctypes.c_void_p]
         L.oracle_stage.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.oracle_sort_raw.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
         L.oracle_step.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
         L.oracle_set_user_targets.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.oracle_read.restype = ctypes.c_size_t
@@ -90,6 +91,10 @@ class OracleSim:
 
     def collide(self):
         self.L.oracle_collide(self.h)
+
+    def sort_raw(self, n: int):
+        """The canonical contact sort alone over the first n raw records (after write("craw"))."""
+        self.L.oracle_sort_raw(self.h, n)
 
     def stage(self, k: int):
         self.L.oracle_stage(self.h, k)

@@ -157,3 +157,27 @@ def test_colors_are_first_fit_in_row_order(oracle_lib):
                 used.setdefault(x, set()).add(expected)
         colors.add(expected)
     assert len(colors) > 3
+
+
+def test_sort_is_independent_of_the_raw_order(oracle_lib):
+    """The canonical order does not depend on the order the narrowphase emitted the contacts in
+    (wgsl.js:3895-3898; the CUDA narrowphase emits them in a different order, by atomics): the raw
+    records of a pile, reversed and shuffled, sort to the same records bit for bit."""
+    from tests import scenes
+    pk = pack(scenes.hull_bin())
+    maxc = pk.C["MAXC"]
+    o = oracle_lib.OracleSim(pk)
+    o.step(40)
+    o.collide()
+    n = int(o.read("collide_counts", np.uint32)[1])
+    assert n > 100
+    raw = o.read("craw").reshape(-1, 4)
+    rec, smu = raw[:n * 5].reshape(n, 5, 4).copy(), raw[maxc * 5:maxc * 5 + n].copy()
+    want = o.read("contacts").view(np.uint32).copy()
+    for perm in (np.arange(n)[::-1], np.random.default_rng(9).permutation(n)):
+        o.write("craw", 0, rec[perm].reshape(-1))
+        o.write("craw", maxc * 5 * 4, smu[perm].reshape(-1))
+        o.sort_raw(n)
+        got = o.read("contacts").view(np.uint32)
+        assert np.array_equal(got[:n * 20], want[:n * 20])
+        assert np.array_equal(got[maxc * 20:maxc * 20 + n * 4], want[maxc * 20:maxc * 20 + n * 4])
