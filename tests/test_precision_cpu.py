@@ -67,3 +67,29 @@ def test_precision_report_small(frames):
         for group in ("quadrupeds", "chains"):
             for q in precision_c3.QUANTITIES:
                 assert 0.0 < e10[group][q] < 1e-3, (leg, group, q, e10[group][q])
+
+
+def test_pd_arm_fp32_within_tolerance_of_fp64_over_1000_frames():
+    """A PD-held three-link arm settling under gravity (no contact, no chaos): the float run stays
+    within 1e-5 relative of the all-FP64 run in poses and joint angles over 1000 frames."""
+    ell = 0.3
+    b = SceneBuilder(fps=240)
+    parent = -1
+    for k in range(3):
+        body = b.add_body(xform=[0.0, 0.0, 2.0 - ell * (k + 0.5), 0, 0, 0, 1])
+        b.add_shape_capsule(body, radius=0.02, half_height=0.1, mass=[1.0, 0.7, 0.4][k])
+        b.add_joint_revolute(parent, body, axis=[0, 1, 0],
+                             parent_xform=[0.0, 0.0, -ell / 2 if parent >= 0 else 2.0, 0, 0, 0, 1],
+                             child_xform=[0.0, 0.0, ell / 2, 0, 0, 0, 1], targetKe=300.0, targetKd=20.0,
+                             targetPos=[0.6, -0.4, 0.8][k])
+        parent = body
+    pk = pack(b.finalize())
+    f32, f64 = OracleSim(pk), OracleSim(pk, f64=True)
+    q0, nq = pk.C["A_Q"], pk.NQ
+    for _ in range(10):
+        f32.step(100)
+        f64.step(100)
+        pa, pb = (o.read("poses")[:pk.NB * 8].astype(np.float64) for o in (f32, f64))
+        qa, qb = (o.read("art")[q0:q0 + nq].astype(np.float64) for o in (f32, f64))
+        assert np.linalg.norm(pa - pb) / np.linalg.norm(pb) < 1e-5
+        assert np.linalg.norm(qa - qb) / np.linalg.norm(qb) < 1e-5
