@@ -516,17 +516,23 @@ void pack_impl(const JV& S, const Bin& bin, const JV* o_in, Packed& P) {
         set(ia->second, ib->second);
         set(ib->second, ia->second);
       }
-    std::vector<int64_t> worlds(NS), groups(NS);
-    for (uint32_t i = 0; i < NS; i++) {
-      worlds[i] = (int64_t)num_or(shapes[i], "world", -1.0);
-      groups[i] = (int64_t)num_or(shapes[i], "group", -1.0);
-    }
+    // The rule depends on a shape's (world, group) alone and is symmetric, so it is decided once per
+    // pair of distinct (world, group) classes, and bits are set only for the members of classes
+    // that do not meet: O(NS + classes^2 + filtered pairs) instead of a test of every shape pair
+    // (the same bits; scenes with one class set none).
+    std::map<std::pair<int64_t, int64_t>, std::vector<uint32_t>> classes;  // members in ascending order
     for (uint32_t i = 0; i < NS; i++)
-      for (uint32_t j = i + 1; j < NS; j++) {
-        const int64_t wa = worlds[i], wb = worlds[j], ga = groups[i], gb = groups[j];
-        const bool gm = ga != 0 && gb != 0 && (ga > 0 ? (ga == gb || gb < 0) : ga != gb);
-        const bool meet = (wa < 0 || wb < 0 || wa == wb) && gm;
-        if (!meet) { set(i, j); set(j, i); }
+      classes[{(int64_t)num_or(shapes[i], "world", -1.0), (int64_t)num_or(shapes[i], "group", -1.0)}].push_back(i);
+    auto meet = [](int64_t wa, int64_t ga, int64_t wb, int64_t gb) {
+      const bool gm = ga != 0 && gb != 0 && (ga > 0 ? (ga == gb || gb < 0) : ga != gb);
+      return (wa < 0 || wb < 0 || wa == wb) && gm;
+    };
+    for (auto ca = classes.begin(); ca != classes.end(); ++ca)
+      for (auto cb = ca; cb != classes.end(); ++cb) {
+        if (meet(ca->first.first, ca->first.second, cb->first.first, cb->first.second)) continue;
+        for (uint32_t i : ca->second)
+          for (uint32_t j : cb->second)
+            if (i != j) { set(i, j); set(j, i); }
       }
   }
 

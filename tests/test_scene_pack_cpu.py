@@ -95,3 +95,22 @@ def test_cpp_packer_errors(steel):
     rc = L.steel_pack(text, len(text), ctypes.cast(b, ctypes.c_void_p), len(sc.bin),
                       b'{"solver": {"friction_mode": "magic"}}', ctypes.byref(p))
     assert rc == 1 and b"friction_mode magic is not supported" in L.steel_last_error()
+
+
+def test_cpp_packer_collision_worlds_and_groups(steel):
+    """Shapes spread over worlds (-1 shared, 0, 1) and collision groups (0 none, positive, negative,
+    -1 all): the filter bitset of sim.js:235-255 from the C++ packer equals the Python packer's."""
+    from steel_webgpu_b200 import SceneBuilder
+    rng = np.random.default_rng(4)
+    b = SceneBuilder(fps=240, box_hulls="direct")
+    b.add_ground_plane()
+    for i in range(60):
+        body = b.add_body(xform=[0.3 * (i % 8), 0.3 * (i // 8), 0.5, 0, 0, 0, 1])
+        b.add_shape_box(body, hx=0.1, hy=0.1, hz=0.1, world=int(rng.choice([-1, 0, 1])),
+                        collisionGroup=int(rng.choice([-1, 0, 1, 2, -2, -3])))
+    sc = b.finalize()
+    pk = pack(sc)
+    ns = pk.C["NS"]
+    bits = pk.statU[pk.C["SU_FILTER"]:pk.C["SU_FILTER"] + (ns * ns + 31) // 32]
+    assert 0 < int(np.unpackbits(bits.view(np.uint8)).sum()) < ns * ns  # some pairs filtered, not all
+    _compare(pk, cpp_pack(json.dumps(sc.json).encode(), sc.bin), "worlds and groups")
