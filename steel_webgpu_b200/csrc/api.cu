@@ -406,10 +406,11 @@ uint32_t stage_flags(const SceneDev& d, uint32_t budget) {
 }
 
 // Blocks of the team launches of prepare and solve (team.cuh) for the batch's block size and shared
-// memory: a batch of one scene without Nesterov momentum; STEEL_TEAM_AUTO takes scenes of at least
-// TEAM_MIN_BODIES bodies or TEAM_MIN_ARTS articulations, with one thread per body or a warp per
-// articulation, capped by the blocks that fit the GPU. Fewer than two blocks: the one-block path. `strict`: a request for more
-// blocks than fit is an error (steel_set_team) rather than capped (a later change of tiles).
+// memory: a batch of one scene without Nesterov momentum, on the 512-thread instances;
+// STEEL_TEAM_AUTO takes scenes of at least TEAM_MIN_BODIES bodies or TEAM_MIN_ARTS articulations,
+// with one thread per body or a warp per articulation, capped by the blocks that fit the GPU. Fewer
+// than two blocks: the one-block path. `strict`: a request for more blocks than fit, or under
+// smaller tiles, is an error (steel_set_team) rather than capped (a later change of tiles).
 int team_blocks_for(const steel_batch* b, uint32_t req, bool strict, uint32_t* out) {
   *out = 0u;
   if (req == 0u || b->sc.size() != 1u || b->sc[0].d.NEST != 0u) return STEEL_OK;
